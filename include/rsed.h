@@ -1,0 +1,248 @@
+/*
+ * rsed.h — C ABI of the B200 symmetry-resolved exact-diagonalization library
+ * (librsed.so, sm_100a).
+ *
+ * Every entry point takes plain device pointers, sizes and a cudaStream_t
+ * passed as `void*` (NULL = legacy default stream), returns 0 on success or a
+ * negative RSED_E* code, and never allocates device memory: scratch buffers
+ * are sized by the matching *_scratch_bytes() query and owned by the caller.
+ * Complex numbers are interleaved (re, im) pairs of double (complex128) or
+ * float (complex64).  Sites are 0-based inside the ABI (the reference's
+ * 1-based site i is bit i-1).
+ *
+ * The reference (realspace_exactdiagonalization_py) has no FFI layer: its
+ * hot path is the set of Python functions in
+ * src/realspace_exactdiagonalization_py/symmetry_resolved_ed.py.  Each entry
+ * point below names the reference function (file:line) it replaces; the
+ * Python binding that calls it is
+ * realspace_exatdiagonalization_py_b200/_lib.py (ctypes).
+ */
+#ifndef RSED_H_
+#define RSED_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RSED_OK 0
+#define RSED_EINVAL -1      /* bad argument (maps to ValueError / AssertionError) */
+#define RSED_ECUDA -2       /* CUDA runtime error (launch or execution) */
+#define RSED_ENOTCONV -3    /* eigensolver hit its iteration cap */
+#define RSED_ERANGE -4      /* size beyond a compiled or documented limit */
+#define RSED_EBREAKDOWN -5  /* Krylov block lost rank (Cholesky pivot <= 0) */
+#define RSED_ESCRATCH -6    /* scratch buffer smaller than the query returned */
+
+/* One representative-table entry (16 bytes), indexed by combinadic rank:
+ * the reference's rep_rank_table / rep_sym_table / rep_amp_table
+ * (symmetry_resolved_ed.py:1359-1361) interleaved per state. */
+typedef struct {
+  int32_t rep;  /* 0-based orbit (representative) index */
+  int32_t g;    /* 0-based group element with g(rep) = mask */
+  float re, im; /* complex64 canonicalisation amplitude alpha_g(rep) */
+} rsed_entry_t;
+
+/* Symmetry group of a catalog (device pointers). */
+typedef struct {
+  int32_t n_site;      /* N <= 63 */
+  int32_t n_filled;    /* k, 0 <= k <= N */
+  int32_t n_group;     /* |G| <= 64 */
+  int32_t fermionic;   /* 1 = fermions (permutation parity), 0 = hard-core bosons */
+  int64_t n_states;    /* C(N, k) */
+  const int64_t* binom; /* (N+1) x (k+1) row-major, C(b, j) */
+  const uint8_t* perm;  /* |G| x N: 0-based image site of site i under g */
+  const double* angle;  /* |G| x N: numpy.angle(eta_g(i)) */
+  const double* eta;    /* |G| x N complex128: eta_g(i) */
+} rsed_group_t;
+
+/* Hopping / density model on the orbit basis of one catalog. */
+typedef struct {
+  int32_t n_site, n_filled, n_group, fermionic;
+  int64_t n_states;
+  int64_t n_orbits;
+  const int64_t* binom;          /* as in rsed_group_t */
+  const rsed_entry_t* table;     /* n_states entries */
+  const uint64_t* repr_masks;    /* n_orbits representative masks (ascending) */
+  int32_t n_terms;               /* directed bilinear terms after merging duplicates */
+  const int32_t* term_begin;     /* N+1: terms grouped by annihilated (source) site */
+  const uint8_t* term_to;        /* n_terms: created (target) site */
+  const double* term_amp;        /* n_terms complex128 amplitudes */
+  const uint64_t* term_jw;       /* n_terms: sites strictly between source and target */
+  const double* hdiag;           /* n_orbits complex128 density-density diagonal */
+} rsed_model_t;
+
+/* A set of momentum sectors evaluated together ("columns" of a block of
+ * vectors laid out row-major as [n_orbits][ld], one row per orbit). */
+typedef struct {
+  int32_t n_sectors;          /* <= 64 */
+  int32_t n_cols;             /* columns in use */
+  int32_t ld;                 /* leading dimension (elements) >= n_cols */
+  int32_t n_group;
+  const uint64_t* member;     /* n_orbits: bit s set if the orbit belongs to sector s */
+  const double* sqrt_stab;    /* n_orbits: sqrt(|Stab|) */
+  const double* chi;          /* n_sectors x n_group complex128 characters */
+  const int32_t* col_sector;  /* n_cols: sector of each column */
+} rsed_sectors_t;
+
+const char* rsed_version(void);
+/* Message of the last error raised on the calling host thread. */
+const char* rsed_last_error(void);
+
+/* ---- K1-K3: orbit catalog -------------------------------------------------
+ * Replaces build_symmetry_orbit_catalog / _build_orbit_catalog_kernel
+ * (symmetry_resolved_ed.py:1298-1404, 433-575).  The caller allocates the
+ * outputs once the counts are known, hence the call sequence
+ *   rsed_catalog_count   representative test over all C(N,k) states -> *n_orbits_out
+ *   rsed_catalog_fill    representative masks (rank order), the whole table
+ *                        (g = 0..|G|-1 written in ascending g so the last writer
+ *                        wins, as the reference does) and stabilizer bitmasks
+ *   rsed_catalog_stab_count  exclusive stabilizer offsets -> *n_stab_out
+ *   rsed_catalog_stab    complex128 stabilizer phases, ascending g per orbit.
+ * The scratch of rsed_catalog_count must be passed unchanged to _fill. */
+size_t rsed_catalog_scratch_bytes(const rsed_group_t* grp);
+int rsed_catalog_count(const rsed_group_t* grp, void* scratch, size_t scratch_bytes,
+                       int64_t* n_orbits_out, void* stream);
+int rsed_catalog_fill(const rsed_group_t* grp, const void* scratch, size_t scratch_bytes,
+                      int64_t n_orbits, uint64_t* repr_masks, rsed_entry_t* table,
+                      uint64_t* stab_mask, void* stream);
+size_t rsed_stab_scratch_bytes(int64_t n_orbits);
+int rsed_catalog_stab_count(int64_t n_orbits, const uint64_t* stab_mask, int64_t* stab_off,
+                            int64_t* n_stab_out, void* scratch, size_t scratch_bytes, void* stream);
+int rsed_catalog_stab(const rsed_group_t* grp, int64_t n_orbits, const uint64_t* repr_masks,
+                      const uint64_t* stab_mask, const int64_t* stab_off, double* stab_phase,
+                      void* stream);
+
+/* ---- K4: flux phase update ------------------------------------------------
+ * Replaces update_orbit_stabilizer_phases (symmetry_resolved_ed.py:1220-1269):
+ * recompute the stabilizer phases and rewrite g / alpha of every table entry
+ * for a group with the same permutations and new per-site phases (product
+ * form, ascending g, last writer wins).  In place.  *err_dev (device int)
+ * becomes non-zero if the catalog does not match the group. */
+int rsed_phase_update(const rsed_group_t* grp, int64_t n_orbits, const uint64_t* repr_masks,
+                      const uint64_t* stab_mask, const int64_t* stab_off, double* stab_phase,
+                      rsed_entry_t* table, int* err_dev, void* stream);
+
+/* ---- K5: sector membership ----------------------------------------------
+ * Replaces _is_orbit_compatible / build_symmetry_sector_basis
+ * (symmetry_resolved_ed.py:1484-1546) for many irreps at once: bit s of
+ * member[o] is set iff |chi_s(h) - alpha_h| <= atol for every h in Stab(o).
+ * sqrt_stab[o] = sqrt(popcount(stab_mask[o])).  sector_dims[s] (device
+ * int64) receives the dimension of sector s. */
+int rsed_sector_members(int64_t n_orbits, int32_t n_group, int32_t n_sectors,
+                        const uint64_t* stab_mask, const int64_t* stab_off,
+                        const double* stab_phase, const double* chi, double atol,
+                        uint64_t* member, double* sqrt_stab, int64_t* sector_dims, void* stream);
+/* Basis of one sector (the reference's Symmetry_Sector_Basis order): orbit of
+ * each basis row (ascending) and the row of each orbit (-1 if absent). */
+size_t rsed_sector_scratch_bytes(int64_t n_orbits, int32_t n_sectors);
+int rsed_sector_rows(int64_t n_orbits, const uint64_t* member, int32_t sector,
+                     int32_t* orbit_of_row, int32_t* row_of_orbit, void* scratch,
+                     size_t scratch_bytes, void* stream);
+
+/* Density-density diagonal per orbit, summed in term order like the
+ * reference's h_diag (symmetry_resolved_ed.py:641-646). */
+int rsed_density_diag(int64_t n_orbits, const uint64_t* repr_masks, int32_t n_density,
+                      const uint8_t* dens_i, const uint8_t* dens_j, const double* dens_v,
+                      double* hdiag, void* stream);
+
+/* ---- K6: matrix-free H|psi> ------------------------------------------------
+ * Replaces MatrixFreeHamiltonian.__call__ / _apply_hamiltonian_kernel
+ * (symmetry_resolved_ed.py:1965-1976, 826-923) for all columns of a block at
+ * once.  Pull form without atomics: row r of a column accumulates
+ * conj(H[s, r]) x[s] over the hops from rep(r), i.e. y = H^dagger x, which is
+ * H x for the Hermitian blocks the reference builds (to the complex64
+ * rounding of its amplitude table).  precision 64: x complex128, FP64
+ * accumulation; precision 32: x complex64, FP32 accumulation; y is always
+ * complex128.  variant 0 picks the lane mapping from n_cols. */
+int rsed_apply_h(const rsed_model_t* model, const rsed_sectors_t* sec, const void* x, void* y,
+                 int32_t precision, int32_t variant, void* stream);
+
+/* ---- K7: matrix mode ---------------------------------------------------
+ * Replaces _vectorized_block_triplets / _build_H_block_kernel
+ * (symmetry_resolved_ed.py:595-736): exact (row, col, value) triplets of one
+ * sector block, value ((((t * s_JW) * alpha) * conj(chi(g))) * sqrt(S_row/S_col))
+ * in the reference's product order, diagonal first per column.  count fills
+ * col_off (n_rows+1 exclusive offsets) and *nnz_out; fill writes the triplets. */
+size_t rsed_triplet_scratch_bytes(int64_t n_rows);
+int rsed_triplets_count(const rsed_model_t* model, int64_t n_rows, const int32_t* orbit_of_row,
+                        const int32_t* row_of_orbit, const double* chi, const uint64_t* stab_mask,
+                        int64_t* col_off, int64_t* nnz_out, void* scratch, size_t scratch_bytes,
+                        void* stream);
+int rsed_triplets_fill(const rsed_model_t* model, int64_t n_rows, const int32_t* orbit_of_row,
+                       const int32_t* row_of_orbit, const double* chi, const uint64_t* stab_mask,
+                       const int64_t* col_off, int64_t* rows, int64_t* cols, double* vals,
+                       void* stream);
+/* y_v = A x_v (v < n_vec, vectors contiguous) for a complex128 CSR matrix
+ * (scipy.sparse csr_matrix @ x, symmetry_resolved_ed.py:1976). */
+int rsed_csr_spmv(int64_t n_rows, const int64_t* row_ptr, const int32_t* col_idx,
+                  const double* vals, int32_t n_vec, const double* x, double* y, void* stream);
+
+/* ---- K8: batched thick-restart block Lanczos -------------------------------
+ * Replaces diagonalize_block_matrixfree / diagonalize_block_arpack
+ * (symmetry_resolved_ed.py:2214-2299, ARPACK eigs(which="SR", tol=1e-10))
+ * for many sector instances at once.  State lives in caller-owned device
+ * buffers described by rsed_lanczos_t.  rsed_lanczos_iterate advances every
+ * active instance by n_iter block steps without host synchronisation or
+ * allocation (capturable in a CUDA graph); per-instance status is read from
+ * state[8*i + 1] (0 running, 1 converged, RSED_E* on failure). */
+typedef struct {
+  int32_t n_inst;        /* instances (sector solves) in the batch */
+  int32_t n_slots;       /* basis blocks before a thick restart (n_slots*bmax <= 64) */
+  int32_t nev;           /* wanted lowest eigenpairs per instance */
+  int32_t keep_blocks;   /* blocks kept at a restart (keep_blocks*bmax <= 16) */
+  int32_t max_restarts;  /* restart cap -> RSED_ENOTCONV */
+  int32_t precision;     /* matvec precision: 64 or 32 */
+  int32_t bmax;          /* largest instance block size (<= 8) */
+  int32_t chunk_rows;    /* rows per reduction chunk */
+  int32_t pm;            /* leading dimension of the projected matrices >= (n_slots+1)*bmax */
+  int32_t reserved;
+  double tol;            /* converged when ||r_j|| <= tol * max(1, |theta_j|) for j < nev */
+  const int32_t* inst_col0;  /* n_inst: first column of each instance */
+  const int32_t* inst_b;     /* n_inst: block size of each instance */
+  double* V;             /* (n_slots+2) x n_orbits x ld complex128: basis slots, last = current block */
+  double* W;             /* n_orbits x ld complex128 */
+  float* Xf;             /* n_orbits x ld complex64 current block (precision 32), else NULL */
+  double* P;             /* n_inst x pm x pm complex128 projected matrices */
+  double* coef;          /* rsed_lanczos_coef_len() doubles */
+  double* partial;       /* partial_len doubles */
+  int64_t partial_len;   /* >= rsed_lanczos_partial_len() */
+  double* ritz_val;      /* n_inst x pm */
+  double* ritz_vec;      /* n_inst x pm x pm complex128 */
+  double* resid;         /* n_inst x pm */
+  int32_t* state;        /* n_inst x 8 */
+} rsed_lanczos_t;
+int64_t rsed_lanczos_partial_len(int64_t n_orbits, int32_t chunk_rows, int32_t n_inst,
+                                 int32_t n_slots);
+int64_t rsed_lanczos_coef_len(int32_t n_inst, int32_t n_slots);
+int rsed_lanczos_max_block(void);
+int rsed_lanczos_max_keep(void);
+int rsed_lanczos_max_projected(void);
+/* One-time kernel attribute set-up; call before capturing a graph. */
+int rsed_lanczos_prepare(void);
+/* The start block is read from the columns of W; it is orthonormalised
+ * (Cholesky QR twice) into basis slot 0. */
+int rsed_lanczos_start(const rsed_model_t* model, const rsed_sectors_t* sec, rsed_lanczos_t* st,
+                       void* stream);
+int rsed_lanczos_iterate(const rsed_model_t* model, const rsed_sectors_t* sec, rsed_lanczos_t* st,
+                         int32_t n_iter, int32_t check_every, int32_t apply_variant, void* stream);
+/* Ritz vectors of the nev lowest pairs of the last check:
+ * U[(inst*nev + j)*u_stride + orbit] (complex128). */
+int rsed_lanczos_extract(const rsed_model_t* model, const rsed_sectors_t* sec, rsed_lanczos_t* st,
+                         double* U, int64_t u_stride, void* stream);
+
+/* Row gather / scatter between a sector's compact basis order and the
+ * orbit-row layout (complex128): dst[r*dst_stride] = src[orbit_of_row[r]*src_ld + src_col]
+ * and the converse. */
+int rsed_gather_rows(int64_t n_rows, const int32_t* orbit_of_row, const double* src, int64_t src_ld,
+                     int32_t src_col, double* dst, int64_t dst_stride, void* stream);
+int rsed_scatter_rows(int64_t n_rows, const int32_t* orbit_of_row, const double* src,
+                      int64_t src_stride, double* dst, int64_t dst_ld, int32_t dst_col, void* stream);
+int rsed_device_sync(void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RSED_H_ */

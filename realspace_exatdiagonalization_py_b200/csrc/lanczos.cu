@@ -1,0 +1,731 @@
+// K8: batched thick-restart block Lanczos with full FP64 reorthogonalisation.
+//
+// One batch holds n_inst independent eigen-solves ("instances", e.g. the
+// momentum sectors of one lattice/flux point).  Instance i owns b_i columns
+// [c0_i, c0_i + b_i) of every block buffer; all blocks share the row-major
+// [n_orbits][ld] layout of the matrix-free apply, so one apply launch serves
+// every instance.  Per iteration (all kernels launched unconditionally, each
+// instance decides from its device-side state whether it has work, so a
+// sequence of iterations can be captured in one CUDA graph):
+//
+//   apply    W = H X                      (X = newest basis block)
+//   pass 1   C1 = V^H W, G1 = W^H W  ->  R1 = chol(G1 - C1^H C1),  W = (W - V C1) R1^-1
+//   pass 2   C2, G2 on the new W     ->  R2,  V_new = (W - V C2) R2^-1
+//            P[:, cur] = C1 + C2 R1,  P[new, cur] = R2 R1   (projected matrix)
+//   ritz     (some iterations) Jacobi eigen-solve of (P + P^H)/2 in shared
+//            memory, residual estimates |R_last S_last,j|, convergence test,
+//            thick restart bookkeeping
+//   restart  V_0..keep-1 = V S_keep, residual block moved behind them
+//
+// The reorthogonalisation is block classical Gram-Schmidt with the Pythagorean
+// Cholesky update, applied twice (one reduction per pass).
+#include <type_traits>
+#include "rsed_internal.cuh"
+
+namespace {
+
+constexpr int kBMax = 8;        // largest block per instance
+constexpr int kKeepMax = 16;    // largest thick-restart basis (columns)
+constexpr int kJacobiMax = 64;  // largest projected matrix
+constexpr int kStateInts = 8;
+// state fields
+constexpr int S_NB = 0, S_STATUS = 1, S_RESTARTS = 2, S_ITERS = 3, S_ACTIVE = 4, S_RESTART_NB = 5,
+              S_NEWSLOT = 6, S_NCONV = 7;
+
+struct LzDims {
+  int64_t n_orb;
+  int ld;
+  int n_inst;
+  int n_slots;
+  int pm;
+  int chunk_rows;
+  int n_chunks;
+  int pslots;  // n_slots + 2 reduction slots per instance
+};
+
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+// conj(a) * b
+__device__ __forceinline__ double2 cdotc(double2 a, double2 b) {
+  return make_double2(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x);
+}
+
+// ---------------------------------------------------------------------------
+// Reduction: partial[chunk][inst][s][p][q] = sum_rows conj(Y_s[row][c0+p]) W[row][c0+q]
+// with Y_s = V[s] for s < nb and Y_nb = W (Gram of W itself).
+__global__ void k_lz_gram(rsed_lanczos_t st, LzDims d) {
+  const int chunk = blockIdx.x;
+  const int inst = blockIdx.y;
+  const int* stt = st.state + inst * kStateInts;
+  if (!stt[S_ACTIVE]) return;
+  const int b = st.inst_b[inst];
+  const int c0 = st.inst_col0[inst];
+  const int nb = stt[S_NB];
+  const int npairs = (nb + 1) * b;
+  const int64_t r0 = (int64_t)chunk * d.chunk_rows;
+  const int64_t r1 = min(r0 + d.chunk_rows, d.n_orb);
+  const double2* V = reinterpret_cast<const double2*>(st.V);
+  const double2* W = reinterpret_cast<const double2*>(st.W);
+  double2* part = reinterpret_cast<double2*>(st.partial);
+  const int64_t slot_stride = d.n_orb * d.ld;
+  for (int pair = threadIdx.x; pair < npairs; pair += blockDim.x) {
+    const int s = pair / b, p = pair % b;
+    const double2* Y = (s < nb) ? V + s * slot_stride : W;
+    double2 acc[kBMax];
+#pragma unroll
+    for (int q = 0; q < kBMax; ++q) acc[q] = make_double2(0.0, 0.0);
+    for (int64_t r = r0; r < r1; ++r) {
+      const double2 y = Y[r * d.ld + c0 + p];
+#pragma unroll
+      for (int q = 0; q < kBMax; ++q) {
+        if (q < b) acc[q] = cadd(acc[q], cdotc(y, W[r * d.ld + c0 + q]));
+      }
+    }
+    double2* out = part + (((int64_t)chunk * d.n_inst + inst) * d.pslots + s) * kBMax * kBMax + p * kBMax;
+#pragma unroll
+    for (int q = 0; q < kBMax; ++q)
+      if (q < b) out[q] = acc[q];
+  }
+}
+
+// Sum the partials, Cholesky of G - C^H C, projected-matrix bookkeeping.
+// coef layout per instance: [pslots][kBMax][kBMax]; slots 0..nb-1 = C, slot
+// pslots-1 = R of this pass; pass-1 results are kept in slots of rbuf.
+__global__ void k_lz_finalize(rsed_lanczos_t st, LzDims d, int pass) {
+  const int inst = blockIdx.x;
+  int* stt = st.state + inst * kStateInts;
+  if (pass == 1 && threadIdx.x == 0) stt[S_RESTART_NB] = 0;
+  if (!stt[S_ACTIVE]) return;
+  const int b = st.inst_b[inst];
+  const int nb = stt[S_NB];
+  if (nb > d.n_slots || b < 1 || b > kBMax) {
+    // the basis is full (no restart happened) or the block size is invalid:
+    // stop this instance instead of writing past its slots
+    if (threadIdx.x == 0) {
+      stt[S_STATUS] = RSED_EINVAL;
+      stt[S_ACTIVE] = 0;
+    }
+    return;
+  }
+  const int nent = (nb + 1) * b * b;
+  const double2* part = reinterpret_cast<const double2*>(st.partial);
+  double2* coef = reinterpret_cast<double2*>(st.coef) + (int64_t)inst * 2 * d.pslots * kBMax * kBMax;
+  // pass-specific area: [pass-1][pslots][kBMax][kBMax]
+  double2* cp = coef + (pass - 1) * d.pslots * kBMax * kBMax;
+  for (int e = threadIdx.x; e < nent; e += blockDim.x) {
+    const int s = e / (b * b), pq = e % (b * b), p = pq / b, q = pq % b;
+    double2 acc = make_double2(0.0, 0.0);
+    for (int c = 0; c < d.n_chunks; ++c)
+      acc = cadd(acc, part[(((int64_t)c * d.n_inst + inst) * d.pslots + s) * kBMax * kBMax + p * kBMax + q]);
+    cp[s * kBMax * kBMax + p * kBMax + q] = acc;
+  }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  // G' = G - C^H C  (G sits in slot nb)
+  double2 G[kBMax][kBMax];
+  double gdiag_max = 0.0;
+  for (int p = 0; p < b; ++p)
+    for (int q = 0; q < b; ++q) {
+      double2 g = cp[nb * kBMax * kBMax + p * kBMax + q];
+      for (int s = 0; s < nb; ++s)
+        for (int r = 0; r < b; ++r) {
+          const double2 a = cp[s * kBMax * kBMax + r * kBMax + p];  // C[s r][p]
+          const double2 c = cp[s * kBMax * kBMax + r * kBMax + q];  // C[s r][q]
+          g = csub(g, cdotc(a, c));
+        }
+      G[p][q] = g;
+      if (p == q) gdiag_max = fmax(gdiag_max, cp[nb * kBMax * kBMax + p * kBMax + p].x);
+    }
+  // Cholesky G' = R^H R, R upper triangular
+  double2 R[kBMax][kBMax];
+  for (int p = 0; p < kBMax; ++p)
+    for (int q = 0; q < kBMax; ++q) R[p][q] = make_double2(0.0, 0.0);
+  bool ok = gdiag_max > 0.0;
+  for (int j = 0; j < b && ok; ++j) {
+    double s = G[j][j].x;
+    for (int k = 0; k < j; ++k) s -= R[k][j].x * R[k][j].x + R[k][j].y * R[k][j].y;
+    if (!(s > 1e-26 * gdiag_max)) {
+      ok = false;
+      break;
+    }
+    const double rjj = sqrt(s);
+    R[j][j] = make_double2(rjj, 0.0);
+    for (int q = j + 1; q < b; ++q) {
+      double2 t = G[j][q];
+      for (int k = 0; k < j; ++k) t = csub(t, cdotc(R[k][j], R[k][q]));
+      R[j][q] = make_double2(t.x / rjj, t.y / rjj);
+    }
+  }
+  if (!ok) {
+    stt[S_STATUS] = RSED_EBREAKDOWN;
+    stt[S_ACTIVE] = 0;
+    return;
+  }
+  double2* Rout = cp + (d.pslots - 1) * kBMax * kBMax;
+  for (int p = 0; p < b; ++p)
+    for (int q = 0; q < b; ++q) Rout[p * kBMax + q] = R[p][q];
+  if (pass == 2) {
+    const int nb_old = nb;
+    stt[S_NEWSLOT] = nb_old;
+    stt[S_NB] = nb_old + 1;
+    stt[S_ITERS] += 1;
+    if (nb_old >= 1) {
+      // combine passes: C = C1 + C2 R1, Rtot = R2 R1 ; column block cb = nb_old-1
+      const double2* c1 = coef;
+      const double2* R1 = coef + (d.pslots - 1) * kBMax * kBMax;
+      double2* P = reinterpret_cast<double2*>(st.P) + (int64_t)inst * d.pm * d.pm;
+      const int cb = nb_old - 1;
+      for (int s = 0; s < nb_old; ++s)
+        for (int p = 0; p < b; ++p)
+          for (int q = 0; q < b; ++q) {
+            double2 v = c1[s * kBMax * kBMax + p * kBMax + q];
+            for (int r = 0; r < b; ++r)
+              v = cadd(v, cmul(cp[s * kBMax * kBMax + p * kBMax + r], R1[r * kBMax + q]));
+            P[(int64_t)(s * b + p) * d.pm + cb * b + q] = v;
+          }
+      for (int p = 0; p < b; ++p)
+        for (int q = 0; q < b; ++q) {
+          double2 v = make_double2(0.0, 0.0);
+          for (int r = 0; r < b; ++r) v = cadd(v, cmul(R[p][r], R1[r * kBMax + q]));
+          P[(int64_t)(nb_old * b + p) * d.pm + cb * b + q] = v;
+        }
+    }
+  }
+}
+
+// W <- (W - V C) R^-1 ; pass 2 writes the new basis block and the matvec input.
+__global__ void k_lz_update(rsed_lanczos_t st, LzDims d, int pass) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t row = t / d.n_inst;
+  const int inst = (int)(t % d.n_inst);
+  if (row >= d.n_orb) return;
+  const int* stt = st.state + inst * kStateInts;
+  if (!stt[S_ACTIVE]) return;
+  const int b = st.inst_b[inst];
+  const int c0 = st.inst_col0[inst];
+  const int nb = (pass == 2) ? stt[S_NEWSLOT] : stt[S_NB];
+  const double2* coef = reinterpret_cast<const double2*>(st.coef) +
+                        (int64_t)inst * 2 * d.pslots * kBMax * kBMax + (pass - 1) * d.pslots * kBMax * kBMax;
+  double2* V = reinterpret_cast<double2*>(st.V);
+  double2* W = reinterpret_cast<double2*>(st.W);
+  const int64_t slot_stride = d.n_orb * d.ld;
+  double2 w[kBMax];
+#pragma unroll
+  for (int q = 0; q < kBMax; ++q) w[q] = (q < b) ? W[row * d.ld + c0 + q] : make_double2(0.0, 0.0);
+  for (int s = 0; s < nb; ++s) {
+    const double2* Vs = V + s * slot_stride + row * d.ld + c0;
+    for (int p = 0; p < b; ++p) {
+      const double2 v = Vs[p];
+#pragma unroll
+      for (int q = 0; q < kBMax; ++q)
+        if (q < b) w[q] = csub(w[q], cmul(v, coef[s * kBMax * kBMax + p * kBMax + q]));
+    }
+  }
+  const double2* R = coef + (d.pslots - 1) * kBMax * kBMax;
+  double2 x[kBMax];
+#pragma unroll
+  for (int q = 0; q < kBMax; ++q) {
+    if (q >= b) break;
+    double2 v = w[q];
+    for (int p = 0; p < q; ++p) v = csub(v, cmul(x[p], R[p * kBMax + q]));
+    const double rr = R[q * kBMax + q].x;
+    x[q] = make_double2(v.x / rr, v.y / rr);
+  }
+  if (pass == 1) {
+    for (int q = 0; q < b; ++q) W[row * d.ld + c0 + q] = x[q];
+  } else {
+    double2* Vn = V + (int64_t)nb * slot_stride + row * d.ld + c0;
+    double2* X = V + (int64_t)(d.n_slots + 1) * slot_stride + row * d.ld + c0;
+    for (int q = 0; q < b; ++q) {
+      Vn[q] = x[q];
+      X[q] = x[q];
+      if (st.Xf) reinterpret_cast<float2*>(st.Xf)[row * d.ld + c0 + q] =
+          make_float2((float)x[q].x, (float)x[q].y);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Jacobi eigen-solver for a Hermitian M x M matrix held in shared memory.
+// Brent-Luk round-robin ordering: M/2 disjoint rotations per step.
+__device__ void jacobi_hermitian(double2* A, double2* Vv, int M, int* pp, int* qq, double* cc,
+                                 double* ss, double2* ee, double* red) {
+  const int Me = (M + 1) & ~1;
+  const int npair = Me / 2;
+  for (int i = threadIdx.x; i < M * M; i += blockDim.x) {
+    const int r = i / M, c = i % M;
+    Vv[i] = make_double2(r == c ? 1.0 : 0.0, 0.0);
+  }
+  __syncthreads();
+  for (int sweep = 0; sweep < 30; ++sweep) {
+    // off-diagonal norm vs total
+    double off = 0.0, tot = 0.0;
+    for (int i = threadIdx.x; i < M * M; i += blockDim.x) {
+      const double2 a = A[i];
+      const double v = a.x * a.x + a.y * a.y;
+      tot += v;
+      if (i / M != i % M) off += v;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      off += __shfl_down_sync(0xffffffffu, off, o);
+      tot += __shfl_down_sync(0xffffffffu, tot, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+      red[2 * (threadIdx.x >> 5)] = off;
+      red[2 * (threadIdx.x >> 5) + 1] = tot;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double o2 = 0.0, t2 = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+        o2 += red[2 * w];
+        t2 += red[2 * w + 1];
+      }
+      red[64] = o2;
+      red[65] = t2;
+    }
+    __syncthreads();
+    const double offn = red[64], totn = red[65];
+    __syncthreads();
+    if (!(offn > 1e-30 * totn) || offn == 0.0) break;
+    for (int step = 0; step < Me - 1; ++step) {
+      for (int k = threadIdx.x; k < npair; k += blockDim.x) {
+        int p, q;
+        if (k == 0) {
+          p = 0;
+          q = (step % (Me - 1)) + 1;
+        } else {
+          p = ((step + k) % (Me - 1)) + 1;
+          q = ((step - k + (Me - 1)) % (Me - 1)) + 1;
+        }
+        if (p > q) {
+          int tmp = p;
+          p = q;
+          q = tmp;
+        }
+        double c = 1.0, s = 0.0;
+        double2 e = make_double2(1.0, 0.0);
+        if (q < M) {
+          const double2 bpq = A[p * M + q];
+          const double ab = hypot(bpq.x, bpq.y);
+          const double app = A[p * M + p].x, aqq = A[q * M + q].x;
+          if (ab > 1e-300 && ab > 1e-18 * (fabs(app) + fabs(aqq))) {
+            const double th = (aqq - app) / (2.0 * ab);
+            const double t = (th >= 0.0 ? 1.0 : -1.0) / (fabs(th) + sqrt(th * th + 1.0));
+            c = 1.0 / sqrt(t * t + 1.0);
+            s = t * c;
+            e = make_double2(bpq.x / ab, bpq.y / ab);
+          }
+        }
+        pp[k] = p;
+        qq[k] = q;
+        cc[k] = c;
+        ss[k] = s;
+        ee[k] = e;
+      }
+      __syncthreads();
+      // rows: A <- J^H A
+      for (int it = threadIdx.x; it < npair * M; it += blockDim.x) {
+        const int k = it / M, j = it % M;
+        const int p = pp[k], q = qq[k];
+        if (q >= M || ss[k] == 0.0) continue;
+        const double c = cc[k], s = ss[k];
+        const double2 e = ee[k];
+        const double2 apj = A[p * M + j], aqj = A[q * M + j];
+        const double2 eq = cmul(e, aqj);
+        A[p * M + j] = make_double2(c * apj.x - s * eq.x, c * apj.y - s * eq.y);
+        A[q * M + j] = make_double2(s * apj.x + c * eq.x, s * apj.y + c * eq.y);
+      }
+      __syncthreads();
+      // cols: A <- A J, V <- V J
+      for (int it = threadIdx.x; it < npair * M; it += blockDim.x) {
+        const int k = it / M, i = it % M;
+        const int p = pp[k], q = qq[k];
+        if (q >= M || ss[k] == 0.0) continue;
+        const double c = cc[k], s = ss[k];
+        const double2 ec = cconj(ee[k]);
+        {
+          const double2 aip = A[i * M + p], aiq = A[i * M + q];
+          const double2 t = cmul(aiq, ec);
+          A[i * M + p] = make_double2(c * aip.x - s * t.x, c * aip.y - s * t.y);
+          A[i * M + q] = make_double2(s * aip.x + c * t.x, s * aip.y + c * t.y);
+        }
+        {
+          const double2 vip = Vv[i * M + p], viq = Vv[i * M + q];
+          const double2 t = cmul(viq, ec);
+          Vv[i * M + p] = make_double2(c * vip.x - s * t.x, c * vip.y - s * t.y);
+          Vv[i * M + q] = make_double2(s * vip.x + c * t.x, s * vip.y + c * t.y);
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// Ritz step: per instance, when due.  Dynamic smem: 2 * kJacobiMax^2 double2.
+__global__ void k_lz_ritz(rsed_lanczos_t st, LzDims d, int check_every, int force) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int inst = blockIdx.x;
+  int* stt = st.state + inst * kStateInts;
+  if (!stt[S_ACTIVE]) return;
+  const int b = st.inst_b[inst];
+  const int nb = stt[S_NB];
+  const int M = (nb - 1) * b;
+  const bool full = (nb >= d.n_slots + 1);
+  const int nev = st.nev;
+  const int K = st.keep_blocks * b;
+  const bool due = full || force || (M >= nev + b && M >= K && (stt[S_ITERS] % check_every) == 0);
+  if (!due) return;
+  if (M < nev || M < K || M > kJacobiMax) {
+    if (full && threadIdx.x == 0) {  // cannot restart: report instead of overrunning
+      stt[S_STATUS] = RSED_EINVAL;
+      stt[S_ACTIVE] = 0;
+    }
+    return;
+  }
+  double2* A = reinterpret_cast<double2*>(smem);
+  double2* Vv = A + kJacobiMax * kJacobiMax;
+  __shared__ int pp[kJacobiMax / 2], qq[kJacobiMax / 2], order[kJacobiMax];
+  __shared__ double cc[kJacobiMax / 2], ss[kJacobiMax / 2], red[72];
+  __shared__ double2 ee[kJacobiMax / 2];
+  __shared__ double theta[kJacobiMax];
+  __shared__ int conv_flag;
+  const double2* P = reinterpret_cast<const double2*>(st.P) + (int64_t)inst * d.pm * d.pm;
+  for (int i = threadIdx.x; i < M * M; i += blockDim.x) {
+    const int r = i / M, c = i % M;
+    const double2 a = P[(int64_t)r * d.pm + c], bt = P[(int64_t)c * d.pm + r];
+    A[i] = make_double2(0.5 * (a.x + bt.x), 0.5 * (a.y - bt.y));
+  }
+  __syncthreads();
+  jacobi_hermitian(A, Vv, M, pp, qq, cc, ss, ee, red);
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < M; ++i) {
+      order[i] = i;
+      theta[i] = A[i * M + i].x;
+    }
+    for (int i = 1; i < M; ++i) {  // insertion sort by eigenvalue
+      int j = i;
+      while (j > 0 && theta[order[j - 1]] > theta[order[j]]) {
+        int t = order[j];
+        order[j] = order[j - 1];
+        order[j - 1] = t;
+        --j;
+      }
+    }
+  }
+  __syncthreads();
+  double* rv = st.ritz_val + (int64_t)inst * d.pm;
+  double2* rvec = reinterpret_cast<double2*>(st.ritz_vec) + (int64_t)inst * d.pm * d.pm;
+  double* res = st.resid + (int64_t)inst * d.pm;
+  for (int i = threadIdx.x; i < M * M; i += blockDim.x) {
+    const int r = i / M, j = i % M;
+    rvec[(int64_t)r * d.pm + j] = Vv[r * M + order[j]];
+  }
+  for (int j = threadIdx.x; j < M; j += blockDim.x) rv[j] = theta[order[j]];
+  __syncthreads();
+  // residual estimates: || Rlast * S[last block rows, j] ||
+  for (int j = threadIdx.x; j < M; j += blockDim.x) {
+    double acc = 0.0;
+    for (int q = 0; q < b; ++q) {
+      double2 v = make_double2(0.0, 0.0);
+      for (int p = 0; p < b; ++p) {
+        const double2 r = P[(int64_t)((nb - 1) * b + q) * d.pm + (nb - 2) * b + p];
+        v = cadd(v, cmul(r, Vv[((nb - 2) * b + p) * M + order[j]]));
+      }
+      acc += v.x * v.x + v.y * v.y;
+    }
+    res[j] = sqrt(acc);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int nconv = 0;
+    for (int j = 0; j < nev; ++j) {
+      if (res[j] <= st.tol * fmax(1.0, fabs(rv[j]))) ++nconv;
+      else break;
+    }
+    stt[S_NCONV] = nconv;
+    conv_flag = (nconv >= nev);
+    if (conv_flag) {
+      stt[S_STATUS] = 1;
+      stt[S_ACTIVE] = 0;
+    } else if (full) {
+      stt[S_RESTARTS] += 1;
+      if (stt[S_RESTARTS] > st.max_restarts) {
+        stt[S_STATUS] = RSED_ENOTCONV;
+        stt[S_ACTIVE] = 0;
+        conv_flag = 1;  // no restart
+      }
+    }
+  }
+  __syncthreads();
+  if (conv_flag || !full) return;
+  // thick restart: new projected matrix diag(theta_0..K-1) + coupling block
+  double2* Pw = reinterpret_cast<double2*>(st.P) + (int64_t)inst * d.pm * d.pm;
+  // coupling rows first (needs old P), staged in smem A (free now)
+  for (int it = threadIdx.x; it < b * K; it += blockDim.x) {
+    const int q = it / K, j = it % K;
+    double2 v = make_double2(0.0, 0.0);
+    for (int p = 0; p < b; ++p) {
+      const double2 r = Pw[(int64_t)((nb - 1) * b + q) * d.pm + (nb - 2) * b + p];
+      v = cadd(v, cmul(r, Vv[((nb - 2) * b + p) * M + order[j]]));
+    }
+    A[it] = v;
+  }
+  __syncthreads();
+  const int Mn = (st.keep_blocks + 1) * b;
+  for (int i = threadIdx.x; i < (nb)*b * (nb)*b; i += blockDim.x) {
+    const int r = i / (nb * b), c = i % (nb * b);
+    Pw[(int64_t)r * d.pm + c] = make_double2(0.0, 0.0);
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < K; j += blockDim.x) Pw[(int64_t)j * d.pm + j] = make_double2(rv[j], 0.0);
+  for (int it = threadIdx.x; it < b * K; it += blockDim.x) {
+    const int q = it / K, j = it % K;
+    Pw[(int64_t)(K + q) * d.pm + j] = A[it];
+  }
+  (void)Mn;
+  if (threadIdx.x == 0) {
+    stt[S_RESTART_NB] = nb;
+    stt[S_NB] = st.keep_blocks + 1;
+  }
+}
+
+// V_0..keep-1 = V S_keep ; residual block (old slot nb_old-1) -> slot keep.
+__global__ void k_lz_restart(rsed_lanczos_t st, LzDims d) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t row = t / d.n_inst;
+  const int inst = (int)(t % d.n_inst);
+  if (row >= d.n_orb) return;
+  const int* stt = st.state + inst * kStateInts;
+  const int nb_old = stt[S_RESTART_NB];
+  if (nb_old == 0) return;
+  const int b = st.inst_b[inst];
+  const int c0 = st.inst_col0[inst];
+  const int K = st.keep_blocks * b;
+  const int Mold = (nb_old - 1) * b;
+  const double2* S = reinterpret_cast<const double2*>(st.ritz_vec) + (int64_t)inst * d.pm * d.pm;
+  double2* V = reinterpret_cast<double2*>(st.V);
+  const int64_t slot_stride = d.n_orb * d.ld;
+  double2 acc[kKeepMax];
+#pragma unroll
+  for (int j = 0; j < kKeepMax; ++j) acc[j] = make_double2(0.0, 0.0);
+  for (int l = 0; l < Mold; ++l) {
+    const double2 v = V[(int64_t)(l / b) * slot_stride + row * d.ld + c0 + (l % b)];
+#pragma unroll
+    for (int j = 0; j < kKeepMax; ++j)
+      if (j < K) acc[j] = cadd(acc[j], cmul(v, S[(int64_t)l * d.pm + j]));
+  }
+  double2 resid[kBMax];
+  for (int q = 0; q < b; ++q) resid[q] = V[(int64_t)(nb_old - 1) * slot_stride + row * d.ld + c0 + q];
+#pragma unroll
+  for (int j = 0; j < kKeepMax; ++j)
+    if (j < K) V[(int64_t)(j / b) * slot_stride + row * d.ld + c0 + (j % b)] = acc[j];
+  for (int q = 0; q < b; ++q) V[(int64_t)st.keep_blocks * slot_stride + row * d.ld + c0 + q] = resid[q];
+}
+
+// U[inst][j][row] = sum_l V_l[row] S[l][j], j < nev (Ritz vectors of the last check).
+__global__ void k_lz_extract(rsed_lanczos_t st, LzDims d, double2* U, int64_t u_stride) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t row = t / d.n_inst;
+  const int inst = (int)(t % d.n_inst);
+  if (row >= d.n_orb) return;
+  const int* stt = st.state + inst * kStateInts;
+  const int b = st.inst_b[inst];
+  const int c0 = st.inst_col0[inst];
+  const int nb = stt[S_NB];
+  const int M = (nb - 1) * b;
+  const double2* S = reinterpret_cast<const double2*>(st.ritz_vec) + (int64_t)inst * d.pm * d.pm;
+  const double2* V = reinterpret_cast<const double2*>(st.V);
+  const int64_t slot_stride = d.n_orb * d.ld;
+  for (int j = 0; j < st.nev; ++j) {
+    double2 acc = make_double2(0.0, 0.0);
+    for (int l = 0; l < M; ++l)
+      acc = cadd(acc, cmul(V[(int64_t)(l / b) * slot_stride + row * d.ld + c0 + (l % b)],
+                           S[(int64_t)l * d.pm + j]));
+    U[((int64_t)inst * st.nev + j) * u_stride + row] = acc;
+  }
+}
+
+LzDims make_dims(const rsed_model_t* md, const rsed_sectors_t* sc, const rsed_lanczos_t* st) {
+  LzDims d;
+  d.n_orb = md->n_orbits;
+  d.ld = sc->ld;
+  d.n_inst = st->n_inst;
+  d.n_slots = st->n_slots;
+  d.pm = st->pm;
+  d.chunk_rows = st->chunk_rows;
+  d.n_chunks = (int)((d.n_orb + d.chunk_rows - 1) / d.chunk_rows);
+  d.pslots = st->n_slots + 3;
+  return d;
+}
+
+int check_lz(const rsed_model_t* md, const rsed_sectors_t* sc, const rsed_lanczos_t* st) {
+  RSED_REQUIRE(md && sc && st, RSED_EINVAL, "NULL descriptor");
+  RSED_REQUIRE(st->n_inst >= 1 && st->n_slots >= 2, RSED_EINVAL, "bad batch shape");
+  RSED_REQUIRE(st->bmax >= 1 && st->bmax <= kBMax, RSED_ERANGE, "block size > %d", kBMax);
+  RSED_REQUIRE(st->keep_blocks >= 1 && st->keep_blocks < st->n_slots, RSED_EINVAL, "bad keep_blocks");
+  RSED_REQUIRE(st->keep_blocks * st->bmax <= kKeepMax, RSED_ERANGE, "keep*b > %d", kKeepMax);
+  RSED_REQUIRE(st->n_slots * st->bmax <= kJacobiMax, RSED_ERANGE, "n_slots*b > %d", kJacobiMax);
+  RSED_REQUIRE(st->pm >= (st->n_slots + 1) * st->bmax, RSED_EINVAL, "pm too small");
+  RSED_REQUIRE(st->nev >= 1 && st->nev <= st->keep_blocks * 1 * st->bmax, RSED_EINVAL, "bad nev");
+  RSED_REQUIRE(st->chunk_rows >= 1, RSED_EINVAL, "bad chunk_rows");
+  RSED_REQUIRE(st->V && st->W && st->P && st->coef && st->partial && st->ritz_val && st->ritz_vec &&
+                   st->resid && st->state && st->inst_b && st->inst_col0,
+               RSED_EINVAL, "Lanczos buffers missing");
+  RSED_REQUIRE(st->precision == 64 || (st->precision == 32 && st->Xf), RSED_EINVAL,
+               "precision 32 needs the complex64 block buffer");
+  const LzDims d = make_dims(md, sc, st);
+  const int64_t need = (int64_t)d.n_chunks * d.n_inst * d.pslots * kBMax * kBMax * 2;
+  RSED_REQUIRE(st->partial_len >= need, RSED_ESCRATCH, "partial buffer too small (%lld < %lld)",
+               (long long)st->partial_len, (long long)need);
+  return RSED_OK;
+}
+
+int launch_pass(const rsed_lanczos_t& st, const LzDims& d, int pass, cudaStream_t stream) {
+  dim3 g1(d.n_chunks, d.n_inst);
+  k_lz_gram<<<g1, 128, 0, stream>>>(st, d);
+  RSED_CHECK_LAUNCH();
+  k_lz_finalize<<<d.n_inst, 128, 0, stream>>>(st, d, pass);
+  RSED_CHECK_LAUNCH();
+  const int64_t tot = d.n_orb * d.n_inst;
+  k_lz_update<<<(unsigned)((tot + 255) / 256), 256, 0, stream>>>(st, d, pass);
+  RSED_CHECK_LAUNCH();
+  return RSED_OK;
+}
+
+__global__ void k_lz_init_state(rsed_lanczos_t st) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= st.n_inst) return;
+  int* s = st.state + i * kStateInts;
+  s[S_NB] = 0;
+  s[S_STATUS] = 0;
+  s[S_RESTARTS] = 0;
+  s[S_ITERS] = 0;
+  s[S_ACTIVE] = 1;
+  s[S_RESTART_NB] = 0;
+  s[S_NEWSLOT] = 0;
+  s[S_NCONV] = 0;
+}
+
+__global__ void k_gather_rows(int64_t n_rows, const int32_t* orbit_of_row, const double2* src,
+                              int64_t src_ld, int src_col, double2* dst, int64_t dst_stride) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r < n_rows) dst[r * dst_stride] = src[(int64_t)orbit_of_row[r] * src_ld + src_col];
+}
+
+__global__ void k_scatter_rows(int64_t n_rows, const int32_t* orbit_of_row, const double2* src,
+                               int64_t src_stride, double2* dst, int64_t dst_ld, int dst_col) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r < n_rows) dst[(int64_t)orbit_of_row[r] * dst_ld + dst_col] = src[r * src_stride];
+}
+
+}  // namespace
+
+extern "C" int64_t rsed_lanczos_partial_len(int64_t n_orbits, int32_t chunk_rows, int32_t n_inst,
+                                            int32_t n_slots) {
+  const int64_t n_chunks = (n_orbits + chunk_rows - 1) / chunk_rows;
+  return n_chunks * n_inst * (int64_t)(n_slots + 3) * kBMax * kBMax * 2;
+}
+
+extern "C" int64_t rsed_lanczos_coef_len(int32_t n_inst, int32_t n_slots) {
+  return (int64_t)n_inst * 2 * (n_slots + 3) * kBMax * kBMax * 2;
+}
+
+extern "C" int rsed_lanczos_max_block(void) { return kBMax; }
+extern "C" int rsed_lanczos_max_keep(void) { return kKeepMax; }
+extern "C" int rsed_lanczos_max_projected(void) { return kJacobiMax; }
+
+static int set_ritz_smem() {
+  static bool done = false;
+  if (!done) {
+    RSED_TRY_CUDA(cudaFuncSetAttribute(k_lz_ritz, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)(2 * sizeof(double2) * kJacobiMax * kJacobiMax)));
+    done = true;
+  }
+  return RSED_OK;
+}
+
+extern "C" int rsed_lanczos_prepare(void) { return set_ritz_smem(); }
+
+extern "C" int rsed_lanczos_start(const rsed_model_t* md, const rsed_sectors_t* sc, rsed_lanczos_t* st,
+                                  void* stream_) {
+  int rc = check_lz(md, sc, st);
+  if (rc) return rc;
+  cudaStream_t stream = as_stream(stream_);
+  const LzDims d = make_dims(md, sc, st);
+  k_lz_init_state<<<(st->n_inst + 63) / 64, 64, 0, stream>>>(*st);
+  RSED_CHECK_LAUNCH();
+  RSED_TRY_CUDA(cudaMemsetAsync(st->P, 0, sizeof(double2) * (size_t)st->n_inst * d.pm * d.pm, stream));
+  // start block sits in W: two CholQR passes with an empty basis
+  rc = launch_pass(*st, d, 1, stream);
+  if (rc) return rc;
+  // pass 2 with nb = 0 appends slot 0 and sets nb = 1
+  return launch_pass(*st, d, 2, stream);
+}
+
+extern "C" int rsed_lanczos_iterate(const rsed_model_t* md, const rsed_sectors_t* sc, rsed_lanczos_t* st,
+                                    int32_t n_iter, int32_t check_every, int32_t apply_variant,
+                                    void* stream_) {
+  int rc = check_lz(md, sc, st);
+  if (rc) return rc;
+  rc = set_ritz_smem();
+  if (rc) return rc;
+  RSED_REQUIRE(check_every >= 1, RSED_EINVAL, "check_every must be >= 1");
+  cudaStream_t stream = as_stream(stream_);
+  const LzDims d = make_dims(md, sc, st);
+  const double2* X = reinterpret_cast<const double2*>(st->V) + (int64_t)(st->n_slots + 1) * d.n_orb * d.ld;
+  for (int it = 0; it < n_iter; ++it) {
+    const void* xin = (st->precision == 32) ? (const void*)st->Xf : (const void*)X;
+    rc = rsed_apply_h(md, sc, xin, st->W, st->precision, apply_variant, stream_);
+    if (rc) return rc;
+    rc = launch_pass(*st, d, 1, stream);
+    if (rc) return rc;
+    rc = launch_pass(*st, d, 2, stream);
+    if (rc) return rc;
+    k_lz_ritz<<<d.n_inst, 256, 2 * sizeof(double2) * kJacobiMax * kJacobiMax, stream>>>(*st, d, check_every, 0);
+    RSED_CHECK_LAUNCH();
+    const int64_t tot = d.n_orb * d.n_inst;
+    k_lz_restart<<<(unsigned)((tot + 255) / 256), 256, 0, stream>>>(*st, d);
+    RSED_CHECK_LAUNCH();
+  }
+  return RSED_OK;
+}
+
+extern "C" int rsed_lanczos_extract(const rsed_model_t* md, const rsed_sectors_t* sc, rsed_lanczos_t* st,
+                                    double* U, int64_t u_stride, void* stream_) {
+  int rc = check_lz(md, sc, st);
+  if (rc) return rc;
+  RSED_REQUIRE(U != nullptr && u_stride >= md->n_orbits, RSED_EINVAL, "bad U buffer");
+  cudaStream_t stream = as_stream(stream_);
+  const LzDims d = make_dims(md, sc, st);
+  const int64_t tot = d.n_orb * d.n_inst;
+  k_lz_extract<<<(unsigned)((tot + 255) / 256), 256, 0, stream>>>(*st, d, reinterpret_cast<double2*>(U),
+                                                                   u_stride);
+  RSED_CHECK_LAUNCH();
+  return RSED_OK;
+}
+
+extern "C" int rsed_gather_rows(int64_t n_rows, const int32_t* orbit_of_row, const double* src,
+                                int64_t src_ld, int32_t src_col, double* dst, int64_t dst_stride,
+                                void* stream_) {
+  RSED_REQUIRE(n_rows >= 0 && orbit_of_row && src && dst, RSED_EINVAL, "bad gather arguments");
+  if (n_rows == 0) return RSED_OK;
+  k_gather_rows<<<(unsigned)((n_rows + 255) / 256), 256, 0, as_stream(stream_)>>>(
+      n_rows, orbit_of_row, reinterpret_cast<const double2*>(src), src_ld, src_col,
+      reinterpret_cast<double2*>(dst), dst_stride);
+  RSED_CHECK_LAUNCH();
+  return RSED_OK;
+}
+
+extern "C" int rsed_scatter_rows(int64_t n_rows, const int32_t* orbit_of_row, const double* src,
+                                 int64_t src_stride, double* dst, int64_t dst_ld, int32_t dst_col,
+                                 void* stream_) {
+  RSED_REQUIRE(n_rows >= 0 && orbit_of_row && src && dst, RSED_EINVAL, "bad scatter arguments");
+  if (n_rows == 0) return RSED_OK;
+  k_scatter_rows<<<(unsigned)((n_rows + 255) / 256), 256, 0, as_stream(stream_)>>>(
+      n_rows, orbit_of_row, reinterpret_cast<const double2*>(src), src_stride,
+      reinterpret_cast<double2*>(dst), dst_ld, dst_col);
+  RSED_CHECK_LAUNCH();
+  return RSED_OK;
+}

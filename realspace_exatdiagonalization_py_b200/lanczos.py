@@ -1,0 +1,336 @@
+"""Batched thick-restart block Lanczos on the device (K8) and the reference's
+``diagonalize_block_*`` API (``symmetry_resolved_ed.py:2180-2299``).
+
+A ``LanczosBatch`` holds any number of sector instances of one catalog; each
+instance owns ``b`` columns of the shared ``[n_orbits, ld]`` blocks.  The
+Lanczos recurrence, the two-pass block Gram-Schmidt, the projected-matrix
+eigen-solve and the restarts are FP64 on the GPU; only the matvec may run in
+FP32 (``precision=32``), in which case ``refine`` finishes the solve with an
+FP64 block Lanczos started from the FP32 Ritz vectors.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _lib
+from .hamiltonian import DeviceModel
+from .sector import SectorSet
+
+S_NB, S_STATUS, S_RESTARTS, S_ITERS, S_ACTIVE = 0, 1, 2, 3, 4
+S_NCONV = 7
+
+__all__ = [
+    "LanczosBatch",
+    "LanczosParams",
+    "start_block",
+    "diagonalize_block_dense",
+    "diagonalize_block_arpack",
+    "diagonalize_block_matrixfree",
+]
+
+
+@dataclass
+class LanczosParams:
+    block: int = 2
+    n_slots: int = 16
+    keep_blocks: int = 0  # 0 = automatic: ceil((nev + block) / block), bounded
+    tol: float = 1e-10
+    max_restarts: int = 200
+    check_every: int = 2
+    precision: int = 64
+    apply_variant: int = 0
+
+
+def start_block(n: int, b: int, seed: int = 12345) -> np.ndarray:
+    """Seeded complex-normal start block ``[n, b]``, each column normalised.
+
+    Column 0 with ``seed=12345`` is the reference's ``v0``
+    (``symmetry_resolved_ed.py:2291-2293``)."""
+    cols = []
+    for j in range(b):
+        rng = np.random.default_rng(seed + 7919 * j)
+        v = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+        cols.append(v / np.linalg.norm(v))
+    return np.stack(cols, axis=1)
+
+
+def _auto_keep(nev: int, b: int, n_slots: int) -> int:
+    kmax = _lib.load().rsed_lanczos_max_keep()
+    keep = max(1, math.ceil((nev + max(b, 2)) / b))
+    keep = min(keep, n_slots - 2, kmax // b)
+    if keep * b < nev:
+        raise ValueError(f"nev={nev} needs keep_blocks*block >= nev (block={b}, n_slots={n_slots})")
+    return keep
+
+
+class LanczosBatch:
+    """Device state of ``len(inst_sectors)`` simultaneous sector solves."""
+
+    def __init__(self, model: DeviceModel, sset: SectorSet, inst_sectors: list[int], nev: int,
+                 params: LanczosParams | None = None, block_sizes: list[int] | None = None):
+        lib = _lib.lib()
+        _lib.check(lib.rsed_lanczos_prepare())
+        p = params or LanczosParams()
+        self.p = p
+        self.model = model
+        self.sset = sset
+        self.nev = nev
+        self.inst_sectors = list(inst_sectors)
+        n_inst = len(inst_sectors)
+        bs = list(block_sizes) if block_sizes else [p.block] * n_inst
+        bmax = max(bs)
+        if bmax > lib.rsed_lanczos_max_block():
+            raise ValueError("block size too large")
+        if p.n_slots * bmax > lib.rsed_lanczos_max_projected():
+            raise ValueError("n_slots * block exceeds the projected-matrix limit")
+        self.block_sizes = bs
+        self.keep = p.keep_blocks or _auto_keep(nev, min(bs), p.n_slots)
+        if self.keep * bmax > lib.rsed_lanczos_max_keep():
+            self.keep = max(1, lib.rsed_lanczos_max_keep() // bmax)
+        if self.keep * min(bs) < nev:
+            raise ValueError("nev larger than the restart basis")
+        dev = model.catalog.table.device
+        self.dev = dev
+        n_orb = model.catalog.n_orbits
+        self.n_orb = n_orb
+        col0 = np.cumsum([0] + bs[:-1]).astype(np.int32)
+        self.col0 = col0
+        self.n_cols = int(sum(bs))
+        self.ld = self.n_cols + (self.n_cols & 1)
+        col_sector = np.concatenate([[s] * b for s, b in zip(inst_sectors, bs)]).astype(np.int32)
+        self.col_sector = torch.from_numpy(col_sector).to(dev)
+        self.inst_col0 = torch.from_numpy(col0).to(dev)
+        self.inst_b = torch.tensor(bs, dtype=torch.int32, device=dev)
+        S = p.n_slots
+        self.pm = (S + 1) * bmax
+        self.chunk_rows = 64 if n_orb <= 65536 else (256 if n_orb <= 1 << 20 else 1024)
+        c128 = torch.complex128
+        self.V = torch.zeros((S + 2, n_orb, self.ld), dtype=c128, device=dev)
+        self.W = torch.zeros((n_orb, self.ld), dtype=c128, device=dev)
+        self.Xf = torch.zeros((n_orb, self.ld), dtype=torch.complex64, device=dev) if p.precision == 32 else None
+        self.P = torch.zeros((n_inst, self.pm, self.pm), dtype=c128, device=dev)
+        self.coef = torch.zeros(int(lib.rsed_lanczos_coef_len(n_inst, S)), dtype=torch.float64, device=dev)
+        plen = int(lib.rsed_lanczos_partial_len(n_orb, self.chunk_rows, n_inst, S))
+        self.partial = torch.zeros(plen, dtype=torch.float64, device=dev)
+        self.ritz_val = torch.zeros((n_inst, self.pm), dtype=torch.float64, device=dev)
+        self.ritz_vec = torch.zeros((n_inst, self.pm, self.pm), dtype=c128, device=dev)
+        self.resid = torch.zeros((n_inst, self.pm), dtype=torch.float64, device=dev)
+        self.state = torch.zeros((n_inst, 8), dtype=torch.int32, device=dev)
+        self.c = _lib.RsedLanczos(
+            n_inst, S, nev, self.keep, p.max_restarts, p.precision, bmax, self.chunk_rows, self.pm, 0,
+            float(p.tol), _lib.ptr(self.inst_col0), _lib.ptr(self.inst_b), _lib.ptr(self.V),
+            _lib.ptr(self.W), _lib.ptr(self.Xf), _lib.ptr(self.P), _lib.ptr(self.coef),
+            _lib.ptr(self.partial), plen, _lib.ptr(self.ritz_val), _lib.ptr(self.ritz_vec),
+            _lib.ptr(self.resid), _lib.ptr(self.state),
+        )
+        self.sc = sset.sectors_struct(self.col_sector, self.n_cols, self.ld)
+
+    @property
+    def n_inst(self) -> int:
+        return len(self.inst_sectors)
+
+    # -- start ------------------------------------------------------------
+    def load_start(self, blocks: list[torch.Tensor | np.ndarray | None], seeds: list[int] | None = None,
+                   stream=None) -> None:
+        """Place each instance's start block ``[D_s, b]`` (compact sector rows)
+        into ``W``; ``None`` draws the seeded block of :func:`start_block`."""
+        self.W.zero_()
+        lib = _lib.lib()
+        sp = _lib.stream_ptr(stream)
+        for i, s in enumerate(self.inst_sectors):
+            d = self.sset.dims[s]
+            b = self.block_sizes[i]
+            blk = blocks[i] if blocks is not None else None
+            if blk is None:
+                seed = 12345 if seeds is None else seeds[i]
+                blk = start_block(d, b, seed)
+            if isinstance(blk, np.ndarray):
+                blk = torch.from_numpy(np.ascontiguousarray(blk, dtype=np.complex128))
+            blk = blk.to(self.dev, non_blocking=True).reshape(d, b).to(torch.complex128)
+            blk = blk.t().contiguous()  # [b, d]
+            oor, _ = self.sset.rows(s)
+            for j in range(b):
+                _lib.check(lib.rsed_scatter_rows(d, _lib.ptr(oor), _lib.ptr(blk[j]), 1, _lib.ptr(self.W),
+                                                 self.ld, int(self.col0[i]) + j, sp))
+
+    def start(self, stream=None) -> None:
+        _lib.check(_lib.lib().rsed_lanczos_start(ctypes.byref(self.model.c), ctypes.byref(self.sc),
+                                                 ctypes.byref(self.c), _lib.stream_ptr(stream)))
+
+    def iterate(self, n_iter: int = 1, stream=None) -> None:
+        _lib.check(_lib.lib().rsed_lanczos_iterate(
+            ctypes.byref(self.model.c), ctypes.byref(self.sc), ctypes.byref(self.c), n_iter,
+            self.p.check_every, self.p.apply_variant, _lib.stream_ptr(stream)))
+
+    def status(self) -> np.ndarray:
+        return self.state.cpu().numpy()
+
+    def done(self) -> bool:
+        return not bool(self.state[:, S_ACTIVE].any().item())
+
+    def run(self, max_iter: int = 4000, poll: int = 8, graph: bool = False, stream=None) -> np.ndarray:
+        """Iterate until every instance converged or failed; returns the state."""
+        it = 0
+        g = None
+        if graph:
+            g = self.capture(poll)
+        while it < max_iter:
+            if g is not None:
+                g.replay()
+            else:
+                self.iterate(poll, stream)
+            it += poll
+            if self.done():
+                break
+        st = self.status()
+        bad = [i for i in range(self.n_inst) if st[i, S_STATUS] != 1]
+        if bad:
+            code = int(st[bad[0], S_STATUS])
+            if code == 0:
+                code = _lib.RSED_ENOTCONV
+            raise _lib.RsedError(code, f"instances {bad} did not converge (state {st[bad[0]].tolist()})")
+        return st
+
+    def capture(self, n_iter: int):
+        """CUDA graph of ``n_iter`` iterations (replayed by ``run(graph=True)``)."""
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            self.iterate(1, s)  # warm-up outside the graph (kernel attributes, lazy loading)
+        torch.cuda.current_stream().wait_stream(s)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=s):
+            self.iterate(n_iter, s)
+        return g
+
+    # -- results ----------------------------------------------------------
+    def eigenvalues(self) -> np.ndarray:
+        return self.ritz_val[:, : self.nev].cpu().numpy()
+
+    def residuals(self) -> np.ndarray:
+        return self.resid[:, : self.nev].cpu().numpy()
+
+    def ritz_vectors_orbit(self, stream=None) -> torch.Tensor:
+        """``U [n_inst, nev, n_orbits]`` in the orbit-row layout."""
+        U = torch.zeros((self.n_inst, self.nev, self.n_orb), dtype=torch.complex128, device=self.dev)
+        _lib.check(_lib.lib().rsed_lanczos_extract(ctypes.byref(self.model.c), ctypes.byref(self.sc),
+                                                   ctypes.byref(self.c), _lib.ptr(U), self.n_orb,
+                                                   _lib.stream_ptr(stream)))
+        return U
+
+    def eigenvectors(self, U: torch.Tensor | None = None, stream=None) -> list[torch.Tensor]:
+        """Per instance ``[D_s, nev]`` eigenvectors in the sector's basis order."""
+        U = self.ritz_vectors_orbit(stream) if U is None else U
+        out = []
+        lib = _lib.lib()
+        sp = _lib.stream_ptr(stream)
+        for i, s in enumerate(self.inst_sectors):
+            d = self.sset.dims[s]
+            oor, _ = self.sset.rows(s)
+            vec = torch.empty((self.nev, d), dtype=torch.complex128, device=self.dev)
+            for j in range(self.nev):
+                _lib.check(lib.rsed_gather_rows(d, _lib.ptr(oor), _lib.ptr(U[i, j]), 1, 0,
+                                                _lib.ptr(vec[j]), 1, sp))
+            out.append(vec.t())
+        return out
+
+
+def refine(batch: LanczosBatch, *, tol: float = 1e-10, n_slots: int = 8, max_restarts: int = 50,
+           poll: int = 4) -> LanczosBatch:
+    """FP64 finish of an FP32-matvec solve: an FP64 block Lanczos per instance
+    whose start block is the ``nev`` FP32 Ritz vectors (block size = nev)."""
+    nev = batch.nev
+    bsz = nev
+    while bsz * n_slots > _lib.load().rsed_lanczos_max_projected():
+        n_slots -= 1
+    keep = max(1, min(_lib.load().rsed_lanczos_max_keep() // bsz, n_slots - 2))
+    p = LanczosParams(block=bsz, n_slots=n_slots, keep_blocks=keep, tol=tol, max_restarts=max_restarts,
+                      check_every=1, precision=64, apply_variant=0)
+    fb = LanczosBatch(batch.model, batch.sset, batch.inst_sectors, nev, p)
+    U = batch.ritz_vectors_orbit()
+    fb.W.zero_()
+    for i in range(batch.n_inst):
+        c0 = int(fb.col0[i])
+        fb.W[:, c0 : c0 + nev] = U[i].t()
+    fb.start()
+    fb.run(poll=poll)
+    return fb
+
+
+# ---------------------------------------------------------------------------
+# reference API
+# ---------------------------------------------------------------------------
+
+
+def diagonalize_block_dense(H, *, nev: int = 5):
+    """Dense Hermitian solve of a small block on its UPPER triangle
+    (``symmetry_resolved_ed.py:2180-2211``); runs ``zheevd`` on the GPU."""
+    n = H.shape[0]
+    if n == 0:
+        return np.zeros(0, dtype=np.float64), np.zeros((0, 0), dtype=np.complex128)
+    dense = H.toarray() if hasattr(H, "toarray") else np.asarray(H)
+    A = torch.from_numpy(np.ascontiguousarray(dense, dtype=np.complex128)).to(
+        torch.device("cuda", torch.cuda.current_device()))
+    vals, vecs = torch.linalg.eigh(A, UPLO="U")
+    k = min(nev, n)
+    return vals[:k].cpu().numpy().real, vecs[:, :k].cpu().numpy()
+
+
+def _solve_sector(model: DeviceModel, sset: SectorSet, s: int, nev: int, params: LanczosParams):
+    b = LanczosBatch(model, sset, [s], nev, params)
+    b.load_start(None)
+    b.start()
+    b.run()
+    if params.precision == 32:
+        b = refine(b)
+    vals = b.eigenvalues()[0]
+    vecs = b.eigenvectors()[0]
+    return vals, vecs
+
+
+def diagonalize_block_arpack(H, *, nev: int = 5, params: LanczosParams | None = None,
+                             basis=None, model: DeviceModel | None = None):
+    """Lowest ``nev`` eigenpairs of a sector block: dense for ``n <= 500``,
+    else the device block Lanczos (``symmetry_resolved_ed.py:2214-2245``)."""
+    n = H.shape[0]
+    if n == 0:
+        return np.zeros(0, dtype=np.float64), np.zeros((0, 0), dtype=np.complex128)
+    if n <= 500 or basis is None or model is None:
+        if n > 500:
+            raise ValueError("diagonalize_block_arpack needs the sector basis for n > 500")
+        return diagonalize_block_dense(H, nev=nev)
+    vals, vecs = _solve_sector(model, basis.sector_set, basis.sector_index, nev,
+                               params or LanczosParams(block=min(4, nev)))
+    return vals, vecs.cpu().numpy()
+
+
+def diagonalize_block_matrixfree(H_op, n: int, *, nev: int = 5, params: LanczosParams | None = None):
+    """Lowest ``nev`` eigenpairs of a matrix-free sector operator
+    (``symmetry_resolved_ed.py:2248-2299``).  ``n <= 500``: the dense block is
+    assembled on the GPU from ``H_op`` applied to the unit vectors and solved
+    on the triangle matching the reference's ``eigh(UPLO="U")``; larger
+    sectors use the device block Lanczos."""
+    if n == 0:
+        return np.zeros(0, dtype=np.float64), np.zeros((0, 0), dtype=np.complex128)
+    if n <= 500:
+        dev = torch.device("cuda", torch.cuda.current_device())
+        cols = []
+        for c0 in range(0, n, 64):
+            c1 = min(n, c0 + 64)
+            E = torch.zeros((n, c1 - c0), dtype=torch.complex128, device=dev)
+            E[torch.arange(c0, c1, device=dev), torch.arange(c1 - c0, device=dev)] = 1.0
+            cols.append(H_op.matvec_device(E, c1 - c0))
+        A = torch.cat(cols, dim=1)
+        # the kernel returns H^dagger; its lower triangle is the reference's upper one
+        vals, vecs = torch.linalg.eigh(A, UPLO="L")
+        k = min(nev, n)
+        return vals[:k].cpu().numpy().real, vecs[:, :k].cpu().numpy()
+    params = params or LanczosParams(block=min(4, nev))
+    vals, vecs = _solve_sector(H_op.model, H_op.basis.sector_set, H_op.basis.sector_index, nev, params)
+    return vals, vecs.cpu().numpy()

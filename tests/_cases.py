@@ -1,0 +1,57 @@
+"""Shared builders of the golden cases (models from this package's builders,
+which the CPU tests pin to the reference's term lists)."""
+
+from fractions import Fraction
+
+import numpy as np
+
+
+def model_for(case):
+    from realspace_exatdiagonalization_py_b200 import models
+
+    if case == "heisenberg16":
+        return models.build_heisenberg_second_quantized_model(16, 1.0)
+    if case == "checkerboard24":
+        p = dict(models.params_Sun_Gu_Katsura_Sarma)
+        p.update({"V1": 1.0, "V2": 0.0, "V3": 0.0})
+        return models.build_zero_flux_fermionic_fci_second_quantized_model(sample_size=[3, 4], params=p)
+    if case.startswith("haldane12"):
+        return models.build_zero_flux_bosonic_fci_second_quantized_model(
+            sample_size=[2, 3], params=models.params_DNSheng)
+    if case == "checkerboard12_flux":
+        return models.build_zero_flux_fermionic_fci_second_quantized_model(
+            sample_size=[2, 3], params=models.params_Sun_Gu_Katsura_Sarma)
+    if case == "haldane24_flux":
+        p = {"t": 1.0, "t'": 0.6, "t''": 0.0, "phi_over_2pi": 0.2, "V1": 1.0, "V2": 0.0}
+        return models.build_zero_flux_bosonic_fci_second_quantized_model(sample_size=[3, 4], params=p)
+    if case == "hubbard12":
+        return models.build_spinful_hubbard_second_quantized_model([2, 3], 1.0, 4.0)
+    raise KeyError(case)
+
+
+def ed_data_for(case, g):
+    import realspace_exatdiagonalization_py_b200 as ed
+
+    m = model_for(case)
+    theta = [float(x) for x in g["theta"]]
+    if any(theta):
+        ed.update_second_quantized_model_with_twisted_phases(m, twisted_phases_over_2π=theta)
+        G = ed.build_translation_group(m.lattice, theta)
+    else:
+        G = ed.build_translation_group(m.lattice)
+    return ed.build_ed_data(m, filling_fraction=Fraction(int(g["n_filled"]), m.lattice.n_site),
+                            symmetry_group=G)
+
+
+def oracle_block(g, s):
+    """The reference's sector block (CSR) rebuilt by the oracle from the
+    golden catalog tables."""
+    from oracle import port
+
+    cat = port.catalog(int(g["n_site"]), int(g["n_filled"]), (g["perm"] - 1).astype(np.uint8), g["eta"],
+                       bool(g["fermionic"]))
+    bil = [(int(i), int(j), t) for (i, j), t in zip(g["bil_ij"], g["bil_t"])]
+    den = [(int(i), int(j), v) for (i, j), v in zip(g["den_ij"], g["den_v"])]
+    chi = g["chi"][s]
+    orbits = port.sector_orbits(cat, chi)
+    return port.csr_block(cat, int(g["n_site"]), orbits, bil, den, chi, bool(g["fermionic"])), orbits

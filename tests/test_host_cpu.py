@@ -1,0 +1,207 @@
+"""CPU tests: model builders, groups/irreps, the scalar mask API, the C ABI
+symbol table.  No GPU needed."""
+
+import math
+import os
+import re
+from collections import Counter
+from fractions import Fraction
+
+import numpy as np
+import pytest
+
+import realspace_exatdiagonalization_py_b200 as ed
+from realspace_exatdiagonalization_py_b200 import _lib, lattice, models
+from realspace_exatdiagonalization_py_b200.symmetry import (
+    _binom_table,
+    _gosper_next,
+    rank_combination,
+    unrank_combination,
+)
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _multiset(terms, digits=14):
+    return Counter((int(i), int(j), round(complex(t).real, digits), round(complex(t).imag, digits))
+                   for (i, j, t) in terms)
+
+
+def _golden_terms(g, key):
+    return [(int(i), int(j), t) for (i, j), t in zip(g[key + "_ij"], g[key + "_t" if key == "bil" else key + "_v"])]
+
+
+# ---- model builders reproduce the reference's term lists --------------------
+
+def _model_for(case):
+    if case == "heisenberg16":
+        return models.build_heisenberg_second_quantized_model(16, 1.0)
+    if case == "checkerboard24":
+        p = dict(models.params_Sun_Gu_Katsura_Sarma)
+        p.update({"V1": 1.0, "V2": 0.0, "V3": 0.0})
+        return models.build_zero_flux_fermionic_fci_second_quantized_model(sample_size=[3, 4], params=p)
+    if case.startswith("haldane12"):
+        return models.build_zero_flux_bosonic_fci_second_quantized_model(
+            sample_size=[2, 3], params=models.params_DNSheng)
+    if case == "checkerboard12_flux":
+        return models.build_zero_flux_fermionic_fci_second_quantized_model(
+            sample_size=[2, 3], params=models.params_Sun_Gu_Katsura_Sarma)
+    if case == "haldane24_flux":
+        p = {"t": 1.0, "t'": 0.6, "t''": 0.0, "phi_over_2pi": 0.2, "V1": 1.0, "V2": 0.0}
+        return models.build_zero_flux_bosonic_fci_second_quantized_model(sample_size=[3, 4], params=p)
+    if case == "hubbard12":
+        return models.build_spinful_hubbard_second_quantized_model([2, 3], 1.0, 4.0)
+    raise KeyError(case)
+
+
+@pytest.mark.parametrize("case", ["heisenberg16", "checkerboard24", "haldane12", "haldane12_flux",
+                                  "checkerboard12_flux", "haldane24_flux", "hubbard12"])
+def test_model_terms_match_reference(golden, case):
+    g = golden(case)
+    m = _model_for(case)
+    theta = list(g["theta"])
+    if any(theta):
+        ed.update_second_quantized_model_with_twisted_phases(m, twisted_phases_over_2π=theta)
+    assert _multiset(m.bilinear_terms) == _multiset(_golden_terms(g, "bil"))
+    assert _multiset(m.density_density_terms) == _multiset(_golden_terms(g, "den"))
+    # group arrays and characters bit for bit
+    G = ed.build_translation_group(m.lattice, theta if any(theta) else None)
+    np.testing.assert_array_equal(np.array([op.perm for op in G.operations]), g["perm"])
+    np.testing.assert_array_equal(np.array([op.perm_phases for op in G.operations]), g["eta"])
+    irreps = ed.build_irrep_list(G, m.lattice)
+    np.testing.assert_array_equal(np.array([ir.values for ir in irreps]), g["chi"])
+
+
+def test_term_counts_of_reference_tests():
+    # test/test_core.py:106-140 of the reference
+    m = models.build_zero_flux_bosonic_fci_second_quantized_model(sample_size=[2, 3],
+                                                                  params=models.params_DNSheng)
+    assert m.lattice.n_site == 12 and len(m.bilinear_terms) == 144
+    summed = {}
+    for (i, j, t) in m.bilinear_terms:
+        summed[(i, j)] = summed.get((i, j), 0j) + t
+    for (i, j), t in summed.items():
+        assert abs(t - np.conj(summed.get((j, i), 0j))) < 1e-12
+    c = models.build_zero_flux_fermionic_fci_second_quantized_model(
+        sample_size=[3, 4], params=models.params_Sun_Gu_Katsura_Sarma)
+    assert c.lattice.n_site == 24 and len(c.density_density_terms) == 96
+    assert c.particle_statistics is ed.Particle_Statistics.FERMIONIC
+    h = models.build_spinful_hubbard_second_quantized_model([2, 2])
+    assert h.lattice.n_site == 8 and len(h.density_density_terms) == 4
+    s = models.build_heisenberg_second_quantized_model(8, J=1.0)
+    assert s.lattice.n_site == 8 and s.particle_statistics is ed.Particle_Statistics.BOSONIC
+
+
+# ---- scalar API known answers (reference test/test_core.py:54-87) ----------
+
+def test_boson_permutation_action():
+    op = ed.Symmetry_Operation("t", [2, 3, 1])
+    m, ph = ed.apply_operation_to_mask(0b101, op, ed.Particle_Statistics.BOSONIC)
+    assert m == 0b011 and abs(ph - 1.0) == 0.0
+
+
+def test_fermion_permutation_sign():
+    op = ed.Symmetry_Operation("id", [1, 2, 3])
+    _, ph = ed.apply_operation_to_mask(0b001, op, ed.Particle_Statistics.FERMIONIC)
+    assert ph == 1.0 + 0.0j
+    swap = ed.Symmetry_Operation("swap", [2, 1, 3])
+    _, ph = ed.apply_operation_to_mask(0b011, swap, ed.Particle_Statistics.FERMIONIC)
+    assert ph == -1.0 + 0.0j
+
+
+def test_canonical_representative():
+    ops = [ed.Symmetry_Operation("id", [1, 2, 3, 4]), ed.Symmetry_Operation("T", [4, 1, 2, 3])]
+    G = ed.Finite_Symmetry_Group("cyclic", ops, identity_idx=0)
+    rep, g, _ = ed.get_canonical_representative(0b1000, G, ed.Particle_Statistics.BOSONIC)
+    assert rep == 0b0100 and g == 1
+
+
+def test_translation_group_structure():
+    lat = lattice.initialize_real_space_lattice(sample_size=[2, 3], lattice_name="honeycomb",
+                                                pbc_indicator=[True, True])
+    G = ed.build_translation_group(lat)
+    assert len(G.operations) == 6 and G.operations[0].label == (0, 0)
+    irreps = ed.build_translation_irrep_list(G, lat)
+    assert len(irreps) == 6 and irreps[0].label == (0, 0)
+
+
+def test_group_validation_errors():
+    with pytest.raises(ValueError):
+        ed.Finite_Symmetry_Group("empty", [])
+    with pytest.raises(ValueError):
+        ed.Finite_Symmetry_Group("bad", [ed.Symmetry_Operation("x", [2, 1])])
+    lat = lattice.initialize_real_space_lattice(sample_size=[2, 3])
+    with pytest.raises(ValueError):
+        ed.build_translation_group(lat, [0.1])
+    G = ed.build_translation_group(lat)
+    G.name = "other"
+    with pytest.raises(ValueError):
+        ed.build_irrep_list(G, lat)
+
+
+def test_rank_unrank_gosper():
+    n, k = 12, 5
+    bt = _binom_table(n, k)
+    m = (1 << k) - 1
+    for r in range(math.comb(n, k)):
+        assert rank_combination(m, bt) == r
+        assert unrank_combination(r, n, k, bt) == m
+        m = _gosper_next(m)
+
+
+def test_hopping_phase():
+    F = ed.Particle_Statistics.FERMIONIC
+    assert ed.hopping_phase_for_stats(F, 0b0100, 1, 4) == -1
+    assert ed.hopping_phase_for_stats(F, 0b0110, 1, 4) == 1
+    assert ed.hopping_phase_for_stats(ed.Particle_Statistics.BOSONIC, 0b0100, 1, 4) == 1
+
+
+def test_filling_assertion_without_gpu():
+    m = models.build_zero_flux_bosonic_fci_second_quantized_model(sample_size=[2, 3],
+                                                                  params=models.params_DNSheng)
+    G = ed.build_translation_group(m.lattice)
+    with pytest.raises(AssertionError):
+        ed.build_ed_data(m, filling_fraction=Fraction(1, 5), symmetry_group=G)
+
+
+def test_term_merging_and_on_site_rejection():
+    from realspace_exatdiagonalization_py_b200.hamiltonian import _merge_terms
+
+    begin, to, amp, jw = _merge_terms([(1, 3, 1.0), (1, 3, 0.5j), (3, 1, 2.0), (2, 1, 1.0)], 4)
+    assert list(begin) == [0, 1, 2, 3, 3]
+    assert list(to) == [2, 0, 0] and amp[0] == 1.0 + 0.5j
+    assert int(jw[0]) == 0b10  # site 2 lies between sites 1 and 3
+    with pytest.raises(ValueError):
+        _merge_terms([(2, 2, 1.0)], 4)
+
+
+# ---- the C ABI --------------------------------------------------------------
+
+def _declared_symbols():
+    text = open(os.path.join(ROOT, "include", "rsed.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(rsed_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _lib.load()
+    names = _declared_symbols()
+    assert len(names) >= 25
+    for n in names:
+        assert hasattr(lib, n), n
+    assert set(names) <= set(_lib.SIGNATURES), set(names) - set(_lib.SIGNATURES)
+    assert lib.rsed_version().startswith(b"rsed-b200")
+
+
+def test_library_rejects_bad_arguments_without_gpu():
+    lib = _lib.load()
+    # descriptor checks run before any CUDA call
+    grp = _lib.RsedGroup(70, 3, 4, 0, 10, None, None, None, None)
+    import ctypes
+
+    n = ctypes.c_int64(0)
+    rc = lib.rsed_catalog_count(ctypes.byref(grp), None, 0, ctypes.byref(n), None)
+    assert rc == _lib.RSED_ERANGE
+    assert b"n_site" in lib.rsed_last_error()
+    with pytest.raises(ValueError):
+        _lib.check(rc)

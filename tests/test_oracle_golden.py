@@ -1,0 +1,83 @@
+"""The CPU oracle (oracle/port.py) against the reference's golden fixtures.
+
+Pins the oracle before it is trusted as the checker of the GPU kernels:
+catalog tables bit for bit, stabilizers, the flux phase update, sector
+dimensions and sector eigenvalues (ARPACK / dense, |dE| < 1e-10).
+"""
+
+import numpy as np
+import pytest
+
+from oracle import port
+
+CASES = ["heisenberg16", "checkerboard24", "haldane12", "haldane12_flux", "checkerboard12_flux",
+         "haldane24_flux", "hubbard12"]
+
+
+def _oracle_catalog(g, eta=None):
+    perm0 = (g["perm"] - 1).astype(np.uint8)
+    return port.catalog(int(g["n_site"]), int(g["n_filled"]), perm0,
+                        g["eta"] if eta is None else eta, bool(g["fermionic"]))
+
+
+def _check_catalog(cat, g, prefix=""):
+    np.testing.assert_array_equal(cat["reprs"], g[prefix + "reprs"])
+    np.testing.assert_array_equal(cat["rep_rank"], g[prefix + "rep_rank"])
+    np.testing.assert_array_equal(cat["rep_sym"], g[prefix + "rep_sym"])
+    np.testing.assert_array_equal(cat["rep_amp"], g[prefix + "rep_amp"])
+    off = g[prefix + "stab_off"]
+    for o in range(len(cat["reprs"])):
+        np.testing.assert_array_equal(cat["stab_g"][o], g[prefix + "stab_g"][off[o]:off[o + 1]])
+        np.testing.assert_array_equal(cat["stab_phase"][o], g[prefix + "stab_phase"][off[o]:off[o + 1]])
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_catalog_matches_reference(golden, case):
+    g = golden(case)
+    _check_catalog(_oracle_catalog(g), g)
+
+
+@pytest.mark.parametrize("case", ["haldane12_flux", "checkerboard12_flux", "haldane24_flux"])
+def test_phase_update_matches_reference(golden, case):
+    g = golden(case)
+    eta0 = np.ones_like(g["eta"])
+    cat = _oracle_catalog(g, eta0)
+    port.update_phases(cat, int(g["n_site"]), (g["perm"] - 1).astype(np.uint8), g["eta"],
+                       bool(g["fermionic"]))
+    _check_catalog(cat, g, "upd_")
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_sector_dims_and_energies(golden, case):
+    g = golden(case)
+    cat = _oracle_catalog(g)
+    bil = [(int(i), int(j), t) for (i, j), t in zip(g["bil_ij"], g["bil_t"])]
+    den = [(int(i), int(j), v) for (i, j), v in zip(g["den_ij"], g["den_v"])]
+    dims = [len(port.sector_orbits(cat, chi)) for chi in g["chi"]]
+    np.testing.assert_array_equal(dims, g["sector_dims"])
+    nev = int(g["nev"])
+    for s, ref in zip(g["eig_sectors"], g["eig_vals"]):
+        chi = g["chi"][s]
+        orbits = port.sector_orbits(cat, chi)
+        H = port.csr_block(cat, int(g["n_site"]), orbits, bil, den, chi, bool(g["fermionic"]))
+        w, _ = port.solve(H, nev)
+        k = min(nev, len(w))
+        np.testing.assert_allclose(w[:k], ref[:k], atol=1e-10, rtol=0)
+
+
+def test_rank_unrank_roundtrip():
+    n, k = 20, 7
+    bt = port.binom_table(n, k)
+    r = np.arange(0, 77520, 37, dtype=np.int64)
+    m = port.unrank(r, n, k, bt)
+    np.testing.assert_array_equal(port.rank(m, n, bt), r)
+    assert np.all(np.bitwise_count(m) == k)
+
+
+def test_rank_beyond_42_sites():
+    # the reference's >42-site fallback returns 0; the oracle's rank is exact
+    n, k = 48, 3
+    bt = port.binom_table(n, k)
+    r = np.array([0, 1, 17295, 17296 - 1], dtype=np.int64)
+    m = port.unrank(r, n, k, bt)
+    np.testing.assert_array_equal(port.rank(m, n, bt), r)
