@@ -1,0 +1,508 @@
+#!/usr/bin/env python
+"""Sector-solve throughput of the symmetry-resolved ED path on B200.
+
+Workload (default ``checkerboard24``): spinless fermions on the 3x4x2
+checkerboard (24 sites, 4 particles, 10,626 states, 892 orbits), translation
+group of order 12; one step = all 12 momentum sectors, lowest 6 eigenvalues
+each, solved in one batched block-Lanczos (FP32 matvec, FP64 recurrence and
+reorthogonalisation, FP64 refinement) to |dE| < 1e-10 against the CPU oracle.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+One JSON line on rank 0.  N > 1 runs independent replicas (one per GPU, no
+collective in the data path); ``value`` is the total over all ranks divided
+by the slowest rank's time.  ``--impl reference`` times the CPU restatement
+of the reference's numpy/ARPACK path on the host cores instead.
+"""
+
+from __future__ import annotations
+
+import os
+
+_NCPU = os.cpu_count() or 1
+for _v in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
+    os.environ.setdefault(_v, str(_NCPU))
+
+import argparse  # noqa: E402
+import json  # noqa: E402
+import statistics  # noqa: E402
+import subprocess  # noqa: E402
+import sys  # noqa: E402
+import threading  # noqa: E402
+import time  # noqa: E402
+from fractions import Fraction  # noqa: E402
+
+import numpy as np  # noqa: E402
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "checkerboard24": dict(nev=6, desc="checkerboard 3x4x2, 24 sites, 4 fermions, |G|=12, 12 sectors"),
+    "heisenberg16": dict(nev=4, desc="Heisenberg ring N=16, 8 up spins, |G|=16, 16 sectors"),
+}
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+# ---------------------------------------------------------------------------
+# CPU side: the oracle (restatement of the reference's numpy/scipy path)
+# ---------------------------------------------------------------------------
+
+
+def cpu_sector_solves(model, n_filled, G, irreps, nev, budget_s=20.0, min_sectors=3):
+    """Time the reference algorithm (projection table + CSR + ARPACK per
+    sector, catalog built outside the timing as in the reference benchmark)
+    on a bounded sample of sectors; returns (solves/s, n_timed, eigvals)."""
+    from oracle import port
+
+    n = G.n_site
+    fermion = model.particle_statistics.name == "FERMIONIC"
+    perm0, eta = port.group_arrays(G)
+    cat = port.catalog(n, n_filled, perm0, eta, fermion)
+    t_all, done, vals = 0.0, 0, {}
+    s = 0
+    while s < len(irreps) and (t_all < budget_s or done < min_sectors):
+        chi = np.asarray(irreps[s].values, dtype=np.complex128)
+        t0 = time.perf_counter()
+        orbits = port.sector_orbits(cat, chi)
+        H = port.csr_block(cat, n, orbits, model.bilinear_terms, model.density_density_terms, chi, fermion)
+        w, _ = port.solve(H, nev)
+        t_all += time.perf_counter() - t0
+        vals[s] = w
+        done += 1
+        s += 1
+    return done / t_all, done, vals, t_all
+
+
+def oracle_eigs(model, n_filled, G, irreps, nev):
+    from oracle import port
+
+    fermion = model.particle_statistics.name == "FERMIONIC"
+    perm0, eta = port.group_arrays(G)
+    cat = port.catalog(G.n_site, n_filled, perm0, eta, fermion)
+    out = {}
+    for s, ir in enumerate(irreps):
+        chi = np.asarray(ir.values, dtype=np.complex128)
+        orbits = port.sector_orbits(cat, chi)
+        H = port.csr_block(cat, G.n_site, orbits, model.bilinear_terms, model.density_density_terms, chi,
+                           fermion)
+        out[s] = port.solve(H, nev)[0]
+    return out
+
+
+def run_reference(args):
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return
+    from realspace_exatdiagonalization_py_b200 import models
+    import realspace_exatdiagonalization_py_b200.symmetry as sym
+
+    wl = WORKLOADS[args.workload]
+    model, nf = models.config_model(args.workload)
+    G = sym.build_translation_group(model.lattice)
+    irreps = sym.build_irrep_list(G, model.lattice)
+    per_step = []
+    for it in range(args.warmup + args.steps):
+        rate, n_done, _, t = cpu_sector_solves(model, nf, G, irreps, wl["nev"], budget_s=8.0, min_sectors=2)
+        if it >= args.warmup:
+            per_step.append((n_done, t))
+    tot_n = sum(n for n, _ in per_step)
+    tot_t = sum(t for _, t in per_step)
+    val = tot_n / tot_t
+    line = {
+        "impl": "reference",
+        "metric": "sector-solves/s",
+        "value": val,
+        "unit": "sector-solves/s",
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 * tot_t / len(per_step),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": args.workload, "desc": wl["desc"], "nev": wl["nev"],
+                   "step": "bounded sample of sectors: projection table + CSR + ARPACK eigs(which=SR)"},
+        "cpu_baseline": {"value": val, "unit": "sector-solves/s", "cores": _NCPU, "kind": "port",
+                         "sample": f"{tot_n} sector solves over {args.steps} steps (catalog built once, untimed)"},
+        "e2e": {"value": val, "unit": "sector-solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# GPU side
+# ---------------------------------------------------------------------------
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 7:
+                continue
+            try:
+                sm.append(float(p[0]))
+                mx = float(p[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, p[3:7]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def count_hops(catalog, model) -> int:
+    """Hops the apply kernel evaluates per row sweep (gate passes from every
+    representative), from the catalog's representative masks."""
+    import torch
+
+    m = catalog.repr_masks.cpu().numpy().astype(np.uint64)
+    h = 0
+    pairs = {(i - 1, j - 1) for (i, j, _) in model.bilinear_terms}
+    for (i, j) in pairs:
+        ok = ((m >> np.uint64(i)) & np.uint64(1)).astype(bool) & ~((m >> np.uint64(j)) & np.uint64(1)).astype(bool)
+        h += int(ok.sum())
+    del torch
+    return h
+
+
+def apply_roofline(ed, data, sset, solver, peak_gbs, n_launch=200):
+    """Average duration of the batch's matvec launch (the FP32 apply over all
+    columns), timed with CUDA events on the launching stream, and its
+    algorithmic bytes per launch."""
+    import torch
+
+    dm, _ = data._device()
+    b = solver.batch
+    n_orb = data.orbit_catalog.n_orbits
+    X = torch.randn((n_orb, b.ld), dtype=torch.complex64, device="cuda")
+    Y = torch.empty((n_orb, b.ld), dtype=torch.complex128, device="cuda")
+    for _ in range(5):
+        dm.apply_block(sset, b.col_sector, X, Y, precision=32)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(n_launch):
+        dm.apply_block(sset, b.col_sector, X, Y, precision=32)
+    e1.record()
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / n_launch * 1e-3
+    hops = count_hops(data.orbit_catalog, data.second_quantized_model)
+    ncols = b.n_cols
+    # algorithmic bytes: per row mask 8 + member 8 + sqrt|Stab| 8 + diag 16,
+    # per row and column x 8 (complex64) in, y 16 (complex128) out,
+    # per hop one 16-B table entry
+    alg = n_orb * (8 + 8 + 8 + 16) + n_orb * ncols * (8 + 16) + hops * 16
+    ach = alg / t / 1e9
+    return {"kernel": "k_apply<LPR,CPL,32> (rsed_apply_h)", "bound": "hbm", "achieved": ach,
+            "peak": peak_gbs, "unit": "GB/s", "frac": ach / peak_gbs, "traffic": None,
+            "alg_bytes_per_launch": alg, "avg_launch_us": t * 1e6, "hops_per_launch": hops,
+            "columns": ncols}
+
+
+def matvec_at_scale(ed, models, peak_gbs, n_launch=20):
+    """HBM-bound matvec at the 32-site Haldane size (10.5M states, table
+    168 MB > L2): all 16 sectors x 2 block columns in one launch, FP64 and FP32."""
+    import torch
+
+    model, nf = models.config_model("haldane32")
+    G = ed.build_translation_group(model.lattice)
+    t0 = time.perf_counter()
+    data = ed.build_ed_data(model, filling_fraction=Fraction(nf, model.lattice.n_site), symmetry_group=G)
+    torch.cuda.synchronize()
+    t_cat = time.perf_counter() - t0
+    dm, sset = data._device()
+    n_orb = data.orbit_catalog.n_orbits
+    ns = len(data.irrep_list)
+    ncol = 2 * ns
+    ld = ncol
+    cs = torch.arange(ns, dtype=torch.int32, device="cuda").repeat_interleave(2)
+    hops = count_hops(data.orbit_catalog, model)
+    out = {"workload": "haldane32: 32 sites, 8 bosons, C=10,518,300, |G|=16, 16 sectors x 2 columns",
+           "n_orbits": n_orb, "hops_per_launch": hops, "catalog_build_s": t_cat}
+    for prec, dt, xb in ((64, torch.complex128, 16), (32, torch.complex64, 8)):
+        X = torch.randn((n_orb, ld), dtype=dt, device="cuda")
+        Y = torch.empty((n_orb, ld), dtype=torch.complex128, device="cuda")
+        for _ in range(3):
+            dm.apply_block(sset, cs, X, Y, precision=prec)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(n_launch):
+            dm.apply_block(sset, cs, X, Y, precision=prec)
+        e1.record()
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / n_launch * 1e-3
+        alg = n_orb * (8 + 8 + 8 + 16) + n_orb * ncol * (xb + 16) + hops * 16
+        out[f"fp{prec}"] = {"avg_launch_ms": t * 1e3, "alg_GBs": alg / t / 1e9,
+                            "frac_of_measured_hbm": alg / t / 1e9 / peak_gbs}
+    return out
+
+
+def run_b200(args):
+    import torch
+
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    import realspace_exatdiagonalization_py_b200 as ed
+    from realspace_exatdiagonalization_py_b200 import _lib, models
+    from realspace_exatdiagonalization_py_b200.batched import BatchedSectorSolver
+
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    peak_gbs = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+
+    wl = WORKLOADS[args.workload]
+    nev = wl["nev"]
+    model, nf = models.config_model(args.workload)
+    G = ed.build_translation_group(model.lattice)
+    data = ed.build_ed_data(model, filling_fraction=Fraction(nf, model.lattice.n_site), symmetry_group=G)
+    dm, sset = data._device()
+    sectors = list(range(len(data.irrep_list)))
+    n_sec = len(sectors)
+    assert all(d > 500 for d in sset.dims), "bench workload expects every sector on the Lanczos path"
+
+    # inputs: seeded start blocks, device-resident copy and pinned host copy
+    params = ed.LanczosParams(block=3, n_slots=16, precision=args.precision)
+    solver = BatchedSectorSolver(dm, sset, sectors, nev, precision=args.precision, params=params)
+    b = solver.batch
+    host_blocks = [ed.lanczos.start_block(sset.dims[s], b.block_sizes[i], 12345 + s)
+                   for i, s in enumerate(sectors)]
+    dev_blocks = [torch.from_numpy(x).cuda() for x in host_blocks]
+    pinned_blocks = [torch.from_numpy(x).pin_memory() for x in host_blocks]
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    # oracle eigenvalues (|dE| check of every step's result)
+    ref = oracle_eigs(model, nf, G, data.irrep_list, nev) if rank == 0 else None
+
+    def step():
+        return solver.solve(dev_blocks, vectors=False, host=False)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if ws > 1:
+        torch.distributed.barrier()
+    lib = _lib.load()
+    times = []
+    max_de = 0.0
+    launches = 0
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            n0 = lib.rsed_launch_count()
+            r0 = (b.replays, solver.refiner.replays if solver.refiner else 0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            vals, _ = step()
+            e1.record()
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1) * 1e-3)
+            launches += int(lib.rsed_launch_count() - n0)
+            launches += (b.replays - r0[0]) * (b.launches_per_graph or 0)
+            if solver.refiner is not None:
+                launches += (solver.refiner.replays - r0[1]) * (solver.refiner.launches_per_graph or 0)
+            if ref is not None:
+                v = vals.cpu().numpy()
+                max_de = max(max_de, max(float(np.max(np.abs(v[i] - ref[s][:nev]))) for i, s in enumerate(sectors)))
+    t_step = float(np.sum(times))
+    if ws > 1:
+        import torch.distributed as dist
+
+        tt = torch.tensor([t_step], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_step = float(tt.item())
+    value = ws * n_sec * args.steps / t_step
+    lat = sorted(times)
+
+    # e2e through the public API: pinned host start blocks in, numpy eigenpairs out
+    e2e_times = []
+    h2d = sum(x.numel() * 16 for x in pinned_blocks)
+    d2h = 0
+    for it in range(args.warmup + args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        res = ed.solve_sectors_batched(data, sectors, nev=nev, precision=args.precision, params=params,
+                                       start_blocks=pinned_blocks)
+        e1.record()
+        torch.cuda.synchronize()
+        if it >= args.warmup:
+            e2e_times.append(e0.elapsed_time(e1) * 1e-3)
+        d2h = sum(res[s][0].nbytes + res[s][1].nbytes for s in sectors)
+    e2e_val = ws * n_sec * len(e2e_times) / sum(e2e_times)
+
+    extra = {}
+    if rank == 0:
+        # plain FP64 GPU path: one sector at a time, block 1, no graph, host
+        # polling every iteration
+        p_plain = ed.LanczosParams(block=1, n_slots=48, precision=64, check_every=1)
+        plain_t = []
+        for s in sectors[: max(3, min(n_sec, args.plain_sectors))]:
+            pb = ed.LanczosBatch(dm, sset, [s], nev, p_plain)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            pb.load_start([dev_blocks[s][:, :1]])
+            pb.start()
+            pb.run(poll=1, graph=False)
+            e1.record()
+            torch.cuda.synchronize()
+            plain_t.append(e0.elapsed_time(e1) * 1e-3)
+            if ref is not None:
+                max_de_plain = float(np.max(np.abs(pb.eigenvalues()[0] - ref[s][:nev])))
+                extra.setdefault("plain_fp64_max_abs_dE", 0.0)
+                extra["plain_fp64_max_abs_dE"] = max(extra["plain_fp64_max_abs_dE"], max_de_plain)
+        plain_rate = len(plain_t) / sum(plain_t)
+        ps = sorted(plain_t)
+        extra.update({
+            "plain_fp64_sector_solves_per_s": plain_rate,
+            "plain_fp64_latency_ms": {"p50": 1e3 * ps[len(ps) // 2], "p99": 1e3 * ps[-1]},
+            "batched_over_plain": value / ws / plain_rate,
+        })
+        # FP64-matvec batched variant
+        s64 = BatchedSectorSolver(dm, sset, sectors, nev, precision=64,
+                                  params=ed.LanczosParams(block=3, n_slots=16, precision=64))
+        for _ in range(2):
+            s64.solve(dev_blocks, vectors=False, host=False)
+        t64 = []
+        for _ in range(max(3, args.steps // 2)):
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            v64, _ = s64.solve(dev_blocks, vectors=False, host=False)
+            e1.record()
+            torch.cuda.synchronize()
+            t64.append(e0.elapsed_time(e1) * 1e-3)
+        extra["fp64_batched_sector_solves_per_s"] = n_sec * len(t64) / sum(t64)
+        extra["fp64_batched_max_abs_dE"] = max(float(np.max(np.abs(v64.cpu().numpy()[i] - ref[s][:nev])))
+                                               for i, s in enumerate(sectors))
+        fe = solver.fp32_error()
+        if fe is not None:
+            extra["fp32_matvec_error_before_refinement"] = {"max": float(fe.max()), "median": float(np.median(fe))}
+        roof = apply_roofline(ed, data, sset, solver, peak_gbs)
+        roof["peak_source"] = peak_src
+        if not args.skip_scale:
+            try:
+                extra["matvec_at_scale"] = matvec_at_scale(ed, models, peak_gbs)
+            except Exception as exc:  # noqa: BLE001 - reported, not fatal
+                extra["matvec_at_scale"] = {"error": repr(exc)}
+        # CPU baseline: the oracle (reference algorithm) on the host cores
+        cpu_rate, cpu_n, _, cpu_t = cpu_sector_solves(model, nf, G, data.irrep_list, nev,
+                                                      budget_s=args.cpu_budget)
+        line = {
+            "metric": "sector-solves/s",
+            "value": value,
+            "unit": "sector-solves/s",
+            "n_gpus": ws,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": 1e3 * t_step / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "c64 matvec / f64 Lanczos" if args.precision == 32 else "f64",
+            "data": "synthetic",
+            "config": {"workload": args.workload, "desc": wl["desc"], "nev": nev,
+                       "sectors_per_step": n_sec, "block": params.block, "precision": args.precision,
+                       "l2": "256 MB buffer written between timed steps",
+                       "parallelism": f"replicas x{ws}"},
+            "latency_ms": {"p50": 1e3 * lat[len(lat) // 2], "p99": 1e3 * lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
+            "parity": {"max_abs_dE_vs_oracle": max_de, "tolerance": 1e-10},
+            "e2e": {"value": e2e_val, "unit": "sector-solves/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h),
+                    "api": "solve_sectors_batched(start_blocks=pinned host) -> numpy eigenpairs"},
+            "roofline": roof,
+            "cpu_baseline": {"value": cpu_rate, "unit": "sector-solves/s", "cores": _NCPU, "kind": "port",
+                             "sample": f"{cpu_n} sectors of the same workload in {cpu_t:.1f} s "
+                                       "(projection table + CSR + ARPACK; catalog untimed)"},
+            "clocks": clk.summary(),
+            "gpu_launches": launches,
+            "extra": extra,
+        }
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="checkerboard24", choices=sorted(WORKLOADS))
+    ap.add_argument("--precision", type=int, default=32, choices=[32, 64])
+    ap.add_argument("--plain-sectors", type=int, default=12)
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--skip-scale", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

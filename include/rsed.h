@@ -240,6 +240,9 @@ int rsed_gather_rows(int64_t n_rows, const int32_t* orbit_of_row, const double* 
 int rsed_scatter_rows(int64_t n_rows, const int32_t* orbit_of_row, const double* src,
                       int64_t src_stride, double* dst, int64_t dst_ld, int32_t dst_col, void* stream);
 int rsed_device_sync(void* stream);
+/* Kernel launches issued by the library so far (process-wide counter; a
+ * CUDA graph replay re-runs the launches counted while it was captured). */
+long long rsed_launch_count(void);
 
 #ifdef __cplusplus
 }

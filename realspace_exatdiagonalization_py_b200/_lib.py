@@ -199,6 +199,7 @@ SIGNATURES = {
         [c_int64, c_void_p, c_void_p, c_int64, c_void_p, c_int64, c_int32, c_void_p],
     ),
     "rsed_device_sync": (c_int, [c_void_p]),
+    "rsed_launch_count": (ctypes.c_longlong, []),
 }
 
 _lib = None

@@ -4,9 +4,16 @@
 #include <string>
 #include "rsed_internal.cuh"
 
+#include <atomic>
+
 namespace {
 thread_local std::string g_last_error;
+std::atomic<long long> g_launches{0};
 }
+
+void rsed_count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+extern "C" long long rsed_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 
 int rsed_set_error(int code, const char* fmt, ...) {
   char buf[512];

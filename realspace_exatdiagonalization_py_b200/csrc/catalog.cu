@@ -177,6 +177,21 @@ __global__ void k_expand(rsed_group_t grp, int64_t n_orb, const uint64_t* repr_m
   stab_mask[o] = smask;
 }
 
+// Entries start as (rep -1, g 0, alpha 0), the reference's initial table
+// (symmetry_resolved_ed.py:1359-1361); every state of a group's catalog is
+// overwritten by k_expand.
+__global__ void k_table_init(int64_t n, RsedEntry* table) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    RsedEntry e;
+    e.rep = -1;
+    e.g = 0;
+    e.re = 0.0f;
+    e.im = 0.0f;
+    table[i] = e;
+  }
+}
+
 __global__ void k_stab_counts(int64_t n_orb, const uint64_t* stab_mask, int64_t* counts) {
   int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (o < n_orb) counts[o] = __popcll(stab_mask[o]);
@@ -558,6 +573,9 @@ extern "C" int rsed_catalog_fill(const rsed_group_t* g, const void* scratch, siz
   GroupSmemLayout lay = group_smem_layout(g->n_site, g->n_filled, g->n_group, true, true);
   int* err = reinterpret_cast<int*>(s.block_count);  // block counts are consumed by now
   RSED_TRY_CUDA(cudaMemsetAsync(err, 0, sizeof(int), stream));
+  k_table_init<<<(unsigned)((g->n_states + 255) / 256), 256, 0, stream>>>(
+      g->n_states, reinterpret_cast<RsedEntry*>(table));
+  RSED_CHECK_LAUNCH();
   const unsigned nb = (unsigned)((n_orbits + 255) / 256);
   k_expand<<<nb, 256, lay.total, stream>>>(*g, n_orbits, repr_masks,
                                            reinterpret_cast<RsedEntry*>(table), stab_mask, lay, err);

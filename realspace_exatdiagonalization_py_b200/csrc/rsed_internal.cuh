@@ -6,6 +6,8 @@
 #include "rsed_common.cuh"
 
 int rsed_set_error(int code, const char* fmt, ...);
+// Number of kernels this library has launched (all host threads).
+void rsed_count_launch();
 
 #define RSED_TRY_CUDA(expr)                                                      \
   do {                                                                           \
@@ -17,6 +19,7 @@ int rsed_set_error(int code, const char* fmt, ...);
 
 #define RSED_CHECK_LAUNCH()                                                      \
   do {                                                                           \
+    rsed_count_launch();                                                         \
     cudaError_t _e = cudaGetLastError();                                         \
     if (_e != cudaSuccess)                                                       \
       return rsed_set_error(RSED_ECUDA, "kernel launch: %s (%s:%d)",             \

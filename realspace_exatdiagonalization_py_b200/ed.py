@@ -68,6 +68,7 @@ class Symmetry_Resolved_ED_Data:
         st = dict(self.__dict__)
         st["orbit_catalog"] = None
         st.pop("_dev", None)
+        st.pop("_solvers", None)
         return st
 
     def __setstate__(self, st):
@@ -178,8 +179,12 @@ def solve_sectors_batched(ed_data, sector_ids: list[int], *, nev: int = 5, preci
     Sectors with ``dim <= 500`` take the dense path (as the reference does);
     the rest run together: every iteration is one apply launch for all of
     them.  ``precision=32`` runs the matvec in FP32 and finishes each sector
-    with an FP64 refinement.  Returns ``{sector: (vals, vecs)}``.
+    with an FP64 refinement.  The batched solver (buffers, captured graphs)
+    is kept on ``ed_data`` and reused by later calls with the same sectors.
+    Returns ``{sector: (vals, vecs)}``.
     """
+    from .batched import BatchedSectorSolver
+
     dm, sset = ed_data._device()
     out = {}
     big = []
@@ -197,20 +202,15 @@ def solve_sectors_batched(ed_data, sector_ids: list[int], *, nev: int = 5, preci
         else:
             big.append(s)
     if big:
-        p = params or _default_params(nev, precision)
-        if p.precision != precision:
-            p = LanczosParams(**{**p.__dict__, "precision": precision})
-        batch = LanczosBatch(dm, sset, big, nev, p)
-        batch.load_start(start_blocks)
-        batch.start()
-        batch.run(graph=graph)
-        if precision == 32:
-            batch = refine(batch)
-        vals = batch.eigenvalues()
-        vecs = batch.eigenvectors() if return_vectors else [None] * len(big)
+        key = (tuple(big), nev, precision, None if params is None else tuple(params.__dict__.items()), graph)
+        cache = ed_data.__dict__.setdefault("_solvers", {})
+        solver = cache.get(key)
+        if solver is None or solver.model is not dm:
+            solver = BatchedSectorSolver(dm, sset, big, nev, precision=precision, params=params, graph=graph)
+            cache[key] = solver
+        vals, vecs = solver.solve(start_blocks, vectors=return_vectors)
         for i, s in enumerate(big):
-            v = vecs[i].cpu().numpy() if vecs[i] is not None else None
-            out[s] = (vals[i].copy(), v)
+            out[s] = (vals[i].copy(), vecs[i] if vecs is not None else None)
     return out
 
 

@@ -41,6 +41,7 @@ class LanczosParams:
     n_slots: int = 16
     keep_blocks: int = 0  # 0 = automatic: ceil((nev + block) / block), bounded
     tol: float = 1e-10
+    tol32: float = 1e-5  # FP32-matvec phase: residual floor of a complex64 operator
     max_restarts: int = 200
     check_every: int = 2
     precision: int = 64
@@ -124,12 +125,16 @@ class LanczosBatch:
         self.state = torch.zeros((n_inst, 8), dtype=torch.int32, device=dev)
         self.c = _lib.RsedLanczos(
             n_inst, S, nev, self.keep, p.max_restarts, p.precision, bmax, self.chunk_rows, self.pm, 0,
-            float(p.tol), _lib.ptr(self.inst_col0), _lib.ptr(self.inst_b), _lib.ptr(self.V),
+            float(p.tol if p.precision == 64 else max(p.tol, p.tol32)), _lib.ptr(self.inst_col0), _lib.ptr(self.inst_b), _lib.ptr(self.V),
             _lib.ptr(self.W), _lib.ptr(self.Xf), _lib.ptr(self.P), _lib.ptr(self.coef),
             _lib.ptr(self.partial), plen, _lib.ptr(self.ritz_val), _lib.ptr(self.ritz_vec),
             _lib.ptr(self.resid), _lib.ptr(self.state),
         )
         self.sc = sset.sectors_struct(self.col_sector, self.n_cols, self.ld)
+        self.replays = 0
+        self.launches_per_graph = None
+        self._graph = None
+        self._graph_iters = None
 
     @property
     def n_inst(self) -> int:
@@ -179,10 +184,15 @@ class LanczosBatch:
         it = 0
         g = None
         if graph:
-            g = self.capture(poll)
+            if getattr(self, "_graph", None) is None or self._graph_iters != poll:
+                self._graph = self.capture(poll)
+                self._graph_iters = poll
+                it += 1  # capture() advanced every instance by one warm-up iteration
+            g = self._graph
         while it < max_iter:
             if g is not None:
                 g.replay()
+                self.replays += 1
             else:
                 self.iterate(poll, stream)
             it += poll
@@ -198,15 +208,20 @@ class LanczosBatch:
         return st
 
     def capture(self, n_iter: int):
-        """CUDA graph of ``n_iter`` iterations (replayed by ``run(graph=True)``)."""
+        """CUDA graph of ``n_iter`` iterations (replayed by ``run(graph=True)``).
+
+        Runs one real iteration first, outside the graph, on the live state."""
+        self.launches_per_graph = None
         s = torch.cuda.Stream()
         s.wait_stream(torch.cuda.current_stream())
         with torch.cuda.stream(s):
             self.iterate(1, s)  # warm-up outside the graph (kernel attributes, lazy loading)
         torch.cuda.current_stream().wait_stream(s)
         g = torch.cuda.CUDAGraph()
+        n0 = _lib.load().rsed_launch_count()
         with torch.cuda.graph(g, stream=s):
             self.iterate(n_iter, s)
+        self.launches_per_graph = int(_lib.load().rsed_launch_count() - n0)
         return g
 
     # -- results ----------------------------------------------------------

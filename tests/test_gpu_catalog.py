@@ -138,8 +138,20 @@ def test_oracle_cross_check_random_groups():
     from oracle import port
 
     rng = np.random.default_rng(7)
-    for n, k, ng, fermion in [(10, 4, 3, False), (11, 5, 4, True), (14, 6, 2, True)]:
-        perms = [list(range(1, n + 1))] + [list(rng.permutation(n) + 1) for _ in range(ng - 1)]
+    for n, k, fermion in [(10, 4, False), (11, 5, True), (14, 6, True), (13, 3, False)]:
+        # cyclic group generated by a random permutation (orbits must be disjoint)
+        while True:
+            gen = rng.permutation(n)
+            perms0 = [np.arange(n)]
+            while True:
+                nxt = gen[perms0[-1]]
+                if np.array_equal(nxt, perms0[0]):
+                    break
+                perms0.append(nxt)
+            if 2 <= len(perms0) <= 24:
+                break
+        ng = len(perms0)
+        perms = [list(p + 1) for p in perms0]
         phases = [np.ones(n)] + [np.exp(2j * np.pi * rng.random(n)) for _ in range(ng - 1)]
         ops = [ed.Symmetry_Operation(i, p, perm_phases=e) for i, (p, e) in enumerate(zip(perms, phases))]
         G = ed.Finite_Symmetry_Group("custom", ops)
