@@ -319,7 +319,7 @@ def run_b200(args):
     assert all(d > 500 for d in sset.dims), "bench workload expects every sector on the Lanczos path"
 
     # inputs: seeded start blocks, device-resident copy and pinned host copy
-    params = ed.LanczosParams(block=3, n_slots=16, precision=args.precision)
+    params = ed.LanczosParams(precision=args.precision)
     solver = BatchedSectorSolver(dm, sset, sectors, nev, precision=args.precision, params=params)
     b = solver.batch
     host_blocks = [ed.lanczos.start_block(sset.dims[s], b.block_sizes[i], 12345 + s)
@@ -348,7 +348,7 @@ def run_b200(args):
             flush.zero_()
             torch.cuda.synchronize()
             n0 = lib.rsed_launch_count()
-            r0 = (b.replays, solver.refiner.replays if solver.refiner else 0)
+            r0 = b.replays
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
             vals, _ = step()
@@ -356,9 +356,7 @@ def run_b200(args):
             torch.cuda.synchronize()
             times.append(e0.elapsed_time(e1) * 1e-3)
             launches += int(lib.rsed_launch_count() - n0)
-            launches += (b.replays - r0[0]) * (b.launches_per_graph or 0)
-            if solver.refiner is not None:
-                launches += (solver.refiner.replays - r0[1]) * (solver.refiner.launches_per_graph or 0)
+            launches += (b.replays - r0) * (b.launches_per_graph or 0)
             if ref is not None:
                 v = vals.cpu().numpy()
                 max_de = max(max_de, max(float(np.max(np.abs(v[i] - ref[s][:nev]))) for i, s in enumerate(sectors)))
@@ -420,7 +418,7 @@ def run_b200(args):
         })
         # FP64-matvec batched variant
         s64 = BatchedSectorSolver(dm, sset, sectors, nev, precision=64,
-                                  params=ed.LanczosParams(block=3, n_slots=16, precision=64))
+                                  params=ed.LanczosParams(precision=64))
         for _ in range(2):
             s64.solve(dev_blocks, vectors=False, host=False)
         t64 = []
@@ -438,6 +436,9 @@ def run_b200(args):
         fe = solver.fp32_error()
         if fe is not None:
             extra["fp32_matvec_error_before_refinement"] = {"max": float(fe.max()), "median": float(np.median(fe))}
+        extra["residual_norm_max"] = float(solver.residuals().max())
+        st = b.status()
+        extra["lanczos_iterations"] = {"min": int(st[:, 3].min()), "max": int(st[:, 3].max())}
         roof = apply_roofline(ed, data, sset, solver, peak_gbs)
         roof["peak_source"] = peak_src
         if not args.skip_scale:

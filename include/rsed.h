@@ -186,7 +186,7 @@ int rsed_csr_spmv(int64_t n_rows, const int64_t* row_ptr, const int32_t* col_idx
  * buffers described by rsed_lanczos_t.  rsed_lanczos_iterate advances every
  * active instance by n_iter block steps without host synchronisation or
  * allocation (capturable in a CUDA graph); per-instance status is read from
- * state[8*i + 1] (0 running, 1 converged, RSED_E* on failure). */
+ * state[16*i + 1] (0 running, 1 converged, RSED_E* on failure). */
 typedef struct {
   int32_t n_inst;        /* instances (sector solves) in the batch */
   int32_t n_slots;       /* basis blocks before a thick restart (n_slots*bmax <= 64) */
@@ -211,7 +211,7 @@ typedef struct {
   double* ritz_val;      /* n_inst x pm */
   double* ritz_vec;      /* n_inst x pm x pm complex128 */
   double* resid;         /* n_inst x pm */
-  int32_t* state;        /* n_inst x 8 */
+  int32_t* state;        /* n_inst x 16 */
 } rsed_lanczos_t;
 int64_t rsed_lanczos_partial_len(int64_t n_orbits, int32_t chunk_rows, int32_t n_inst,
                                  int32_t n_slots);
@@ -227,6 +227,13 @@ int rsed_lanczos_start(const rsed_model_t* model, const rsed_sectors_t* sec, rse
                        void* stream);
 int rsed_lanczos_iterate(const rsed_model_t* model, const rsed_sectors_t* sec, rsed_lanczos_t* st,
                          int32_t n_iter, int32_t check_every, int32_t apply_variant, void* stream);
+/* FP64 Rayleigh-Ritz refinement of converged instances (typically after an
+ * FP32-matvec solve): the thick-restart basis (keep_blocks*b Ritz vectors
+ * plus the residual block) is re-projected with the FP64 operator, the
+ * Ritz pairs recomputed, and the true FP64 residual norms ||H u - theta u||
+ * written to resid[inst*pm + j].  Needs n_slots >= 2*keep_blocks + 1. */
+int rsed_lanczos_rayleigh_ritz(const rsed_model_t* model, const rsed_sectors_t* sec,
+                               rsed_lanczos_t* st, int32_t apply_variant, void* stream);
 /* Ritz vectors of the nev lowest pairs of the last check:
  * U[(inst*nev + j)*u_stride + orbit] (complex128). */
 int rsed_lanczos_extract(const rsed_model_t* model, const rsed_sectors_t* sec, rsed_lanczos_t* st,

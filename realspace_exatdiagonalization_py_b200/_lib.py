@@ -186,6 +186,10 @@ SIGNATURES = {
         [POINTER(RsedModel), POINTER(RsedSectors), POINTER(RsedLanczos), c_int32, c_int32, c_int32,
          c_void_p],
     ),
+    "rsed_lanczos_rayleigh_ritz": (
+        c_int,
+        [POINTER(RsedModel), POINTER(RsedSectors), POINTER(RsedLanczos), c_int32, c_void_p],
+    ),
     "rsed_lanczos_extract": (
         c_int,
         [POINTER(RsedModel), POINTER(RsedSectors), POINTER(RsedLanczos), c_void_p, c_int64, c_void_p],

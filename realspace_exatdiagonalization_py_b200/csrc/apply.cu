@@ -106,7 +106,10 @@ struct XLoad<float2> {
 // LPR lanes cooperate on one row; lane q owns columns q, q+LPR, ... (CPL of them).
 // PREC 64: complex128 input and accumulation.  PREC 32: complex64 input and
 // accumulation (the per-hop weight is formed in FP64 and rounded once).
-template <int LPR, int CPL, int PREC>
+// Hops are gathered HB at a time: all table entries of a batch are loaded
+// together, then the member masks, sqrt|Stab| and x rows of their targets,
+// so each batch costs two dependent memory round trips instead of 3*HB.
+template <int LPR, int CPL, int PREC, int HB>
 __global__ void __launch_bounds__(256) k_apply(rsed_model_t md, rsed_sectors_t sc, const void* xin,
                                                double2* __restrict__ y, ApplySmemLayout lay) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -146,6 +149,59 @@ __global__ void __launch_bounds__(256) k_apply(rsed_model_t md, rsed_sectors_t s
       acc[j].x += c.x;
       acc[j].y += c.y;
     }
+    int bt[HB];
+    int64_t bidx[HB];
+    int nh = 0;
+    auto process = [&](int cnt) {
+      RsedEntry e[HB];
+#pragma unroll
+      for (int h = 0; h < HB; ++h)
+        if (h < cnt) e[h] = load_entry(reinterpret_cast<const RsedEntry*>(md.table), bidx[h]);
+      uint64_t mc[HB];
+      double sq[HB];
+      XT xv[HB][CPL];
+#pragma unroll
+      for (int h = 0; h < HB; ++h) {
+        if (h < cnt) {
+          const int64_t c = e[h].rep;
+          mc[h] = __ldg(sc.member + c);
+          sq[h] = __ldg(sc.sqrt_stab + c);
+#pragma unroll
+          for (int j = 0; j < CPL; ++j)
+            if (on[j]) xv[h][j] = __ldg(x + c * sc.ld + col[j]);
+        }
+      }
+#pragma unroll
+      for (int h = 0; h < HB; ++h) {
+        if (h >= cnt || (mc[h] & memr) == 0ull) continue;
+        const int t = bt[h];
+        // H[c, row] = t * s_JW * alpha * conj(chi(g)) * sqrt(S_c / S_row); we
+        // accumulate its conjugate: w * chi(g) with w = conj(t s alpha) * ratio.
+        double2 ta = cmul(v.tamp[t], make_double2(e[h].re, e[h].im));
+        if (md.fermionic && (__popcll(m & v.tjw[t]) & 1)) {
+          ta.x = -ta.x;
+          ta.y = -ta.y;
+        }
+        const double ratio = sq[h] / sr;
+        const double2 w = make_double2(ta.x * ratio, -ta.y * ratio);
+#pragma unroll
+        for (int j = 0; j < CPL; ++j) {
+          if (!on[j] || !((mc[h] >> sec[j]) & 1ull)) continue;
+          const double2 ch = v.chi[sec[j] * md.n_group + e[h].g];
+          const double2 wc = cmul(w, ch);
+          if constexpr (PREC == 64) {
+            const double2 xx = xv[h][j];
+            acc[j].x += wc.x * xx.x - wc.y * xx.y;
+            acc[j].y += wc.x * xx.y + wc.y * xx.x;
+          } else {
+            const float2 xx = xv[h][j];
+            const float2 wf = make_float2((float)wc.x, (float)wc.y);
+            acc[j].x += wf.x * xx.x - wf.y * xx.y;
+            acc[j].y += wf.x * xx.y + wf.y * xx.x;
+          }
+        }
+      }
+    };
     uint64_t occ = m;
     while (occ) {
       const int i = __ffsll((long long)occ) - 1;
@@ -154,39 +210,15 @@ __global__ void __launch_bounds__(256) k_apply(rsed_model_t md, rsed_sectors_t s
       for (int t = v.tbeg[i]; t < t1; ++t) {
         const int jj = v.tto[t];
         if ((m >> jj) & 1ull) continue;
-        const uint64_t m2 = m ^ (1ull << i) ^ (1ull << jj);
-        const int64_t idx = rsed_rank(m2, v.binom, kp1);
-        const RsedEntry e = load_entry(reinterpret_cast<const RsedEntry*>(md.table), idx);
-        const int64_t c = e.rep;
-        const uint64_t memc = __ldg(sc.member + c);
-        if ((memc & memr) == 0ull) continue;
-        // H[c, row] = t * s_JW * alpha * conj(chi(g)) * sqrt(S_c / S_row); we
-        // accumulate its conjugate: w * chi(g) with w = conj(t s alpha) * ratio.
-        double2 ta = cmul(v.tamp[t], make_double2(e.re, e.im));
-        if (md.fermionic && (__popcll(m & v.tjw[t]) & 1)) {
-          ta.x = -ta.x;
-          ta.y = -ta.y;
-        }
-        const double ratio = __ldg(sc.sqrt_stab + c) / sr;
-        const double2 w = make_double2(ta.x * ratio, -ta.y * ratio);
-#pragma unroll
-        for (int j = 0; j < CPL; ++j) {
-          if (!on[j] || !((memc >> sec[j]) & 1ull)) continue;
-          const double2 ch = v.chi[sec[j] * md.n_group + e.g];
-          const double2 wc = cmul(w, ch);
-          if constexpr (PREC == 64) {
-            const double2 xv = XLoad<double2>::ld(reinterpret_cast<const double2*>(x) + c * sc.ld + col[j]);
-            acc[j].x += wc.x * xv.x - wc.y * xv.y;
-            acc[j].y += wc.x * xv.y + wc.y * xv.x;
-          } else {
-            const float2 xv = __ldg(reinterpret_cast<const float2*>(x) + c * sc.ld + col[j]);
-            const float2 wf = make_float2((float)wc.x, (float)wc.y);
-            acc[j].x += wf.x * xv.x - wf.y * xv.y;
-            acc[j].y += wf.x * xv.y + wf.y * xv.x;
-          }
+        bt[nh] = t;
+        bidx[nh] = rsed_rank(m ^ (1ull << i) ^ (1ull << jj), v.binom, kp1);
+        if (++nh == HB) {
+          process(HB);
+          nh = 0;
         }
       }
     }
+    if (nh) process(nh);
   }
 #pragma unroll
   for (int j = 0; j < CPL; ++j) {
@@ -197,18 +229,18 @@ __global__ void __launch_bounds__(256) k_apply(rsed_model_t md, rsed_sectors_t s
   }
 }
 
-template <int LPR, int CPL, int PREC>
+template <int LPR, int CPL, int PREC, int HB = 4>
 int launch_apply(const rsed_model_t& md, const rsed_sectors_t& sc, const void* x, double2* y,
                  cudaStream_t stream) {
   ApplySmemLayout lay = apply_layout(md, sc);
   if (lay.total > 48 * 1024) {
-    RSED_TRY_CUDA(cudaFuncSetAttribute(k_apply<LPR, CPL, PREC>,
+    RSED_TRY_CUDA(cudaFuncSetAttribute(k_apply<LPR, CPL, PREC, HB>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lay.total));
   }
   const int threads = 256;
   const int64_t total = md.n_orbits * LPR;
   const unsigned blocks = (unsigned)((total + threads - 1) / threads);
-  k_apply<LPR, CPL, PREC><<<blocks, threads, lay.total, stream>>>(md, sc, x, y, lay);
+  k_apply<LPR, CPL, PREC, HB><<<blocks, threads, lay.total, stream>>>(md, sc, x, y, lay);
   RSED_CHECK_LAUNCH();
   return RSED_OK;
 }
@@ -242,6 +274,15 @@ int dispatch_apply(const rsed_model_t& md, const rsed_sectors_t& sc, const void*
     case 11: if (n <= 8) return launch_apply<8, 1, PREC>(md, sc, x, y, stream); break;
     case 12: if (n <= 4) return launch_apply<2, 2, PREC>(md, sc, x, y, stream); break;
     case 13: if (n <= 64) return launch_apply<16, 4, PREC>(md, sc, x, y, stream); break;
+    // one hop at a time (no batching), for comparison
+    case 101: if (n <= 1) return launch_apply<1, 1, PREC, 1>(md, sc, x, y, stream); break;
+    case 106: if (n <= 32) return launch_apply<16, 2, PREC, 1>(md, sc, x, y, stream); break;
+    case 107: if (n <= 64) return launch_apply<32, 2, PREC, 1>(md, sc, x, y, stream); break;
+    // deeper hop batches
+    case 201: if (n <= 1) return launch_apply<1, 1, PREC, 8>(md, sc, x, y, stream); break;
+    case 206: if (n <= 32) return launch_apply<16, 2, PREC, 8>(md, sc, x, y, stream); break;
+    case 207: if (n <= 64) return launch_apply<32, 2, PREC, 8>(md, sc, x, y, stream); break;
+    case 209: if (n <= 32) return launch_apply<32, 1, PREC, 8>(md, sc, x, y, stream); break;
     default: break;
   }
   return rsed_set_error(RSED_EINVAL, "apply variant %d cannot hold %d columns", variant, n);

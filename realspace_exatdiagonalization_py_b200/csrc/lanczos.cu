@@ -22,15 +22,19 @@
 #include <type_traits>
 #include "rsed_internal.cuh"
 
+extern "C" int64_t rsed_lanczos_partial_len(int64_t n_orbits, int32_t chunk_rows, int32_t n_inst,
+                                            int32_t n_slots);
+
 namespace {
 
 constexpr int kBMax = 8;        // largest block per instance
 constexpr int kKeepMax = 16;    // largest thick-restart basis (columns)
 constexpr int kJacobiMax = 64;  // largest projected matrix
-constexpr int kStateInts = 8;
+constexpr int kRRMax = kKeepMax + kBMax;  // Rayleigh-Ritz basis (restart basis + residual block)
+constexpr int kStateInts = 16;
 // state fields
 constexpr int S_NB = 0, S_STATUS = 1, S_RESTARTS = 2, S_ITERS = 3, S_ACTIVE = 4, S_RESTART_NB = 5,
-              S_NEWSLOT = 6, S_NCONV = 7;
+              S_NEWSLOT = 6, S_NCONV = 7, S_TICKET = 8, S_RR = 9;
 
 struct LzDims {
   int64_t n_orb;
@@ -52,16 +56,35 @@ __device__ __forceinline__ double2 cdotc(double2 a, double2 b) {
 }
 
 // ---------------------------------------------------------------------------
-// Reduction: partial[chunk][inst][s][p][q] = sum_rows conj(Y_s[row][c0+p]) W[row][c0+q]
-// with Y_s = V[s] for s < nb and Y_nb = W (Gram of W itself).
-__global__ void k_lz_gram(rsed_lanczos_t st, LzDims d) {
+// Reduction + finalisation in one launch.  Block (chunk, inst) forms
+//   partial[chunk][inst][s][p][q] = sum_rows conj(Y_s[row][c0+p]) W[row][c0+q]
+// with Y_s = V[s] for s < nb and Y_nb = W (Gram of W itself); the last block
+// of an instance to finish (atomic ticket, no waiting) sums the partials in
+// chunk order, forms G' = G - C^H C, its Cholesky factor R and the
+// projected-matrix entries.
+__global__ void __launch_bounds__(128) k_lz_reduce(rsed_lanczos_t st, LzDims d, int pass) {
   const int chunk = blockIdx.x;
   const int inst = blockIdx.y;
-  const int* stt = st.state + inst * kStateInts;
+  int* stt = st.state + inst * kStateInts;
+  if (pass == 1 && chunk == 0 && threadIdx.x == 0) stt[S_RESTART_NB] = 0;
   if (!stt[S_ACTIVE]) return;
   const int b = st.inst_b[inst];
   const int c0 = st.inst_col0[inst];
   const int nb = stt[S_NB];
+  __shared__ int s_last;
+  __shared__ double2 sc[(kJacobiMax / 1 + kBMax + kBMax) * kBMax];  // C (nb*b rows) + G rows
+  __shared__ double2 sR[kBMax * kBMax];
+  __shared__ double2 sG[kBMax * kBMax];
+  __shared__ int s_ok;
+  if (nb > d.n_slots || b < 1 || b > kBMax || nb * b > kJacobiMax + kBMax) {
+    // the basis is full (no restart happened) or the block size is invalid:
+    // stop this instance instead of writing past its slots
+    if (chunk == 0 && threadIdx.x == 0) {
+      stt[S_STATUS] = RSED_EINVAL;
+      stt[S_ACTIVE] = 0;
+    }
+    return;
+  }
   const int npairs = (nb + 1) * b;
   const int64_t r0 = (int64_t)chunk * d.chunk_rows;
   const int64_t r1 = min(r0 + d.chunk_rows, d.n_orb);
@@ -69,127 +92,119 @@ __global__ void k_lz_gram(rsed_lanczos_t st, LzDims d) {
   const double2* W = reinterpret_cast<const double2*>(st.W);
   double2* part = reinterpret_cast<double2*>(st.partial);
   const int64_t slot_stride = d.n_orb * d.ld;
+  const int64_t pbase = ((int64_t)chunk * d.n_inst + inst) * (int64_t)d.pslots * kBMax * kBMax;
   for (int pair = threadIdx.x; pair < npairs; pair += blockDim.x) {
-    const int s = pair / b, p = pair % b;
-    const double2* Y = (s < nb) ? V + s * slot_stride : W;
+    const int sl = pair / b, p = pair % b;
+    const double2* Y = (sl < nb) ? V + sl * slot_stride : W;
     double2 acc[kBMax];
 #pragma unroll
     for (int q = 0; q < kBMax; ++q) acc[q] = make_double2(0.0, 0.0);
+#pragma unroll 4
     for (int64_t r = r0; r < r1; ++r) {
       const double2 y = Y[r * d.ld + c0 + p];
+      const double2* wr = W + r * d.ld + c0;
 #pragma unroll
-      for (int q = 0; q < kBMax; ++q) {
-        if (q < b) acc[q] = cadd(acc[q], cdotc(y, W[r * d.ld + c0 + q]));
-      }
+      for (int q = 0; q < kBMax; ++q)
+        if (q < b) acc[q] = cadd(acc[q], cdotc(y, wr[q]));
     }
-    double2* out = part + (((int64_t)chunk * d.n_inst + inst) * d.pslots + s) * kBMax * kBMax + p * kBMax;
+    double2* out = part + pbase + sl * kBMax * kBMax + p * kBMax;
 #pragma unroll
     for (int q = 0; q < kBMax; ++q)
       if (q < b) out[q] = acc[q];
   }
-}
-
-// Sum the partials, Cholesky of G - C^H C, projected-matrix bookkeeping.
-// coef layout per instance: [pslots][kBMax][kBMax]; slots 0..nb-1 = C, slot
-// pslots-1 = R of this pass; pass-1 results are kept in slots of rbuf.
-__global__ void k_lz_finalize(rsed_lanczos_t st, LzDims d, int pass) {
-  const int inst = blockIdx.x;
-  int* stt = st.state + inst * kStateInts;
-  if (pass == 1 && threadIdx.x == 0) stt[S_RESTART_NB] = 0;
-  if (!stt[S_ACTIVE]) return;
-  const int b = st.inst_b[inst];
-  const int nb = stt[S_NB];
-  if (nb > d.n_slots || b < 1 || b > kBMax) {
-    // the basis is full (no restart happened) or the block size is invalid:
-    // stop this instance instead of writing past its slots
-    if (threadIdx.x == 0) {
-      stt[S_STATUS] = RSED_EINVAL;
-      stt[S_ACTIVE] = 0;
-    }
-    return;
-  }
-  const int nent = (nb + 1) * b * b;
-  const double2* part = reinterpret_cast<const double2*>(st.partial);
-  double2* coef = reinterpret_cast<double2*>(st.coef) + (int64_t)inst * 2 * d.pslots * kBMax * kBMax;
-  // pass-specific area: [pass-1][pslots][kBMax][kBMax]
-  double2* cp = coef + (pass - 1) * d.pslots * kBMax * kBMax;
-  for (int e = threadIdx.x; e < nent; e += blockDim.x) {
-    const int s = e / (b * b), pq = e % (b * b), p = pq / b, q = pq % b;
-    double2 acc = make_double2(0.0, 0.0);
-    for (int c = 0; c < d.n_chunks; ++c)
-      acc = cadd(acc, part[(((int64_t)c * d.n_inst + inst) * d.pslots + s) * kBMax * kBMax + p * kBMax + q]);
-    cp[s * kBMax * kBMax + p * kBMax + q] = acc;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int t = atomicAdd(&stt[S_TICKET], 1);
+    s_last = (t == d.n_chunks - 1);
   }
   __syncthreads();
-  if (threadIdx.x != 0) return;
-  // G' = G - C^H C  (G sits in slot nb)
-  double2 G[kBMax][kBMax];
-  double gdiag_max = 0.0;
-  for (int p = 0; p < b; ++p)
-    for (int q = 0; q < b; ++q) {
-      double2 g = cp[nb * kBMax * kBMax + p * kBMax + q];
-      for (int s = 0; s < nb; ++s)
-        for (int r = 0; r < b; ++r) {
-          const double2 a = cp[s * kBMax * kBMax + r * kBMax + p];  // C[s r][p]
-          const double2 c = cp[s * kBMax * kBMax + r * kBMax + q];  // C[s r][q]
-          g = csub(g, cdotc(a, c));
-        }
-      G[p][q] = g;
-      if (p == q) gdiag_max = fmax(gdiag_max, cp[nb * kBMax * kBMax + p * kBMax + p].x);
+  if (!s_last) return;
+  __threadfence();
+  if (threadIdx.x == 0) stt[S_TICKET] = 0;
+  // ---- finalisation (one block per instance) ----
+  const int nent = (nb + 1) * b * b;
+  for (int e = threadIdx.x; e < nent; e += blockDim.x) {
+    const int sl = e / (b * b), pq = e % (b * b), p = pq / b, q = pq % b;
+    double2 a = make_double2(0.0, 0.0);
+    for (int c = 0; c < d.n_chunks; ++c) {
+      const double2* src = part + ((int64_t)c * d.n_inst + inst) * (int64_t)d.pslots * kBMax * kBMax +
+                           sl * kBMax * kBMax + p * kBMax + q;
+      a = cadd(a, __ldcg(src));
     }
-  // Cholesky G' = R^H R, R upper triangular
-  double2 R[kBMax][kBMax];
-  for (int p = 0; p < kBMax; ++p)
-    for (int q = 0; q < kBMax; ++q) R[p][q] = make_double2(0.0, 0.0);
-  bool ok = gdiag_max > 0.0;
-  for (int j = 0; j < b && ok; ++j) {
-    double s = G[j][j].x;
-    for (int k = 0; k < j; ++k) s -= R[k][j].x * R[k][j].x + R[k][j].y * R[k][j].y;
-    if (!(s > 1e-26 * gdiag_max)) {
-      ok = false;
-      break;
+    sc[(sl * b + p) * kBMax + q] = a;  // row (sl*b + p), column q
+  }
+  __syncthreads();
+  // G' = G - C^H C, one thread per (p, q)
+  for (int e = threadIdx.x; e < b * b; e += blockDim.x) {
+    const int p = e / b, q = e % b;
+    double2 g = sc[(nb * b + p) * kBMax + q];
+    for (int r = 0; r < nb * b; ++r) g = csub(g, cdotc(sc[r * kBMax + p], sc[r * kBMax + q]));
+    sG[p * kBMax + q] = g;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double gmax = 0.0;
+    for (int p = 0; p < b; ++p) gmax = fmax(gmax, sc[(nb * b + p) * kBMax + p].x);
+    for (int i = 0; i < kBMax * kBMax; ++i) sR[i] = make_double2(0.0, 0.0);
+    bool ok = gmax > 0.0;
+    for (int j = 0; j < b && ok; ++j) {
+      double sdiag = sG[j * kBMax + j].x;
+      for (int k = 0; k < j; ++k) sdiag -= sR[k * kBMax + j].x * sR[k * kBMax + j].x + sR[k * kBMax + j].y * sR[k * kBMax + j].y;
+      if (!(sdiag > 1e-26 * gmax)) {
+        ok = false;
+        break;
+      }
+      const double rjj = sqrt(sdiag);
+      sR[j * kBMax + j] = make_double2(rjj, 0.0);
+      for (int q = j + 1; q < b; ++q) {
+        double2 t = sG[j * kBMax + q];
+        for (int k = 0; k < j; ++k) t = csub(t, cdotc(sR[k * kBMax + j], sR[k * kBMax + q]));
+        sR[j * kBMax + q] = make_double2(t.x / rjj, t.y / rjj);
+      }
     }
-    const double rjj = sqrt(s);
-    R[j][j] = make_double2(rjj, 0.0);
-    for (int q = j + 1; q < b; ++q) {
-      double2 t = G[j][q];
-      for (int k = 0; k < j; ++k) t = csub(t, cdotc(R[k][j], R[k][q]));
-      R[j][q] = make_double2(t.x / rjj, t.y / rjj);
+    s_ok = ok;
+    if (!ok) {
+      stt[S_STATUS] = RSED_EBREAKDOWN;
+      stt[S_ACTIVE] = 0;
     }
   }
-  if (!ok) {
-    stt[S_STATUS] = RSED_EBREAKDOWN;
-    stt[S_ACTIVE] = 0;
-    return;
+  __syncthreads();
+  if (!s_ok) return;
+  double2* coef = reinterpret_cast<double2*>(st.coef) + (int64_t)inst * 2 * d.pslots * kBMax * kBMax;
+  double2* cp = coef + (pass - 1) * d.pslots * kBMax * kBMax;
+  for (int e = threadIdx.x; e < nb * b * b; e += blockDim.x) {
+    const int r = e / b, q = e % b;  // C[s r'][q] stored slot-major as before
+    cp[(r / b) * kBMax * kBMax + (r % b) * kBMax + q] = sc[r * kBMax + q];
   }
   double2* Rout = cp + (d.pslots - 1) * kBMax * kBMax;
-  for (int p = 0; p < b; ++p)
-    for (int q = 0; q < b; ++q) Rout[p * kBMax + q] = R[p][q];
+  for (int e = threadIdx.x; e < kBMax * kBMax; e += blockDim.x) Rout[e] = sR[e];
   if (pass == 2) {
     const int nb_old = nb;
-    stt[S_NEWSLOT] = nb_old;
-    stt[S_NB] = nb_old + 1;
-    stt[S_ITERS] += 1;
     if (nb_old >= 1) {
       // combine passes: C = C1 + C2 R1, Rtot = R2 R1 ; column block cb = nb_old-1
       const double2* c1 = coef;
       const double2* R1 = coef + (d.pslots - 1) * kBMax * kBMax;
       double2* P = reinterpret_cast<double2*>(st.P) + (int64_t)inst * d.pm * d.pm;
       const int cb = nb_old - 1;
-      for (int s = 0; s < nb_old; ++s)
-        for (int p = 0; p < b; ++p)
-          for (int q = 0; q < b; ++q) {
-            double2 v = c1[s * kBMax * kBMax + p * kBMax + q];
-            for (int r = 0; r < b; ++r)
-              v = cadd(v, cmul(cp[s * kBMax * kBMax + p * kBMax + r], R1[r * kBMax + q]));
-            P[(int64_t)(s * b + p) * d.pm + cb * b + q] = v;
-          }
-      for (int p = 0; p < b; ++p)
-        for (int q = 0; q < b; ++q) {
-          double2 v = make_double2(0.0, 0.0);
-          for (int r = 0; r < b; ++r) v = cadd(v, cmul(R[p][r], R1[r * kBMax + q]));
-          P[(int64_t)(nb_old * b + p) * d.pm + cb * b + q] = v;
-        }
+      for (int e = threadIdx.x; e < nb_old * b * b; e += blockDim.x) {
+        const int r = e / b, q = e % b, sl = r / b, p = r % b;
+        double2 v = c1[sl * kBMax * kBMax + p * kBMax + q];
+        for (int k = 0; k < b; ++k) v = cadd(v, cmul(sc[r * kBMax + k], R1[k * kBMax + q]));
+        P[(int64_t)r * d.pm + cb * b + q] = v;
+      }
+      for (int e = threadIdx.x; e < b * b; e += blockDim.x) {
+        const int p = e / b, q = e % b;
+        double2 v = make_double2(0.0, 0.0);
+        for (int k = 0; k < b; ++k) v = cadd(v, cmul(sR[p * kBMax + k], R1[k * kBMax + q]));
+        P[(int64_t)(nb_old * b + p) * d.pm + cb * b + q] = v;
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      stt[S_NEWSLOT] = nb_old;
+      stt[S_NB] = nb_old + 1;
+      stt[S_ITERS] += 1;
     }
   }
 }
@@ -213,6 +228,7 @@ __global__ void k_lz_update(rsed_lanczos_t st, LzDims d, int pass) {
   double2 w[kBMax];
 #pragma unroll
   for (int q = 0; q < kBMax; ++q) w[q] = (q < b) ? W[row * d.ld + c0 + q] : make_double2(0.0, 0.0);
+#pragma unroll 4
   for (int s = 0; s < nb; ++s) {
     const double2* Vs = V + s * slot_stride + row * d.ld + c0;
     for (int p = 0; p < b; ++p) {
@@ -364,18 +380,22 @@ __device__ void jacobi_hermitian(double2* A, double2* Vv, int M, int* pp, int* q
 }
 
 // Ritz step: per instance, when due.  Dynamic smem: 2 * kJacobiMax^2 double2.
-__global__ void k_lz_ritz(rsed_lanczos_t st, LzDims d, int check_every, int force) {
+__global__ void k_lz_ritz(rsed_lanczos_t st, LzDims d, int check_every, int force, int rr) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int inst = blockIdx.x;
   int* stt = st.state + inst * kStateInts;
-  if (!stt[S_ACTIVE]) return;
+  if (rr) {
+    if (stt[S_RR] != 1) return;
+  } else if (!stt[S_ACTIVE]) {
+    return;
+  }
   const int b = st.inst_b[inst];
-  const int nb = stt[S_NB];
+  const int nb = rr ? st.keep_blocks + 2 : stt[S_NB];
   const int M = (nb - 1) * b;
-  const bool full = (nb >= d.n_slots + 1);
+  const bool full = !rr && (nb >= d.n_slots + 1);
   const int nev = st.nev;
   const int K = st.keep_blocks * b;
-  const bool due = full || force || (M >= nev + b && M >= K && (stt[S_ITERS] % check_every) == 0);
+  const bool due = rr || full || force || (M >= nev + b && M >= K && (stt[S_ITERS] % check_every) == 0);
   if (!due) return;
   if (M < nev || M < K || M > kJacobiMax) {
     if (full && threadIdx.x == 0) {  // cannot restart: report instead of overrunning
@@ -424,6 +444,13 @@ __global__ void k_lz_ritz(rsed_lanczos_t st, LzDims d, int check_every, int forc
   }
   for (int j = threadIdx.x; j < M; j += blockDim.x) rv[j] = theta[order[j]];
   __syncthreads();
+  if (rr) {  // Rayleigh-Ritz refinement: eigenpairs only, residuals come from k_rr_resid
+    if (threadIdx.x == 0) {
+      stt[S_NB] = nb;
+      stt[S_RR] = 2;
+    }
+    return;
+  }
   // residual estimates: || Rlast * S[last block rows, j] ||
   for (int j = threadIdx.x; j < M; j += blockDim.x) {
     double acc = 0.0;
@@ -547,6 +574,142 @@ __global__ void k_lz_extract(rsed_lanczos_t st, LzDims d, double2* U, int64_t u_
   }
 }
 
+// ---------------------------------------------------------------------------
+// FP64 Rayleigh-Ritz refinement of a converged (FP32-matvec) solve.
+// k_rr_prepare flags converged instances and schedules the thick-restart
+// combination (V_0..keep-1 = Ritz vectors, residual block -> slot keep);
+// the caller then applies H in FP64 to slots 0..keep (into slots keep+1..),
+// k_rr_gram forms T = Q^H H Q over those K + b vectors, k_lz_ritz(rr)
+// diagonalises its Hermitian part and k_rr_resid measures the true FP64
+// residuals ||H u_j - theta_j u_j||.
+__global__ void k_rr_prepare(rsed_lanczos_t st) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= st.n_inst) return;
+  int* s = st.state + i * kStateInts;
+  if (s[S_STATUS] == 1 && s[S_RR] == 0) {
+    s[S_RESTART_NB] = s[S_NB];
+    s[S_NB] = st.keep_blocks + 1;
+    s[S_RR] = 1;
+  }
+}
+
+__global__ void __launch_bounds__(128) k_rr_gram(rsed_lanczos_t st, LzDims d) {
+  const int chunk = blockIdx.x;
+  const int inst = blockIdx.y;
+  int* stt = st.state + inst * kStateInts;
+  if (stt[S_RR] != 1) return;
+  const int b = st.inst_b[inst];
+  const int c0 = st.inst_col0[inst];
+  const int nq = st.keep_blocks + 1;  // blocks of Q
+  const int M = nq * b;
+  const int64_t r0 = (int64_t)chunk * d.chunk_rows;
+  const int64_t r1 = min(r0 + d.chunk_rows, d.n_orb);
+  const double2* V = reinterpret_cast<const double2*>(st.V);
+  const int64_t slot_stride = d.n_orb * d.ld;
+  double2* part = reinterpret_cast<double2*>(st.partial);
+  const int64_t pbase = ((int64_t)chunk * d.n_inst + inst) * (int64_t)kRRMax * kRRMax;
+  __shared__ int s_last;
+  // thread task: (row of T, column block l2) -> b accumulators
+  for (int task = threadIdx.x; task < M * nq; task += blockDim.x) {
+    const int r = task / nq, l2 = task % nq;
+    const double2* Q = V + (int64_t)(r / b) * slot_stride + c0 + (r % b);
+    const double2* Z = V + (int64_t)(nq + l2) * slot_stride + c0;
+    double2 acc[kBMax];
+#pragma unroll
+    for (int q = 0; q < kBMax; ++q) acc[q] = make_double2(0.0, 0.0);
+#pragma unroll 4
+    for (int64_t row = r0; row < r1; ++row) {
+      const double2 qv = Q[row * d.ld];
+#pragma unroll
+      for (int q = 0; q < kBMax; ++q)
+        if (q < b) acc[q] = cadd(acc[q], cdotc(qv, Z[row * d.ld + q]));
+    }
+    for (int q = 0; q < b; ++q) part[pbase + r * kRRMax + l2 * b + q] = acc[q];
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int t = atomicAdd(&stt[S_TICKET], 1);
+    s_last = (t == d.n_chunks - 1);
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  if (threadIdx.x == 0) {
+    stt[S_TICKET] = 0;
+    stt[S_RESTART_NB] = 0;
+  }
+  double2* P = reinterpret_cast<double2*>(st.P) + (int64_t)inst * d.pm * d.pm;
+  for (int e = threadIdx.x; e < M * M; e += blockDim.x) {
+    const int r = e / M, c = e % M;
+    double2 a = make_double2(0.0, 0.0);
+    for (int ch = 0; ch < d.n_chunks; ++ch)
+      a = cadd(a, __ldcg(part + ((int64_t)ch * d.n_inst + inst) * (int64_t)kRRMax * kRRMax + r * kRRMax + c));
+    P[(int64_t)r * d.pm + c] = a;
+  }
+}
+
+// True FP64 residual norms of the nev refined pairs.
+__global__ void __launch_bounds__(128) k_rr_resid(rsed_lanczos_t st, LzDims d) {
+  const int chunk = blockIdx.x;
+  const int inst = blockIdx.y;
+  int* stt = st.state + inst * kStateInts;
+  if (stt[S_RR] != 2) return;
+  const int b = st.inst_b[inst];
+  const int c0 = st.inst_col0[inst];
+  const int nq = st.keep_blocks + 1;
+  const int M = nq * b;
+  const int nev = st.nev;
+  const int64_t r0 = (int64_t)chunk * d.chunk_rows;
+  const int64_t r1 = min(r0 + d.chunk_rows, d.n_orb);
+  const double2* V = reinterpret_cast<const double2*>(st.V);
+  const int64_t slot_stride = d.n_orb * d.ld;
+  const double2* S = reinterpret_cast<const double2*>(st.ritz_vec) + (int64_t)inst * d.pm * d.pm;
+  const double* th = st.ritz_val + (int64_t)inst * d.pm;
+  double* part = st.partial;
+  __shared__ double red[kKeepMax][128];
+  __shared__ int s_last;
+  for (int j = 0; j < nev; ++j) red[j][threadIdx.x] = 0.0;
+  for (int64_t row = r0 + threadIdx.x; row < r1; row += blockDim.x) {
+    for (int j = 0; j < nev; ++j) {
+      double2 hu = make_double2(0.0, 0.0), u = make_double2(0.0, 0.0);
+      for (int l = 0; l < M; ++l) {
+        const double2 sj = S[(int64_t)l * d.pm + j];
+        const int64_t off = row * d.ld + c0 + (l % b);
+        u = cadd(u, cmul(V[(int64_t)(l / b) * slot_stride + off], sj));
+        hu = cadd(hu, cmul(V[(int64_t)(nq + l / b) * slot_stride + off], sj));
+      }
+      const double2 r = make_double2(hu.x - th[j] * u.x, hu.y - th[j] * u.y);
+      red[j][threadIdx.x] += r.x * r.x + r.y * r.y;
+    }
+  }
+  __syncthreads();
+  for (int w = 64; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w)
+      for (int j = 0; j < nev; ++j) red[j][threadIdx.x] += red[j][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x < nev)
+    part[((int64_t)chunk * d.n_inst + inst) * kKeepMax + threadIdx.x] = red[threadIdx.x][0];
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int t = atomicAdd(&stt[S_TICKET], 1);
+    s_last = (t == d.n_chunks - 1);
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  if (threadIdx.x == 0) stt[S_TICKET] = 0;
+  if (threadIdx.x < nev) {
+    double a = 0.0;
+    for (int ch = 0; ch < d.n_chunks; ++ch)
+      a += __ldcg(part + ((int64_t)ch * d.n_inst + inst) * kKeepMax + threadIdx.x);
+    st.resid[(int64_t)inst * d.pm + threadIdx.x] = sqrt(a);
+  }
+  if (threadIdx.x == 0) stt[S_RR] = 3;
+}
+
 LzDims make_dims(const rsed_model_t* md, const rsed_sectors_t* sc, const rsed_lanczos_t* st) {
   LzDims d;
   d.n_orb = md->n_orbits;
@@ -576,7 +739,7 @@ int check_lz(const rsed_model_t* md, const rsed_sectors_t* sc, const rsed_lanczo
   RSED_REQUIRE(st->precision == 64 || (st->precision == 32 && st->Xf), RSED_EINVAL,
                "precision 32 needs the complex64 block buffer");
   const LzDims d = make_dims(md, sc, st);
-  const int64_t need = (int64_t)d.n_chunks * d.n_inst * d.pslots * kBMax * kBMax * 2;
+  const int64_t need = rsed_lanczos_partial_len(d.n_orb, d.chunk_rows, d.n_inst, d.n_slots);
   RSED_REQUIRE(st->partial_len >= need, RSED_ESCRATCH, "partial buffer too small (%lld < %lld)",
                (long long)st->partial_len, (long long)need);
   return RSED_OK;
@@ -584,9 +747,7 @@ int check_lz(const rsed_model_t* md, const rsed_sectors_t* sc, const rsed_lanczo
 
 int launch_pass(const rsed_lanczos_t& st, const LzDims& d, int pass, cudaStream_t stream) {
   dim3 g1(d.n_chunks, d.n_inst);
-  k_lz_gram<<<g1, 128, 0, stream>>>(st, d);
-  RSED_CHECK_LAUNCH();
-  k_lz_finalize<<<d.n_inst, 128, 0, stream>>>(st, d, pass);
+  k_lz_reduce<<<g1, 128, 0, stream>>>(st, d, pass);
   RSED_CHECK_LAUNCH();
   const int64_t tot = d.n_orb * d.n_inst;
   k_lz_update<<<(unsigned)((tot + 255) / 256), 256, 0, stream>>>(st, d, pass);
@@ -606,6 +767,7 @@ __global__ void k_lz_init_state(rsed_lanczos_t st) {
   s[S_RESTART_NB] = 0;
   s[S_NEWSLOT] = 0;
   s[S_NCONV] = 0;
+  for (int k = S_TICKET; k < kStateInts; ++k) s[k] = 0;
 }
 
 __global__ void k_gather_rows(int64_t n_rows, const int32_t* orbit_of_row, const double2* src,
@@ -625,7 +787,9 @@ __global__ void k_scatter_rows(int64_t n_rows, const int32_t* orbit_of_row, cons
 extern "C" int64_t rsed_lanczos_partial_len(int64_t n_orbits, int32_t chunk_rows, int32_t n_inst,
                                             int32_t n_slots) {
   const int64_t n_chunks = (n_orbits + chunk_rows - 1) / chunk_rows;
-  return n_chunks * n_inst * (int64_t)(n_slots + 3) * kBMax * kBMax * 2;
+  const int64_t lz = (int64_t)(n_slots + 3) * kBMax * kBMax * 2;
+  const int64_t rr = (int64_t)kRRMax * kRRMax * 2;
+  return n_chunks * n_inst * (lz > rr ? lz : rr);
 }
 
 extern "C" int64_t rsed_lanczos_coef_len(int32_t n_inst, int32_t n_slots) {
@@ -683,12 +847,43 @@ extern "C" int rsed_lanczos_iterate(const rsed_model_t* md, const rsed_sectors_t
     if (rc) return rc;
     rc = launch_pass(*st, d, 2, stream);
     if (rc) return rc;
-    k_lz_ritz<<<d.n_inst, 256, 2 * sizeof(double2) * kJacobiMax * kJacobiMax, stream>>>(*st, d, check_every, 0);
+    k_lz_ritz<<<d.n_inst, 256, 2 * sizeof(double2) * kJacobiMax * kJacobiMax, stream>>>(*st, d, check_every, 0, 0);
     RSED_CHECK_LAUNCH();
     const int64_t tot = d.n_orb * d.n_inst;
     k_lz_restart<<<(unsigned)((tot + 255) / 256), 256, 0, stream>>>(*st, d);
     RSED_CHECK_LAUNCH();
   }
+  return RSED_OK;
+}
+
+extern "C" int rsed_lanczos_rayleigh_ritz(const rsed_model_t* md, const rsed_sectors_t* sc,
+                                          rsed_lanczos_t* st, int32_t apply_variant, void* stream_) {
+  int rc = check_lz(md, sc, st);
+  if (rc) return rc;
+  rc = set_ritz_smem();
+  if (rc) return rc;
+  RSED_REQUIRE(st->n_slots >= 2 * st->keep_blocks + 1, RSED_EINVAL,
+               "Rayleigh-Ritz needs n_slots >= 2*keep_blocks + 1");
+  cudaStream_t stream = as_stream(stream_);
+  const LzDims d = make_dims(md, sc, st);
+  k_rr_prepare<<<(st->n_inst + 63) / 64, 64, 0, stream>>>(*st);
+  RSED_CHECK_LAUNCH();
+  const int64_t tot = d.n_orb * d.n_inst;
+  k_lz_restart<<<(unsigned)((tot + 255) / 256), 256, 0, stream>>>(*st, d);
+  RSED_CHECK_LAUNCH();
+  const int64_t slot = d.n_orb * d.ld;
+  double2* V = reinterpret_cast<double2*>(st->V);
+  for (int l = 0; l <= st->keep_blocks; ++l) {
+    rc = rsed_apply_h(md, sc, V + l * slot, V + (st->keep_blocks + 1 + l) * slot, 64, apply_variant, stream_);
+    if (rc) return rc;
+  }
+  dim3 g(d.n_chunks, d.n_inst);
+  k_rr_gram<<<g, 128, 0, stream>>>(*st, d);
+  RSED_CHECK_LAUNCH();
+  k_lz_ritz<<<d.n_inst, 256, 2 * sizeof(double2) * kJacobiMax * kJacobiMax, stream>>>(*st, d, 1, 1, 1);
+  RSED_CHECK_LAUNCH();
+  k_rr_resid<<<g, 128, 0, stream>>>(*st, d);
+  RSED_CHECK_LAUNCH();
   return RSED_OK;
 }
 

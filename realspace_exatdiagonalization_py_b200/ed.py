@@ -123,8 +123,7 @@ def _empty():
 
 
 def _default_params(nev: int, precision: int = 64) -> LanczosParams:
-    b = 2 if nev <= 4 else 3
-    return LanczosParams(block=b, n_slots=min(16, 64 // b), precision=precision)
+    return LanczosParams(precision=precision)
 
 
 def ed_scan_at_irrep_matrixfree(irrep_label, ed_data, *, nev: int = 5,

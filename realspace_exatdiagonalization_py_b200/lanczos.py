@@ -23,7 +23,8 @@ from .hamiltonian import DeviceModel
 from .sector import SectorSet
 
 S_NB, S_STATUS, S_RESTARTS, S_ITERS, S_ACTIVE = 0, 1, 2, 3, 4
-S_NCONV = 7
+S_NCONV, S_RR = 7, 9
+STATE_INTS = 16
 
 __all__ = [
     "LanczosBatch",
@@ -37,13 +38,22 @@ __all__ = [
 
 @dataclass
 class LanczosParams:
-    block: int = 2
+    """Thick-restart block Lanczos settings.
+
+    ``tol`` is the FP64 convergence test ``||r_j|| <= tol * max(1, |theta_j|)``
+    (the reference's ARPACK tolerance).  With ``precision=32`` the FP32-matvec
+    phase stops at ``tol32`` and the eigenpairs are then recomputed by an FP64
+    Rayleigh-Ritz step over the thick-restart basis: the eigenvalue error is
+    second order in the FP32 residual.  Ritz checks run at every restart and
+    every ``check_every`` iterations."""
+
+    block: int = 4
     n_slots: int = 16
-    keep_blocks: int = 0  # 0 = automatic: ceil((nev + block) / block), bounded
+    keep_blocks: int = 0  # 0 = automatic
     tol: float = 1e-10
-    tol32: float = 1e-5  # FP32-matvec phase: residual floor of a complex64 operator
+    tol32: float = 1e-6
     max_restarts: int = 200
-    check_every: int = 2
+    check_every: int = 1000
     precision: int = 64
     apply_variant: int = 0
 
@@ -62,9 +72,11 @@ def start_block(n: int, b: int, seed: int = 12345) -> np.ndarray:
 
 
 def _auto_keep(nev: int, b: int, n_slots: int) -> int:
+    """Largest restart basis the kernels hold (<= 16 vectors) that leaves room
+    for the FP64 Rayleigh-Ritz step (n_slots >= 2*keep + 1)."""
     kmax = _lib.load().rsed_lanczos_max_keep()
-    keep = max(1, math.ceil((nev + max(b, 2)) / b))
-    keep = min(keep, n_slots - 2, kmax // b)
+    keep = min(kmax // b, (n_slots - 1) // 2)
+    keep = max(keep, math.ceil(nev / b))
     if keep * b < nev:
         raise ValueError(f"nev={nev} needs keep_blocks*block >= nev (block={b}, n_slots={n_slots})")
     return keep
@@ -122,7 +134,7 @@ class LanczosBatch:
         self.ritz_val = torch.zeros((n_inst, self.pm), dtype=torch.float64, device=dev)
         self.ritz_vec = torch.zeros((n_inst, self.pm, self.pm), dtype=c128, device=dev)
         self.resid = torch.zeros((n_inst, self.pm), dtype=torch.float64, device=dev)
-        self.state = torch.zeros((n_inst, 8), dtype=torch.int32, device=dev)
+        self.state = torch.zeros((n_inst, STATE_INTS), dtype=torch.int32, device=dev)
         self.c = _lib.RsedLanczos(
             n_inst, S, nev, self.keep, p.max_restarts, p.precision, bmax, self.chunk_rows, self.pm, 0,
             float(p.tol if p.precision == 64 else max(p.tol, p.tol32)), _lib.ptr(self.inst_col0), _lib.ptr(self.inst_b), _lib.ptr(self.V),
@@ -175,6 +187,13 @@ class LanczosBatch:
 
     def status(self) -> np.ndarray:
         return self.state.cpu().numpy()
+
+    def rayleigh_ritz(self, stream=None) -> None:
+        """FP64 Rayleigh-Ritz over the restart basis of every converged
+        instance; afterwards ``residuals()`` are true FP64 residual norms."""
+        _lib.check(_lib.lib().rsed_lanczos_rayleigh_ritz(
+            ctypes.byref(self.model.c), ctypes.byref(self.sc), ctypes.byref(self.c),
+            self.p.apply_variant, _lib.stream_ptr(stream)))
 
     def done(self) -> bool:
         return not bool(self.state[:, S_ACTIVE].any().item())
@@ -256,26 +275,11 @@ class LanczosBatch:
         return out
 
 
-def refine(batch: LanczosBatch, *, tol: float = 1e-10, n_slots: int = 8, max_restarts: int = 50,
-           poll: int = 4) -> LanczosBatch:
-    """FP64 finish of an FP32-matvec solve: an FP64 block Lanczos per instance
-    whose start block is the ``nev`` FP32 Ritz vectors (block size = nev)."""
-    nev = batch.nev
-    bsz = nev
-    while bsz * n_slots > _lib.load().rsed_lanczos_max_projected():
-        n_slots -= 1
-    keep = max(1, min(_lib.load().rsed_lanczos_max_keep() // bsz, n_slots - 2))
-    p = LanczosParams(block=bsz, n_slots=n_slots, keep_blocks=keep, tol=tol, max_restarts=max_restarts,
-                      check_every=1, precision=64, apply_variant=0)
-    fb = LanczosBatch(batch.model, batch.sset, batch.inst_sectors, nev, p)
-    U = batch.ritz_vectors_orbit()
-    fb.W.zero_()
-    for i in range(batch.n_inst):
-        c0 = int(fb.col0[i])
-        fb.W[:, c0 : c0 + nev] = U[i].t()
-    fb.start()
-    fb.run(poll=poll)
-    return fb
+def refine(batch: LanczosBatch) -> LanczosBatch:
+    """FP64 finish of an FP32-matvec solve (in place): Rayleigh-Ritz with the
+    FP64 operator over the thick-restart basis; returns the same batch."""
+    batch.rayleigh_ritz()
+    return batch
 
 
 # ---------------------------------------------------------------------------
@@ -303,7 +307,7 @@ def _solve_sector(model: DeviceModel, sset: SectorSet, s: int, nev: int, params:
     b.start()
     b.run()
     if params.precision == 32:
-        b = refine(b)
+        refine(b)
     vals = b.eigenvalues()[0]
     vecs = b.eigenvectors()[0]
     return vals, vecs
@@ -321,7 +325,7 @@ def diagonalize_block_arpack(H, *, nev: int = 5, params: LanczosParams | None = 
             raise ValueError("diagonalize_block_arpack needs the sector basis for n > 500")
         return diagonalize_block_dense(H, nev=nev)
     vals, vecs = _solve_sector(model, basis.sector_set, basis.sector_index, nev,
-                               params or LanczosParams(block=min(4, nev)))
+                               params or LanczosParams())
     return vals, vecs.cpu().numpy()
 
 
@@ -346,6 +350,6 @@ def diagonalize_block_matrixfree(H_op, n: int, *, nev: int = 5, params: LanczosP
         vals, vecs = torch.linalg.eigh(A, UPLO="L")
         k = min(nev, n)
         return vals[:k].cpu().numpy().real, vecs[:, :k].cpu().numpy()
-    params = params or LanczosParams(block=min(4, nev))
+    params = params or LanczosParams()
     vals, vecs = _solve_sector(H_op.model, H_op.basis.sector_set, H_op.basis.sector_index, nev, params)
     return vals, vecs.cpu().numpy()
