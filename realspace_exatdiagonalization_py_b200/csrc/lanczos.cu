@@ -263,120 +263,248 @@ __global__ void k_lz_update(rsed_lanczos_t st, LzDims d, int pass) {
 }
 
 // ---------------------------------------------------------------------------
-// Jacobi eigen-solver for a Hermitian M x M matrix held in shared memory.
-// Brent-Luk round-robin ordering: M/2 disjoint rotations per step.
-__device__ void jacobi_hermitian(double2* A, double2* Vv, int M, int* pp, int* qq, double* cc,
-                                 double* ss, double2* ee, double* red) {
-  const int Me = (M + 1) & ~1;
-  const int npair = Me / 2;
-  for (int i = threadIdx.x; i < M * M; i += blockDim.x) {
-    const int r = i / M, c = i % M;
-    Vv[i] = make_double2(r == c ? 1.0 : 0.0, 0.0);
+// Lowest Kp eigenpairs of a Hermitian M x M matrix held in shared memory
+// (full row-major storage, destroyed), one thread block:
+//   1. Householder reduction to a real symmetric tridiagonal T = Q^H A Q
+//      (lower variant of LAPACK zhetd2: reflectors H_k = I - tau_k v v^H
+//      chosen so the sub-diagonal comes out real), ~5 block barriers per column;
+//   2. eigenvalues of T by Sturm-sequence bisection, one thread per eigenvalue;
+//   3. eigenvectors of T by inverse iteration (tridiagonal LU with partial
+//      pivoting, three solves), one thread per eigenvector, then modified
+//      Gram-Schmidt in ascending order (orthonormal bases of degenerate
+//      clusters);
+//   4. back-transformation s = H_0 H_1 ... H_{M-2} z, one warp per vector.
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ int sturm_count(const double* dd, const double* ee, int M, double x, double pivmin) {
+  int c = 0;
+  double q = dd[0] - x;
+  if (fabs(q) < pivmin) q = -pivmin;
+  if (q < 0.0) ++c;
+  for (int i = 1; i < M; ++i) {
+    q = dd[i] - x - ee[i - 1] * ee[i - 1] / q;
+    if (fabs(q) < pivmin) q = -pivmin;
+    if (q < 0.0) ++c;
+  }
+  return c;
+}
+
+__device__ void herm_lowest(double2* A, int M, int Kp, double* theta, double2* S, double* Z, double2* tau,
+                            double* dd, double* ee, double* red) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int lane = tid & 31, warp = tid >> 5, nwarp = nt >> 5;
+  double2* pw = S;  // scratch vector (M entries) for p / w during the reduction
+  // ---- 1. tridiagonalisation ----
+  for (int k = 0; k < M - 1; ++k) {
+    if (warp == 0) {
+      double sq = 0.0;
+      for (int i = k + 2 + lane; i < M; i += 32) {
+        const double2 v = A[i * M + k];
+        sq += v.x * v.x + v.y * v.y;
+      }
+      sq = warp_sum(sq);
+      if (lane == 0) {
+        const double2 al = A[(k + 1) * M + k];
+        double2 t = make_double2(0.0, 0.0), scl = make_double2(0.0, 0.0);
+        double beta = al.x;
+        if (sq != 0.0 || al.y != 0.0) {
+          beta = -copysign(sqrt(al.x * al.x + al.y * al.y + sq), al.x);
+          t = make_double2((beta - al.x) / beta, -al.y / beta);
+          const double2 den = make_double2(al.x - beta, al.y);
+          const double dn = den.x * den.x + den.y * den.y;
+          scl = make_double2(den.x / dn, -den.y / dn);
+        }
+        tau[k] = t;
+        ee[k] = beta;
+        red[0] = scl.x;
+        red[1] = scl.y;
+      }
+    }
+    __syncthreads();
+    const double2 scl = make_double2(red[0], red[1]);
+    for (int i = k + 2 + tid; i < M; i += nt) A[i * M + k] = cmul(A[i * M + k], scl);
+    if (tid == 0) A[(k + 1) * M + k] = make_double2(1.0, 0.0);
+    __syncthreads();
+    const double2 t = tau[k];
+    if (t.x == 0.0 && t.y == 0.0) continue;
+    // p = tau * A22 v  (warp per row)
+    for (int i = k + 1 + warp; i < M; i += nwarp) {
+      double sx = 0.0, sy = 0.0;
+      for (int j = k + 1 + lane; j < M; j += 32) {
+        const double2 a = A[i * M + j], v = A[j * M + k];
+        sx += a.x * v.x - a.y * v.y;
+        sy += a.x * v.y + a.y * v.x;
+      }
+      sx = warp_sum(sx);
+      sy = warp_sum(sy);
+      if (lane == 0) pw[i] = cmul(t, make_double2(sx, sy));
+    }
+    __syncthreads();
+    // alpha = -1/2 tau (p^H v)
+    if (warp == 0) {
+      double sx = 0.0, sy = 0.0;
+      for (int i = k + 1 + lane; i < M; i += 32) {
+        const double2 c = cdotc(pw[i], A[i * M + k]);
+        sx += c.x;
+        sy += c.y;
+      }
+      sx = warp_sum(sx);
+      sy = warp_sum(sy);
+      if (lane == 0) {
+        const double2 al = cmul(t, make_double2(sx, sy));
+        red[2] = -0.5 * al.x;
+        red[3] = -0.5 * al.y;
+      }
+    }
+    __syncthreads();
+    const double2 alpha = make_double2(red[2], red[3]);
+    for (int i = k + 1 + tid; i < M; i += nt) pw[i] = cadd(pw[i], cmul(alpha, A[i * M + k]));
+    __syncthreads();
+    // A22 -= v w^H + w v^H
+    const int L = M - k - 1;
+    for (int idx = tid; idx < L * L; idx += nt) {
+      const int i = k + 1 + idx / L, j = k + 1 + idx % L;
+      const double2 vi = A[i * M + k], vj = A[j * M + k];
+      const double2 wi = pw[i], wj = pw[j];
+      const double2 u = cadd(make_double2(vi.x * wj.x + vi.y * wj.y, vi.y * wj.x - vi.x * wj.y),
+                             make_double2(wi.x * vj.x + wi.y * vj.y, wi.y * vj.x - wi.x * vj.y));
+      A[i * M + j] = csub(A[i * M + j], u);
+    }
+    __syncthreads();
+  }
+  for (int k = tid; k < M; k += nt) dd[k] = A[k * M + k].x;
+  if (tid == 0 && M >= 1) ee[M - 1] = 0.0;
+  __syncthreads();
+  // ---- 2. bisection ----
+  double lo = 1e300, hi = -1e300, emax2 = 0.0;
+  for (int i = 0; i < M; ++i) {
+    const double r = (i > 0 ? fabs(ee[i - 1]) : 0.0) + (i < M - 1 ? fabs(ee[i]) : 0.0);
+    lo = fmin(lo, dd[i] - r);
+    hi = fmax(hi, dd[i] + r);
+    if (i < M - 1) emax2 = fmax(emax2, ee[i] * ee[i]);
+  }
+  const double tnorm = fmax(fabs(lo), fabs(hi));
+  const double pivmin = 1e-300 * fmax(1.0, emax2);
+  if (tid < Kp) {
+    double a = lo - 1e-12 * tnorm - 1e-300, bnd = hi + 1e-12 * tnorm + 1e-300;
+    for (int it = 0; it < 200 && bnd - a > 2.2e-16 * fmax(fabs(a), fabs(bnd)) + pivmin; ++it) {
+      const double mid = 0.5 * (a + bnd);
+      if (sturm_count(dd, ee, M, mid, pivmin) <= tid) a = mid;
+      else bnd = mid;
+    }
+    theta[tid] = 0.5 * (a + bnd);
   }
   __syncthreads();
-  for (int sweep = 0; sweep < 30; ++sweep) {
-    // off-diagonal norm vs total
-    double off = 0.0, tot = 0.0;
-    for (int i = threadIdx.x; i < M * M; i += blockDim.x) {
-      const double2 a = A[i];
-      const double v = a.x * a.x + a.y * a.y;
-      tot += v;
-      if (i / M != i % M) off += v;
+  // ---- 3. inverse iteration ----
+  if (tid < Kp) {
+    const int j = tid;
+    double lam = theta[j];
+    const double sep = 1e-14 * fmax(tnorm, 1e-300);
+    for (int i = 0; i < j; ++i)  // separate shifts of (nearly) equal eigenvalues
+      if (fabs(lam - theta[i]) < sep) lam = theta[i] + sep * (j - i + 1);
+    double dl[kJacobiMax], dg[kJacobiMax], du[kJacobiMax], du2[kJacobiMax], z[kJacobiMax];
+    unsigned char piv[kJacobiMax];
+    for (int i = 0; i < M; ++i) {
+      dg[i] = dd[i] - lam;
+      dl[i] = (i < M - 1) ? ee[i] : 0.0;
+      du[i] = (i < M - 1) ? ee[i] : 0.0;
+      du2[i] = 0.0;
     }
-    for (int o = 16; o > 0; o >>= 1) {
-      off += __shfl_down_sync(0xffffffffu, off, o);
-      tot += __shfl_down_sync(0xffffffffu, tot, o);
-    }
-    if ((threadIdx.x & 31) == 0) {
-      red[2 * (threadIdx.x >> 5)] = off;
-      red[2 * (threadIdx.x >> 5) + 1] = tot;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double o2 = 0.0, t2 = 0.0;
-      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
-        o2 += red[2 * w];
-        t2 += red[2 * w + 1];
+    const double tiny = 1e-15 * fmax(tnorm, 1e-300);
+    for (int i = 0; i < M - 1; ++i) {
+      if (fabs(dg[i]) >= fabs(dl[i])) {
+        piv[i] = 0;
+        if (dg[i] == 0.0) dg[i] = tiny;
+        const double f = dl[i] / dg[i];
+        dl[i] = f;
+        dg[i + 1] -= f * du[i];
+      } else {
+        piv[i] = 1;
+        const double f = dg[i] / dl[i];
+        dg[i] = dl[i];
+        dl[i] = f;
+        const double tmp = du[i];
+        du[i] = dg[i + 1];
+        dg[i + 1] = tmp - f * dg[i + 1];
+        if (i < M - 2) {
+          du2[i] = du[i + 1];
+          du[i + 1] = -f * du[i + 1];
+        }
       }
-      red[64] = o2;
-      red[65] = t2;
     }
-    __syncthreads();
-    const double offn = red[64], totn = red[65];
-    __syncthreads();
-    if (!(offn > 1e-30 * totn) || offn == 0.0) break;
-    for (int step = 0; step < Me - 1; ++step) {
-      for (int k = threadIdx.x; k < npair; k += blockDim.x) {
-        int p, q;
-        if (k == 0) {
-          p = 0;
-          q = (step % (Me - 1)) + 1;
+    if (dg[M - 1] == 0.0) dg[M - 1] = tiny;
+    unsigned h = 2166136261u ^ (unsigned)(j * 16777619u);
+    for (int i = 0; i < M; ++i) {
+      h = h * 1664525u + 1013904223u;
+      z[i] = ((h >> 8) * (1.0 / 16777216.0)) - 0.5;
+    }
+    for (int rep = 0; rep < 3; ++rep) {
+      for (int i = 0; i < M - 1; ++i) {
+        if (piv[i] == 0) {
+          z[i + 1] -= dl[i] * z[i];
         } else {
-          p = ((step + k) % (Me - 1)) + 1;
-          q = ((step - k + (Me - 1)) % (Me - 1)) + 1;
-        }
-        if (p > q) {
-          int tmp = p;
-          p = q;
-          q = tmp;
-        }
-        double c = 1.0, s = 0.0;
-        double2 e = make_double2(1.0, 0.0);
-        if (q < M) {
-          const double2 bpq = A[p * M + q];
-          const double ab = hypot(bpq.x, bpq.y);
-          const double app = A[p * M + p].x, aqq = A[q * M + q].x;
-          if (ab > 1e-300 && ab > 1e-18 * (fabs(app) + fabs(aqq))) {
-            const double th = (aqq - app) / (2.0 * ab);
-            const double t = (th >= 0.0 ? 1.0 : -1.0) / (fabs(th) + sqrt(th * th + 1.0));
-            c = 1.0 / sqrt(t * t + 1.0);
-            s = t * c;
-            e = make_double2(bpq.x / ab, bpq.y / ab);
-          }
-        }
-        pp[k] = p;
-        qq[k] = q;
-        cc[k] = c;
-        ss[k] = s;
-        ee[k] = e;
-      }
-      __syncthreads();
-      // rows: A <- J^H A
-      for (int it = threadIdx.x; it < npair * M; it += blockDim.x) {
-        const int k = it / M, j = it % M;
-        const int p = pp[k], q = qq[k];
-        if (q >= M || ss[k] == 0.0) continue;
-        const double c = cc[k], s = ss[k];
-        const double2 e = ee[k];
-        const double2 apj = A[p * M + j], aqj = A[q * M + j];
-        const double2 eq = cmul(e, aqj);
-        A[p * M + j] = make_double2(c * apj.x - s * eq.x, c * apj.y - s * eq.y);
-        A[q * M + j] = make_double2(s * apj.x + c * eq.x, s * apj.y + c * eq.y);
-      }
-      __syncthreads();
-      // cols: A <- A J, V <- V J
-      for (int it = threadIdx.x; it < npair * M; it += blockDim.x) {
-        const int k = it / M, i = it % M;
-        const int p = pp[k], q = qq[k];
-        if (q >= M || ss[k] == 0.0) continue;
-        const double c = cc[k], s = ss[k];
-        const double2 ec = cconj(ee[k]);
-        {
-          const double2 aip = A[i * M + p], aiq = A[i * M + q];
-          const double2 t = cmul(aiq, ec);
-          A[i * M + p] = make_double2(c * aip.x - s * t.x, c * aip.y - s * t.y);
-          A[i * M + q] = make_double2(s * aip.x + c * t.x, s * aip.y + c * t.y);
-        }
-        {
-          const double2 vip = Vv[i * M + p], viq = Vv[i * M + q];
-          const double2 t = cmul(viq, ec);
-          Vv[i * M + p] = make_double2(c * vip.x - s * t.x, c * vip.y - s * t.y);
-          Vv[i * M + q] = make_double2(s * vip.x + c * t.x, s * vip.y + c * t.y);
+          const double tmp = z[i];
+          z[i] = z[i + 1];
+          z[i + 1] = tmp - dl[i] * z[i];
         }
       }
-      __syncthreads();
+      z[M - 1] /= dg[M - 1];
+      if (M > 1) z[M - 2] = (z[M - 2] - du[M - 2] * z[M - 1]) / dg[M - 2];
+      for (int i = M - 3; i >= 0; --i) z[i] = (z[i] - du[i] * z[i + 1] - du2[i] * z[i + 2]) / dg[i];
+      double nrm = 0.0;
+      for (int i = 0; i < M; ++i) nrm = fmax(nrm, fabs(z[i]));
+      const double inv = nrm > 0.0 ? 1.0 / nrm : 1.0;
+      for (int i = 0; i < M; ++i) z[i] *= inv;
+    }
+    double n2 = 0.0;
+    for (int i = 0; i < M; ++i) n2 += z[i] * z[i];
+    const double inv = 1.0 / sqrt(n2);
+    for (int i = 0; i < M; ++i) Z[i * Kp + j] = z[i] * inv;
+  }
+  __syncthreads();
+  // modified Gram-Schmidt in ascending order (one warp)
+  if (warp == 0) {
+    for (int j = 0; j < Kp; ++j) {
+      for (int i = 0; i < j; ++i) {
+        double dt = 0.0;
+        for (int r = lane; r < M; r += 32) dt += Z[r * Kp + i] * Z[r * Kp + j];
+        dt = warp_sum(dt);
+        for (int r = lane; r < M; r += 32) Z[r * Kp + j] -= dt * Z[r * Kp + i];
+        __syncwarp();
+      }
+      double n2 = 0.0;
+      for (int r = lane; r < M; r += 32) n2 += Z[r * Kp + j] * Z[r * Kp + j];
+      n2 = warp_sum(n2);
+      const double inv = 1.0 / sqrt(n2);
+      for (int r = lane; r < M; r += 32) Z[r * Kp + j] *= inv;
+      __syncwarp();
     }
   }
+  __syncthreads();
+  // ---- 4. back-transformation (warp per vector) ----
+  for (int j = warp; j < Kp; j += nwarp) {
+    for (int r = lane; r < M; r += 32) S[r * Kp + j] = make_double2(Z[r * Kp + j], 0.0);
+    __syncwarp();
+    for (int k = M - 2; k >= 0; --k) {
+      const double2 t = tau[k];
+      if (t.x == 0.0 && t.y == 0.0) continue;
+      double sx = 0.0, sy = 0.0;
+      for (int r = k + 1 + lane; r < M; r += 32) {
+        const double2 c = cdotc(A[r * M + k], S[r * Kp + j]);
+        sx += c.x;
+        sy += c.y;
+      }
+      sx = warp_sum(sx);
+      sy = warp_sum(sy);
+      const double2 f = cmul(t, make_double2(sx, sy));
+      for (int r = k + 1 + lane; r < M; r += 32) S[r * Kp + j] = csub(S[r * Kp + j], cmul(A[r * M + k], f));
+      __syncwarp();
+    }
+  }
+  __syncthreads();
 }
 
 // Ritz step: per instance, when due.  Dynamic smem: 2 * kJacobiMax^2 double2.
@@ -405,12 +533,13 @@ __global__ void k_lz_ritz(rsed_lanczos_t st, LzDims d, int check_every, int forc
     return;
   }
   double2* A = reinterpret_cast<double2*>(smem);
-  double2* Vv = A + kJacobiMax * kJacobiMax;
-  __shared__ int pp[kJacobiMax / 2], qq[kJacobiMax / 2], order[kJacobiMax];
-  __shared__ double cc[kJacobiMax / 2], ss[kJacobiMax / 2], red[72];
-  __shared__ double2 ee[kJacobiMax / 2];
-  __shared__ double theta[kJacobiMax];
+  double2* Sv = A + kJacobiMax * kJacobiMax;                      // M x Kp eigenvectors
+  double* Z = reinterpret_cast<double*>(Sv + kJacobiMax * kKeepMax);  // M x Kp real scratch
+  __shared__ double2 tau[kJacobiMax];
+  __shared__ double dd[kJacobiMax], ee[kJacobiMax], red[8];
+  __shared__ double theta[kKeepMax];
   __shared__ int conv_flag;
+  const int Kp = min(M, max(nev, K));
   const double2* P = reinterpret_cast<const double2*>(st.P) + (int64_t)inst * d.pm * d.pm;
   for (int i = threadIdx.x; i < M * M; i += blockDim.x) {
     const int r = i / M, c = i % M;
@@ -418,31 +547,15 @@ __global__ void k_lz_ritz(rsed_lanczos_t st, LzDims d, int check_every, int forc
     A[i] = make_double2(0.5 * (a.x + bt.x), 0.5 * (a.y - bt.y));
   }
   __syncthreads();
-  jacobi_hermitian(A, Vv, M, pp, qq, cc, ss, ee, red);
-  if (threadIdx.x == 0) {
-    for (int i = 0; i < M; ++i) {
-      order[i] = i;
-      theta[i] = A[i * M + i].x;
-    }
-    for (int i = 1; i < M; ++i) {  // insertion sort by eigenvalue
-      int j = i;
-      while (j > 0 && theta[order[j - 1]] > theta[order[j]]) {
-        int t = order[j];
-        order[j] = order[j - 1];
-        order[j - 1] = t;
-        --j;
-      }
-    }
-  }
-  __syncthreads();
+  herm_lowest(A, M, Kp, theta, Sv, Z, tau, dd, ee, red);
   double* rv = st.ritz_val + (int64_t)inst * d.pm;
   double2* rvec = reinterpret_cast<double2*>(st.ritz_vec) + (int64_t)inst * d.pm * d.pm;
   double* res = st.resid + (int64_t)inst * d.pm;
-  for (int i = threadIdx.x; i < M * M; i += blockDim.x) {
-    const int r = i / M, j = i % M;
-    rvec[(int64_t)r * d.pm + j] = Vv[r * M + order[j]];
+  for (int i = threadIdx.x; i < M * Kp; i += blockDim.x) {
+    const int r = i / Kp, j = i % Kp;
+    rvec[(int64_t)r * d.pm + j] = Sv[r * Kp + j];
   }
-  for (int j = threadIdx.x; j < M; j += blockDim.x) rv[j] = theta[order[j]];
+  for (int j = threadIdx.x; j < Kp; j += blockDim.x) rv[j] = theta[j];
   __syncthreads();
   if (rr) {  // Rayleigh-Ritz refinement: eigenpairs only, residuals come from k_rr_resid
     if (threadIdx.x == 0) {
@@ -452,13 +565,13 @@ __global__ void k_lz_ritz(rsed_lanczos_t st, LzDims d, int check_every, int forc
     return;
   }
   // residual estimates: || Rlast * S[last block rows, j] ||
-  for (int j = threadIdx.x; j < M; j += blockDim.x) {
+  for (int j = threadIdx.x; j < Kp; j += blockDim.x) {
     double acc = 0.0;
     for (int q = 0; q < b; ++q) {
       double2 v = make_double2(0.0, 0.0);
       for (int p = 0; p < b; ++p) {
         const double2 r = P[(int64_t)((nb - 1) * b + q) * d.pm + (nb - 2) * b + p];
-        v = cadd(v, cmul(r, Vv[((nb - 2) * b + p) * M + order[j]]));
+        v = cadd(v, cmul(r, Sv[((nb - 2) * b + p) * Kp + j]));
       }
       acc += v.x * v.x + v.y * v.y;
     }
@@ -495,7 +608,7 @@ __global__ void k_lz_ritz(rsed_lanczos_t st, LzDims d, int check_every, int forc
     double2 v = make_double2(0.0, 0.0);
     for (int p = 0; p < b; ++p) {
       const double2 r = Pw[(int64_t)((nb - 1) * b + q) * d.pm + (nb - 2) * b + p];
-      v = cadd(v, cmul(r, Vv[((nb - 2) * b + p) * M + order[j]]));
+      v = cadd(v, cmul(r, Sv[((nb - 2) * b + p) * Kp + j]));
     }
     A[it] = v;
   }
