@@ -141,6 +141,23 @@ int rsed_sector_rows(int64_t n_orbits, const uint64_t* member, int32_t sector,
                      int32_t* orbit_of_row, int32_t* row_of_orbit, void* scratch,
                      size_t scratch_bytes, void* stream);
 
+/* Same output as rsed_sector_rows, without any caller scratch: for callers
+ * that cannot allocate device memory -- services that reserve the GPU's
+ * memory up front in their own pool and forbid later allocations, and
+ * latency-critical loops that must not hit the device-wide synchronisation
+ * that cudaFree performs.  No counterpart in the reference (it has no C
+ * interface at all).  The scan's tile sums live in a file-scope __device__
+ * array sized for at most rsed_sector_rows_noalloc_max_orbits() = 2^27 orbits
+ * (128 KiB, present on every GPU that loads the library until the process
+ * exits); larger inputs return RSED_ERANGE.  The array's device address is
+ * looked up on the first call on each device, so make that first call before
+ * any stream capture.  All calls share the array: calls that can overlap on
+ * the GPU (different streams, different host threads) race and must be
+ * serialised by the caller.  It calls no cudaMalloc/cudaFree. */
+int rsed_sector_rows_noalloc(int64_t n_orbits, const uint64_t* member, int32_t sector,
+                             int32_t* orbit_of_row, int32_t* row_of_orbit, void* stream);
+int64_t rsed_sector_rows_noalloc_max_orbits(void);
+
 /* Density-density diagonal per orbit, summed in term order like the
  * reference's h_diag (symmetry_resolved_ed.py:641-646). */
 int rsed_density_diag(int64_t n_orbits, const uint64_t* repr_masks, int32_t n_density,

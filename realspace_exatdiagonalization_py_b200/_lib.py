@@ -148,6 +148,8 @@ SIGNATURES = {
         c_int,
         [c_int64, c_void_p, c_int32, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p],
     ),
+    "rsed_sector_rows_noalloc": (c_int, [c_int64, c_void_p, c_int32, c_void_p, c_void_p, c_void_p]),
+    "rsed_sector_rows_noalloc_max_orbits": (c_int64, []),
     "rsed_density_diag": (
         c_int,
         [c_int64, c_void_p, c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p],

@@ -8,6 +8,7 @@
 //   stab_off    n_orb+1 x 8 B   exclusive offsets into stab_phase
 //   stab_phase  sum|Stab| x 16 B complex128 alpha_h(rep), ascending h
 #include <cstring>
+#include <mutex>
 #include "rsed_internal.cuh"
 
 namespace {
@@ -717,3 +718,105 @@ extern "C" int rsed_density_diag(int64_t n_orbits, const uint64_t* repr_masks, i
   RSED_CHECK_LAUNCH();
   return RSED_OK;
 }
+
+// ---- sector rows without device allocation ----------------------------------
+// rsed_sector_rows_noalloc: the same result as rsed_sector_rows, for callers
+// that cannot hand the library a scratch buffer.  Its only scratch is the
+// per-tile sums of the scan, held in this file-scope device array (one copy
+// on every GPU that loads the library, kept until the process exits).  The
+// member bit is re-derived from `member` in both passes instead of being
+// stored, so no buffer proportional to n_orbits is needed.
+namespace {
+
+constexpr int64_t kNoAllocMaxTiles = 16384;  // 16384 tiles x 8192 orbits = 2^27 orbits
+constexpr int64_t kNoAllocMaxOrbits = kNoAllocMaxTiles * kScanTile;
+
+// tile sums (kNoAllocMaxTiles) followed by the total
+static __device__ __align__(256) int64_t g_rows_scan_scratch[kNoAllocMaxTiles + 1];
+
+__global__ void k_nb_tile_counts(int64_t n, const uint64_t* member, int sector, int64_t* tile_sum) {
+  __shared__ int64_t tot;
+  const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+  int64_t c = 0;
+  for (int j = 0; j < kScanItems; ++j) {
+    const int64_t i = base + j;
+    if (i < n) c += (member[i] >> sector) & 1ull;
+  }
+  block_exclusive_scan(c, &tot);
+  if (threadIdx.x == 0) tile_sum[blockIdx.x] = tot;
+}
+
+__global__ void k_nb_tile_rows(int64_t n, const uint64_t* member, int sector, const int64_t* tile_off,
+                               int32_t* orbit_of_row, int32_t* row_of_orbit) {
+  __shared__ int64_t tot;
+  const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+  int flag[kScanItems];
+  int64_t c = 0;
+  for (int j = 0; j < kScanItems; ++j) {
+    const int64_t i = base + j;
+    flag[j] = (i < n) ? (int)((member[i] >> sector) & 1ull) : 0;
+    c += flag[j];
+  }
+  int64_t pos = block_exclusive_scan(c, &tot) + tile_off[blockIdx.x];
+  for (int j = 0; j < kScanItems; ++j) {
+    const int64_t i = base + j;
+    if (i >= n) break;
+    if (flag[j]) {
+      if (orbit_of_row) orbit_of_row[pos] = (int32_t)i;
+      if (row_of_orbit) row_of_orbit[i] = (int32_t)pos;
+      ++pos;
+    } else if (row_of_orbit) {
+      row_of_orbit[i] = -1;
+    }
+  }
+}
+
+// Device address of the scratch array, looked up once per device.
+std::mutex g_noalloc_mu;
+int64_t* g_noalloc_ptr[64] = {nullptr};
+
+int noalloc_scratch(int64_t** out) {
+  int dev = -1;
+  RSED_TRY_CUDA(cudaGetDevice(&dev));
+  RSED_REQUIRE(dev >= 0 && dev < 64, RSED_ERANGE, "device ordinal %d outside [0, 64)", dev);
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (g_noalloc_ptr[dev] == nullptr) {
+    void* p = nullptr;
+    RSED_TRY_CUDA(cudaGetSymbolAddress(&p, g_rows_scan_scratch));
+    g_noalloc_ptr[dev] = reinterpret_cast<int64_t*>(p);
+  }
+  *out = g_noalloc_ptr[dev];
+  return RSED_OK;
+}
+
+}  // namespace
+
+extern "C" int rsed_sector_rows_noalloc(int64_t n_orbits, const uint64_t* member, int32_t sector,
+                                        int32_t* orbit_of_row, int32_t* row_of_orbit, void* stream_) {
+  RSED_REQUIRE(n_orbits >= 1 && member && sector >= 0 && sector < 64, RSED_EINVAL,
+               "bad sector-rows arguments");
+  RSED_REQUIRE(orbit_of_row || row_of_orbit, RSED_EINVAL, "no output buffer");
+  RSED_REQUIRE(n_orbits <= kNoAllocMaxOrbits, RSED_ERANGE,
+               "rsed_sector_rows_noalloc handles at most %lld orbits (got %lld); "
+               "use rsed_sector_rows with a caller-owned scratch buffer",
+               (long long)kNoAllocMaxOrbits, (long long)n_orbits);
+  int64_t* scratch = nullptr;
+  int rc = noalloc_scratch(&scratch);
+  if (rc) return rc;
+  cudaStream_t stream = as_stream(stream_);
+  const int64_t tiles = (n_orbits + kScanTile - 1) / kScanTile;
+  int64_t* tile_sum = scratch;
+  int64_t* total = scratch + kNoAllocMaxTiles;
+  // every tile sum and the total are rewritten below, so the contents left
+  // by an earlier call need no clearing
+  k_nb_tile_counts<<<(unsigned)tiles, kScanThreads, 0, stream>>>(n_orbits, member, sector, tile_sum);
+  RSED_CHECK_LAUNCH();
+  k_scan_tiles<<<1, kScanThreads, 0, stream>>>(tile_sum, tiles, total);
+  RSED_CHECK_LAUNCH();
+  k_nb_tile_rows<<<(unsigned)tiles, kScanThreads, 0, stream>>>(n_orbits, member, sector, tile_sum,
+                                                               orbit_of_row, row_of_orbit);
+  RSED_CHECK_LAUNCH();
+  return RSED_OK;
+}
+
+extern "C" int64_t rsed_sector_rows_noalloc_max_orbits(void) { return kNoAllocMaxOrbits; }
