@@ -498,7 +498,19 @@ def main():
     ap.add_argument("--plain-sectors", type=int, default=12)
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--skip-scale", action="store_true")
+    ap.add_argument("--matvec-only", action="store_true",
+                    help="only the 32-site matvec at scale (for kernel profiling)")
+    ap.add_argument("--matvec-launches", type=int, default=20)
     args = ap.parse_args()
+    if args.matvec_only:
+        import realspace_exatdiagonalization_py_b200 as ed
+        from realspace_exatdiagonalization_py_b200 import models
+
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+            os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+        print(json.dumps(matvec_at_scale(ed, models, float(peaks.get("hbm_gbs", 6650.0)),
+                                         n_launch=args.matvec_launches)), flush=True)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -251,6 +251,15 @@ int rsed_lanczos_iterate(const rsed_model_t* model, const rsed_sectors_t* sec, r
  * written to resid[inst*pm + j].  Needs n_slots >= 2*keep_blocks + 1. */
 int rsed_lanczos_rayleigh_ritz(const rsed_model_t* model, const rsed_sectors_t* sec,
                                rsed_lanczos_t* st, int32_t apply_variant, void* stream);
+/* The whole thick-restart loop for every active instance in ONE launch: one
+ * thread-block cluster of cluster_size (1..8) CTAs per instance, each CTA
+ * owning a slice of the orbit rows; Gram reductions go through distributed
+ * shared memory, the projected eigenproblem is solved by the cluster's first
+ * CTA.  Block sizes must divide 32.  Runs at most max_iter block steps;
+ * per-instance status and the Ritz data are left in `st` as after
+ * rsed_lanczos_iterate, so rsed_lanczos_rayleigh_ritz/_extract follow. */
+int rsed_lanczos_persistent(const rsed_model_t* model, const rsed_sectors_t* sec, rsed_lanczos_t* st,
+                            int32_t cluster_size, int32_t max_iter, void* stream);
 /* Ritz vectors of the nev lowest pairs of the last check:
  * U[(inst*nev + j)*u_stride + orbit] (complex128). */
 int rsed_lanczos_extract(const rsed_model_t* model, const rsed_sectors_t* sec, rsed_lanczos_t* st,

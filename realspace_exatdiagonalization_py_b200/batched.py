@@ -22,7 +22,7 @@ class BatchedSectorSolver:
 
     def __init__(self, model: DeviceModel, sset: SectorSet, sectors: list[int], nev: int, *,
                  precision: int = 64, params: LanczosParams | None = None, poll: int = 16,
-                 graph: bool = True):
+                 graph: bool = True, persistent: int = 4):
         p = params or LanczosParams()
         if p.precision != precision:
             p = LanczosParams(**{**p.__dict__, "precision": precision})
@@ -30,13 +30,18 @@ class BatchedSectorSolver:
         self.precision = precision
         self.poll = poll
         self.graph = graph
+        # cluster size of the one-launch solve (0 = per-iteration kernels in a CUDA graph)
+        self.persistent = persistent if (p.block & (p.block - 1)) == 0 and p.block <= 4 else 0
         self.batch = LanczosBatch(model, sset, self.sectors, nev, p)
         self.refiner = None
         self.last_fp32_vals = None
 
     def _run(self, b: LanczosBatch, poll: int):
         b.start()
-        b.run(poll=poll, graph=self.graph)
+        if self.persistent:
+            b.run_persistent(self.persistent)
+        else:
+            b.run(poll=poll, graph=self.graph)
 
     def solve(self, start_blocks=None, *, vectors: bool = True, host: bool = True):
         """Solve every sector; ``start_blocks`` as in ``LanczosBatch.load_start``.

@@ -19,8 +19,12 @@
 //
 // The reorthogonalisation is block classical Gram-Schmidt with the Pythagorean
 // Cholesky update, applied twice (one reduction per pass).
+#include <cooperative_groups.h>
 #include <type_traits>
 #include "rsed_internal.cuh"
+#include "rsed_apply.cuh"
+
+namespace cg = cooperative_groups;
 
 extern "C" int64_t rsed_lanczos_partial_len(int64_t n_orbits, int32_t chunk_rows, int32_t n_inst,
                                             int32_t n_slots);
@@ -32,6 +36,9 @@ constexpr int kKeepMax = 16;    // largest thick-restart basis (columns)
 constexpr int kJacobiMax = 64;  // largest projected matrix
 constexpr int kRRMax = kKeepMax + kBMax;  // Rayleigh-Ritz basis (restart basis + residual block)
 constexpr int kStateInts = 16;
+// dynamic shared memory of k_lz_ritz: padded A (M x (M+1)), S (M x 16 complex), Z (M x 16 real)
+constexpr size_t kRitzSmem = sizeof(double2) * (kJacobiMax * (kJacobiMax + 1) + kJacobiMax * kKeepMax) +
+                             sizeof(double) * kJacobiMax * kKeepMax;
 // state fields
 constexpr int S_NB = 0, S_STATUS = 1, S_RESTARTS = 2, S_ITERS = 3, S_ACTIVE = 4, S_RESTART_NB = 5,
               S_NEWSLOT = 6, S_NCONV = 7, S_TICKET = 8, S_RR = 9;
@@ -228,7 +235,7 @@ __global__ void k_lz_update(rsed_lanczos_t st, LzDims d, int pass) {
   double2 w[kBMax];
 #pragma unroll
   for (int q = 0; q < kBMax; ++q) w[q] = (q < b) ? W[row * d.ld + c0 + q] : make_double2(0.0, 0.0);
-#pragma unroll 4
+#pragma unroll 2
   for (int s = 0; s < nb; ++s) {
     const double2* Vs = V + s * slot_stride + row * d.ld + c0;
     for (int p = 0; p < b; ++p) {
@@ -293,92 +300,96 @@ __device__ int sturm_count(const double* dd, const double* ee, int M, double x, 
 }
 
 __device__ void herm_lowest(double2* A, int M, int Kp, double* theta, double2* S, double* Z, double2* tau,
-                            double* dd, double* ee, double* red) {
+                            double* dd, double* ee, double* red, double2* vv, double2* pw) {
+  // A is M x M with row stride lda = M + 1 (odd, so column walks hit distinct banks)
+  const int lda = M + 1;
   const int tid = threadIdx.x, nt = blockDim.x;
   const int lane = tid & 31, warp = tid >> 5, nwarp = nt >> 5;
-  double2* pw = S;  // scratch vector (M entries) for p / w during the reduction
-  // ---- 1. tridiagonalisation ----
+  // ---- 1. tridiagonalisation: three barriers per column ----
   for (int k = 0; k < M - 1; ++k) {
+    // phase A (warp 0): reflector of column k, scaled v into vv and back into A
     if (warp == 0) {
       double sq = 0.0;
       for (int i = k + 2 + lane; i < M; i += 32) {
-        const double2 v = A[i * M + k];
+        const double2 v = A[i * lda + k];
         sq += v.x * v.x + v.y * v.y;
       }
       sq = warp_sum(sq);
+      const double2 al = A[(k + 1) * lda + k];
+      double2 t = make_double2(0.0, 0.0), scl = make_double2(0.0, 0.0);
+      double beta = al.x;
+      if (sq != 0.0 || al.y != 0.0) {
+        beta = -copysign(sqrt(al.x * al.x + al.y * al.y + sq), al.x);
+        t = make_double2((beta - al.x) / beta, -al.y / beta);
+        const double2 den = make_double2(al.x - beta, al.y);
+        const double dn = den.x * den.x + den.y * den.y;
+        scl = make_double2(den.x / dn, -den.y / dn);
+      }
+      for (int i = k + 2 + lane; i < M; i += 32) {
+        const double2 v = cmul(A[i * lda + k], scl);
+        A[i * lda + k] = v;
+        vv[i] = v;
+      }
       if (lane == 0) {
-        const double2 al = A[(k + 1) * M + k];
-        double2 t = make_double2(0.0, 0.0), scl = make_double2(0.0, 0.0);
-        double beta = al.x;
-        if (sq != 0.0 || al.y != 0.0) {
-          beta = -copysign(sqrt(al.x * al.x + al.y * al.y + sq), al.x);
-          t = make_double2((beta - al.x) / beta, -al.y / beta);
-          const double2 den = make_double2(al.x - beta, al.y);
-          const double dn = den.x * den.x + den.y * den.y;
-          scl = make_double2(den.x / dn, -den.y / dn);
-        }
+        vv[k + 1] = make_double2(1.0, 0.0);
+        A[(k + 1) * lda + k] = make_double2(1.0, 0.0);
         tau[k] = t;
         ee[k] = beta;
-        red[0] = scl.x;
-        red[1] = scl.y;
       }
     }
-    __syncthreads();
-    const double2 scl = make_double2(red[0], red[1]);
-    for (int i = k + 2 + tid; i < M; i += nt) A[i * M + k] = cmul(A[i * M + k], scl);
-    if (tid == 0) A[(k + 1) * M + k] = make_double2(1.0, 0.0);
     __syncthreads();
     const double2 t = tau[k];
     if (t.x == 0.0 && t.y == 0.0) continue;
-    // p = tau * A22 v  (warp per row)
-    for (int i = k + 1 + warp; i < M; i += nwarp) {
+    // phase B: p = tau * A22 v, one thread per row (odd stride: no bank conflicts)
+    if (tid < M - k - 1) {
+      const int i = k + 1 + tid;
       double sx = 0.0, sy = 0.0;
-      for (int j = k + 1 + lane; j < M; j += 32) {
-        const double2 a = A[i * M + j], v = A[j * M + k];
+      const double2* Ar = A + i * lda;
+      for (int j = k + 1; j < M; ++j) {
+        const double2 a = Ar[j], v = vv[j];
         sx += a.x * v.x - a.y * v.y;
         sy += a.x * v.y + a.y * v.x;
       }
-      sx = warp_sum(sx);
-      sy = warp_sum(sy);
-      if (lane == 0) pw[i] = cmul(t, make_double2(sx, sy));
+      pw[i] = cmul(t, make_double2(sx, sy));
     }
     __syncthreads();
-    // alpha = -1/2 tau (p^H v)
+    // p^H v (warp 0) into red[0..1]
     if (warp == 0) {
       double sx = 0.0, sy = 0.0;
       for (int i = k + 1 + lane; i < M; i += 32) {
-        const double2 c = cdotc(pw[i], A[i * M + k]);
+        const double2 c = cdotc(pw[i], vv[i]);
         sx += c.x;
         sy += c.y;
       }
       sx = warp_sum(sx);
       sy = warp_sum(sy);
       if (lane == 0) {
-        const double2 al = cmul(t, make_double2(sx, sy));
-        red[2] = -0.5 * al.x;
-        red[3] = -0.5 * al.y;
+        red[0] = sx;
+        red[1] = sy;
       }
     }
     __syncthreads();
-    const double2 alpha = make_double2(red[2], red[3]);
-    for (int i = k + 1 + tid; i < M; i += nt) pw[i] = cadd(pw[i], cmul(alpha, A[i * M + k]));
-    __syncthreads();
-    // A22 -= v w^H + w v^H
-    const int L = M - k - 1;
-    for (int idx = tid; idx < L * L; idx += nt) {
-      const int i = k + 1 + idx / L, j = k + 1 + idx % L;
-      const double2 vi = A[i * M + k], vj = A[j * M + k];
-      const double2 wi = pw[i], wj = pw[j];
-      const double2 u = cadd(make_double2(vi.x * wj.x + vi.y * wj.y, vi.y * wj.x - vi.x * wj.y),
-                             make_double2(wi.x * vj.x + wi.y * vj.y, wi.y * vj.x - wi.x * vj.y));
-      A[i * M + j] = csub(A[i * M + j], u);
+    // phase C: alpha = -1/2 tau (p^H v); A22 -= v w^H + w v^H with w = p + alpha v
+    const double2 pv = make_double2(red[0], red[1]);
+    const double2 ta = cmul(t, pv);
+    const double2 alpha = make_double2(-0.5 * ta.x, -0.5 * ta.y);
+    for (int i = k + 1 + warp; i < M; i += nwarp) {
+      const double2 vi = vv[i];
+      const double2 wi = cadd(pw[i], cmul(alpha, vi));
+      for (int j = k + 1 + lane; j < M; j += 32) {
+        const double2 vj = vv[j];
+        const double2 wj = cadd(pw[j], cmul(alpha, vj));
+        const double2 u = cadd(make_double2(vi.x * wj.x + vi.y * wj.y, vi.y * wj.x - vi.x * wj.y),
+                               make_double2(wi.x * vj.x + wi.y * vj.y, wi.y * vj.x - wi.x * vj.y));
+        A[i * lda + j] = csub(A[i * lda + j], u);
+      }
     }
     __syncthreads();
   }
-  for (int k = tid; k < M; k += nt) dd[k] = A[k * M + k].x;
+  for (int k = tid; k < M; k += nt) dd[k] = A[k * lda + k].x;
   if (tid == 0 && M >= 1) ee[M - 1] = 0.0;
   __syncthreads();
-  // ---- 2. bisection ----
+  // ---- 2. eigenvalues: 16-way multisection, 16 threads per eigenvalue ----
   double lo = 1e300, hi = -1e300, emax2 = 0.0;
   for (int i = 0; i < M; ++i) {
     const double r = (i > 0 ? fabs(ee[i - 1]) : 0.0) + (i < M - 1 ? fabs(ee[i]) : 0.0);
@@ -388,14 +399,24 @@ __device__ void herm_lowest(double2* A, int M, int Kp, double* theta, double2* S
   }
   const double tnorm = fmax(fabs(lo), fabs(hi));
   const double pivmin = 1e-300 * fmax(1.0, emax2);
-  if (tid < Kp) {
+  {
+    const int j = tid >> 4, sub = tid & 15;  // eigenvalue j, sample point sub
     double a = lo - 1e-12 * tnorm - 1e-300, bnd = hi + 1e-12 * tnorm + 1e-300;
-    for (int it = 0; it < 200 && bnd - a > 2.2e-16 * fmax(fabs(a), fabs(bnd)) + pivmin; ++it) {
-      const double mid = 0.5 * (a + bnd);
-      if (sturm_count(dd, ee, M, mid, pivmin) <= tid) a = mid;
-      else bnd = mid;
+    // 16 rounds shrink the Gershgorin interval by 16^16 ~ 1.8e19: below one ulp.
+    // No early exit, so every lane of the warp stays in the ballot.
+    for (int round = 0; round < 16; ++round) {
+      const double w = (bnd - a) * (1.0 / 16.0);
+      const double x = a + w * (sub + 1);
+      const int c = (j < Kp && sub < 15) ? sturm_count(dd, ee, M, x, pivmin) : 1 << 30;
+      // first sample whose count exceeds j bounds the eigenvalue from above
+      const unsigned ballot = __ballot_sync(0xffffffffu, c > j);
+      const unsigned mine = (ballot >> ((lane >> 4) << 4)) & 0xFFFFu;
+      const int first = __ffs(mine) - 1;  // 0..15 (15 = the upper end)
+      const double na = a + w * first;
+      bnd = a + w * (first + 1);
+      a = na;
     }
-    theta[tid] = 0.5 * (a + bnd);
+    if (j < Kp && sub == 0) theta[j] = 0.5 * (a + bnd);
   }
   __syncthreads();
   // ---- 3. inverse iteration ----
@@ -484,25 +505,27 @@ __device__ void herm_lowest(double2* A, int M, int Kp, double* theta, double2* S
     }
   }
   __syncthreads();
-  // ---- 4. back-transformation (warp per vector) ----
-  for (int j = warp; j < Kp; j += nwarp) {
-    for (int r = lane; r < M; r += 32) S[r * Kp + j] = make_double2(Z[r * Kp + j], 0.0);
-    __syncwarp();
-    for (int k = M - 2; k >= 0; --k) {
-      const double2 t = tau[k];
-      if (t.x == 0.0 && t.y == 0.0) continue;
+  // ---- 4. back-transformation: s = H_0 (H_1 (... H_{M-2} z)), all vectors at once ----
+  for (int i = tid; i < M * Kp; i += nt) S[i] = make_double2(Z[i], 0.0);
+  __syncthreads();
+  for (int k = M - 2; k >= 0; --k) {
+    const double2 t = tau[k];
+    if (t.x == 0.0 && t.y == 0.0) continue;
+    if (tid < Kp) {  // f_j = tau (v^H s_j)
       double sx = 0.0, sy = 0.0;
-      for (int r = k + 1 + lane; r < M; r += 32) {
-        const double2 c = cdotc(A[r * M + k], S[r * Kp + j]);
+      for (int r = k + 1; r < M; ++r) {
+        const double2 c = cdotc(A[r * lda + k], S[r * Kp + tid]);
         sx += c.x;
         sy += c.y;
       }
-      sx = warp_sum(sx);
-      sy = warp_sum(sy);
-      const double2 f = cmul(t, make_double2(sx, sy));
-      for (int r = k + 1 + lane; r < M; r += 32) S[r * Kp + j] = csub(S[r * Kp + j], cmul(A[r * M + k], f));
-      __syncwarp();
+      pw[tid] = cmul(t, make_double2(sx, sy));
     }
+    __syncthreads();
+    for (int i = tid; i < (M - k - 1) * Kp; i += nt) {
+      const int r = k + 1 + i / Kp, j = i % Kp;
+      S[r * Kp + j] = csub(S[r * Kp + j], cmul(A[r * lda + k], pw[j]));
+    }
+    __syncthreads();
   }
   __syncthreads();
 }
@@ -533,10 +556,10 @@ __global__ void k_lz_ritz(rsed_lanczos_t st, LzDims d, int check_every, int forc
     return;
   }
   double2* A = reinterpret_cast<double2*>(smem);
-  double2* Sv = A + kJacobiMax * kJacobiMax;                      // M x Kp eigenvectors
+  double2* Sv = A + kJacobiMax * (kJacobiMax + 1);                // M x Kp eigenvectors
   double* Z = reinterpret_cast<double*>(Sv + kJacobiMax * kKeepMax);  // M x Kp real scratch
-  __shared__ double2 tau[kJacobiMax];
-  __shared__ double dd[kJacobiMax], ee[kJacobiMax], red[8];
+  __shared__ double2 tau[kJacobiMax], vv[kJacobiMax], pw[kJacobiMax];
+  __shared__ double dd[kJacobiMax], ee[kJacobiMax], red[64];
   __shared__ double theta[kKeepMax];
   __shared__ int conv_flag;
   const int Kp = min(M, max(nev, K));
@@ -544,10 +567,10 @@ __global__ void k_lz_ritz(rsed_lanczos_t st, LzDims d, int check_every, int forc
   for (int i = threadIdx.x; i < M * M; i += blockDim.x) {
     const int r = i / M, c = i % M;
     const double2 a = P[(int64_t)r * d.pm + c], bt = P[(int64_t)c * d.pm + r];
-    A[i] = make_double2(0.5 * (a.x + bt.x), 0.5 * (a.y - bt.y));
+    A[r * (M + 1) + c] = make_double2(0.5 * (a.x + bt.x), 0.5 * (a.y - bt.y));
   }
   __syncthreads();
-  herm_lowest(A, M, Kp, theta, Sv, Z, tau, dd, ee, red);
+  herm_lowest(A, M, Kp, theta, Sv, Z, tau, dd, ee, red, vv, pw);
   double* rv = st.ritz_val + (int64_t)inst * d.pm;
   double2* rvec = reinterpret_cast<double2*>(st.ritz_vec) + (int64_t)inst * d.pm * d.pm;
   double* res = st.resid + (int64_t)inst * d.pm;
@@ -823,6 +846,508 @@ __global__ void __launch_bounds__(128) k_rr_resid(rsed_lanczos_t st, LzDims d) {
   if (threadIdx.x == 0) stt[S_RR] = 3;
 }
 
+// ---------------------------------------------------------------------------
+// Persistent form: one thread-block cluster per instance runs the whole
+// thick-restart loop in one launch.  CTA r of the cluster owns a contiguous
+// slice of the orbit rows; per iteration
+//   matvec (own rows, x gathered from every row) -> Gram partials of own rows
+//   -> cluster barrier -> CTA 0 sums the partials through distributed shared
+//   memory, factors, updates P -> cluster barrier -> every CTA reads C, R
+//   from CTA 0 and updates its rows -> (second pass likewise) -> at a full
+//   basis CTA 0 solves the projected eigenproblem and every CTA recombines
+//   its rows for the thick restart.
+// Control values live in CTA 0's shared memory and are read by all CTAs after
+// a cluster barrier, so every CTA takes the same branch and executes the same
+// number of barriers.  Waiting is only on hardware cluster barriers; the loop
+// is bounded by max_iter.
+constexpr int kPT = 512;          // threads per CTA
+constexpr int kHopLanes = 4;      // lanes sharing one row's hops in the matvec
+constexpr int kPHB = 4;           // hops whose loads are issued together
+constexpr int kPB = 4;            // largest block size of the persistent form
+constexpr int kPRows = kJacobiMax + kBMax;  // max rows of the Gram matrices
+
+struct PersistLayout {
+  size_t part, tot, c1, c2, r1, r2, sg, sloc, eigA, eigS, eigZ, total;
+};
+
+enum { C_NB = 0, C_ACTIVE, C_ITERS, C_RESTARTS, C_STATUS, C_OK, C_RESTART, C_NBOLD, C_NCONV, C_N };
+
+template <int PREC>
+__global__ void __launch_bounds__(kPT, 1)
+k_lz_persist(rsed_model_t md, rsed_sectors_t sc, rsed_lanczos_t st, LzDims d, rsed_apply::ApplySmemLayout alay,
+             PersistLayout pl, int max_iter) {
+  using XT = typename std::conditional<PREC == 64, double2, float2>::type;
+  cg::cluster_group cluster = cg::this_cluster();
+  const int CS = (int)cluster.num_blocks();
+  const int rank = (int)cluster.block_rank();
+  const int inst = blockIdx.x / CS;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = kPT >> 5;
+  extern __shared__ __align__(16) unsigned char smem[];
+  rsed_apply::ApplyView av = rsed_apply::stage_apply(md, sc, alay, smem);
+  double2* part = reinterpret_cast<double2*>(smem + pl.part);  // [kPRows][kBMax]
+  double2* tot = reinterpret_cast<double2*>(smem + pl.tot);
+  double2* C1 = reinterpret_cast<double2*>(smem + pl.c1);
+  double2* C2 = reinterpret_cast<double2*>(smem + pl.c2);
+  double2* R1 = reinterpret_cast<double2*>(smem + pl.r1);     // [kBMax][kBMax]
+  double2* R2 = reinterpret_cast<double2*>(smem + pl.r2);
+  double2* sG = reinterpret_cast<double2*>(smem + pl.sg);
+  double2* Sloc = reinterpret_cast<double2*>(smem + pl.sloc);  // [kJacobiMax][kKeepMax]
+  __shared__ int ctl[C_N];
+  __shared__ double2 tau[kJacobiMax], vv[kJacobiMax], pw[kJacobiMax];
+  __shared__ double dd[kJacobiMax], ee[kJacobiMax], red[64], theta[kKeepMax], resj[kKeepMax];
+
+  int* stt = st.state + inst * kStateInts;
+  const int b = st.inst_b[inst];
+  const int c0 = st.inst_col0[inst];
+  const int sector = av.csec[c0];
+  const int nev = st.nev, keep = st.keep_blocks, K = keep * b;
+  const int64_t slot = d.n_orb * d.ld;
+  const int64_t per = (d.n_orb + CS - 1) / CS;
+  const int64_t rb = (int64_t)rank * per, re = min(rb + per, d.n_orb);
+  double2* V = reinterpret_cast<double2*>(st.V);
+  double2* W = reinterpret_cast<double2*>(st.W);
+  double2* X = V + (int64_t)(d.n_slots + 1) * slot;
+  const XT* xin = (PREC == 64) ? reinterpret_cast<const XT*>(X) : reinterpret_cast<const XT*>(st.Xf);
+  double2* P = reinterpret_cast<double2*>(st.P) + (int64_t)inst * d.pm * d.pm;
+  const int kp1 = md.n_filled + 1;
+  const bool bad_block = (b < 1 || b > kPB || (32 % b) != 0);
+
+  if (rank == 0 && tid == 0) {
+    ctl[C_NB] = stt[S_NB];
+    ctl[C_ACTIVE] = stt[S_ACTIVE] && !bad_block;
+    ctl[C_ITERS] = stt[S_ITERS];
+    ctl[C_RESTARTS] = stt[S_RESTARTS];
+    ctl[C_STATUS] = bad_block ? RSED_EINVAL : stt[S_STATUS];
+    ctl[C_OK] = 1;
+    ctl[C_RESTART] = 0;
+    ctl[C_NBOLD] = 0;
+    ctl[C_NCONV] = stt[S_NCONV];
+  }
+  int* ctl0 = cluster.map_shared_rank(ctl, 0);
+
+  for (int it = 0; it < max_iter; ++it) {
+    cluster.sync();  // (A) X complete, control stable
+    const int nb = ctl0[C_NB];
+    if (!ctl0[C_ACTIVE]) break;
+    // C_RESTART is next read after barrier (C) of this iteration's second pass
+    if (rank == 0 && tid == 0) ctl[C_RESTART] = 0;
+    // ---- matvec: W = H^dagger X on own rows (own columns) ----
+    {
+      const int ng = kPT / kHopLanes;
+      const int hl = tid % kHopLanes;
+      for (int64_t r0 = rb; r0 < re; r0 += ng) {
+        const int64_t row = r0 + tid / kHopLanes;
+        double2 acc[kPB];
+#pragma unroll
+        for (int q = 0; q < kPB; ++q) acc[q] = make_double2(0.0, 0.0);
+        bool on = false;
+        if (row < re) {
+          const uint64_t memr = sc.member[row];
+          on = (memr >> sector) & 1ull;
+          if (on) {
+            const uint64_t m = md.repr_masks[row];
+            const double sr = sc.sqrt_stab[row];
+            if (hl == 0) {
+              const double2 hd = reinterpret_cast<const double2*>(md.hdiag)[row];
+              for (int q = 0; q < b; ++q) {
+                const XT xv = xin[row * d.ld + c0 + q];
+                const double2 xx = make_double2((double)xv.x, (double)xv.y);
+                acc[q] = cadd(acc[q], make_double2(hd.x * xx.x + hd.y * xx.y, hd.x * xx.y - hd.y * xx.x));
+              }
+            }
+            int hop = 0;
+            int bt[kPHB];
+            int64_t bidx[kPHB];
+            int nh = 0;
+            auto process = [&](int cnt) {
+              RsedEntry e[kPHB];
+#pragma unroll
+              for (int h = 0; h < kPHB; ++h)
+                if (h < cnt) e[h] = rsed_apply::load_entry(reinterpret_cast<const RsedEntry*>(md.table), bidx[h]);
+              uint64_t mc[kPHB];
+              double sq[kPHB];
+              XT xv[kPHB][kPB];
+#pragma unroll
+              for (int h = 0; h < kPHB; ++h) {
+                if (h < cnt) {
+                  const int64_t c = e[h].rep;
+                  mc[h] = __ldg(sc.member + c);
+                  sq[h] = __ldg(sc.sqrt_stab + c);
+#pragma unroll
+                  for (int q = 0; q < kPB; ++q)
+                    if (q < b) xv[h][q] = xin[c * d.ld + c0 + q];
+                }
+              }
+#pragma unroll
+              for (int h = 0; h < kPHB; ++h) {
+                if (h >= cnt || !((mc[h] >> sector) & 1ull)) continue;
+                const int t = bt[h];
+                double2 ta = cmul(av.tamp[t], make_double2(e[h].re, e[h].im));
+                if (md.fermionic && (__popcll(m & av.tjw[t]) & 1)) {
+                  ta.x = -ta.x;
+                  ta.y = -ta.y;
+                }
+                const double ratio = sq[h] / sr;
+                const double2 w =
+                    cmul(make_double2(ta.x * ratio, -ta.y * ratio), av.chi[sector * md.n_group + e[h].g]);
+#pragma unroll
+                for (int q = 0; q < kPB; ++q) {
+                  if (q < b) {
+                    const double2 xx = make_double2((double)xv[h][q].x, (double)xv[h][q].y);
+                    acc[q] = cadd(acc[q], cmul(w, xx));
+                  }
+                }
+              }
+            };
+            uint64_t occ = m;
+            while (occ) {
+              const int i = __ffsll((long long)occ) - 1;
+              occ &= occ - 1;
+              const int t1 = av.tbeg[i + 1];
+              for (int t = av.tbeg[i]; t < t1; ++t) {
+                const int jj = av.tto[t];
+                if ((m >> jj) & 1ull) continue;
+                if ((hop++ % kHopLanes) != hl) continue;
+                bt[nh] = t;
+                bidx[nh] = rsed_rank(m ^ (1ull << i) ^ (1ull << jj), av.binom, kp1);
+                if (++nh == kPHB) {
+                  process(kPHB);
+                  nh = 0;
+                }
+              }
+            }
+            if (nh) process(nh);
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < kPB; ++q) {
+          for (int o = 1; o < kHopLanes; o <<= 1) {
+            acc[q].x += __shfl_xor_sync(0xffffffffu, acc[q].x, o);
+            acc[q].y += __shfl_xor_sync(0xffffffffu, acc[q].y, o);
+          }
+        }
+        if (row < re && hl == 0)
+          for (int q = 0; q < b; ++q) W[row * d.ld + c0 + q] = on ? acc[q] : make_double2(0.0, 0.0);
+      }
+    }
+    __syncthreads();
+    // ---- two Gram-Schmidt passes ----
+    for (int pass = 1; pass <= 2; ++pass) {
+      const int npairs = (nb + 1) * b;
+      const int rl_n = 32 / b;           // row lanes per pair in a warp
+      const int q = lane % b, rl = lane / b;
+      for (int pair = warp; pair < npairs; pair += nwarp) {
+        const int sl = pair / b, p = pair % b;
+        const double2* Y = (sl < nb) ? V + sl * slot : W;
+        double2 a = make_double2(0.0, 0.0);
+        for (int64_t row = rb + rl; row < re; row += 4 * rl_n) {
+          double2 yv[4], wv[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const int64_t r = row + u * rl_n;
+            yv[u] = (r < re) ? Y[r * d.ld + c0 + p] : make_double2(0.0, 0.0);
+            wv[u] = (r < re) ? W[r * d.ld + c0 + q] : make_double2(0.0, 0.0);
+          }
+#pragma unroll
+          for (int u = 0; u < 4; ++u) a = cadd(a, cdotc(yv[u], wv[u]));
+        }
+        for (int o = b; o < 32; o <<= 1) {
+          a.x += __shfl_xor_sync(0xffffffffu, a.x, o);
+          a.y += __shfl_xor_sync(0xffffffffu, a.y, o);
+        }
+        if (rl == 0) part[pair * kBMax + q] = a;
+      }
+      cluster.sync();  // (B) partials of every CTA ready
+      if (rank == 0) {
+        // sum partials over the cluster in rank order
+        for (int e = tid; e < npairs * b; e += kPT) {
+          const int pr = e / b, qq = e % b;
+          double2 a = make_double2(0.0, 0.0);
+          for (int r = 0; r < CS; ++r) a = cadd(a, cluster.map_shared_rank(part, r)[pr * kBMax + qq]);
+          tot[pr * kBMax + qq] = a;
+        }
+        __syncthreads();
+        // G' = G - C^H C
+        for (int e = tid; e < b * b; e += kPT) {
+          const int pp = e / b, qq = e % b;
+          double2 g = tot[(nb * b + pp) * kBMax + qq];
+          for (int r = 0; r < nb * b; ++r) g = csub(g, cdotc(tot[r * kBMax + pp], tot[r * kBMax + qq]));
+          sG[pp * kBMax + qq] = g;
+        }
+        __syncthreads();
+        double2* Rx = (pass == 1) ? R1 : R2;
+        double2* Cx = (pass == 1) ? C1 : C2;
+        if (tid == 0) {
+          double gmax = 0.0;
+          for (int pp = 0; pp < b; ++pp) gmax = fmax(gmax, tot[(nb * b + pp) * kBMax + pp].x);
+          for (int i = 0; i < kBMax * kBMax; ++i) Rx[i] = make_double2(0.0, 0.0);
+          bool ok = gmax > 0.0;
+          for (int j = 0; j < b && ok; ++j) {
+            double sdg = sG[j * kBMax + j].x;
+            for (int k = 0; k < j; ++k) sdg -= Rx[k * kBMax + j].x * Rx[k * kBMax + j].x + Rx[k * kBMax + j].y * Rx[k * kBMax + j].y;
+            if (!(sdg > 1e-26 * gmax)) {
+              ok = false;
+              break;
+            }
+            const double rjj = sqrt(sdg);
+            Rx[j * kBMax + j] = make_double2(rjj, 0.0);
+            for (int qq = j + 1; qq < b; ++qq) {
+              double2 tt = sG[j * kBMax + qq];
+              for (int k = 0; k < j; ++k) tt = csub(tt, cdotc(Rx[k * kBMax + j], Rx[k * kBMax + qq]));
+              Rx[j * kBMax + qq] = make_double2(tt.x / rjj, tt.y / rjj);
+            }
+          }
+          ctl[C_OK] = ok;
+          if (!ok) {
+            ctl[C_STATUS] = RSED_EBREAKDOWN;
+            ctl[C_ACTIVE] = 0;
+            ctl[C_RESTART] = 0;
+          }
+        }
+        for (int e = tid; e < nb * b * kBMax; e += kPT) Cx[e] = tot[e];
+        __syncthreads();
+        if (pass == 2 && ctl[C_OK]) {
+          // projected matrix: column block cb = nb-1 gets C1 + C2 R1, row block nb gets R2 R1
+          const int cb = nb - 1;
+          if (nb >= 1) {
+            for (int e = tid; e < nb * b * b; e += kPT) {
+              const int r = e / b, qq = e % b;
+              double2 v = C1[r * kBMax + qq];
+              for (int k = 0; k < b; ++k) v = cadd(v, cmul(C2[r * kBMax + k], R1[k * kBMax + qq]));
+              P[(int64_t)r * d.pm + cb * b + qq] = v;
+            }
+            for (int e = tid; e < b * b; e += kPT) {
+              const int pp = e / b, qq = e % b;
+              double2 v = make_double2(0.0, 0.0);
+              for (int k = 0; k < b; ++k) v = cadd(v, cmul(R2[pp * kBMax + k], R1[k * kBMax + qq]));
+              P[(int64_t)(nb * b + pp) * d.pm + cb * b + qq] = v;
+            }
+          }
+          __syncthreads();
+          const int nbn = nb + 1;
+          const bool full = nbn >= d.n_slots + 1;
+          if (tid == 0) {
+            ctl[C_NB] = nbn;
+            ctl[C_NBOLD] = nb;
+            ctl[C_ITERS] += 1;
+            ctl[C_RESTART] = 0;
+          }
+          if (full) {
+            // projected eigenproblem (blocks 0..nb-1), restart bookkeeping
+            const int M = nb * b;
+            const int Kp = min(M, max(nev, K));
+            double2* A = reinterpret_cast<double2*>(smem + pl.eigA);
+            double2* Sv = reinterpret_cast<double2*>(smem + pl.eigS);
+            double* Zs = reinterpret_cast<double*>(smem + pl.eigZ);
+            for (int i = tid; i < M * M; i += kPT) {
+              const int r = i / M, c = i % M;
+              const double2 a = P[(int64_t)r * d.pm + c], bt = P[(int64_t)c * d.pm + r];
+              A[r * (M + 1) + c] = make_double2(0.5 * (a.x + bt.x), 0.5 * (a.y - bt.y));
+            }
+            __syncthreads();
+            herm_lowest(A, M, Kp, theta, Sv, Zs, tau, dd, ee, red, vv, pw);
+            double* rv = st.ritz_val + (int64_t)inst * d.pm;
+            double2* rvec = reinterpret_cast<double2*>(st.ritz_vec) + (int64_t)inst * d.pm * d.pm;
+            double* res = st.resid + (int64_t)inst * d.pm;
+            for (int i = tid; i < M * Kp; i += kPT) {
+              const int r = i / Kp, j = i % Kp;
+              rvec[(int64_t)r * d.pm + j] = Sv[r * Kp + j];
+            }
+            for (int j = tid; j < Kp; j += kPT) {
+              rv[j] = theta[j];
+              double a2 = 0.0;
+              for (int qq = 0; qq < b; ++qq) {
+                double2 v = make_double2(0.0, 0.0);
+                for (int pp = 0; pp < b; ++pp)
+                  v = cadd(v, cmul(P[(int64_t)(nb * b + qq) * d.pm + (nb - 1) * b + pp], Sv[((nb - 1) * b + pp) * Kp + j]));
+                a2 += v.x * v.x + v.y * v.y;
+              }
+              resj[j] = sqrt(a2);
+              res[j] = resj[j];
+            }
+            __syncthreads();
+            if (tid == 0) {
+              int nconv = 0;
+              for (int j = 0; j < nev; ++j) {
+                if (resj[j] <= st.tol * fmax(1.0, fabs(theta[j]))) ++nconv;
+                else break;
+              }
+              ctl[C_NCONV] = nconv;
+              if (nconv >= nev) {
+                ctl[C_STATUS] = 1;
+                ctl[C_ACTIVE] = 0;
+              } else if (++ctl[C_RESTARTS] > st.max_restarts) {
+                ctl[C_STATUS] = RSED_ENOTCONV;
+                ctl[C_ACTIVE] = 0;
+              } else {
+                ctl[C_RESTART] = 1;
+              }
+            }
+            __syncthreads();
+            if (ctl[C_RESTART]) {
+              // coupling rows (from the old P) then the new P: diag(theta) + coupling
+              for (int i = tid; i < b * K; i += kPT) {
+                const int qq = i / K, j = i % K;
+                double2 v = make_double2(0.0, 0.0);
+                for (int pp = 0; pp < b; ++pp)
+                  v = cadd(v, cmul(P[(int64_t)(nb * b + qq) * d.pm + (nb - 1) * b + pp], Sv[((nb - 1) * b + pp) * Kp + j]));
+                A[i] = v;  // staged in A (free now)
+              }
+              __syncthreads();
+              for (int i = tid; i < (nbn * b) * (nbn * b); i += kPT) {
+                const int r = i / (nbn * b), c = i % (nbn * b);
+                P[(int64_t)r * d.pm + c] = make_double2(0.0, 0.0);
+              }
+              __syncthreads();
+              for (int j = tid; j < K; j += kPT) P[(int64_t)j * d.pm + j] = make_double2(theta[j], 0.0);
+              for (int i = tid; i < b * K; i += kPT) {
+                const int qq = i / K, j = i % K;
+                P[(int64_t)(K + qq) * d.pm + j] = A[i];
+              }
+              for (int i = tid; i < M * K; i += kPT) {
+                const int r = i / K, j = i % K;
+                Sloc[r * kKeepMax + j] = Sv[r * Kp + j];
+              }
+              if (tid == 0) ctl[C_NB] = keep + 1;
+            }
+          }
+        }
+        __syncthreads();
+      }
+      cluster.sync();  // (C) C, R (and restart data) ready in CTA 0
+      if (!cluster.map_shared_rank(ctl, 0)[C_OK]) break;
+      // copy this pass's coefficients from CTA 0
+      {
+        const double2* Cs = cluster.map_shared_rank(pass == 1 ? C1 : C2, 0);
+        const double2* Rs = cluster.map_shared_rank(pass == 1 ? R1 : R2, 0);
+        if (rank != 0) {
+          double2* Cd = (pass == 1) ? C1 : C2;
+          double2* Rd = (pass == 1) ? R1 : R2;
+          for (int e = tid; e < nb * b * kBMax; e += kPT) Cd[e] = Cs[e];
+          for (int e = tid; e < kBMax * kBMax; e += kPT) Rd[e] = Rs[e];
+        }
+        __syncthreads();
+      }
+      // ---- update own rows: W <- (W - V C) R^-1 (pass 1) or new block (pass 2) ----
+      {
+        const double2* Cx = (pass == 1) ? C1 : C2;
+        const double2* Rx = (pass == 1) ? R1 : R2;
+        const int rows_per_iter = kPT / b;
+        const int qq = tid % b;
+        for (int64_t r0 = rb; r0 < re; r0 += rows_per_iter) {
+          const int64_t row = r0 + tid / b;
+          double2 w = make_double2(0.0, 0.0);
+          if (row < re) {
+            w = W[row * d.ld + c0 + qq];
+            for (int sl = 0; sl < nb; sl += 4) {
+              double2 vr[4][kPB];
+#pragma unroll
+              for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int pp = 0; pp < kPB; ++pp)
+                  vr[u][pp] = (sl + u < nb && pp < b) ? V[(int64_t)(sl + u) * slot + row * d.ld + c0 + pp]
+                                                     : make_double2(0.0, 0.0);
+#pragma unroll
+              for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int pp = 0; pp < kPB; ++pp)
+                  if (sl + u < nb && pp < b) w = csub(w, cmul(vr[u][pp], Cx[((sl + u) * b + pp) * kBMax + qq]));
+            }
+          }
+          // triangular solve across the b lanes of this row (lanes base..base+b-1)
+          const int base = lane - (lane % b);
+          double2 acc = make_double2(0.0, 0.0), xq = make_double2(0.0, 0.0);
+          for (int pp = 0; pp < b; ++pp) {
+            if (qq == pp) {
+              const double rr = Rx[pp * kBMax + pp].x;
+              xq = make_double2((w.x - acc.x) / rr, (w.y - acc.y) / rr);
+            }
+            const double xpx = __shfl_sync(0xffffffffu, xq.x, base + pp);
+            const double xpy = __shfl_sync(0xffffffffu, xq.y, base + pp);
+            if (qq > pp) acc = cadd(acc, cmul(make_double2(xpx, xpy), Rx[pp * kBMax + qq]));
+          }
+          if (row < re) {
+            if (pass == 1) {
+              W[row * d.ld + c0 + qq] = xq;
+            } else {
+              V[(int64_t)nb * slot + row * d.ld + c0 + qq] = xq;
+              X[row * d.ld + c0 + qq] = xq;
+              if (st.Xf) reinterpret_cast<float2*>(st.Xf)[row * d.ld + c0 + qq] = make_float2((float)xq.x, (float)xq.y);
+            }
+          }
+        }
+        __syncthreads();
+      }
+    }
+    // ---- thick restart of own rows ----
+    if (cluster.map_shared_rank(ctl, 0)[C_RESTART]) {
+      const int nb_old = cluster.map_shared_rank(ctl, 0)[C_NBOLD];  // blocks 0..nb_old-1 + residual nb_old
+      const int M = nb_old * b;
+      if (rank != 0) {
+        const double2* Ss = cluster.map_shared_rank(Sloc, 0);
+        for (int e = tid; e < M * kKeepMax; e += kPT) Sloc[e] = Ss[e];
+      }
+      __syncthreads();
+      const int rows_per_iter = kPT / b;
+      const int pp = tid % b;
+      for (int64_t r0 = rb; r0 < re; r0 += rows_per_iter) {
+        const int64_t row = r0 + tid / b;
+        double2 acc[kKeepMax];
+        for (int t = 0; t < kKeepMax; ++t) acc[t] = make_double2(0.0, 0.0);
+        if (row < re) {
+          for (int l0 = 0; l0 < M; l0 += 8) {
+            double2 v[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+              v[u] = (l0 + u < M) ? V[(int64_t)((l0 + u) / b) * slot + row * d.ld + c0 + ((l0 + u) % b)]
+                                  : make_double2(0.0, 0.0);
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+              if (l0 + u < M)
+                for (int t = 0; t < keep; ++t)
+                  acc[t] = cadd(acc[t], cmul(v[u], Sloc[(l0 + u) * kKeepMax + t * b + pp]));
+          }
+        }
+        __syncthreads();  // every read of the old slots of these rows is done
+        if (row < re) {
+          for (int t = 0; t < keep; ++t) V[(int64_t)t * slot + row * d.ld + c0 + pp] = acc[t];
+          V[(int64_t)keep * slot + row * d.ld + c0 + pp] = V[(int64_t)nb_old * slot + row * d.ld + c0 + pp];
+        }
+        __syncthreads();
+      }
+    }
+  }
+  cluster.sync();  // no CTA leaves while another may still read its shared memory
+  if (rank == 0 && tid == 0) {
+    stt[S_NB] = ctl[C_NB];
+    stt[S_ACTIVE] = ctl[C_ACTIVE];
+    stt[S_ITERS] = ctl[C_ITERS];
+    stt[S_RESTARTS] = ctl[C_RESTARTS];
+    stt[S_STATUS] = ctl[C_ACTIVE] ? 0 : ctl[C_STATUS];
+    stt[S_NCONV] = ctl[C_NCONV];
+    stt[S_RESTART_NB] = 0;
+  }
+}
+
+PersistLayout persist_layout(size_t base) {
+  PersistLayout l{};
+  size_t off = align_up(base, 16);
+  const size_t g = sizeof(double2) * kPRows * kBMax;
+  l.part = off; off += g;
+  l.tot = off; off += g;
+  l.c1 = off; off += g;
+  l.c2 = off; off += g;
+  l.r1 = off; off += sizeof(double2) * kBMax * kBMax;
+  l.r2 = off; off += sizeof(double2) * kBMax * kBMax;
+  l.sg = off; off += sizeof(double2) * kBMax * kBMax;
+  l.sloc = off; off += sizeof(double2) * kJacobiMax * kKeepMax;
+  l.eigA = off; off += sizeof(double2) * kJacobiMax * (kJacobiMax + 1);
+  l.eigS = off; off += sizeof(double2) * kJacobiMax * kKeepMax;
+  l.eigZ = off; off += sizeof(double) * kJacobiMax * kKeepMax;
+  l.total = align_up(off, 16);
+  return l;
+}
+
 LzDims make_dims(const rsed_model_t* md, const rsed_sectors_t* sc, const rsed_lanczos_t* st) {
   LzDims d;
   d.n_orb = md->n_orbits;
@@ -917,7 +1442,7 @@ static int set_ritz_smem() {
   static bool done = false;
   if (!done) {
     RSED_TRY_CUDA(cudaFuncSetAttribute(k_lz_ritz, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)(2 * sizeof(double2) * kJacobiMax * kJacobiMax)));
+                                       (int)kRitzSmem));
     done = true;
   }
   return RSED_OK;
@@ -960,7 +1485,7 @@ extern "C" int rsed_lanczos_iterate(const rsed_model_t* md, const rsed_sectors_t
     if (rc) return rc;
     rc = launch_pass(*st, d, 2, stream);
     if (rc) return rc;
-    k_lz_ritz<<<d.n_inst, 256, 2 * sizeof(double2) * kJacobiMax * kJacobiMax, stream>>>(*st, d, check_every, 0, 0);
+    k_lz_ritz<<<d.n_inst, 256, kRitzSmem, stream>>>(*st, d, check_every, 0, 0);
     RSED_CHECK_LAUNCH();
     const int64_t tot = d.n_orb * d.n_inst;
     k_lz_restart<<<(unsigned)((tot + 255) / 256), 256, 0, stream>>>(*st, d);
@@ -993,10 +1518,49 @@ extern "C" int rsed_lanczos_rayleigh_ritz(const rsed_model_t* md, const rsed_sec
   dim3 g(d.n_chunks, d.n_inst);
   k_rr_gram<<<g, 128, 0, stream>>>(*st, d);
   RSED_CHECK_LAUNCH();
-  k_lz_ritz<<<d.n_inst, 256, 2 * sizeof(double2) * kJacobiMax * kJacobiMax, stream>>>(*st, d, 1, 1, 1);
+  k_lz_ritz<<<d.n_inst, 256, kRitzSmem, stream>>>(*st, d, 1, 1, 1);
   RSED_CHECK_LAUNCH();
   k_rr_resid<<<g, 128, 0, stream>>>(*st, d);
   RSED_CHECK_LAUNCH();
+  return RSED_OK;
+}
+
+extern "C" int rsed_lanczos_persistent(const rsed_model_t* md, const rsed_sectors_t* sc, rsed_lanczos_t* st,
+                                       int32_t cluster_size, int32_t max_iter, void* stream_) {
+  int rc = check_lz(md, sc, st);
+  if (rc) return rc;
+  RSED_REQUIRE(cluster_size >= 1 && cluster_size <= 8, RSED_ERANGE, "cluster size %d outside [1, 8]",
+               cluster_size);
+  RSED_REQUIRE(max_iter >= 1, RSED_EINVAL, "max_iter must be >= 1");
+  RSED_REQUIRE(md->n_terms >= 0, RSED_EINVAL, "bad model");
+  const LzDims d = make_dims(md, sc, st);
+  RSED_REQUIRE(d.n_slots * st->bmax <= kJacobiMax, RSED_ERANGE, "n_slots*b > %d", kJacobiMax);
+  RSED_REQUIRE(st->bmax <= kPB, RSED_ERANGE, "the persistent form takes blocks of at most %d", kPB);
+  rsed_apply::ApplySmemLayout alay = rsed_apply::apply_layout(*md, *sc);
+  PersistLayout pl = persist_layout(alay.total);
+  RSED_REQUIRE(pl.total <= 220 * 1024, RSED_ERANGE, "persistent kernel needs %zu B of shared memory",
+               pl.total);
+  cudaStream_t stream = as_stream(stream_);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(st->n_inst * cluster_size), 1, 1);
+  cfg.blockDim = dim3(kPT, 1, 1);
+  cfg.dynamicSmemBytes = pl.total;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)cluster_size;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if (st->precision == 64) {
+    RSED_TRY_CUDA(cudaFuncSetAttribute(k_lz_persist<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.total));
+    RSED_TRY_CUDA(cudaLaunchKernelEx(&cfg, k_lz_persist<64>, *md, *sc, *st, d, alay, pl, (int)max_iter));
+  } else {
+    RSED_TRY_CUDA(cudaFuncSetAttribute(k_lz_persist<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.total));
+    RSED_TRY_CUDA(cudaLaunchKernelEx(&cfg, k_lz_persist<32>, *md, *sc, *st, d, alay, pl, (int)max_iter));
+  }
+  rsed_count_launch();
   return RSED_OK;
 }
 

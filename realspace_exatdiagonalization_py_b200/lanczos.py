@@ -226,6 +226,19 @@ class LanczosBatch:
             raise _lib.RsedError(code, f"instances {bad} did not converge (state {st[bad[0]].tolist()})")
         return st
 
+    def run_persistent(self, cluster_size: int = 4, max_iter: int = 4000, stream=None) -> np.ndarray:
+        """Whole solve in one launch (one thread-block cluster per instance);
+        raises if an instance did not converge."""
+        _lib.check(_lib.lib().rsed_lanczos_persistent(
+            ctypes.byref(self.model.c), ctypes.byref(self.sc), ctypes.byref(self.c), int(cluster_size),
+            int(max_iter), _lib.stream_ptr(stream)))
+        st = self.status()
+        bad = [i for i in range(self.n_inst) if st[i, S_STATUS] != 1]
+        if bad:
+            code = int(st[bad[0], S_STATUS]) or _lib.RSED_ENOTCONV
+            raise _lib.RsedError(code, f"instances {bad} did not converge (state {st[bad[0]].tolist()})")
+        return st
+
     def capture(self, n_iter: int):
         """CUDA graph of ``n_iter`` iterations (replayed by ``run(graph=True)``).
 

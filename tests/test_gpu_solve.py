@@ -230,3 +230,25 @@ def test_reference_energy_alignment():
     ed.ed_scan(data, nev=5, mode="matrix", scanned_sectors=list(JULIA_REF_FERMION_34))
     for k, ref in JULIA_REF_FERMION_34.items():
         np.testing.assert_allclose(_sector_vals(data, k)[:5], ref, atol=1e-9)
+
+
+@pytest.mark.parametrize("cluster", [1, 2, 8])
+def test_persistent_cluster_solve(golden, cluster):
+    """The one-launch solve (one thread-block cluster per sector) agrees with
+    the oracle for every cluster size, and is deterministic."""
+    import realspace_exatdiagonalization_py_b200 as ed
+    from realspace_exatdiagonalization_py_b200.batched import BatchedSectorSolver
+
+    g = golden("checkerboard24")
+    data = ed_data_for("checkerboard24", g)
+    dm, sset = data._device()
+    sectors = [int(s) for s in g["eig_sectors"]]
+    for prec in (64, 32):
+        sol = BatchedSectorSolver(dm, sset, sectors, 6, precision=prec,
+                                  params=ed.LanczosParams(precision=prec), persistent=cluster)
+        v1, _ = sol.solve(None, vectors=False)
+        v2, _ = sol.solve(None, vectors=False)
+        np.testing.assert_array_equal(v1, v2)
+        for i, s in enumerate(sectors):
+            np.testing.assert_allclose(v1[i], g["eig_vals"][list(g["eig_sectors"]).index(s)][:6], atol=1e-10,
+                                       rtol=0)
