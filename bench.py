@@ -197,58 +197,74 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def count_hops(catalog, model) -> int:
-    """Hops the apply kernel evaluates per row sweep (gate passes from every
-    representative), from the catalog's representative masks."""
+def sector_matvec_bytes(dm, sset, col_sector, x_bytes):
+    """Algorithmic bytes of one apply over the given columns: per column
+    (one sector matvec) D_s * (8 + 2 s) + H_s * 16 -- the representative
+    mask, x read and y write per row and one 16-B table entry per hop of the
+    sector's rows.  H_s comes from the projection table's row lengths."""
     import torch
 
-    m = catalog.repr_masks.cpu().numpy().astype(np.uint64)
-    h = 0
-    pairs = {(i - 1, j - 1) for (i, j, _) in model.bilinear_terms}
-    for (i, j) in pairs:
-        ok = ((m >> np.uint64(i)) & np.uint64(1)).astype(bool) & ~((m >> np.uint64(j)) & np.uint64(1)).astype(bool)
-        h += int(ok.sum())
-    del torch
-    return h
+    rp = dm.proj["rowptr"]
+    hops_row = (rp[1:] - rp[:-1]).to(torch.float64)
+    mem = sset.member
+    total = 0.0
+    for s in col_sector.tolist():
+        on = ((mem >> int(s)) & 1).to(torch.bool)
+        d = int(on.sum().item())
+        h = float(hops_row[on].sum().item())
+        total += d * (8 + 2 * x_bytes) + h * 16
+    return total
+
+
+def _zero_outside(X, sset, col_sector):
+    import torch
+
+    for c, s in enumerate(col_sector.tolist()):
+        X[((sset.member >> int(s)) & 1) == 0, c] = 0
+    X[:, len(col_sector):] = 0
+    return X
+
+
+def time_apply(dm, sset, cs, X, Y, prec, variant, n_launch, warm=3):
+    """Average time of one apply (CUDA events on the current stream)."""
+    import torch
+
+    for _ in range(warm):
+        dm.apply_block(sset, cs, X, Y, precision=prec, variant=variant)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(n_launch):
+        dm.apply_block(sset, cs, X, Y, precision=prec, variant=variant)
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / n_launch * 1e-3
 
 
 def apply_roofline(ed, data, sset, solver, peak_gbs, n_launch=200):
-    """Average duration of the batch's matvec launch (the FP32 apply over all
-    columns), timed with CUDA events on the launching stream, and its
-    algorithmic bytes per launch."""
+    """The batch's FP32 matvec (all columns of the bench workload) timed with
+    CUDA events, against the per-sector-matvec algorithmic bytes."""
     import torch
 
     dm, _ = data._device()
     b = solver.batch
     n_orb = data.orbit_catalog.n_orbits
-    X = torch.randn((n_orb, b.ld), dtype=torch.complex64, device="cuda")
+    X = _zero_outside(torch.randn((n_orb, b.ld), dtype=torch.complex64, device="cuda"), sset, b.col_sector)
     Y = torch.empty((n_orb, b.ld), dtype=torch.complex128, device="cuda")
-    for _ in range(5):
-        dm.apply_block(sset, b.col_sector, X, Y, precision=32)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(n_launch):
-        dm.apply_block(sset, b.col_sector, X, Y, precision=32)
-    e1.record()
-    torch.cuda.synchronize()
-    t = e0.elapsed_time(e1) / n_launch * 1e-3
-    hops = count_hops(data.orbit_catalog, data.second_quantized_model)
-    ncols = b.n_cols
-    # algorithmic bytes: per row mask 8 + member 8 + sqrt|Stab| 8 + diag 16,
-    # per row and column x 8 (complex64) in, y 16 (complex128) out,
-    # per hop one 16-B table entry
-    alg = n_orb * (8 + 8 + 8 + 16) + n_orb * ncols * (8 + 16) + hops * 16
+    t = time_apply(dm, sset, b.col_sector, X, Y, 32, 0, n_launch, warm=5)
+    alg = sector_matvec_bytes(dm, sset, b.col_sector, 8)
     ach = alg / t / 1e9
-    return {"kernel": "k_apply<LPR,CPL,32> (rsed_apply_h)", "bound": "hbm", "achieved": ach,
-            "peak": peak_gbs, "unit": "GB/s", "frac": ach / peak_gbs, "traffic": None,
-            "alg_bytes_per_launch": alg, "avg_launch_us": t * 1e6, "hops_per_launch": hops,
-            "columns": ncols}
+    return {"kernel": "k_proj_spmv<32,*> (rsed_apply_h, projection table)", "bound": "hbm",
+            "achieved": ach, "peak": peak_gbs, "unit": "GB/s", "frac": ach / peak_gbs, "traffic": None,
+            "alg_bytes_per_launch": alg, "avg_launch_us": t * 1e6, "hops_per_launch": dm.proj["n_hops"],
+            "columns": b.n_cols, "note": "latency-bound size (892 orbits): see matvec_at_scale"}
 
 
-def matvec_at_scale(ed, models, peak_gbs, n_launch=20):
-    """HBM-bound matvec at the 32-site Haldane size (10.5M states, table
-    168 MB > L2): all 16 sectors x 2 block columns in one launch, FP64 and FP32."""
+def matvec_at_scale(ed, models, peak_gbs, n_launch=20, precisions=(32, 64), per_sector=4, otf=True):
+    """The HBM-bound matvec at the 32-site Haldane size (10.5M states, 657,756
+    orbits, table 168 MB > L2): 16 sectors x 4 block columns, the shape of one
+    batched Lanczos step, through the projection table (and, for comparison,
+    the on-the-fly apply)."""
     import torch
 
     model, nf = models.config_model("haldane32")
@@ -258,30 +274,42 @@ def matvec_at_scale(ed, models, peak_gbs, n_launch=20):
     torch.cuda.synchronize()
     t_cat = time.perf_counter() - t0
     dm, sset = data._device()
+    t0 = time.perf_counter()
+    dm.build_projection(sset.sqrt_stab, precisions=precisions)
+    torch.cuda.synchronize()
+    t_proj = time.perf_counter() - t0
     n_orb = data.orbit_catalog.n_orbits
     ns = len(data.irrep_list)
-    ncol = 2 * ns
-    ld = ncol
-    cs = torch.arange(ns, dtype=torch.int32, device="cuda").repeat_interleave(2)
-    hops = count_hops(data.orbit_catalog, model)
-    out = {"workload": "haldane32: 32 sites, 8 bosons, C=10,518,300, |G|=16, 16 sectors x 2 columns",
-           "n_orbits": n_orb, "hops_per_launch": hops, "catalog_build_s": t_cat}
-    for prec, dt, xb in ((64, torch.complex128, 16), (32, torch.complex64, 8)):
-        X = torch.randn((n_orb, ld), dtype=dt, device="cuda")
+    ncol = per_sector * ns
+    ld = ncol + (ncol & 1)
+    cs = torch.arange(ns, dtype=torch.int32, device="cuda").repeat_interleave(per_sector)
+    nh = dm.proj["n_hops"]
+    out = {"workload": f"haldane32: 32 sites, 8 bosons, C=10,518,300, |G|=16, {ns} sectors x {per_sector} columns",
+           "n_orbits": n_orb, "hops_per_apply": nh, "catalog_build_s": t_cat, "projection_build_s": t_proj,
+           "projection_bytes": dm.projection_bytes(), "l2": "x > L2 for every precision (no flush needed)"}
+    for prec in precisions:
+        dt, xb = (torch.complex128, 16) if prec == 64 else (torch.complex64, 8)
+        X = _zero_outside(torch.randn((n_orb, ld), dtype=dt, device="cuda"), sset, cs)
         Y = torch.empty((n_orb, ld), dtype=torch.complex128, device="cuda")
-        for _ in range(3):
-            dm.apply_block(sset, cs, X, Y, precision=prec)
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for _ in range(n_launch):
-            dm.apply_block(sset, cs, X, Y, precision=prec)
-        e1.record()
-        torch.cuda.synchronize()
-        t = e0.elapsed_time(e1) / n_launch * 1e-3
-        alg = n_orb * (8 + 8 + 8 + 16) + n_orb * ncol * (xb + 16) + hops * 16
-        out[f"fp{prec}"] = {"avg_launch_ms": t * 1e3, "alg_GBs": alg / t / 1e9,
-                            "frac_of_measured_hbm": alg / t / 1e9 / peak_gbs}
+        t = time_apply(dm, sset, cs, X, Y, prec, 0, n_launch)
+        alg = sector_matvec_bytes(dm, sset, cs, xb)
+        wb = 16 if prec == 64 else 8
+        uniq = nh * (4 + wb) + n_orb * (8 + 8 + 16) + n_orb * ncol * (xb + 16)
+        gathered = nh * ncol * xb
+        r = {"avg_apply_ms": t * 1e3, "alg_bytes": alg, "alg_GBs": alg / t / 1e9,
+             "frac_of_measured_hbm": alg / t / 1e9 / peak_gbs,
+             "unique_bytes": uniq, "unique_GBs": uniq / t / 1e9,
+             "gathered_x_bytes": gathered, "gathered_x_GBs": gathered / t / 1e9}
+        if otf:
+            proj = dm.proj
+            dm.proj = None
+            dm.refresh()
+            t_otf = time_apply(dm, sset, cs, X, Y, prec, 0, max(3, n_launch // 4))
+            dm.proj = proj
+            dm.refresh()
+            r["on_the_fly_apply_ms"] = t_otf * 1e3
+        out[f"fp{prec}"] = r
+        del X, Y
     return out
 
 
@@ -314,13 +342,19 @@ def run_b200(args):
     G = ed.build_translation_group(model.lattice)
     data = ed.build_ed_data(model, filling_fraction=Fraction(nf, model.lattice.n_site), symmetry_group=G)
     dm, sset = data._device()
+    dm.build_projection(sset.sqrt_stab)
     sectors = list(range(len(data.irrep_list)))
     n_sec = len(sectors)
     assert all(d > 500 for d in sset.dims), "bench workload expects every sector on the Lanczos path"
 
-    # inputs: seeded start blocks, device-resident copy and pinned host copy
+    # how the batch runs (block sizes, persistent cluster or graph path,
+    # projection table) is picked by the autotuner, untimed, before warm-up
     params = ed.LanczosParams(precision=args.precision)
-    solver = BatchedSectorSolver(dm, sset, sectors, nev, precision=args.precision, params=params)
+    tuner = ed.Autotuner(trials=2)
+    t0 = time.perf_counter()
+    config, tune_table = tuner.tune(dm, sset, sectors, nev, precision=args.precision, params=params)
+    tune_s = time.perf_counter() - t0
+    solver = BatchedSectorSolver(dm, sset, sectors, nev, precision=args.precision, params=params, config=config)
     b = solver.batch
     host_blocks = [ed.lanczos.start_block(sset.dims[s], b.block_sizes[i], 12345 + s)
                    for i, s in enumerate(sectors)]
@@ -380,7 +414,7 @@ def run_b200(args):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         res = ed.solve_sectors_batched(data, sectors, nev=nev, precision=args.precision, params=params,
-                                       start_blocks=pinned_blocks)
+                                       start_blocks=pinned_blocks, config=config)
         e1.record()
         torch.cuda.synchronize()
         if it >= args.warmup:
@@ -416,17 +450,19 @@ def run_b200(args):
             "plain_fp64_latency_ms": {"p50": 1e3 * ps[len(ps) // 2], "p99": 1e3 * ps[-1]},
             "batched_over_plain": value / ws / plain_rate,
         })
-        # FP64-matvec batched variant
+        # FP64-matvec batched variant (its own tuned configuration)
+        cfg64, _ = tuner.tune(dm, sset, sectors, nev, precision=64, params=ed.LanczosParams(precision=64))
+        extra["fp64_batched_config"] = cfg64.describe()
         s64 = BatchedSectorSolver(dm, sset, sectors, nev, precision=64,
-                                  params=ed.LanczosParams(precision=64))
+                                  params=ed.LanczosParams(precision=64), config=cfg64)
         for _ in range(2):
-            s64.solve(dev_blocks, vectors=False, host=False)
+            s64.solve(None, vectors=False, host=False)
         t64 = []
         for _ in range(max(3, args.steps // 2)):
             torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
-            v64, _ = s64.solve(dev_blocks, vectors=False, host=False)
+            v64, _ = s64.solve(None, vectors=False, host=False)
             e1.record()
             torch.cuda.synchronize()
             t64.append(e0.elapsed_time(e1) * 1e-3)
@@ -437,6 +473,9 @@ def run_b200(args):
         if fe is not None:
             extra["fp32_matvec_error_before_refinement"] = {"max": float(fe.max()), "median": float(np.median(fe))}
         extra["residual_norm_max"] = float(solver.residuals().max())
+        extra["autotune"] = {"chosen": config.describe(), "tune_s": tune_s,
+                             "candidates": [{"config": r["config"], "solve_ms": None if r["time_s"] is None
+                                             else 1e3 * r["time_s"], "ok": r["ok"]} for r in tune_table]}
         st = b.status()
         extra["lanczos_iterations"] = {"min": int(st[:, 3].min()), "max": int(st[:, 3].max())}
         roof = apply_roofline(ed, data, sset, solver, peak_gbs)
@@ -463,7 +502,7 @@ def run_b200(args):
             "dtype": "c64 matvec / f64 Lanczos" if args.precision == 32 else "f64",
             "data": "synthetic",
             "config": {"workload": args.workload, "desc": wl["desc"], "nev": nev,
-                       "sectors_per_step": n_sec, "block": params.block, "precision": args.precision,
+                       "sectors_per_step": n_sec, "solver": config.describe(), "precision": args.precision,
                        "l2": "256 MB buffer written between timed steps",
                        "parallelism": f"replicas x{ws}"},
             "latency_ms": {"p50": 1e3 * lat[len(lat) // 2], "p99": 1e3 * lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
@@ -501,6 +540,8 @@ def main():
     ap.add_argument("--matvec-only", action="store_true",
                     help="only the 32-site matvec at scale (for kernel profiling)")
     ap.add_argument("--matvec-launches", type=int, default=20)
+    ap.add_argument("--matvec-precision", type=int, default=0, choices=[0, 32, 64])
+    ap.add_argument("--matvec-no-otf", action="store_true")
     args = ap.parse_args()
     if args.matvec_only:
         import realspace_exatdiagonalization_py_b200 as ed
@@ -508,8 +549,10 @@ def main():
 
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
             os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+        precs = (args.matvec_precision,) if args.matvec_precision else (32, 64)
         print(json.dumps(matvec_at_scale(ed, models, float(peaks.get("hbm_gbs", 6650.0)),
-                                         n_launch=args.matvec_launches)), flush=True)
+                                         n_launch=args.matvec_launches, precisions=precs,
+                                         otf=not args.matvec_no_otf)), flush=True)
         return
     if args.impl == "reference":
         run_reference(args)

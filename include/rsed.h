@@ -71,6 +71,13 @@ typedef struct {
   const double* term_amp;        /* n_terms complex128 amplitudes */
   const uint64_t* term_jw;       /* n_terms: sites strictly between source and target */
   const double* hdiag;           /* n_orbits complex128 density-density diagonal */
+  /* Optional orbit-space projection table (rsed_proj_fill); proj_rowptr NULL
+   * = none.  When present, rsed_apply_h streams it instead of re-deriving
+   * every hop (variants 0 and 3xx/4xx). */
+  const int64_t* proj_rowptr;    /* n_orbits + 1 entry offsets */
+  const uint32_t* proj_cg;       /* per hop: target orbit | g << 26 */
+  const double* proj_w64;        /* per hop complex128 weight, or NULL */
+  const float* proj_w32;         /* per hop complex64 weight, or NULL */
 } rsed_model_t;
 
 /* A set of momentum sectors evaluated together ("columns" of a block of
@@ -172,9 +179,37 @@ int rsed_density_diag(int64_t n_orbits, const uint64_t* repr_masks, int32_t n_de
  * H x for the Hermitian blocks the reference builds (to the complex64
  * rounding of its amplitude table).  precision 64: x complex128, FP64
  * accumulation; precision 32: x complex64, FP32 accumulation; y is always
- * complex128.  variant 0 picks the lane mapping from n_cols. */
+ * complex128.  variant 0 streams the model's projection table when it has one
+ * (K6b below) and otherwise picks the on-the-fly lane mapping from n_cols;
+ * 999 always picks the on-the-fly mapping; 1..299 name one on-the-fly
+ * mapping. */
 int rsed_apply_h(const rsed_model_t* model, const rsed_sectors_t* sec, const void* x, void* y,
                  int32_t precision, int32_t variant, void* stream);
+
+/* ---- K6b: orbit-space projection table ---------------------------------
+ * The sector-independent part of every hop of every orbit row, built once per
+ * catalog state (the device form of build_matrixfree_projection_table /
+ * _build_matrixfree_table_kernel, symmetry_resolved_ed.py:1719-1769, 751-799,
+ * shared by all sectors instead of one table per sector).  Row r holds, in the
+ * hop order of rsed_apply_h (occupied source site ascending, then term order),
+ *   cg = c | g << 26     target orbit c, group element g of the table entry
+ *   w  = conj(t * s_JW * alpha) * sqrt(S_c) / sqrt(S_r)
+ * so that column j of y = H^dagger x gets sum_hops w * chi_s(g) * x[c][j]
+ * (s = sector of column j) plus conj(h_diag[r]) x[r][j].  Needs n_orbits <
+ * 2^26 and |G| <= 64.  rsed_proj_count writes rowptr (n_orbits + 1) and the
+ * number of hops; rsed_proj_fill writes cg and either weight array (NULL =
+ * skip).  With the table set in the model, rsed_apply_h variant 3NN streams
+ * it over column chunks of NN columns one chunk after another (the chunk of x
+ * stays in L2 while the table streams from HBM), 4NN runs all chunks in one
+ * launch; 5NN / 6NN are the same with 8 instead of 4 hops in flight per lane;
+ * NN in {2,4,8,16,32} at precision 64 and {4,8,16,32,64} at 32.
+ * These variants read x only at rows of the column's sector: rows outside it
+ * must hold zero (the Lanczos buffers keep them zero). */
+size_t rsed_proj_scratch_bytes(int64_t n_orbits);
+int rsed_proj_count(const rsed_model_t* model, int64_t* rowptr, int64_t* n_hops_out, void* scratch,
+                    size_t scratch_bytes, void* stream);
+int rsed_proj_fill(const rsed_model_t* model, const double* sqrt_stab, const int64_t* rowptr,
+                   uint32_t* cg, double* w64, float* w32, void* stream);
 
 /* ---- K7: matrix mode ---------------------------------------------------
  * Replaces _vectorized_block_triplets / _build_H_block_kernel

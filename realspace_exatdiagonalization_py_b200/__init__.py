@@ -9,6 +9,8 @@ solves with FP64 refinement and a continuous-batching solver service sit
 beside the plain API.
 """
 
+from .autotune import Autotuner, candidate_configs, default_tuner
+from .batched import BatchedSectorSolver, SolverConfig
 from .catalog import Symmetry_Orbit_Catalog, build_symmetry_orbit_catalog, update_orbit_stabilizer_phases
 from .ed import (
     Symmetry_Resolved_ED_Data,

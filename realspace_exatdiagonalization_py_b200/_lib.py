@@ -70,6 +70,10 @@ class RsedModel(ctypes.Structure):
         ("term_amp", c_void_p),
         ("term_jw", c_void_p),
         ("hdiag", c_void_p),
+        ("proj_rowptr", c_void_p),
+        ("proj_cg", c_void_p),
+        ("proj_w64", c_void_p),
+        ("proj_w32", c_void_p),
     ]
 
 
@@ -158,6 +162,9 @@ SIGNATURES = {
         c_int,
         [POINTER(RsedModel), POINTER(RsedSectors), c_void_p, c_void_p, c_int32, c_int32, c_void_p],
     ),
+    "rsed_proj_scratch_bytes": (c_size_t, [c_int64]),
+    "rsed_proj_count": (c_int, [POINTER(RsedModel), c_void_p, POINTER(c_int64), c_void_p, c_size_t, c_void_p]),
+    "rsed_proj_fill": (c_int, [POINTER(RsedModel), c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "rsed_triplet_scratch_bytes": (c_size_t, [c_int64]),
     "rsed_triplets_count": (
         c_int,

@@ -90,6 +90,9 @@ class Symmetry_Orbit_Catalog:
         self.n_orbits = int(repr_masks.shape[0])
         self._host: dict = {}
         self._lin = None
+        # bumped by every in-place amplitude update; device-side derived
+        # tables (the projection table) record the version they were built at
+        self.version = 0
 
     # -- host views --------------------------------------------------------
     def invalidate_host(self) -> None:
@@ -266,5 +269,6 @@ def update_orbit_stabilizer_phases(
         raise ValueError("update_orbit_stabilizer_phases: catalog does not match the group.")
     catalog.symmetry_group = new_group
     catalog.dgroup = dg
+    catalog.version += 1
     catalog.invalidate_host()
     return catalog

@@ -341,6 +341,14 @@ extern "C" int rsed_apply_h(const rsed_model_t* md, const rsed_sectors_t* sc, co
   RSED_REQUIRE(sc->n_group == md->n_group, RSED_EINVAL, "sector/model group order mismatch");
   RSED_REQUIRE(x && y, RSED_EINVAL, "x or y is NULL");
   cudaStream_t stream = as_stream(stream_);
+  RSED_REQUIRE(precision == 64 || precision == 32, RSED_EINVAL, "precision must be 64 or 32");
+  const bool have_proj =
+      md->proj_rowptr && md->proj_cg && (precision == 64 ? md->proj_w64 != nullptr : md->proj_w32 != nullptr);
+  if (variant == 999) {
+    variant = 0;  // automatic on-the-fly mapping even when a projection table is present
+  } else if (variant >= 300 || (variant == 0 && have_proj)) {
+    return rsed_proj_apply(*md, *sc, x, reinterpret_cast<double2*>(y), precision, variant, stream);
+  }
   if (precision == 64)
     return dispatch_apply<64>(*md, *sc, x, reinterpret_cast<double2*>(y), variant, stream);
   if (precision == 32)

@@ -69,7 +69,8 @@ __device__ __forceinline__ double2 cdotc(double2 a, double2 b) {
 // of an instance to finish (atomic ticket, no waiting) sums the partials in
 // chunk order, forms G' = G - C^H C, its Cholesky factor R and the
 // projected-matrix entries.
-__global__ void __launch_bounds__(128) k_lz_reduce(rsed_lanczos_t st, LzDims d, int pass) {
+constexpr int kRT = 256;  // threads of k_lz_reduce
+__global__ void __launch_bounds__(kRT) k_lz_reduce(rsed_lanczos_t st, LzDims d, int pass) {
   const int chunk = blockIdx.x;
   const int inst = blockIdx.y;
   int* stt = st.state + inst * kStateInts;
@@ -100,24 +101,37 @@ __global__ void __launch_bounds__(128) k_lz_reduce(rsed_lanczos_t st, LzDims d, 
   double2* part = reinterpret_cast<double2*>(st.partial);
   const int64_t slot_stride = d.n_orb * d.ld;
   const int64_t pbase = ((int64_t)chunk * d.n_inst + inst) * (int64_t)d.pslots * kBMax * kBMax;
-  for (int pair = threadIdx.x; pair < npairs; pair += blockDim.x) {
-    const int sl = pair / b, p = pair % b;
-    const double2* Y = (sl < nb) ? V + sl * slot_stride : W;
-    double2 acc[kBMax];
+  {
+    // threads = (row group, pair); the row groups split the chunk's rows and
+    // are summed through shared memory
+    __shared__ double2 red[kRT * kBMax];
+    const int groups = kRT / npairs;  // >= 3 since npairs <= kJacobiMax + kBMax
+    const int pair = threadIdx.x % npairs, rg = threadIdx.x / npairs;
+    if (rg < groups) {
+      const int sl = pair / b, p = pair % b;
+      const double2* Y = (sl < nb) ? V + sl * slot_stride : W;
+      double2 acc[kBMax];
 #pragma unroll
-    for (int q = 0; q < kBMax; ++q) acc[q] = make_double2(0.0, 0.0);
+      for (int q = 0; q < kBMax; ++q) acc[q] = make_double2(0.0, 0.0);
 #pragma unroll 4
-    for (int64_t r = r0; r < r1; ++r) {
-      const double2 y = Y[r * d.ld + c0 + p];
-      const double2* wr = W + r * d.ld + c0;
+      for (int64_t r = r0 + rg; r < r1; r += groups) {
+        const double2 y = Y[r * d.ld + c0 + p];
+        const double2* wr = W + r * d.ld + c0;
+#pragma unroll
+        for (int q = 0; q < kBMax; ++q)
+          if (q < b) acc[q] = cadd(acc[q], cdotc(y, wr[q]));
+      }
 #pragma unroll
       for (int q = 0; q < kBMax; ++q)
-        if (q < b) acc[q] = cadd(acc[q], cdotc(y, wr[q]));
+        if (q < b) red[(rg * npairs + pair) * kBMax + q] = acc[q];
     }
-    double2* out = part + pbase + sl * kBMax * kBMax + p * kBMax;
-#pragma unroll
-    for (int q = 0; q < kBMax; ++q)
-      if (q < b) out[q] = acc[q];
+    __syncthreads();
+    for (int e = threadIdx.x; e < npairs * b; e += kRT) {
+      const int pr = e / b, q = e % b, sl = pr / b, p = pr % b;
+      double2 a = make_double2(0.0, 0.0);
+      for (int g = 0; g < groups; ++g) a = cadd(a, red[(g * npairs + pr) * kBMax + q]);
+      part[pbase + sl * kBMax * kBMax + p * kBMax + q] = a;
+    }
   }
   __threadfence();
   __syncthreads();
@@ -134,11 +148,10 @@ __global__ void __launch_bounds__(128) k_lz_reduce(rsed_lanczos_t st, LzDims d, 
   for (int e = threadIdx.x; e < nent; e += blockDim.x) {
     const int sl = e / (b * b), pq = e % (b * b), p = pq / b, q = pq % b;
     double2 a = make_double2(0.0, 0.0);
-    for (int c = 0; c < d.n_chunks; ++c) {
-      const double2* src = part + ((int64_t)c * d.n_inst + inst) * (int64_t)d.pslots * kBMax * kBMax +
-                           sl * kBMax * kBMax + p * kBMax + q;
-      a = cadd(a, __ldcg(src));
-    }
+    const int64_t cstride = (int64_t)d.n_inst * d.pslots * kBMax * kBMax;
+    const double2* src = part + (int64_t)inst * d.pslots * kBMax * kBMax + sl * kBMax * kBMax + p * kBMax + q;
+#pragma unroll 8
+    for (int c = 0; c < d.n_chunks; ++c) a = cadd(a, __ldcg(src + c * cstride));
     sc[(sl * b + p) * kBMax + q] = a;  // row (sl*b + p), column q
   }
   __syncthreads();
@@ -217,18 +230,29 @@ __global__ void __launch_bounds__(128) k_lz_reduce(rsed_lanczos_t st, LzDims d, 
 }
 
 // W <- (W - V C) R^-1 ; pass 2 writes the new basis block and the matvec input.
-__global__ void k_lz_update(rsed_lanczos_t st, LzDims d, int pass) {
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int64_t row = t / d.n_inst;
-  const int inst = (int)(t % d.n_inst);
-  if (row >= d.n_orb) return;
+// Block (row range, instance): the instance's coefficients are staged in
+// shared memory (read by every thread of the block as broadcasts), one row
+// per thread.
+__global__ void __launch_bounds__(256) k_lz_update(rsed_lanczos_t st, LzDims d, int pass) {
+  const int inst = blockIdx.y;
   const int* stt = st.state + inst * kStateInts;
   if (!stt[S_ACTIVE]) return;
   const int b = st.inst_b[inst];
   const int c0 = st.inst_col0[inst];
   const int nb = (pass == 2) ? stt[S_NEWSLOT] : stt[S_NB];
+  if (nb * b > kJacobiMax || b > kBMax) return;  // guarded by k_lz_reduce (status set there)
   const double2* coef = reinterpret_cast<const double2*>(st.coef) +
                         (int64_t)inst * 2 * d.pslots * kBMax * kBMax + (pass - 1) * d.pslots * kBMax * kBMax;
+  __shared__ double2 cs[kJacobiMax * kBMax];
+  __shared__ double2 Rs[kBMax * kBMax];
+  for (int e = threadIdx.x; e < nb * b * b; e += blockDim.x) {
+    const int r = e / b, q = e % b;  // r = s * b + p
+    cs[r * kBMax + q] = coef[(r / b) * kBMax * kBMax + (r % b) * kBMax + q];
+  }
+  for (int e = threadIdx.x; e < kBMax * kBMax; e += blockDim.x) Rs[e] = coef[(d.pslots - 1) * kBMax * kBMax + e];
+  __syncthreads();
+  const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= d.n_orb) return;
   double2* V = reinterpret_cast<double2*>(st.V);
   double2* W = reinterpret_cast<double2*>(st.W);
   const int64_t slot_stride = d.n_orb * d.ld;
@@ -238,29 +262,36 @@ __global__ void k_lz_update(rsed_lanczos_t st, LzDims d, int pass) {
 #pragma unroll 2
   for (int s = 0; s < nb; ++s) {
     const double2* Vs = V + s * slot_stride + row * d.ld + c0;
-    for (int p = 0; p < b; ++p) {
-      const double2 v = Vs[p];
+    double2 v[kBMax];
+#pragma unroll
+    for (int p = 0; p < kBMax; ++p) v[p] = (p < b) ? Vs[p] : make_double2(0.0, 0.0);
+#pragma unroll
+    for (int p = 0; p < kBMax; ++p) {
+      if (p >= b) break;
 #pragma unroll
       for (int q = 0; q < kBMax; ++q)
-        if (q < b) w[q] = csub(w[q], cmul(v, coef[s * kBMax * kBMax + p * kBMax + q]));
+        if (q < b) w[q] = csub(w[q], cmul(v[p], cs[(s * b + p) * kBMax + q]));
     }
   }
-  const double2* R = coef + (d.pslots - 1) * kBMax * kBMax;
   double2 x[kBMax];
 #pragma unroll
   for (int q = 0; q < kBMax; ++q) {
     if (q >= b) break;
     double2 v = w[q];
-    for (int p = 0; p < q; ++p) v = csub(v, cmul(x[p], R[p * kBMax + q]));
-    const double rr = R[q * kBMax + q].x;
+    for (int p = 0; p < q; ++p) v = csub(v, cmul(x[p], Rs[p * kBMax + q]));
+    const double rr = Rs[q * kBMax + q].x;
     x[q] = make_double2(v.x / rr, v.y / rr);
   }
   if (pass == 1) {
-    for (int q = 0; q < b; ++q) W[row * d.ld + c0 + q] = x[q];
+#pragma unroll
+    for (int q = 0; q < kBMax; ++q)
+      if (q < b) W[row * d.ld + c0 + q] = x[q];
   } else {
     double2* Vn = V + (int64_t)nb * slot_stride + row * d.ld + c0;
     double2* X = V + (int64_t)(d.n_slots + 1) * slot_stride + row * d.ld + c0;
-    for (int q = 0; q < b; ++q) {
+#pragma unroll
+    for (int q = 0; q < kBMax; ++q) {
+      if (q >= b) break;
       Vn[q] = x[q];
       X[q] = x[q];
       if (st.Xf) reinterpret_cast<float2*>(st.Xf)[row * d.ld + c0 + q] =
@@ -655,11 +686,10 @@ __global__ void k_lz_ritz(rsed_lanczos_t st, LzDims d, int check_every, int forc
 }
 
 // V_0..keep-1 = V S_keep ; residual block (old slot nb_old-1) -> slot keep.
-__global__ void k_lz_restart(rsed_lanczos_t st, LzDims d) {
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int64_t row = t / d.n_inst;
-  const int inst = (int)(t % d.n_inst);
-  if (row >= d.n_orb) return;
+// Block (row range, instance) with the instance's Ritz coefficients staged in
+// shared memory; one row per thread.
+__global__ void __launch_bounds__(256) k_lz_restart(rsed_lanczos_t st, LzDims d) {
+  const int inst = blockIdx.y;
   const int* stt = st.state + inst * kStateInts;
   const int nb_old = stt[S_RESTART_NB];
   if (nb_old == 0) return;
@@ -667,47 +697,68 @@ __global__ void k_lz_restart(rsed_lanczos_t st, LzDims d) {
   const int c0 = st.inst_col0[inst];
   const int K = st.keep_blocks * b;
   const int Mold = (nb_old - 1) * b;
+  if (Mold > kJacobiMax || K > kKeepMax) return;
+  __shared__ double2 Ss[kJacobiMax * kKeepMax];
   const double2* S = reinterpret_cast<const double2*>(st.ritz_vec) + (int64_t)inst * d.pm * d.pm;
+  for (int e = threadIdx.x; e < Mold * K; e += blockDim.x) Ss[(e / K) * kKeepMax + e % K] = S[(int64_t)(e / K) * d.pm + e % K];
+  __syncthreads();
+  const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= d.n_orb) return;
   double2* V = reinterpret_cast<double2*>(st.V);
   const int64_t slot_stride = d.n_orb * d.ld;
   double2 acc[kKeepMax];
 #pragma unroll
   for (int j = 0; j < kKeepMax; ++j) acc[j] = make_double2(0.0, 0.0);
+#pragma unroll 2
   for (int l = 0; l < Mold; ++l) {
     const double2 v = V[(int64_t)(l / b) * slot_stride + row * d.ld + c0 + (l % b)];
 #pragma unroll
     for (int j = 0; j < kKeepMax; ++j)
-      if (j < K) acc[j] = cadd(acc[j], cmul(v, S[(int64_t)l * d.pm + j]));
+      if (j < K) acc[j] = cadd(acc[j], cmul(v, Ss[l * kKeepMax + j]));
   }
   double2 resid[kBMax];
-  for (int q = 0; q < b; ++q) resid[q] = V[(int64_t)(nb_old - 1) * slot_stride + row * d.ld + c0 + q];
+#pragma unroll
+  for (int q = 0; q < kBMax; ++q)
+    if (q < b) resid[q] = V[(int64_t)(nb_old - 1) * slot_stride + row * d.ld + c0 + q];
 #pragma unroll
   for (int j = 0; j < kKeepMax; ++j)
     if (j < K) V[(int64_t)(j / b) * slot_stride + row * d.ld + c0 + (j % b)] = acc[j];
-  for (int q = 0; q < b; ++q) V[(int64_t)st.keep_blocks * slot_stride + row * d.ld + c0 + q] = resid[q];
+#pragma unroll
+  for (int q = 0; q < kBMax; ++q)
+    if (q < b) V[(int64_t)st.keep_blocks * slot_stride + row * d.ld + c0 + q] = resid[q];
 }
 
 // U[inst][j][row] = sum_l V_l[row] S[l][j], j < nev (Ritz vectors of the last check).
-__global__ void k_lz_extract(rsed_lanczos_t st, LzDims d, double2* U, int64_t u_stride) {
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int64_t row = t / d.n_inst;
-  const int inst = (int)(t % d.n_inst);
-  if (row >= d.n_orb) return;
+__global__ void __launch_bounds__(256) k_lz_extract(rsed_lanczos_t st, LzDims d, double2* U, int64_t u_stride) {
+  const int inst = blockIdx.y;
   const int* stt = st.state + inst * kStateInts;
   const int b = st.inst_b[inst];
   const int c0 = st.inst_col0[inst];
   const int nb = stt[S_NB];
   const int M = (nb - 1) * b;
+  const int nev = st.nev;
+  if (M > kJacobiMax + kBMax || nev > kKeepMax) return;
+  __shared__ double2 Ss[(kJacobiMax + kBMax) * kKeepMax];
   const double2* S = reinterpret_cast<const double2*>(st.ritz_vec) + (int64_t)inst * d.pm * d.pm;
+  for (int e = threadIdx.x; e < M * nev; e += blockDim.x)
+    Ss[(e / nev) * kKeepMax + e % nev] = S[(int64_t)(e / nev) * d.pm + e % nev];
+  __syncthreads();
+  const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= d.n_orb) return;
   const double2* V = reinterpret_cast<const double2*>(st.V);
   const int64_t slot_stride = d.n_orb * d.ld;
-  for (int j = 0; j < st.nev; ++j) {
-    double2 acc = make_double2(0.0, 0.0);
-    for (int l = 0; l < M; ++l)
-      acc = cadd(acc, cmul(V[(int64_t)(l / b) * slot_stride + row * d.ld + c0 + (l % b)],
-                           S[(int64_t)l * d.pm + j]));
-    U[((int64_t)inst * st.nev + j) * u_stride + row] = acc;
+  double2 acc[kKeepMax];
+#pragma unroll
+  for (int j = 0; j < kKeepMax; ++j) acc[j] = make_double2(0.0, 0.0);
+  for (int l = 0; l < M; ++l) {
+    const double2 v = V[(int64_t)(l / b) * slot_stride + row * d.ld + c0 + (l % b)];
+#pragma unroll
+    for (int j = 0; j < kKeepMax; ++j)
+      if (j < nev) acc[j] = cadd(acc[j], cmul(v, Ss[l * kKeepMax + j]));
   }
+#pragma unroll
+  for (int j = 0; j < kKeepMax; ++j)
+    if (j < nev) U[((int64_t)inst * nev + j) * u_stride + row] = acc[j];
 }
 
 // ---------------------------------------------------------------------------
@@ -1385,10 +1436,9 @@ int check_lz(const rsed_model_t* md, const rsed_sectors_t* sc, const rsed_lanczo
 
 int launch_pass(const rsed_lanczos_t& st, const LzDims& d, int pass, cudaStream_t stream) {
   dim3 g1(d.n_chunks, d.n_inst);
-  k_lz_reduce<<<g1, 128, 0, stream>>>(st, d, pass);
+  k_lz_reduce<<<g1, kRT, 0, stream>>>(st, d, pass);
   RSED_CHECK_LAUNCH();
-  const int64_t tot = d.n_orb * d.n_inst;
-  k_lz_update<<<(unsigned)((tot + 255) / 256), 256, 0, stream>>>(st, d, pass);
+  k_lz_update<<<dim3((unsigned)((d.n_orb + 255) / 256), d.n_inst), 256, 0, stream>>>(st, d, pass);
   RSED_CHECK_LAUNCH();
   return RSED_OK;
 }
@@ -1487,8 +1537,7 @@ extern "C" int rsed_lanczos_iterate(const rsed_model_t* md, const rsed_sectors_t
     if (rc) return rc;
     k_lz_ritz<<<d.n_inst, 256, kRitzSmem, stream>>>(*st, d, check_every, 0, 0);
     RSED_CHECK_LAUNCH();
-    const int64_t tot = d.n_orb * d.n_inst;
-    k_lz_restart<<<(unsigned)((tot + 255) / 256), 256, 0, stream>>>(*st, d);
+    k_lz_restart<<<dim3((unsigned)((d.n_orb + 255) / 256), d.n_inst), 256, 0, stream>>>(*st, d);
     RSED_CHECK_LAUNCH();
   }
   return RSED_OK;
@@ -1506,8 +1555,7 @@ extern "C" int rsed_lanczos_rayleigh_ritz(const rsed_model_t* md, const rsed_sec
   const LzDims d = make_dims(md, sc, st);
   k_rr_prepare<<<(st->n_inst + 63) / 64, 64, 0, stream>>>(*st);
   RSED_CHECK_LAUNCH();
-  const int64_t tot = d.n_orb * d.n_inst;
-  k_lz_restart<<<(unsigned)((tot + 255) / 256), 256, 0, stream>>>(*st, d);
+  k_lz_restart<<<dim3((unsigned)((d.n_orb + 255) / 256), d.n_inst), 256, 0, stream>>>(*st, d);
   RSED_CHECK_LAUNCH();
   const int64_t slot = d.n_orb * d.ld;
   double2* V = reinterpret_cast<double2*>(st->V);
@@ -1571,9 +1619,8 @@ extern "C" int rsed_lanczos_extract(const rsed_model_t* md, const rsed_sectors_t
   RSED_REQUIRE(U != nullptr && u_stride >= md->n_orbits, RSED_EINVAL, "bad U buffer");
   cudaStream_t stream = as_stream(stream_);
   const LzDims d = make_dims(md, sc, st);
-  const int64_t tot = d.n_orb * d.n_inst;
-  k_lz_extract<<<(unsigned)((tot + 255) / 256), 256, 0, stream>>>(*st, d, reinterpret_cast<double2*>(U),
-                                                                   u_stride);
+  k_lz_extract<<<dim3((unsigned)((d.n_orb + 255) / 256), d.n_inst), 256, 0, stream>>>(
+      *st, d, reinterpret_cast<double2*>(U), u_stride);
   RSED_CHECK_LAUNCH();
   return RSED_OK;
 }

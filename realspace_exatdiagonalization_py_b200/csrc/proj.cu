@@ -1,0 +1,431 @@
+// K6b: orbit-space projection table and its streaming SpMV.
+//
+// The on-the-fly apply (apply.cu) re-derives every hop on every call: gate
+// test, combinadic rank, a random 16-B gather from the C(N,k)-sized table.
+// Across the ~100 matvecs of one eigen-solve those hops never change, so this
+// file builds them once per catalog state into a CSR over orbit rows whose
+// entries carry only what does not depend on the sector:
+//   cg = c | g << 26   (target orbit, group element)
+//   w  = conj(t * s_JW * alpha) * sqrt(S_c) / sqrt(S_r)
+// A matvec then streams the table from HBM once per column chunk and gathers
+// x[c][chunk] rows; chunks are sized by the caller so that x[:, chunk] stays
+// resident in L2 while the table streams past it.
+#include <type_traits>
+#include "rsed_internal.cuh"
+#include "rsed_apply.cuh"
+
+using namespace rsed_apply;
+
+namespace {
+
+constexpr int kOrbitBits = 26;
+constexpr uint32_t kOrbitMask = (1u << kOrbitBits) - 1u;
+
+// Hops of row r in the order of the on-the-fly apply: occupied source site
+// ascending, then the terms of that site in order, skipping occupied targets.
+__global__ void __launch_bounds__(256) k_proj_count(rsed_model_t md, int64_t* counts, ApplySmemLayout lay) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  rsed_sectors_t none{};
+  ApplyView v = stage_apply(md, none, lay, smem);
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= md.n_orbits) return;
+  const uint64_t m = md.repr_masks[r];
+  int64_t n = 0;
+  uint64_t occ = m;
+  while (occ) {
+    const int i = __ffsll((long long)occ) - 1;
+    occ &= occ - 1;
+    for (int t = v.tbeg[i]; t < v.tbeg[i + 1]; ++t) n += ((m >> v.tto[t]) & 1ull) ? 0 : 1;
+  }
+  counts[r] = n;
+}
+
+// Table entries are gathered HB hops at a time so each thread keeps several
+// random 16-B loads in flight.
+template <int HB>
+__global__ void __launch_bounds__(256) k_proj_fill(rsed_model_t md, const double* __restrict__ sqrt_stab,
+                                                   const int64_t* __restrict__ rowptr, uint32_t* __restrict__ cg,
+                                                   double2* __restrict__ w64, float2* __restrict__ w32,
+                                                   ApplySmemLayout lay) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  rsed_sectors_t none{};
+  ApplyView v = stage_apply(md, none, lay, smem);
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= md.n_orbits) return;
+  const int kp1 = md.n_filled + 1;
+  const uint64_t m = md.repr_masks[r];
+  const double sr = sqrt_stab[r];
+  int64_t pos = rowptr[r];
+  int bt[HB];
+  int64_t bidx[HB];
+  int nh = 0;
+  auto flush = [&](int cnt) {
+    RsedEntry e[HB];
+#pragma unroll
+    for (int h = 0; h < HB; ++h)
+      if (h < cnt) e[h] = load_entry(reinterpret_cast<const RsedEntry*>(md.table), bidx[h]);
+    double sq[HB];
+#pragma unroll
+    for (int h = 0; h < HB; ++h)
+      if (h < cnt) sq[h] = __ldg(sqrt_stab + e[h].rep);
+#pragma unroll
+    for (int h = 0; h < HB; ++h) {
+      if (h >= cnt) continue;
+      const int t = bt[h];
+      double2 ta = cmul(v.tamp[t], make_double2(e[h].re, e[h].im));
+      if (md.fermionic && (__popcll(m & v.tjw[t]) & 1)) {
+        ta.x = -ta.x;
+        ta.y = -ta.y;
+      }
+      const double ratio = sq[h] / sr;
+      const double2 w = make_double2(ta.x * ratio, -ta.y * ratio);
+      cg[pos] = (uint32_t)e[h].rep | ((uint32_t)e[h].g << kOrbitBits);
+      if (w64) w64[pos] = w;
+      if (w32) w32[pos] = make_float2((float)w.x, (float)w.y);
+      ++pos;
+    }
+  };
+  uint64_t occ = m;
+  while (occ) {
+    const int i = __ffsll((long long)occ) - 1;
+    occ &= occ - 1;
+    for (int t = v.tbeg[i]; t < v.tbeg[i + 1]; ++t) {
+      const int jj = v.tto[t];
+      if ((m >> jj) & 1ull) continue;
+      bt[nh] = t;
+      bidx[nh] = rsed_rank(m ^ (1ull << i) ^ (1ull << jj), v.binom, kp1);
+      if (++nh == HB) {
+        flush(HB);
+        nh = 0;
+      }
+    }
+  }
+  if (nh) flush(nh);
+}
+
+// ---- streaming SpMV --------------------------------------------------------
+// One warp per orbit row (grid-stride).  The warp's lanes form EPW = 32/L
+// entry slots of L lanes; the L lanes of a slot cover the NC = L*CPL columns
+// of the chunk, CPL contiguous columns each (one 16-B gather per lane and
+// hop).  Entry slots walk the row's hops EPW at a time, U hops per batch
+// (all U table entries, then all U x rows, then the arithmetic), and are
+// summed with xor-shuffles at the end of the row.
+template <int PREC>
+struct ProjTypes;
+template <>
+struct ProjTypes<64> {
+  using W = double2;
+  using Real = double;
+};
+template <>
+struct ProjTypes<32> {
+  using W = float2;
+  using Real = float;
+};
+
+template <int PREC, int CPL>
+struct XVec;
+template <>
+struct XVec<64, 1> {
+  double2 v[1];
+  __device__ __forceinline__ void load(const void* base) { v[0] = __ldg(reinterpret_cast<const double2*>(base)); }
+  __device__ __forceinline__ void zero() { v[0] = make_double2(0.0, 0.0); }
+};
+template <>
+struct XVec<32, 2> {
+  float2 v[2];
+  __device__ __forceinline__ void load(const void* base) {
+    const float4 q = __ldg(reinterpret_cast<const float4*>(base));
+    v[0] = make_float2(q.x, q.y);
+    v[1] = make_float2(q.z, q.w);
+  }
+  __device__ __forceinline__ void zero() {
+    v[0] = make_float2(0.f, 0.f);
+    v[1] = make_float2(0.f, 0.f);
+  }
+};
+
+template <typename T>
+__device__ __forceinline__ T ld_stream(const T* p) {
+  return __ldcs(p);
+}
+
+template <int PREC, int L, int U>
+__global__ void __launch_bounds__(256) k_proj_spmv(rsed_model_t md, rsed_sectors_t sc, const void* __restrict__ xin,
+                                                   double2* __restrict__ y, int chunk0) {
+  using W = typename ProjTypes<PREC>::W;
+  using Real = typename ProjTypes<PREC>::Real;
+  constexpr int CPL = (PREC == 64) ? 1 : 2;
+  constexpr int EPW = 32 / L;
+  constexpr int NC = L * CPL;
+  extern __shared__ __align__(16) unsigned char smem[];
+  // characters transposed to [g][sector]: the L lanes of an entry slot share
+  // g and read consecutive words
+  W* chi = reinterpret_cast<W*>(smem);
+  const double2* gchi = reinterpret_cast<const double2*>(sc.chi);
+  const int nsec = sc.n_sectors;
+  const int nchi = nsec * md.n_group;
+  for (int i = threadIdx.x; i < nchi; i += blockDim.x) {
+    const int s = i / md.n_group, g = i % md.n_group;
+    const double2 c = gchi[i];
+    chi[g * nsec + s].x = (Real)c.x;
+    chi[g * nsec + s].y = (Real)c.y;
+  }
+  __syncthreads();
+  const W* __restrict__ wt = reinterpret_cast<const W*>(PREC == 64 ? (const void*)md.proj_w64
+                                                                    : (const void*)md.proj_w32);
+  const uint32_t* __restrict__ cgt = md.proj_cg;
+  const int64_t* __restrict__ rp = md.proj_rowptr;
+  const int lane = threadIdx.x & 31;
+  const int eslot = lane / L;
+  const int c0 = (chunk0 + (int)blockIdx.y) * NC + (lane % L) * CPL;
+  const int64_t ld = sc.ld;
+  int sec[CPL];
+  bool colv[CPL];
+#pragma unroll
+  for (int j = 0; j < CPL; ++j) {
+    colv[j] = c0 + j < sc.n_cols;
+    sec[j] = colv[j] ? sc.col_sector[c0 + j] : 0;
+  }
+  bool same = true;
+#pragma unroll
+  for (int j = 1; j < CPL; ++j) same = same && sec[j] == sec[0];
+  const char* xb = reinterpret_cast<const char*>(xin) + (size_t)c0 * sizeof(W);
+  constexpr size_t kRowBytes = sizeof(W);
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t r = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < md.n_orbits; r += warps) {
+    const uint64_t memr = sc.member[r];
+    bool on[CPL];
+    bool any = false;
+#pragma unroll
+    for (int j = 0; j < CPL; ++j) {
+      on[j] = colv[j] && ((memr >> sec[j]) & 1ull);
+      any |= on[j];
+    }
+    W acc[CPL];
+#pragma unroll
+    for (int j = 0; j < CPL; ++j) acc[j].x = acc[j].y = (Real)0;
+    if (__any_sync(0xffffffffu, any)) {
+      const int64_t e0 = rp[r], e1 = rp[r + 1];
+      for (int64_t base = e0; base < e1; base += EPW * U) {
+        uint32_t cgv[U];
+        W wv[U];
+        XVec<PREC, CPL> xv[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const int64_t idx = base + u * EPW + eslot;
+          if (idx < e1) {
+            cgv[u] = ld_stream(cgt + idx);
+            wv[u] = ld_stream(wt + idx);
+          } else {
+            cgv[u] = 0xffffffffu;
+            wv[u].x = wv[u].y = (Real)0;
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          if (cgv[u] != 0xffffffffu && any)
+            xv[u].load(xb + (size_t)(cgv[u] & kOrbitMask) * ld * kRowBytes);
+          else
+            xv[u].zero();
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          if (cgv[u] == 0xffffffffu) continue;
+          const W* chg = chi + (int)(cgv[u] >> kOrbitBits) * nsec;
+          Real wcx = 0, wcy = 0;
+#pragma unroll
+          for (int j = 0; j < CPL; ++j) {
+            if (!on[j]) continue;
+            // the block vectors of one sector sit in adjacent columns, so a
+            // lane's columns usually share the weight
+            if (j == 0 || !same) {
+              const W ch = chg[sec[j]];
+              wcx = wv[u].x * ch.x - wv[u].y * ch.y;
+              wcy = wv[u].x * ch.y + wv[u].y * ch.x;
+            }
+            const W xx = xv[u].v[j];
+            acc[j].x += wcx * xx.x - wcy * xx.y;
+            acc[j].y += wcx * xx.y + wcy * xx.x;
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int off = L; off < 32; off <<= 1) {
+#pragma unroll
+      for (int j = 0; j < CPL; ++j) {
+        acc[j].x += __shfl_xor_sync(0xffffffffu, acc[j].x, off);
+        acc[j].y += __shfl_xor_sync(0xffffffffu, acc[j].y, off);
+      }
+    }
+    if (eslot == 0) {
+      const double2 hd = reinterpret_cast<const double2*>(md.hdiag)[r];
+#pragma unroll
+      for (int j = 0; j < CPL; ++j) {
+        if (!colv[j]) continue;
+        double2 o = make_double2(0.0, 0.0);
+        if (on[j]) {
+          const W xr = reinterpret_cast<const W*>(xin)[r * ld + c0 + j];
+          const double xx = (double)xr.x, xy = (double)xr.y;
+          o.x = (double)acc[j].x + (hd.x * xx + hd.y * xy);
+          o.y = (double)acc[j].y + (hd.x * xy - hd.y * xx);
+        }
+        y[r * ld + c0 + j] = o;
+      }
+    }
+  }
+}
+
+template <int PREC, int L, int U>
+int launch_spmv(const rsed_model_t& md, const rsed_sectors_t& sc, const void* x, double2* y, bool sequential,
+                cudaStream_t stream) {
+  using W = typename ProjTypes<PREC>::W;
+  constexpr int NC = L * ((PREC == 64) ? 1 : 2);
+  const size_t smem = sizeof(W) * (size_t)sc.n_sectors * md.n_group;
+  static int blocks_per_sm[16] = {0};  // per device, computed once
+  int dev = 0;
+  RSED_TRY_CUDA(cudaGetDevice(&dev));
+  int& bps = blocks_per_sm[dev & 15];
+  if (smem > 48 * 1024)
+    RSED_TRY_CUDA(cudaFuncSetAttribute(k_proj_spmv<PREC, L, U>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem));
+  if (bps == 0) {
+    RSED_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_proj_spmv<PREC, L, U>, 256, smem));
+    if (bps < 1) bps = 1;
+  }
+  static int n_sm = 0;
+  if (n_sm == 0) RSED_TRY_CUDA(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
+  const int n_chunks = (sc.n_cols + NC - 1) / NC;
+  const int64_t row_blocks = (md.n_orbits + 7) / 8;
+  const int64_t gx = row_blocks < (int64_t)n_sm * bps ? row_blocks : (int64_t)n_sm * bps;
+  if (sequential) {
+    for (int c = 0; c < n_chunks; ++c) {
+      k_proj_spmv<PREC, L, U><<<dim3((unsigned)gx, 1), 256, smem, stream>>>(md, sc, x, y, c);
+      RSED_CHECK_LAUNCH();
+    }
+  } else {
+    k_proj_spmv<PREC, L, U><<<dim3((unsigned)gx, (unsigned)n_chunks), 256, smem, stream>>>(md, sc, x, y, 0);
+    RSED_CHECK_LAUNCH();
+  }
+  return RSED_OK;
+}
+
+int check_proj_model(const rsed_model_t* md) {
+  RSED_REQUIRE(md != nullptr, RSED_EINVAL, "model descriptor is NULL");
+  RSED_REQUIRE(md->n_site >= 1 && md->n_site <= RSED_MAX_SITES, RSED_ERANGE, "bad n_site");
+  RSED_REQUIRE(md->n_group >= 1 && md->n_group <= RSED_MAX_GROUP, RSED_ERANGE, "bad |G|");
+  RSED_REQUIRE(md->n_orbits >= 1 && md->table && md->repr_masks && md->binom && md->hdiag, RSED_EINVAL,
+               "model tables missing");
+  RSED_REQUIRE(md->n_terms >= 0 && md->term_begin, RSED_EINVAL, "terms missing");
+  RSED_REQUIRE(md->n_orbits <= (int64_t)kOrbitMask, RSED_ERANGE,
+               "projection table holds at most 2^26 - 1 orbits");
+  return RSED_OK;
+}
+
+}  // namespace
+
+// Called by rsed_apply_h for variants 0 (with a table present), 3NN and 4NN.
+int rsed_proj_apply(const rsed_model_t& md, const rsed_sectors_t& sc, const void* x, double2* y, int precision,
+                    int variant, cudaStream_t stream) {
+  RSED_REQUIRE(md.proj_rowptr && md.proj_cg, RSED_EINVAL, "no projection table in the model");
+  RSED_REQUIRE(precision == 64 ? md.proj_w64 != nullptr : md.proj_w32 != nullptr, RSED_EINVAL,
+               "projection table has no weights for precision %d", precision);
+  RSED_REQUIRE((sc.ld & 1) == 0 && (reinterpret_cast<uintptr_t>(x) & 15) == 0, RSED_EINVAL,
+               "projection apply needs an even leading dimension and a 16-byte aligned x");
+  const size_t s = precision == 64 ? 16 : 8;
+  (void)s;
+  if (variant == 0) {
+    // Measured on B200: at scale (x larger than L2) the widest chunk wins,
+    // since the gathered row segments then use whole 128-B lines and the
+    // table streams once; small bases (latency-bound) prefer 16 columns per
+    // chunk with all chunks in one launch for more warps in flight.
+    const int opts64[5] = {2, 4, 8, 16, 32}, opts32[5] = {4, 8, 16, 32, 64};
+    const int* opts = precision == 64 ? opts64 : opts32;
+    int nc = opts[4];
+    if (md.n_orbits < 65536) {
+      nc = 16;
+    } else {
+      for (int i = 0; i < 5; ++i)
+        if (opts[i] >= sc.n_cols) {
+          nc = opts[i];
+          break;
+        }
+    }
+    variant = (md.n_orbits < 65536 ? 400 : 300) + nc;
+  }
+  const int family = variant / 100;  // 3/4: 4 hops per slot and batch, 5/6: 8
+  const bool seq = family == 3 || family == 5;
+  const bool deep = family >= 5;
+  const int nc = variant % 100;
+  if (family >= 3 && family <= 6) {
+#define RSED_PROJ_CASE(P, NCOLS, LANES)                                                     \
+  case NCOLS:                                                                               \
+    return deep ? launch_spmv<P, LANES, 8>(md, sc, x, y, seq, stream)                       \
+                : launch_spmv<P, LANES, 4>(md, sc, x, y, seq, stream);
+    if (precision == 64) {
+      switch (nc) {
+        RSED_PROJ_CASE(64, 2, 2)
+        RSED_PROJ_CASE(64, 4, 4)
+        RSED_PROJ_CASE(64, 8, 8)
+        RSED_PROJ_CASE(64, 16, 16)
+        RSED_PROJ_CASE(64, 32, 32)
+        default: break;
+      }
+    } else {
+      switch (nc) {
+        RSED_PROJ_CASE(32, 4, 2)
+        RSED_PROJ_CASE(32, 8, 4)
+        RSED_PROJ_CASE(32, 16, 8)
+        RSED_PROJ_CASE(32, 32, 16)
+        RSED_PROJ_CASE(32, 64, 32)
+        default: break;
+      }
+    }
+#undef RSED_PROJ_CASE
+  }
+  return rsed_set_error(RSED_EINVAL, "projection apply variant %d invalid at precision %d", variant, precision);
+}
+
+extern "C" size_t rsed_proj_scratch_bytes(int64_t n_orbits) {
+  return align_up(sizeof(int64_t) * (size_t)(n_orbits + 1), 256) + rsed_scan_scratch_bytes(n_orbits);
+}
+
+extern "C" int rsed_proj_count(const rsed_model_t* md, int64_t* rowptr, int64_t* n_hops_out, void* scratch,
+                               size_t scratch_bytes, void* stream_) {
+  int rc = check_proj_model(md);
+  if (rc) return rc;
+  RSED_REQUIRE(rowptr && n_hops_out && scratch, RSED_EINVAL, "bad projection count arguments");
+  RSED_REQUIRE(scratch_bytes >= rsed_proj_scratch_bytes(md->n_orbits), RSED_ESCRATCH,
+               "projection scratch too small");
+  cudaStream_t stream = as_stream(stream_);
+  int64_t* counts = reinterpret_cast<int64_t*>(scratch);
+  char* scan = reinterpret_cast<char*>(scratch) + align_up(sizeof(int64_t) * (size_t)(md->n_orbits + 1), 256);
+  rsed_sectors_t none{};
+  ApplySmemLayout lay = apply_layout(*md, none);
+  RSED_REQUIRE(lay.total <= 48 * 1024, RSED_ERANGE, "term tables exceed 48 KB of shared memory");
+  k_proj_count<<<(unsigned)((md->n_orbits + 255) / 256), 256, lay.total, stream>>>(*md, counts, lay);
+  RSED_CHECK_LAUNCH();
+  rc = rsed_exclusive_scan_i64(counts, rowptr, md->n_orbits, scan, rsed_scan_scratch_bytes(md->n_orbits),
+                               stream);
+  if (rc) return rc;
+  RSED_TRY_CUDA(cudaMemcpyAsync(n_hops_out, rowptr + md->n_orbits, sizeof(int64_t), cudaMemcpyDeviceToHost,
+                                stream));
+  RSED_TRY_CUDA(cudaStreamSynchronize(stream));
+  return RSED_OK;
+}
+
+extern "C" int rsed_proj_fill(const rsed_model_t* md, const double* sqrt_stab, const int64_t* rowptr,
+                              uint32_t* cg, double* w64, float* w32, void* stream_) {
+  int rc = check_proj_model(md);
+  if (rc) return rc;
+  RSED_REQUIRE(sqrt_stab && rowptr && cg, RSED_EINVAL, "bad projection fill arguments");
+  cudaStream_t stream = as_stream(stream_);
+  rsed_sectors_t none{};
+  ApplySmemLayout lay = apply_layout(*md, none);
+  RSED_REQUIRE(lay.total <= 48 * 1024, RSED_ERANGE, "term tables exceed 48 KB of shared memory");
+  k_proj_fill<4><<<(unsigned)((md->n_orbits + 255) / 256), 256, lay.total, stream>>>(
+      *md, sqrt_stab, rowptr, cg, reinterpret_cast<double2*>(w64), reinterpret_cast<float2*>(w32), lay);
+  RSED_CHECK_LAUNCH();
+  return RSED_OK;
+}

@@ -49,3 +49,7 @@ struct GroupSmemLayout {
 GroupSmemLayout group_smem_layout(int n_site, int n_filled, int n_group, bool with_eta,
                                   bool with_angle);
 int check_group(const rsed_group_t* g);
+// Streaming apply over the model's projection table (proj.cu); variant 0
+// picks the column chunk, 3NN / 4NN as documented at rsed_apply_h.
+int rsed_proj_apply(const rsed_model_t& md, const rsed_sectors_t& sc, const void* x, double2* y, int precision,
+                    int variant, cudaStream_t stream);

@@ -80,7 +80,7 @@ class Symmetry_Resolved_ED_Data:
         cat = self.orbit_catalog
         model = self.second_quantized_model
         key = (id(cat), id(model.bilinear_terms), id(model.density_density_terms),
-               id(cat.symmetry_group))
+               id(cat.symmetry_group), cat.version)
         if dv is None or dv[0] != key:
             dm = DeviceModel(cat, model.bilinear_terms, model.density_density_terms)
             sset = SectorSet(cat, self.irrep_list[:64]) if len(self.irrep_list) <= 64 else None
@@ -172,7 +172,8 @@ def ed_scan_at_irrep_matrix(irrep_label, ed_data, *, nev: int = 5,
 
 def solve_sectors_batched(ed_data, sector_ids: list[int], *, nev: int = 5, precision: int = 64,
                           params: LanczosParams | None = None, graph: bool = True,
-                          return_vectors: bool = True, start_blocks=None):
+                          return_vectors: bool = True, start_blocks=None, config=None,
+                          autotune: bool = False):
     """Solve many sectors of one catalog in one batched block Lanczos.
 
     Sectors with ``dim <= 500`` take the dense path (as the reference does);
@@ -180,6 +181,8 @@ def solve_sectors_batched(ed_data, sector_ids: list[int], *, nev: int = 5, preci
     them.  ``precision=32`` runs the matvec in FP32 and finishes each sector
     with an FP64 refinement.  The batched solver (buffers, captured graphs)
     is kept on ``ed_data`` and reused by later calls with the same sectors.
+    ``config`` (a ``SolverConfig``) fixes how the batch runs; ``autotune``
+    picks it by measurement (``autotune.default_tuner``, cached per shape).
     Returns ``{sector: (vals, vecs)}``.
     """
     from .batched import BatchedSectorSolver
@@ -201,11 +204,17 @@ def solve_sectors_batched(ed_data, sector_ids: list[int], *, nev: int = 5, preci
         else:
             big.append(s)
     if big:
-        key = (tuple(big), nev, precision, None if params is None else tuple(params.__dict__.items()), graph)
+        if config is None and autotune:
+            from .autotune import default_tuner
+
+            config = default_tuner().best(dm, sset, big, nev, precision, params)
+        key = (tuple(big), nev, precision, None if params is None else tuple(params.__dict__.items()), graph,
+               config)
         cache = ed_data.__dict__.setdefault("_solvers", {})
         solver = cache.get(key)
         if solver is None or solver.model is not dm:
-            solver = BatchedSectorSolver(dm, sset, big, nev, precision=precision, params=params, graph=graph)
+            solver = BatchedSectorSolver(dm, sset, big, nev, precision=precision, params=params, graph=graph,
+                                         config=config)
             cache[key] = solver
         vals, vecs = solver.solve(start_blocks, vectors=return_vectors)
         for i, s in enumerate(big):

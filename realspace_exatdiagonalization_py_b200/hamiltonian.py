@@ -95,18 +95,70 @@ class DeviceModel:
         _lib.check(lib.rsed_density_diag(catalog.n_orbits, _lib.ptr(catalog.repr_masks), nd,
                                          _lib.ptr(self._di), _lib.ptr(self._dj), _lib.ptr(self._dv),
                                          _lib.ptr(self.hdiag), _lib.stream_ptr(stream)))
+        self.proj = None
         self.refresh()
 
     def refresh(self) -> None:
-        """Rebuild the C descriptor (after an in-place catalog update)."""
+        """Rebuild the C descriptor (after an in-place catalog update, which
+        also drops the projection table built from the old amplitudes)."""
         cat = self.catalog
         dg = cat.dgroup
+        if self.proj is not None and self.proj["table_version"] != cat.version:
+            self.proj = None
+        pj = self.proj or {}
         self.c = _lib.RsedModel(
             dg.n_site, dg.n_filled, dg.n_group, int(dg.fermionic), dg.n_states, cat.n_orbits,
             _lib.ptr(dg.binom), _lib.ptr(cat.table), _lib.ptr(cat.repr_masks), self.n_terms,
             _lib.ptr(self.term_begin), _lib.ptr(self.term_to), _lib.ptr(self.term_amp),
             _lib.ptr(self.term_jw), _lib.ptr(self.hdiag),
+            _lib.ptr(pj.get("rowptr")), _lib.ptr(pj.get("cg")), _lib.ptr(pj.get("w64")),
+            _lib.ptr(pj.get("w32")),
         )
+
+    def projection_bytes(self, precisions=(64, 32)) -> int:
+        """Device bytes of the projection table (exact hop count; one pass)."""
+        if self.proj is not None:
+            return sum(int(t.numel() * t.element_size()) for k, t in self.proj.items() if torch.is_tensor(t))
+        n = self.count_hops()
+        return 8 * (self.catalog.n_orbits + 1) + n * (4 + (16 if 64 in precisions else 0)
+                                                      + (8 if 32 in precisions else 0))
+
+    def count_hops(self, stream=None) -> int:
+        """Hops over all orbit rows (the projection table's entry count)."""
+        lib = _lib.lib()
+        n_orb = self.catalog.n_orbits
+        dev = self.hdiag.device
+        rowptr = torch.empty(n_orb + 1, dtype=torch.int64, device=dev)
+        scratch = torch.empty(lib.rsed_proj_scratch_bytes(n_orb), dtype=torch.uint8, device=dev)
+        n = ctypes.c_int64()
+        _lib.check(lib.rsed_proj_count(ctypes.byref(self.c), _lib.ptr(rowptr), ctypes.byref(n),
+                                       _lib.ptr(scratch), scratch.numel(), _lib.stream_ptr(stream)))
+        self._rowptr_cache = rowptr
+        return int(n.value)
+
+    def build_projection(self, sqrt_stab: torch.Tensor, precisions=(64, 32), stream=None) -> None:
+        """Build the orbit-space projection table (K6b) for the current
+        catalog amplitudes; afterwards ``rsed_apply_h`` variant 0 streams it."""
+        lib = _lib.lib()
+        want = tuple(sorted(set(precisions)))
+        if self.proj is not None and self.proj["table_version"] == self.catalog.version and \
+                set(want) <= set(self.proj["precisions"]):
+            return
+        n = self.count_hops(stream)
+        rowptr = self._rowptr_cache
+        dev = rowptr.device
+        cg = torch.empty(max(n, 1), dtype=torch.int32, device=dev)
+        w64 = torch.empty(max(n, 1), dtype=torch.complex128, device=dev) if 64 in want else None
+        w32 = torch.empty(max(n, 1), dtype=torch.complex64, device=dev) if 32 in want else None
+        _lib.check(lib.rsed_proj_fill(ctypes.byref(self.c), _lib.ptr(sqrt_stab), _lib.ptr(rowptr),
+                                      _lib.ptr(cg), _lib.ptr(w64), _lib.ptr(w32), _lib.stream_ptr(stream)))
+        self.proj = {"rowptr": rowptr, "cg": cg, "w64": w64, "w32": w32, "n_hops": n,
+                     "precisions": want, "table_version": self.catalog.version}
+        self.refresh()
+
+    def drop_projection(self) -> None:
+        self.proj = None
+        self.refresh()
 
     def apply_block(self, sset: SectorSet, col_sector: torch.Tensor, X: torch.Tensor,
                     Y: torch.Tensor, precision: int = 64, variant: int = 0, stream=None) -> None:

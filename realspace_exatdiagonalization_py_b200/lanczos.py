@@ -122,7 +122,10 @@ class LanczosBatch:
         self.inst_b = torch.tensor(bs, dtype=torch.int32, device=dev)
         S = p.n_slots
         self.pm = (S + 1) * bmax
-        self.chunk_rows = 64 if n_orb <= 65536 else (256 if n_orb <= 1 << 20 else 1024)
+        # reduction chunks: about 8 blocks per SM over all instances, >= 64 rows
+        n_sm = torch.cuda.get_device_properties(dev).multi_processor_count if dev.type == "cuda" else 148
+        target = max(1, (8 * n_sm) // n_inst)
+        self.chunk_rows = max(64, -(-n_orb // target))
         c128 = torch.complex128
         self.V = torch.zeros((S + 2, n_orb, self.ld), dtype=c128, device=dev)
         self.W = torch.zeros((n_orb, self.ld), dtype=c128, device=dev)
@@ -155,8 +158,9 @@ class LanczosBatch:
     # -- start ------------------------------------------------------------
     def load_start(self, blocks: list[torch.Tensor | np.ndarray | None], seeds: list[int] | None = None,
                    stream=None) -> None:
-        """Place each instance's start block ``[D_s, b]`` (compact sector rows)
-        into ``W``; ``None`` draws the seeded block of :func:`start_block`."""
+        """Place each instance's start block ``[D_s, >= b]`` (compact sector
+        rows; the first ``b`` columns are used) into ``W``; ``None`` draws the
+        seeded block of :func:`start_block`."""
         self.W.zero_()
         lib = _lib.lib()
         sp = _lib.stream_ptr(stream)
@@ -169,7 +173,10 @@ class LanczosBatch:
                 blk = start_block(d, b, seed)
             if isinstance(blk, np.ndarray):
                 blk = torch.from_numpy(np.ascontiguousarray(blk, dtype=np.complex128))
-            blk = blk.to(self.dev, non_blocking=True).reshape(d, b).to(torch.complex128)
+            blk = blk.to(self.dev, non_blocking=True).reshape(d, -1)
+            if blk.shape[1] < b:
+                raise ValueError(f"start block of sector {s} has {blk.shape[1]} columns, the instance needs {b}")
+            blk = blk[:, :b].to(torch.complex128)
             blk = blk.t().contiguous()  # [b, d]
             oor, _ = self.sset.rows(s)
             for j in range(b):
