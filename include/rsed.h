@@ -201,8 +201,10 @@ int rsed_apply_h(const rsed_model_t* model, const rsed_sectors_t* sec, const voi
  * skip).  With the table set in the model, rsed_apply_h variant 3NN streams
  * it over column chunks of NN columns one chunk after another (the chunk of x
  * stays in L2 while the table streams from HBM), 4NN runs all chunks in one
- * launch; 5NN / 6NN are the same with 8 instead of 4 hops in flight per lane;
- * NN in {2,4,8,16,32} at precision 64 and {4,8,16,32,64} at 32.
+ * launch; NN in {2,4,8,16,32} at precision 64 and {4,8,16,32,64} at 32.
+ * 5NN / 6NN are the same with a 32-B instead of a 16-B segment of x per lane
+ * and hop; NN in {4,8,16,32,64} at precision 64 and {8,16,32,64} at 32, and
+ * 528 / 628 for 128 columns at precision 32.
  * These variants read x only at rows of the column's sector: rows outside it
  * must hold zero (the Lanczos buffers keep them zero). */
 size_t rsed_proj_scratch_bytes(int64_t n_orbits);

@@ -123,25 +123,35 @@ struct ProjTypes<32> {
   using Real = float;
 };
 
+// CPL contiguous columns of one x row, loaded as 16-B vectors (two FP32 or one
+// FP64 complex value each); vectors at or beyond the row's leading dimension
+// read as zero, so a lane's segment never leaves its row.
 template <int PREC, int CPL>
-struct XVec;
-template <>
-struct XVec<64, 1> {
-  double2 v[1];
-  __device__ __forceinline__ void load(const void* base) { v[0] = __ldg(reinterpret_cast<const double2*>(base)); }
-  __device__ __forceinline__ void zero() { v[0] = make_double2(0.0, 0.0); }
-};
-template <>
-struct XVec<32, 2> {
-  float2 v[2];
-  __device__ __forceinline__ void load(const void* base) {
-    const float4 q = __ldg(reinterpret_cast<const float4*>(base));
-    v[0] = make_float2(q.x, q.y);
-    v[1] = make_float2(q.z, q.w);
+struct XVec {
+  using W = typename ProjTypes<PREC>::W;
+  static constexpr int kPer = (PREC == 64) ? 1 : 2;  // columns per 16-B vector
+  static constexpr int kVec = CPL / kPer;
+  W v[CPL];
+  __device__ __forceinline__ void load(const char* base, int avail) {
+#pragma unroll
+    for (int k = 0; k < kVec; ++k) {
+      if (k * kPer < avail) {
+        if constexpr (PREC == 64) {
+          v[k] = __ldg(reinterpret_cast<const double2*>(base) + k);
+        } else {
+          const float4 q = __ldg(reinterpret_cast<const float4*>(base) + k);
+          v[2 * k] = make_float2(q.x, q.y);
+          v[2 * k + 1] = make_float2(q.z, q.w);
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < kPer; ++j) v[k * kPer + j].x = v[k * kPer + j].y = 0;
+      }
+    }
   }
   __device__ __forceinline__ void zero() {
-    v[0] = make_float2(0.f, 0.f);
-    v[1] = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int j = 0; j < CPL; ++j) v[j].x = v[j].y = 0;
   }
 };
 
@@ -150,12 +160,11 @@ __device__ __forceinline__ T ld_stream(const T* p) {
   return __ldcs(p);
 }
 
-template <int PREC, int L, int U>
+template <int PREC, int L, int CPL, int U>
 __global__ void __launch_bounds__(256) k_proj_spmv(rsed_model_t md, rsed_sectors_t sc, const void* __restrict__ xin,
                                                    double2* __restrict__ y, int chunk0) {
   using W = typename ProjTypes<PREC>::W;
   using Real = typename ProjTypes<PREC>::Real;
-  constexpr int CPL = (PREC == 64) ? 1 : 2;
   constexpr int EPW = 32 / L;
   constexpr int NC = L * CPL;
   extern __shared__ __align__(16) unsigned char smem[];
@@ -180,18 +189,18 @@ __global__ void __launch_bounds__(256) k_proj_spmv(rsed_model_t md, rsed_sectors
   const int eslot = lane / L;
   const int c0 = (chunk0 + (int)blockIdx.y) * NC + (lane % L) * CPL;
   const int64_t ld = sc.ld;
+  const int avail = (int)ld - c0;
   int sec[CPL];
-  bool colv[CPL];
+  bool colv[CPL], fresh[CPL];
 #pragma unroll
   for (int j = 0; j < CPL; ++j) {
     colv[j] = c0 + j < sc.n_cols;
-    sec[j] = colv[j] ? sc.col_sector[c0 + j] : 0;
+    sec[j] = colv[j] ? sc.col_sector[c0 + j] : -1;
+    // the block vectors of one sector sit in adjacent columns, so a lane's
+    // columns usually share the hop weight
+    fresh[j] = (j == 0) || sec[j] != sec[j - 1];
   }
-  bool same = true;
-#pragma unroll
-  for (int j = 1; j < CPL; ++j) same = same && sec[j] == sec[0];
   const char* xb = reinterpret_cast<const char*>(xin) + (size_t)c0 * sizeof(W);
-  constexpr size_t kRowBytes = sizeof(W);
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
   for (int64_t r = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < md.n_orbits; r += warps) {
     const uint64_t memr = sc.member[r];
@@ -225,7 +234,7 @@ __global__ void __launch_bounds__(256) k_proj_spmv(rsed_model_t md, rsed_sectors
 #pragma unroll
         for (int u = 0; u < U; ++u) {
           if (cgv[u] != 0xffffffffu && any)
-            xv[u].load(xb + (size_t)(cgv[u] & kOrbitMask) * ld * kRowBytes);
+            xv[u].load(xb + (size_t)(cgv[u] & kOrbitMask) * ld * sizeof(W), avail);
           else
             xv[u].zero();
         }
@@ -237,9 +246,7 @@ __global__ void __launch_bounds__(256) k_proj_spmv(rsed_model_t md, rsed_sectors
 #pragma unroll
           for (int j = 0; j < CPL; ++j) {
             if (!on[j]) continue;
-            // the block vectors of one sector sit in adjacent columns, so a
-            // lane's columns usually share the weight
-            if (j == 0 || !same) {
+            if (fresh[j] || !on[j - (j > 0)]) {
               const W ch = chg[sec[j]];
               wcx = wv[u].x * ch.x - wv[u].y * ch.y;
               wcy = wv[u].x * ch.y + wv[u].y * ch.x;
@@ -277,21 +284,22 @@ __global__ void __launch_bounds__(256) k_proj_spmv(rsed_model_t md, rsed_sectors
   }
 }
 
-template <int PREC, int L, int U>
+template <int PREC, int L, int CPL>
 int launch_spmv(const rsed_model_t& md, const rsed_sectors_t& sc, const void* x, double2* y, bool sequential,
                 cudaStream_t stream) {
   using W = typename ProjTypes<PREC>::W;
-  constexpr int NC = L * ((PREC == 64) ? 1 : 2);
+  constexpr int U = 4;
+  constexpr int NC = L * CPL;
+  auto kern = k_proj_spmv<PREC, L, CPL, U>;
   const size_t smem = sizeof(W) * (size_t)sc.n_sectors * md.n_group;
   static int blocks_per_sm[16] = {0};  // per device, computed once
   int dev = 0;
   RSED_TRY_CUDA(cudaGetDevice(&dev));
   int& bps = blocks_per_sm[dev & 15];
   if (smem > 48 * 1024)
-    RSED_TRY_CUDA(cudaFuncSetAttribute(k_proj_spmv<PREC, L, U>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem));
+    RSED_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   if (bps == 0) {
-    RSED_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_proj_spmv<PREC, L, U>, 256, smem));
+    RSED_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, 256, smem));
     if (bps < 1) bps = 1;
   }
   static int n_sm = 0;
@@ -301,11 +309,11 @@ int launch_spmv(const rsed_model_t& md, const rsed_sectors_t& sc, const void* x,
   const int64_t gx = row_blocks < (int64_t)n_sm * bps ? row_blocks : (int64_t)n_sm * bps;
   if (sequential) {
     for (int c = 0; c < n_chunks; ++c) {
-      k_proj_spmv<PREC, L, U><<<dim3((unsigned)gx, 1), 256, smem, stream>>>(md, sc, x, y, c);
+      kern<<<dim3((unsigned)gx, 1), 256, smem, stream>>>(md, sc, x, y, c);
       RSED_CHECK_LAUNCH();
     }
   } else {
-    k_proj_spmv<PREC, L, U><<<dim3((unsigned)gx, (unsigned)n_chunks), 256, smem, stream>>>(md, sc, x, y, 0);
+    kern<<<dim3((unsigned)gx, (unsigned)n_chunks), 256, smem, stream>>>(md, sc, x, y, 0);
     RSED_CHECK_LAUNCH();
   }
   return RSED_OK;
@@ -325,7 +333,7 @@ int check_proj_model(const rsed_model_t* md) {
 
 }  // namespace
 
-// Called by rsed_apply_h for variants 0 (with a table present), 3NN and 4NN.
+// Called by rsed_apply_h for variants 0 (with a table present), 3NN-6NN.
 int rsed_proj_apply(const rsed_model_t& md, const rsed_sectors_t& sc, const void* x, double2* y, int precision,
                     int variant, cudaStream_t stream) {
   RSED_REQUIRE(md.proj_rowptr && md.proj_cg, RSED_EINVAL, "no projection table in the model");
@@ -333,56 +341,71 @@ int rsed_proj_apply(const rsed_model_t& md, const rsed_sectors_t& sc, const void
                "projection table has no weights for precision %d", precision);
   RSED_REQUIRE((sc.ld & 1) == 0 && (reinterpret_cast<uintptr_t>(x) & 15) == 0, RSED_EINVAL,
                "projection apply needs an even leading dimension and a 16-byte aligned x");
-  const size_t s = precision == 64 ? 16 : 8;
-  (void)s;
   if (variant == 0) {
-    // Measured on B200: at scale (x larger than L2) the widest chunk wins,
-    // since the gathered row segments then use whole 128-B lines and the
-    // table streams once; small bases (latency-bound) prefer 16 columns per
-    // chunk with all chunks in one launch for more warps in flight.
-    const int opts64[5] = {2, 4, 8, 16, 32}, opts32[5] = {4, 8, 16, 32, 64};
-    const int* opts = precision == 64 ? opts64 : opts32;
-    int nc = opts[4];
+    // Measured on B200 (657,756 orbits, 64 columns): FP32 runs best with a
+    // 32-B x segment per lane (4 columns) and one chunk covering up to 64
+    // columns (3.7 ms vs 4.5 ms with 16-B segments); FP64 with 16-B segments
+    // and 16-column chunks, one after another (7.5 ms; wider segments spill
+    // into lower occupancy).  Small (latency-bound) bases prefer 16 columns
+    // per chunk with all chunks in one launch, for more warps in flight.
     if (md.n_orbits < 65536) {
-      nc = 16;
+      variant = 416;
+    } else if (precision == 32) {
+      int nc = 8;
+      while (nc < sc.n_cols && nc < 64) nc *= 2;
+      variant = 500 + nc;
     } else {
-      for (int i = 0; i < 5; ++i)
-        if (opts[i] >= sc.n_cols) {
-          nc = opts[i];
-          break;
-        }
+      int nc = 2;
+      while (nc < sc.n_cols && nc < 16) nc *= 2;
+      variant = 300 + nc;
     }
-    variant = (md.n_orbits < 65536 ? 400 : 300) + nc;
   }
-  const int family = variant / 100;  // 3/4: 4 hops per slot and batch, 5/6: 8
+  const int family = variant / 100;  // 3/4: 16-B segment per lane, 5/6: 32-B segment
   const bool seq = family == 3 || family == 5;
-  const bool deep = family >= 5;
-  const int nc = variant % 100;
+  const bool wide = family >= 5;
+  const int nc = variant % 100 + (variant % 100 == 28 ? 100 : 0);  // 528 / 628 = 128 columns
   if (family >= 3 && family <= 6) {
-#define RSED_PROJ_CASE(P, NCOLS, LANES)                                                     \
-  case NCOLS:                                                                               \
-    return deep ? launch_spmv<P, LANES, 8>(md, sc, x, y, seq, stream)                       \
-                : launch_spmv<P, LANES, 4>(md, sc, x, y, seq, stream);
     if (precision == 64) {
-      switch (nc) {
-        RSED_PROJ_CASE(64, 2, 2)
-        RSED_PROJ_CASE(64, 4, 4)
-        RSED_PROJ_CASE(64, 8, 8)
-        RSED_PROJ_CASE(64, 16, 16)
-        RSED_PROJ_CASE(64, 32, 32)
-        default: break;
+      if (!wide) {
+        switch (nc) {
+          case 2: return launch_spmv<64, 2, 1>(md, sc, x, y, seq, stream);
+          case 4: return launch_spmv<64, 4, 1>(md, sc, x, y, seq, stream);
+          case 8: return launch_spmv<64, 8, 1>(md, sc, x, y, seq, stream);
+          case 16: return launch_spmv<64, 16, 1>(md, sc, x, y, seq, stream);
+          case 32: return launch_spmv<64, 32, 1>(md, sc, x, y, seq, stream);
+          default: break;
+        }
+      } else {
+        switch (nc) {
+          case 4: return launch_spmv<64, 2, 2>(md, sc, x, y, seq, stream);
+          case 8: return launch_spmv<64, 4, 2>(md, sc, x, y, seq, stream);
+          case 16: return launch_spmv<64, 8, 2>(md, sc, x, y, seq, stream);
+          case 32: return launch_spmv<64, 16, 2>(md, sc, x, y, seq, stream);
+          case 64: return launch_spmv<64, 32, 2>(md, sc, x, y, seq, stream);
+          default: break;
+        }
       }
     } else {
-      switch (nc) {
-        RSED_PROJ_CASE(32, 4, 2)
-        RSED_PROJ_CASE(32, 8, 4)
-        RSED_PROJ_CASE(32, 16, 8)
-        RSED_PROJ_CASE(32, 32, 16)
-        RSED_PROJ_CASE(32, 64, 32)
-        default: break;
+      if (!wide) {
+        switch (nc) {
+          case 4: return launch_spmv<32, 2, 2>(md, sc, x, y, seq, stream);
+          case 8: return launch_spmv<32, 4, 2>(md, sc, x, y, seq, stream);
+          case 16: return launch_spmv<32, 8, 2>(md, sc, x, y, seq, stream);
+          case 32: return launch_spmv<32, 16, 2>(md, sc, x, y, seq, stream);
+          case 64: return launch_spmv<32, 32, 2>(md, sc, x, y, seq, stream);
+          default: break;
+        }
+      } else {
+        switch (nc) {
+          case 8: return launch_spmv<32, 2, 4>(md, sc, x, y, seq, stream);
+          case 16: return launch_spmv<32, 4, 4>(md, sc, x, y, seq, stream);
+          case 32: return launch_spmv<32, 8, 4>(md, sc, x, y, seq, stream);
+          case 64: return launch_spmv<32, 16, 4>(md, sc, x, y, seq, stream);
+          case 128: return launch_spmv<32, 32, 4>(md, sc, x, y, seq, stream);
+          default: break;
+        }
       }
     }
-#undef RSED_PROJ_CASE
   }
   return rsed_set_error(RSED_EINVAL, "projection apply variant %d invalid at precision %d", variant, precision);
 }

@@ -73,12 +73,14 @@ def test_projection_variants_match_on_the_fly(golden, case):
     dm.apply_block(sset, cs, Xf, Yref32, precision=32, variant=0)
     dm.build_projection(sset.sqrt_stab)
     try:
-        for v in (302, 304, 308, 316, 332, 402, 404, 408, 416, 432):
+        for v in (302, 304, 308, 316, 332, 402, 404, 408, 416, 432, 504, 508, 516, 532, 564, 604, 608, 616,
+                  632, 664):
             Y = torch.full_like(X, complex("nan"))
             dm.apply_block(sset, cs, X, Y, variant=v)
             assert (Y[:, :ns] - Yref[:, :ns]).abs().max().item() < 1e-13, v
         nrm = Yref32[:, :ns].abs().max().item()
-        for v in (304, 308, 316, 332, 364, 404, 408, 416, 432, 464):
+        for v in (304, 308, 316, 332, 364, 404, 408, 416, 432, 464, 508, 516, 532, 564, 528, 608, 616, 632,
+                  664, 628):
             Y = torch.full_like(X, complex("nan"))
             dm.apply_block(sset, cs, Xf, Y, precision=32, variant=v)
             assert (Y[:, :ns] - Yref32[:, :ns]).abs().max().item() < 2e-6 * nrm, v
@@ -99,8 +101,9 @@ def test_projection_rejects_bad_variant(golden):
     try:
         with pytest.raises(ValueError):
             dm.apply_block(sset, cs, X.to(torch.complex64), Y, precision=32, variant=308)  # no FP32 weights
-        with pytest.raises(ValueError):
-            dm.apply_block(sset, cs, X, Y, variant=303)
+        for bad in (303, 502, 700):
+            with pytest.raises(ValueError):
+                dm.apply_block(sset, cs, X, Y, variant=bad)
     finally:
         dm.drop_projection()
     assert _lib.lib() is not None
