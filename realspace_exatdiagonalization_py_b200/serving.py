@@ -1,0 +1,420 @@
+"""Continuous-batching eigen-solve service.
+
+A request is one (lattice model, momentum sector, flux point) eigen-solve.
+The server keeps, per lattice model, the zero-flux orbit catalog, and per flux
+point a ``FluxContext``: a copy of that catalog whose amplitudes were moved to
+the flux point by ``update_orbit_stabilizer_phases`` (no rebuild), the twisted
+device model, the sector membership and the projection table.  Requests run in
+*lanes*: a lane is a resident ``LanczosBatch`` (Krylov basis, projected
+matrices, state) of 1..``max_width`` instances on its own CUDA stream, bound
+to one flux point and reused by later requests of that flux point.
+
+Scheduling (``step``), one host thread, no blocking waits on the device:
+  * admission: pending requests are grouped by (model, flux); a group takes an
+    idle lane of its flux point or a new one, as many requests per lane as
+    arrived together (up to ``max_width``).  A new lane or flux context is
+    admitted only while the device bytes they need (measured for contexts,
+    computed for lanes) fit the budget; idle contexts and lanes are evicted
+    (least recently used) to make room.  Requests that do not fit wait.
+  * progress: every running lane gets ``poll`` more Lanczos iterations on its
+    stream, followed by an asynchronous copy of its state into pinned host
+    memory and an event; lanes whose event completed and whose instances all
+    stopped move on to the FP64 Rayleigh-Ritz refinement (FP32 matvec) and
+    the asynchronous copy of their eigenvalues.  Lanes on different streams
+    overlap on the device; a request arriving while others run is admitted at
+    the next step as soon as a lane and memory are free.
+
+Each request's start block is drawn on the device from a generator seeded with
+``12345 + seed`` (the request id by default), so a result does not depend on
+which other requests share the device or its lane.
+"""
+
+from __future__ import annotations
+
+import time
+from collections import OrderedDict
+from dataclasses import dataclass, field
+from fractions import Fraction
+
+import numpy as np
+import torch
+
+from . import _lib
+from .batched import APPLY_AUTO, lanczos_footprint_bytes
+from .catalog import build_symmetry_orbit_catalog, update_orbit_stabilizer_phases
+from .hamiltonian import DeviceModel
+from .lanczos import S_ACTIVE, S_ITERS, S_STATUS, LanczosBatch, LanczosParams
+from .lattice import generate_bilinear_terms
+from .sector import SectorSet
+from .symmetry import build_irrep_list, build_translation_group
+
+__all__ = ["ServingModel", "FluxContext", "SolveRequest", "SolveResult", "SolveServer", "latency_summary"]
+
+
+@dataclass
+class SolveRequest:
+    rid: int
+    sector: int                      # irrep index (0-based, the reference's result key)
+    flux: tuple = ()                 # twisted phases over 2 pi, one per lattice dimension
+    model: str = "default"
+    arrival: float = 0.0             # seconds after the start of the run
+    seed: int | None = None          # start-block seed offset (default: rid)
+
+
+@dataclass
+class SolveResult:
+    rid: int
+    sector: int
+    flux: tuple
+    model: str
+    eigenvalues: np.ndarray
+    residuals: np.ndarray
+    fp32_error: np.ndarray | None
+    iterations: int
+    dim: int
+    arrival: float
+    admitted: float
+    finished: float
+    lane: int
+    lane_width: int
+
+    @property
+    def latency(self) -> float:
+        return self.finished - self.arrival
+
+
+class ServingModel:
+    """One lattice model: its zero-flux catalog, shared by every flux point."""
+
+    def __init__(self, second_quantized_model, n_filled: int, name: str = "default"):
+        self.name = name
+        self.model = second_quantized_model
+        self.n_filled = int(n_filled)
+        self.lattice = second_quantized_model.lattice
+        self.stats = second_quantized_model.particle_statistics
+        self.group0 = build_translation_group(self.lattice)
+        self.catalog = build_symmetry_orbit_catalog(
+            second_quantized_model=second_quantized_model, n_filled=self.n_filled,
+            symmetry_group=self.group0, particle_statistics=self.stats)
+        self.n_orbits = self.catalog.n_orbits
+        self.n_sectors = len(build_irrep_list(self.group0, self.lattice))
+        self.ctx_bytes: int | None = None  # measured device bytes of a flux point, once one was built
+
+    def normalize_flux(self, flux) -> tuple:
+        f = tuple(float(x) for x in (flux or ()))
+        if not f:
+            f = (0.0,) * self.lattice.dim
+        if len(f) != self.lattice.dim:
+            raise ValueError(f"flux needs {self.lattice.dim} components")
+        return f
+
+
+class FluxContext:
+    """Device state of one flux point of one model."""
+
+    def __init__(self, sm: ServingModel, flux: tuple, precision: int, projection: bool = True):
+        self.sm = sm
+        self.flux = flux
+        before = torch.cuda.memory_allocated()
+        if any(flux):
+            terms = generate_bilinear_terms(sm.model.tb_model, twisted_phases_over_2π=list(flux))
+            group = build_translation_group(sm.lattice, list(flux))
+            cat = sm.catalog.clone()
+            update_orbit_stabilizer_phases(cat, group, sm.stats)
+        else:
+            terms, group, cat = sm.model.bilinear_terms, sm.group0, sm.catalog
+        self.catalog = cat
+        self.irreps = build_irrep_list(group, sm.lattice)
+        self.dm = DeviceModel(cat, terms, sm.model.density_density_terms)
+        self.sset = SectorSet(cat, self.irreps)
+        if projection:
+            self.dm.build_projection(self.sset.sqrt_stab, precisions=(precision,))
+        torch.cuda.synchronize()
+        self.bytes = max(0, torch.cuda.memory_allocated() - before)
+        if any(flux):
+            sm.ctx_bytes = max(sm.ctx_bytes or 0, self.bytes)
+        self.lanes: list[_Lane] = []
+        self.last_used = time.perf_counter()
+
+    def busy(self) -> bool:
+        return any(ln.state != "idle" for ln in self.lanes)
+
+
+class _Lane:
+    _ids = 0
+
+    def __init__(self, ctx: FluxContext, width: int, nev: int, params: LanczosParams, poll: int,
+                 graph: bool):
+        _Lane._ids += 1
+        self.id = _Lane._ids
+        self.ctx = ctx
+        self.width = width
+        self.nev = nev
+        self.params = params
+        self.poll = poll
+        self.use_graph = graph
+        self.stream = torch.cuda.Stream()
+        self.batch: LanczosBatch | None = None
+        self.graph = None
+        self.state = "idle"
+        self.reqs: list[SolveRequest] = []
+        self.admitted = 0.0
+        self.event = torch.cuda.Event()
+        self.h_state = None
+        self.h_vals = self.h_res = self.h_fp32 = None
+        self.bytes = lanczos_footprint_bytes(ctx.sset.catalog.n_orbits, width * params.block, params.n_slots,
+                                             params.precision)
+
+    # -- device work (all on the lane's stream) ----------------------------
+    def _start_blocks(self):
+        out = []
+        for r in self.reqs:
+            d = self.ctx.sset.dims[r.sector]
+            g = torch.Generator(device="cuda")
+            g.manual_seed(12345 + (r.rid if r.seed is None else r.seed))
+            blk = torch.randn((d, self.params.block), dtype=torch.complex128, device="cuda", generator=g)
+            out.append(blk / torch.linalg.vector_norm(blk, dim=0, keepdim=True))
+        return out
+
+    def begin(self, reqs: list[SolveRequest], now: float) -> None:
+        assert len(reqs) == self.width and self.state == "idle"
+        self.reqs = list(reqs)
+        self.admitted = now
+        sectors = [r.sector for r in reqs]
+        with torch.cuda.stream(self.stream):
+            if self.batch is None:
+                self.batch = LanczosBatch(self.ctx.dm, self.ctx.sset, sectors, self.nev, self.params,
+                                          block_sizes=[self.params.block] * self.width)
+                self.h_state = torch.empty(self.batch.state.shape, dtype=torch.int32).pin_memory()
+                self.h_vals = torch.empty((self.width, self.nev), dtype=torch.float64).pin_memory()
+                self.h_res = torch.empty((self.width, self.nev), dtype=torch.float64).pin_memory()
+                self.h_fp32 = torch.empty((self.width, self.nev), dtype=torch.float64).pin_memory()
+            else:
+                b = self.batch
+                b.inst_sectors = sectors
+                cs = np.concatenate([[s] * self.params.block for s in sectors]).astype(np.int32)
+                b.col_sector.copy_(torch.from_numpy(cs), non_blocking=False)
+            self.batch.load_start(self._start_blocks())
+            self.batch.start()
+            if self.use_graph and self.graph is None:
+                self.graph = self.batch.capture(self.poll)
+            self._advance()
+        self.state = "running"
+        self.ctx.last_used = time.perf_counter()
+
+    def _advance(self) -> None:
+        b = self.batch
+        if self.graph is not None:
+            self.graph.replay()
+        else:
+            b.iterate(self.poll)
+        self.h_state.copy_(b.state, non_blocking=True)
+        self.event.record(self.stream)
+
+    def _finish(self) -> None:
+        b = self.batch
+        if self.params.precision == 32:
+            fp32 = b.ritz_val[:, : self.nev].clone()
+            b.rayleigh_ritz()
+            self.h_fp32.copy_((fp32 - b.ritz_val[:, : self.nev]).abs(), non_blocking=True)
+        self.h_vals.copy_(b.ritz_val[:, : self.nev], non_blocking=True)
+        self.h_res.copy_(b.resid[:, : self.nev], non_blocking=True)
+        self.h_state.copy_(b.state, non_blocking=True)
+        self.event.record(self.stream)
+
+    def poll_once(self, now: float, max_iter: int) -> list[SolveResult] | None:
+        """Advance the lane if its last work completed; results when done."""
+        if self.state == "idle" or not self.event.query():
+            return None
+        st = self.h_state.numpy()
+        with torch.cuda.stream(self.stream):
+            if self.state == "running":
+                if st[:, S_ACTIVE].any() and st[:, S_ITERS].max() < max_iter:
+                    self._advance()
+                    return None
+                bad = [i for i in range(self.width) if st[i, S_STATUS] != 1]
+                if bad:
+                    code = int(st[bad[0], S_STATUS]) or _lib.RSED_ENOTCONV
+                    self.state = "idle"
+                    raise _lib.RsedError(code, f"lane {self.id}: requests {[self.reqs[i].rid for i in bad]} "
+                                               f"did not converge")
+                self._finish()
+                self.state = "finishing"
+                return None
+        # finishing: results are in pinned memory
+        out = []
+        for i, r in enumerate(self.reqs):
+            out.append(SolveResult(
+                rid=r.rid, sector=r.sector, flux=r.flux, model=r.model,
+                eigenvalues=self.h_vals[i].numpy().copy(), residuals=self.h_res[i].numpy().copy(),
+                fp32_error=self.h_fp32[i].numpy().copy() if self.params.precision == 32 else None,
+                iterations=int(st[i, S_ITERS]), dim=int(self.ctx.sset.dims[r.sector]), arrival=r.arrival,
+                admitted=self.admitted, finished=now, lane=self.id, lane_width=self.width))
+        self.state = "idle"
+        self.reqs = []
+        self.ctx.last_used = time.perf_counter()
+        return out
+
+
+class SolveServer:
+    """Continuous-batching server over one or more ``ServingModel``s."""
+
+    def __init__(self, models: dict[str, ServingModel] | ServingModel, *, nev: int = 4, precision: int = 32,
+                 block: int = 4, n_slots: int = 16, poll: int = 16, max_width: int = 4,
+                 memory_budget: int | None = None, projection: bool = True, graph: bool | None = None,
+                 max_iter: int = 4000):
+        if isinstance(models, ServingModel):
+            models = {models.name: models}
+        self.models = dict(models)
+        self.nev = nev
+        self.precision = precision
+        self.params = LanczosParams(block=block, n_slots=n_slots, precision=precision,
+                                    apply_variant=APPLY_AUTO)
+        self.poll = poll
+        self.max_width = max_width
+        self.projection = projection
+        self.graph = graph
+        self.max_iter = max_iter
+        if memory_budget is None:
+            free, _ = torch.cuda.mem_get_info()
+            memory_budget = int(0.8 * free)
+        self.budget = memory_budget
+        self.contexts: OrderedDict[tuple, FluxContext] = OrderedDict()
+        self.pending: list[SolveRequest] = []
+        self.t0 = time.perf_counter()
+        self.peak_running = 0
+        self.admissions = 0
+
+    # -- memory ------------------------------------------------------------
+    def used_bytes(self) -> int:
+        return sum(c.bytes + sum(ln.bytes for ln in c.lanes) for c in self.contexts.values())
+
+    def _ctx_estimate(self, sm: ServingModel) -> int:
+        if sm.ctx_bytes:
+            return sm.ctx_bytes
+        n = sm.n_orbits
+        return int(sm.catalog.n_states * 16 + n * 64 + n * 74 * (4 + 8 * (self.precision // 32)))
+
+    def _evict(self, need: int) -> bool:
+        """Drop idle lanes, then idle contexts, least recently used first,
+        until ``need`` more bytes fit; False if they cannot."""
+        if self.used_bytes() + need <= self.budget:
+            return True
+        for key, c in sorted(self.contexts.items(), key=lambda kv: kv[1].last_used):
+            for ln in [ln for ln in c.lanes if ln.state == "idle"]:
+                c.lanes.remove(ln)
+                if self.used_bytes() + need <= self.budget:
+                    torch.cuda.empty_cache()
+                    return True
+            if not c.lanes and not c.busy():
+                del self.contexts[key]
+                if self.used_bytes() + need <= self.budget:
+                    torch.cuda.empty_cache()
+                    return True
+        torch.cuda.empty_cache()
+        return self.used_bytes() + need <= self.budget
+
+    def _lane_bytes(self, sm: ServingModel, width: int) -> int:
+        return lanczos_footprint_bytes(sm.n_orbits, width * self.params.block, self.params.n_slots, self.precision)
+
+    # -- API -----------------------------------------------------------------
+    def now(self) -> float:
+        return time.perf_counter() - self.t0
+
+    def submit(self, req: SolveRequest) -> None:
+        sm = self.models[req.model]
+        req.flux = sm.normalize_flux(req.flux)
+        if not 0 <= req.sector < sm.n_sectors:
+            raise ValueError(f"request {req.rid}: no sector {req.sector}")
+        self.pending.append(req)
+
+    def running(self) -> int:
+        return sum(1 for c in self.contexts.values() for ln in c.lanes if ln.state != "idle")
+
+    def _admit(self, now: float) -> None:
+        groups: OrderedDict[tuple, list[SolveRequest]] = OrderedDict()
+        for r in self.pending:
+            groups.setdefault((r.model, r.flux), []).append(r)
+        admitted: set[int] = set()
+        for key, reqs in groups.items():
+            sm = self.models[key[0]]
+            while reqs:
+                ctx = self.contexts.get(key)
+                if ctx is not None:
+                    idle = [ln for ln in ctx.lanes if ln.state == "idle" and ln.width <= len(reqs)]
+                    lane = max(idle, key=lambda ln: ln.width) if idle else None
+                else:
+                    lane = None
+                if lane is None:
+                    width = min(len(reqs), self.max_width)
+                    need = self._lane_bytes(sm, width) + (0 if ctx is not None else self._ctx_estimate(sm))
+                    if not self._evict(need):
+                        break
+                    if ctx is None:
+                        ctx = FluxContext(sm, key[1], self.precision, self.projection)
+                        self.contexts[key] = ctx
+                    use_graph = self.graph if self.graph is not None else sm.n_orbits < 65536
+                    lane = _Lane(ctx, width, self.nev, self.params, self.poll, use_graph)
+                    ctx.lanes.append(lane)
+                take, reqs[:] = reqs[: lane.width], reqs[lane.width:]
+                lane.begin(take, now)
+                self.admissions += 1
+                admitted.update(r.rid for r in take)
+        if admitted:
+            self.pending = [r for r in self.pending if r.rid not in admitted]
+
+    def step(self) -> list[SolveResult]:
+        """One scheduling round; returns the requests that finished in it."""
+        now = self.now()
+        done: list[SolveResult] = []
+        for c in list(self.contexts.values()):
+            for ln in c.lanes:
+                res = ln.poll_once(now, self.max_iter)
+                if res:
+                    done.extend(res)
+        if self.pending:
+            self._admit(self.now())
+        self.peak_running = max(self.peak_running, self.running())
+        return done
+
+    def run(self, requests: list[SolveRequest], *, realtime: bool = True, timeout: float = 600.0
+            ) -> list[SolveResult]:
+        """Serve ``requests``, each submitted at its ``arrival`` time (seconds
+        after the start of this call; all at once if ``realtime`` is false)."""
+        order = sorted(requests, key=lambda r: r.arrival)
+        self.t0 = time.perf_counter()
+        results: list[SolveResult] = []
+        i = 0
+        while len(results) < len(order):
+            now = self.now()
+            if now > timeout:
+                raise TimeoutError(f"{len(order) - len(results)} requests unfinished after {timeout} s")
+            while i < len(order) and (not realtime or order[i].arrival <= now):
+                self.submit(order[i])
+                i += 1
+            got = self.step()
+            results.extend(got)
+            if not got and self.running() == 0 and not self.pending and i < len(order):
+                time.sleep(max(0.0, min(0.002, order[i].arrival - self.now())))
+        return results
+
+
+def latency_summary(results: list[SolveResult]) -> dict:
+    lat = np.array([r.latency for r in results])
+    span = max(r.finished for r in results) - min(r.arrival for r in results)
+    return {"requests": len(results), "throughput_per_s": len(results) / span if span > 0 else None,
+            "p50_ms": 1e3 * float(np.percentile(lat, 50)), "p99_ms": 1e3 * float(np.percentile(lat, 99)),
+            "mean_ms": 1e3 * float(lat.mean()), "max_ms": 1e3 * float(lat.max())}
+
+
+def poisson_requests(n: int, rate: float, n_sectors: int, flux_grid: int, *, dim: int = 2, seed: int = 0,
+                     model: str = "default") -> list[SolveRequest]:
+    """``n`` requests with exponential inter-arrival times (rate per second),
+    uniform sector and uniform flux point on a ``flux_grid``^dim grid in
+    [0, 1)^dim (units of 2 pi), all from ``numpy.random.default_rng(seed)``."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, size=n)) if rate > 0 else np.zeros(n)
+    sec = rng.integers(0, n_sectors, size=n)
+    fl = rng.integers(0, flux_grid, size=(n, dim))
+    return [SolveRequest(rid=i, sector=int(sec[i]), flux=tuple(float(Fraction(int(k), flux_grid)) for k in fl[i]),
+                         model=model, arrival=float(t[i])) for i in range(n)]
