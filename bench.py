@@ -313,6 +313,54 @@ def matvec_at_scale(ed, models, peak_gbs, n_launch=20, precisions=(32, 64), per_
     return out
 
 
+def serving_at_scale(ed, models, n_req=32, rate=20.0, block=2, plain_samples=2):
+    """The request loop at the 32-site Haldane size: a Poisson stream (seed 0)
+    of (sector, flux) requests over a 16 x 16 flux grid and 16 sectors,
+    served with continuous batching (FP32 matvec + FP64 refinement, nev 4),
+    against the plain FP64 path (one request at a time, block 1, no graph,
+    host polling every iteration) on the first requests of the stream."""
+    import torch
+    from realspace_exatdiagonalization_py_b200.serving import poisson_requests
+
+    model, nf = models.config_model("haldane32")
+    sm = ed.ServingModel(model, nf, name="haldane32")
+    reqs = poisson_requests(n_req, rate=rate, n_sectors=sm.n_sectors, flux_grid=16, model="haldane32", seed=0)
+    srv = ed.SolveServer(sm, nev=4, precision=32, block=block, poll=8)
+    srv.run([ed.SolveRequest(10 ** 6, 0, (0.5, 0.5), "haldane32")], realtime=False)  # warm-up
+    res = srv.run([ed.SolveRequest(r.rid, r.sector, r.flux, r.model, r.arrival) for r in reqs], realtime=True)
+    summ = ed.latency_summary(res)
+    by_id = {r.rid: r for r in res}
+    out = {"workload": f"haldane32 requests: {n_req} Poisson arrivals at {rate}/s (seed 0), uniform sector of "
+                       f"{sm.n_sectors}, uniform flux on 16x16, nev 4", **summ,
+           "block": block, "peak_concurrent_lanes": srv.peak_running, "flux_contexts": len(srv.contexts),
+           "device_GB_in_use": srv.used_bytes() / 1e9,
+           "fp32_error_before_refinement_max": float(max(r.fp32_error.max() for r in res)),
+           "iterations": [min(r.iterations for r in res), max(r.iterations for r in res)]}
+    del srv
+    torch.cuda.empty_cache()
+    # plain FP64 path on the first requests
+    plain_t, dE = [], []
+    for r in reqs[:plain_samples]:
+        ctx = ed.FluxContext(sm, sm.normalize_flux(r.flux), 64, projection=True)
+        p = ed.LanczosParams(block=1, n_slots=48, precision=64, check_every=1)
+        b = ed.LanczosBatch(ctx.dm, ctx.sset, [r.sector], 4, p)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        b.load_start(None)
+        b.start()
+        b.run(poll=1, graph=False)
+        torch.cuda.synchronize()
+        plain_t.append(time.perf_counter() - t0)
+        dE.append(float(np.max(np.abs(b.eigenvalues()[0] - by_id[r.rid].eigenvalues))))
+        del b, ctx
+        torch.cuda.empty_cache()
+    plain_rate = len(plain_t) / sum(plain_t)
+    out.update({"plain_fp64_solves_per_s": plain_rate, "plain_fp64_s_per_solve": plain_t,
+                "served_over_plain": summ["throughput_per_s"] / plain_rate,
+                "max_abs_dE_served_vs_plain_fp64": max(dE)})
+    return out
+
+
 def run_b200(args):
     import torch
 
@@ -485,6 +533,11 @@ def run_b200(args):
                 extra["matvec_at_scale"] = matvec_at_scale(ed, models, peak_gbs)
             except Exception as exc:  # noqa: BLE001 - reported, not fatal
                 extra["matvec_at_scale"] = {"error": repr(exc)}
+            torch.cuda.empty_cache()
+            try:
+                extra["serving_at_scale"] = serving_at_scale(ed, models)
+            except Exception as exc:  # noqa: BLE001 - reported, not fatal
+                extra["serving_at_scale"] = {"error": repr(exc)}
         # CPU baseline: the oracle (reference algorithm) on the host cores
         cpu_rate, cpu_n, _, cpu_t = cpu_sector_solves(model, nf, G, data.irrep_list, nev,
                                                       budget_s=args.cpu_budget)

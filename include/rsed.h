@@ -55,6 +55,15 @@ typedef struct {
   const uint8_t* perm;  /* |G| x N: 0-based image site of site i under g */
   const double* angle;  /* |G| x N: numpy.angle(eta_g(i)) */
   const double* eta;    /* |G| x N complex128: eta_g(i) */
+  /* Two-species bases (particle number fixed per species, e.g. per spin):
+   * species_b marks the sites of species B, which hold n_filled_b of the
+   * n_filled particles; 0 = one species.  States are ranked
+   * rank_A * C(|B|, n_filled_b) + rank_B, each species in colex order over its
+   * own sites; n_states = C(N - |B|, n_filled - n_filled_b) * C(|B|, n_filled_b).
+   * Every group element must map species B onto itself. */
+  uint64_t species_b;
+  int32_t n_filled_b;
+  int32_t reserved_b;
 } rsed_group_t;
 
 /* Hopping / density model on the orbit basis of one catalog. */
@@ -78,6 +87,9 @@ typedef struct {
   const uint32_t* proj_cg;       /* per hop: target orbit | g << 26 */
   const double* proj_w64;        /* per hop complex128 weight, or NULL */
   const float* proj_w32;         /* per hop complex64 weight, or NULL */
+  uint64_t species_b;            /* as in rsed_group_t */
+  int32_t n_filled_b;
+  int32_t reserved_b;
 } rsed_model_t;
 
 /* A set of momentum sectors evaluated together ("columns" of a block of

@@ -67,6 +67,42 @@ def rank(masks: np.ndarray, n: int, bt: np.ndarray) -> np.ndarray:
     return out
 
 
+def species_basis(n: int, k: int, species, bt: np.ndarray):
+    """(C, rank_fn, unrank_fn) of a basis.  ``species = (sb, kb)``: the sites
+    in mask ``sb`` hold ``kb`` particles; rank = rank_A * C(|B|, kb) + rank_B,
+    each species in colex order over its own sites (the device convention;
+    the reference ranks one species only, SRE:122-140)."""
+    if not species:
+        return math.comb(n, k), (lambda m: rank(m, n, bt)), (lambda r: unrank(r, n, k, bt))
+    sb, kb = species
+    sites_b = [i for i in range(n) if (sb >> i) & 1]
+    sites_a = [i for i in range(n) if not (sb >> i) & 1]
+    na, nb, ka = len(sites_a), len(sites_b), k - kb
+    cb = math.comb(nb, kb)
+
+    def compact(m, sites):
+        m = np.asarray(m, dtype=np.uint64)
+        out = np.zeros(m.shape, dtype=np.uint64)
+        for p, st in enumerate(sites):
+            out |= ((m >> np.uint64(st)) & np.uint64(1)) << np.uint64(p)
+        return out
+
+    def deposit(cm, sites):
+        out = np.zeros(cm.shape, dtype=np.uint64)
+        for p, st in enumerate(sites):
+            out |= ((cm >> np.uint64(p)) & np.uint64(1)) << np.uint64(st)
+        return out
+
+    def rank2(m):
+        return rank(compact(m, sites_a), na, bt) * cb + rank(compact(m, sites_b), nb, bt)
+
+    def unrank2(r):
+        r = np.asarray(r, dtype=np.int64)
+        return deposit(unrank(r // cb, na, ka, bt), sites_a) | deposit(unrank(r % cb, nb, kb, bt), sites_b)
+
+    return math.comb(na, ka) * cb, rank2, unrank2
+
+
 def _byte_tables(n: int, perm0: np.ndarray, angle: np.ndarray):
     """Per (g, byte, value): image bits and the byte's angle partial sum,
     bits ascending (SRE:346-374)."""
@@ -106,13 +142,15 @@ def apply_product(m: int, perm0: np.ndarray, eta: np.ndarray, fermion: bool):
     return new, ph * par
 
 
-def catalog(n: int, k: int, perm0: np.ndarray, eta: np.ndarray, fermion: bool, chunk: int = 1 << 16):
+def catalog(n: int, k: int, perm0: np.ndarray, eta: np.ndarray, fermion: bool, chunk: int = 1 << 16,
+            species=None):
     """Orbit catalog: dict with reprs (uint64), stab_g (list of int arrays),
     stab_phase (list of complex128 arrays), rep_rank/rep_sym (int32),
-    rep_amp (complex64) over all C(n, k) states."""
+    rep_amp (complex64) over all C(n, k) states (or the two-species basis of
+    :func:`species_basis`)."""
     ng = perm0.shape[0]
-    C = math.comb(n, k)
     bt = binom_table(n, k)
+    C, rank_fn, unrank_fn = species_basis(n, k, species, bt)
     rep_rank = np.full(C, -1, dtype=np.int32)
     rep_sym = np.zeros(C, dtype=np.int32)
     rep_amp = np.zeros(C, dtype=np.complex64)
@@ -130,12 +168,12 @@ def catalog(n: int, k: int, perm0: np.ndarray, eta: np.ndarray, fermion: bool, c
         stab_ph.append(np.array(ps, dtype=np.complex128))
         for g in range(ng):
             img, a = apply_product(m, perm0[g], eta[g], fermion)
-            idx = int(rank(np.array([img], dtype=np.uint64), n, bt)[0])
+            idx = int(rank_fn(np.array([img], dtype=np.uint64))[0])
             rep_rank[idx] = 0
             rep_sym[idx] = g
             rep_amp[idx] = np.complex64(a)
         return dict(reprs=np.array(reprs, dtype=np.uint64), stab_g=stab_g, stab_phase=stab_ph,
-                    rep_rank=rep_rank, rep_sym=rep_sym, rep_amp=rep_amp, binom=bt)
+                    rep_rank=rep_rank, rep_sym=rep_sym, rep_amp=rep_amp, binom=bt, rank=rank_fn)
     angle = np.angle(eta)
     ptab, atab, nbytes = _byte_tables(n, perm0, angle)
     inv = np.zeros((ng, n, n), dtype=np.int64)
@@ -147,7 +185,7 @@ def catalog(n: int, k: int, perm0: np.ndarray, eta: np.ndarray, fermion: bool, c
                         inv[g, i, j] = 1
     for start in range(0, C, chunk):
         stop = min(start + chunk, C)
-        masks = unrank(np.arange(start, stop, dtype=np.int64), n, k, bt)
+        masks = unrank_fn(np.arange(start, stop, dtype=np.int64))
         best = np.full(stop - start, np.iinfo(np.uint64).max, dtype=np.uint64)
         for g in range(ng):
             img = np.zeros(stop - start, dtype=np.uint64)
@@ -172,7 +210,7 @@ def catalog(n: int, k: int, perm0: np.ndarray, eta: np.ndarray, fermion: bool, c
             for g in range(ng):
                 ninv = (bits * (bits @ inv[g])).sum(axis=1)
                 ph[g, (ninv & 1) == 1] *= -1.0 + 0.0j
-        rk = rank(imgs, n, bt)
+        rk = rank_fn(imgs)
         ids = np.arange(idx0, idx0 + pos.size, dtype=np.int64)
         for g in range(ng):  # ascending g, last writer wins (SRE:556-560)
             rep_rank[rk[g]] = ids
@@ -185,7 +223,12 @@ def catalog(n: int, k: int, perm0: np.ndarray, eta: np.ndarray, fermion: bool, c
             stab_g.append(gs.astype(np.int64))
             stab_ph.append(ph[gs, j].astype(np.complex128))
     return dict(reprs=np.array(reprs, dtype=np.uint64), stab_g=stab_g, stab_phase=stab_ph,
-                rep_rank=rep_rank, rep_sym=rep_sym, rep_amp=rep_amp, binom=bt)
+                rep_rank=rep_rank, rep_sym=rep_sym, rep_amp=rep_amp, binom=bt, rank=rank_fn)
+
+
+def _rank_of(cat: dict, masks, n: int):
+    fn = cat.get("rank")
+    return fn(masks) if fn is not None else rank(masks, n, cat["binom"])
 
 
 def update_phases(cat: dict, n: int, perm0: np.ndarray, eta_new: np.ndarray, fermion: bool) -> dict:
@@ -200,7 +243,7 @@ def update_phases(cat: dict, n: int, perm0: np.ndarray, eta_new: np.ndarray, fer
         m = int(m)
         for g in range(ng):
             img, a = apply_product(m, perm0[g], eta_new[g], fermion)
-            idx = int(rank(np.array([img], dtype=np.uint64), n, bt)[0])
+            idx = int(_rank_of(cat, np.array([img], dtype=np.uint64), n)[0])
             if cat["rep_rank"][idx] == o:
                 cat["rep_sym"][idx] = g
                 cat["rep_amp"][idx] = np.complex64(a)
@@ -248,7 +291,7 @@ def triplets(cat: dict, n: int, orbits: np.ndarray, bilinear, density, chi, ferm
         c = np.nonzero((rm & hop) == frm)[0]
         if c.size == 0:
             continue
-        idx = rank(rm[c] ^ hop, n, bt)
+        idx = _rank_of(cat, rm[c] ^ hop, n)
         crep = cat["rep_rank"][idx]
         keep = np.nonzero(in_basis[crep])[0]
         if keep.size == 0:

@@ -50,6 +50,9 @@ class RsedGroup(ctypes.Structure):
         ("perm", c_void_p),
         ("angle", c_void_p),
         ("eta", c_void_p),
+        ("species_b", ctypes.c_uint64),
+        ("n_filled_b", c_int32),
+        ("reserved_b", c_int32),
     ]
 
 
@@ -74,6 +77,9 @@ class RsedModel(ctypes.Structure):
         ("proj_cg", c_void_p),
         ("proj_w64", c_void_p),
         ("proj_w32", c_void_p),
+        ("species_b", ctypes.c_uint64),
+        ("n_filled_b", c_int32),
+        ("reserved_b", c_int32),
     ]
 
 

@@ -26,6 +26,8 @@ from .symmetry import (
     _lin_table,
     group_arrays,
     group_order,
+    rank_combination,
+    rank_two_species,
 )
 
 __all__ = [
@@ -44,14 +46,22 @@ class DeviceGroup:
     """Group tables uploaded for the kernels (``rsed_group_t``)."""
 
     def __init__(self, G: Finite_Symmetry_Group, n_filled: int, stats: Particle_Statistics,
-                 binom_dev: torch.Tensor | None = None):
+                 binom_dev: torch.Tensor | None = None, species: tuple[int, int] | None = None):
         dev = _device()
         self.group = G
         self.n_site = G.n_site
         self.n_filled = n_filled
         self.n_group = group_order(G)
         self.fermionic = stats is Particle_Statistics.FERMIONIC
-        self.n_states = math.comb(self.n_site, n_filled)
+        # species = (mask of species-B sites, particles on them) or None
+        self.species_b, self.n_filled_b = species if species else (0, 0)
+        if self.species_b:
+            nb = int(self.species_b).bit_count()
+            self.c_b = math.comb(nb, self.n_filled_b)
+            self.n_states = math.comb(self.n_site - nb, n_filled - self.n_filled_b) * self.c_b
+        else:
+            self.c_b = 1
+            self.n_states = math.comb(self.n_site, n_filled)
         perm0, eta, angle = group_arrays(G)
         self.binom_host = _binom_table(self.n_site, n_filled)
         self.binom = binom_dev if binom_dev is not None else torch.from_numpy(self.binom_host).to(dev)
@@ -61,6 +71,7 @@ class DeviceGroup:
         self.c = _lib.RsedGroup(
             self.n_site, n_filled, self.n_group, int(self.fermionic), self.n_states,
             _lib.ptr(self.binom), _lib.ptr(self.perm), _lib.ptr(self.angle), _lib.ptr(self.eta),
+            int(self.species_b), int(self.n_filled_b), 0,
         )
 
 
@@ -174,6 +185,27 @@ class Symmetry_Orbit_Catalog:
             + self.stab_off.numel() * 8 + self.stab_phase.numel() * 16
         )
 
+    @property
+    def species(self) -> tuple[int, int] | None:
+        """(species-B site mask, particles on species B) of a two-species
+        basis, ``None`` for one species."""
+        dg = self.dgroup
+        return (dg.species_b, dg.n_filled_b) if dg.species_b else None
+
+    def rank_of(self, m: int) -> int:
+        """Table index of a basis mask."""
+        dg = self.dgroup
+        if dg.species_b:
+            return rank_two_species(int(m), dg.species_b, self.binom_table, dg.c_b)
+        return rank_combination(int(m), self.binom_table)
+
+    def in_basis(self, m: int) -> bool:
+        m = int(m)
+        if m.bit_count() != self.n_filled or m >> self.n_site:
+            return False
+        dg = self.dgroup
+        return not dg.species_b or (m & dg.species_b).bit_count() == dg.n_filled_b
+
     def clone(self) -> "Symmetry_Orbit_Catalog":
         """Independent copy of the flux-dependent parts (table, stabilizer
         phases); the representative list and stabilizer masks are shared."""
@@ -195,6 +227,7 @@ def build_symmetry_orbit_catalog(
     symmetry_group: Finite_Symmetry_Group,
     particle_statistics: Particle_Statistics,
     stream=None,
+    species: tuple[list[int], int] | None = None,
 ) -> Symmetry_Orbit_Catalog:
     """Partition the fixed-filling Hilbert space into orbits on the GPU.
 
@@ -202,6 +235,12 @@ def build_symmetry_orbit_catalog(
     asserts ``symmetry_group.n_site == lattice.n_site``, ``ValueError`` above
     63 sites; the tables equal the reference's bit for bit (integer tables
     exactly, complex64 amplitudes to the last bit of ``sincos``).
+
+    ``species = (sites_b, n_filled_b)`` (1-based sites) fixes the particle
+    number on those sites as well (e.g. spin-down orbitals at fixed N_down):
+    the basis is then the product of two fixed-filling spaces, ranked
+    ``rank_A * C(|B|, n_filled_b) + rank_B``.  Every group element must map
+    the species-B sites onto themselves.
     """
     n_site = symmetry_group.n_site
     assert n_site == second_quantized_model.lattice.n_site, (
@@ -215,7 +254,8 @@ def build_symmetry_orbit_catalog(
     assert 0 <= n_filled <= n_site
     lib = _lib.lib()
     dev = _device()
-    dg = DeviceGroup(symmetry_group, n_filled, particle_statistics)
+    sp_mask = _species_mask(species, symmetry_group, n_site, n_filled)
+    dg = DeviceGroup(symmetry_group, n_filled, particle_statistics, species=sp_mask)
     sp = _lib.stream_ptr(stream)
     nbytes = lib.rsed_catalog_scratch_bytes(ctypes.byref(dg.c))
     scratch = torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=dev)
@@ -242,6 +282,28 @@ def build_symmetry_orbit_catalog(
                                   repr_masks, stab_mask, stab_off, stab_phase)
 
 
+def _species_mask(species, G: Finite_Symmetry_Group, n_site: int, n_filled: int):
+    if not species:
+        return None
+    sites, kb = species
+    sb = 0
+    for i in sites:
+        if not 1 <= int(i) <= n_site:
+            raise ValueError(f"species site {i} outside 1..{n_site}")
+        sb |= 1 << (int(i) - 1)
+    nb = sb.bit_count()
+    if not (0 < nb < n_site and 0 <= kb <= nb and 0 <= n_filled - kb <= n_site - nb):
+        raise ValueError("species: particle numbers do not fit the two site sets")
+    for op in G.operations:
+        img = 0
+        for i in range(n_site):
+            if (sb >> i) & 1:
+                img |= 1 << (int(op.perm[i]) - 1)
+        if img != sb:
+            raise ValueError(f"symmetry operation {op.label!r} mixes the two species")
+    return sb, int(kb)
+
+
 def update_orbit_stabilizer_phases(
     catalog: Symmetry_Orbit_Catalog,
     new_group: Finite_Symmetry_Group,
@@ -258,7 +320,8 @@ def update_orbit_stabilizer_phases(
     ):
         raise ValueError("update_orbit_stabilizer_phases: the new group must have the same permutations.")
     lib = _lib.lib()
-    dg = DeviceGroup(new_group, catalog.n_filled, particle_statistics, binom_dev=catalog.dgroup.binom)
+    dg = DeviceGroup(new_group, catalog.n_filled, particle_statistics, binom_dev=catalog.dgroup.binom,
+                     species=catalog.species)
     err = torch.zeros(1, dtype=torch.int32, device=catalog.table.device)
     sp = _lib.stream_ptr(stream)
     _lib.check(lib.rsed_phase_update(

@@ -47,6 +47,7 @@ __global__ void __launch_bounds__(256) k_apply(rsed_model_t md, rsed_sectors_t s
   const int q = (int)(gt % LPR);
   if (row >= md.n_orbits) return;
   const int kp1 = md.n_filled + 1;
+  const int64_t cbs = md.species_b ? v.binom[__popcll(md.species_b) * kp1 + md.n_filled_b] : 1;
   const uint64_t m = md.repr_masks[row];
   const uint64_t memr = sc.member[row];
   int col[CPL], sec[CPL];
@@ -136,7 +137,7 @@ __global__ void __launch_bounds__(256) k_apply(rsed_model_t md, rsed_sectors_t s
         const int jj = v.tto[t];
         if ((m >> jj) & 1ull) continue;
         bt[nh] = t;
-        bidx[nh] = rsed_rank(m ^ (1ull << i) ^ (1ull << jj), v.binom, kp1);
+        bidx[nh] = rsed_rank_any(m ^ (1ull << i) ^ (1ull << jj), v.binom, kp1, md.species_b, cbs);
         if (++nh == HB) {
           process(HB);
           nh = 0;
@@ -256,6 +257,7 @@ __global__ void k_triplets(rsed_model_t md, int64_t n_rows, const int32_t* orbit
   const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= n_rows) return;
   const int kp1 = md.n_filled + 1;
+  const int64_t cbs = md.species_b ? b[__popcll(md.species_b) * kp1 + md.n_filled_b] : 1;
   const int64_t o = orbit_of_row[r];
   const uint64_t m = md.repr_masks[o];
   const int s_col = stab_order_of(stab_mask, o);
@@ -275,7 +277,7 @@ __global__ void k_triplets(rsed_model_t md, int64_t n_rows, const int32_t* orbit
       const int jj = tt[t];
       if ((m >> jj) & 1ull) continue;
       const uint64_t m2 = m ^ (1ull << i) ^ (1ull << jj);
-      const int64_t idx = rsed_rank(m2, b, kp1);
+      const int64_t idx = rsed_rank_any(m2, b, kp1, md.species_b, cbs);
       const RsedEntry e = load_entry(reinterpret_cast<const RsedEntry*>(md.table), idx);
       const int32_t rr = row_of_orbit[e.rep];
       if (rr < 0) continue;

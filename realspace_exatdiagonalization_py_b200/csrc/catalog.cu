@@ -60,6 +60,48 @@ __device__ __forceinline__ bool is_representative(uint64_t m, const uint8_t* per
   return true;
 }
 
+// Walks masks in rank order from rank r0: Gosper's successor for one
+// species; for two species the B part advances first and wraps into the A part.
+struct RankWalker {
+  uint64_t m, ca, cbm;
+  int64_t rb;
+  bool two;
+  RsedSpecies sp;
+  __device__ void init(int64_t r0, const rsed_group_t& grp, const int64_t* binom, int kp1) {
+    two = grp.species_b != 0ull;
+    if (!two) {
+      m = rsed_unrank(r0, grp.n_site, grp.n_filled, binom, kp1);
+      return;
+    }
+    sp = rsed_species(grp.species_b, grp.n_site, grp.n_filled, grp.n_filled_b, binom, kp1);
+    const int64_t ra = r0 / sp.cb;
+    rb = r0 % sp.cb;
+    ca = rsed_unrank(ra, sp.na, sp.ka, binom, kp1);
+    cbm = rsed_unrank(rb, sp.nb, sp.kb, binom, kp1);
+    m = rsed_deposit(ca, sp.sa) | rsed_deposit(cbm, sp.sb);
+  }
+  // call only while a next rank exists
+  __device__ void next() {
+    if (!two) {
+      m = rsed_gosper_next(m);
+      return;
+    }
+    if (rb + 1 < sp.cb) {
+      cbm = rsed_gosper_next(cbm);
+      ++rb;
+    } else {
+      cbm = (sp.kb > 0) ? ((1ull << sp.kb) - 1ull) : 0ull;
+      rb = 0;
+      ca = rsed_gosper_next(ca);
+    }
+    m = rsed_deposit(ca, sp.sa) | rsed_deposit(cbm, sp.sb);
+  }
+};
+
+__device__ __forceinline__ int64_t group_cb(const rsed_group_t& grp, const int64_t* binom, int kp1) {
+  return grp.species_b ? binom[__popcll(grp.species_b) * kp1 + grp.n_filled_b] : 1;
+}
+
 // Pass 1: representative flags as a bitmap, one 32-rank word per thread
 // (symmetry_resolved_ed.py:519-528).
 __global__ void k_rep_flags(rsed_group_t grp, uint32_t* bitmap, int64_t* block_count,
@@ -72,12 +114,13 @@ __global__ void k_rep_flags(rsed_group_t grp, uint32_t* bitmap, int64_t* block_c
   const int64_t r0 = word * kRanksPerThread;
   uint32_t bits = 0;
   if (r0 < grp.n_states) {
-    uint64_t m = rsed_unrank(r0, grp.n_site, grp.n_filled, gv.binom, kp1);
+    RankWalker w;
+    w.init(r0, grp, gv.binom, kp1);
     for (int i = 0; i < kRanksPerThread; ++i) {
       const int64_t r = r0 + i;
       if (r >= grp.n_states) break;
-      if (is_representative(m, gv.perm, grp.n_site, grp.n_group)) bits |= 1u << i;
-      if (r + 1 < grp.n_states) m = rsed_gosper_next(m);
+      if (is_representative(w.m, gv.perm, grp.n_site, grp.n_group)) bits |= 1u << i;
+      if (r + 1 < grp.n_states) w.next();
     }
     bitmap[word] = bits;
   }
@@ -117,12 +160,13 @@ __global__ void k_rep_list(rsed_group_t grp, const uint32_t* bitmap, const int64
   for (int w = 0; w < (int)(threadIdx.x >> 5); ++w) warp_prefix += warp_tot[w];
   int64_t off = block_off[blockIdx.x] + warp_prefix + (incl - c);
   if (bits) {
-    uint64_t m = rsed_unrank(r0, grp.n_site, grp.n_filled, gv.binom, kp1);
+    RankWalker w;
+    w.init(r0, grp, gv.binom, kp1);
     for (int i = 0; i < kRanksPerThread; ++i) {
-      if ((bits >> i) & 1u) repr_masks[off++] = m;
+      if ((bits >> i) & 1u) repr_masks[off++] = w.m;
       const uint32_t rest = (i < kRanksPerThread - 1) ? (bits >> (i + 1)) : 0u;
       if (rest == 0u) break;
-      m = rsed_gosper_next(m);
+      w.next();
     }
   }
 }
@@ -162,7 +206,7 @@ __global__ void k_expand(rsed_group_t grp, int64_t n_orb, const uint64_t* repr_m
   for (int g = 0; g < grp.n_group; ++g) {
     uint64_t img;
     double2 a = catalog_alpha(m, g, grp, gv, product_form, &img);
-    int64_t idx = rsed_rank(img, gv.binom, kp1);
+    int64_t idx = rsed_rank_any(img, gv.binom, kp1, grp.species_b, group_cb(grp, gv.binom, kp1));
     if (idx < 0 || idx >= grp.n_states) {
       rsed_flag_error(err, 1);
       continue;
@@ -244,7 +288,7 @@ __global__ void k_phase_update(rsed_group_t grp, int64_t n_orb, const uint64_t* 
     uint64_t img;
     double2 a =
         rsed_phase_product(m, gv.perm + g * grp.n_site, gv.eta + g * grp.n_site, grp.fermionic, &img);
-    int64_t idx = rsed_rank(img, gv.binom, kp1);
+    int64_t idx = rsed_rank_any(img, gv.binom, kp1, grp.species_b, group_cb(grp, gv.binom, kp1));
     if (idx < 0 || idx >= grp.n_states) {
       rsed_flag_error(err, 1);
       continue;
@@ -488,6 +532,15 @@ int check_group(const rsed_group_t* g) {
                "|G| = %d outside [1, %d]", g->n_group, RSED_MAX_GROUP);
   RSED_REQUIRE(g->n_states >= 1, RSED_EINVAL, "n_states must be >= 1");
   RSED_REQUIRE(g->binom && g->perm, RSED_EINVAL, "group tables missing");
+  if (g->species_b) {
+    const uint64_t all = (g->n_site >= 64) ? ~0ull : ((1ull << g->n_site) - 1ull);
+    const int nb = __builtin_popcountll(g->species_b);
+    RSED_REQUIRE((g->species_b & ~all) == 0ull && nb < g->n_site, RSED_EINVAL,
+                 "species_b must mark a proper subset of the sites");
+    RSED_REQUIRE(g->n_filled_b >= 0 && g->n_filled_b <= nb && g->n_filled_b <= g->n_filled &&
+                     g->n_filled - g->n_filled_b <= g->n_site - nb,
+                 RSED_EINVAL, "n_filled_b = %d does not fit the two species", g->n_filled_b);
+  }
   return RSED_OK;
 }
 

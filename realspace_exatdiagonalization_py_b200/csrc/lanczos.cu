@@ -1060,7 +1060,9 @@ k_lz_persist(rsed_model_t md, rsed_sectors_t sc, rsed_lanczos_t st, LzDims d, rs
                 if ((m >> jj) & 1ull) continue;
                 if ((hop++ % kHopLanes) != hl) continue;
                 bt[nh] = t;
-                bidx[nh] = rsed_rank(m ^ (1ull << i) ^ (1ull << jj), av.binom, kp1);
+                bidx[nh] = rsed_rank_any(m ^ (1ull << i) ^ (1ull << jj), av.binom, kp1, md.species_b,
+                                         md.species_b ? av.binom[__popcll(md.species_b) * kp1 + md.n_filled_b]
+                                                      : 1);
                 if (++nh == kPHB) {
                   process(kPHB);
                   nh = 0;

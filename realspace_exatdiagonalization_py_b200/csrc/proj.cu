@@ -53,6 +53,7 @@ __global__ void __launch_bounds__(256) k_proj_fill(rsed_model_t md, const double
   const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= md.n_orbits) return;
   const int kp1 = md.n_filled + 1;
+  const int64_t cbs = md.species_b ? v.binom[__popcll(md.species_b) * kp1 + md.n_filled_b] : 1;
   const uint64_t m = md.repr_masks[r];
   const double sr = sqrt_stab[r];
   int64_t pos = rowptr[r];
@@ -93,7 +94,7 @@ __global__ void __launch_bounds__(256) k_proj_fill(rsed_model_t md, const double
       const int jj = v.tto[t];
       if ((m >> jj) & 1ull) continue;
       bt[nh] = t;
-      bidx[nh] = rsed_rank(m ^ (1ull << i) ^ (1ull << jj), v.binom, kp1);
+      bidx[nh] = rsed_rank_any(m ^ (1ull << i) ^ (1ull << jj), v.binom, kp1, md.species_b, cbs);
       if (++nh == HB) {
         flush(HB);
         nh = 0;

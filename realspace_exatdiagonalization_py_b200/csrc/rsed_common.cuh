@@ -54,6 +54,66 @@ __device__ __forceinline__ uint64_t rsed_unrank(int64_t r, int n, int k,
   return mask;
 }
 
+// ---------------------------------------------------------------------------
+// Two-species bases: the sites in species_b hold exactly n_filled_b of the
+// particles, the other sites the rest (e.g. spin up / spin down at fixed
+// N_up, N_down).  Each species is ranked in colex order over its own sites in
+// ascending order, and rank = rank_A * C(|B|, n_filled_b) + rank_B; the
+// representative of an orbit is still its smallest mask.
+// ---------------------------------------------------------------------------
+struct RsedSpecies {
+  uint64_t sb, sa;  // site masks of species B and A
+  int kb, ka, nb, na;
+  int64_t cb;       // C(nb, kb)
+};
+
+__device__ __forceinline__ RsedSpecies rsed_species(uint64_t sb, int n_site, int n_filled, int kb,
+                                                    const int64_t* __restrict__ binom, int kp1) {
+  RsedSpecies s;
+  const uint64_t all = (n_site >= 64) ? ~0ull : ((1ull << n_site) - 1ull);
+  s.sb = sb;
+  s.sa = all & ~sb;
+  s.kb = kb;
+  s.ka = n_filled - kb;
+  s.nb = __popcll(sb);
+  s.na = n_site - s.nb;
+  s.cb = binom[s.nb * kp1 + kb];
+  return s;
+}
+
+__device__ __forceinline__ int64_t rsed_rank2(uint64_t m, const int64_t* __restrict__ binom, int kp1,
+                                              uint64_t sb, int64_t cb) {
+  int64_t ra = 0, rb = 0;
+  int ja = 1, jb = 1;
+  while (m) {
+    const int b = __ffsll((long long)m) - 1;
+    const int below_b = __popcll(sb & ((1ull << b) - 1ull));
+    if ((sb >> b) & 1ull) {
+      rb += binom[below_b * kp1 + jb];
+      ++jb;
+    } else {
+      ra += binom[(b - below_b) * kp1 + ja];
+      ++ja;
+    }
+    m &= m - 1;
+  }
+  return ra * cb + rb;
+}
+
+// rank for either basis kind (sb == 0: one species)
+__device__ __forceinline__ int64_t rsed_rank_any(uint64_t m, const int64_t* __restrict__ binom, int kp1,
+                                                 uint64_t sb, int64_t cb) {
+  return sb ? rsed_rank2(m, binom, kp1, sb, cb) : rsed_rank(m, binom, kp1);
+}
+
+// Place bit p of `compact` at the p-th set bit of `sel` (ascending).
+__device__ __forceinline__ uint64_t rsed_deposit(uint64_t compact, uint64_t sel) {
+  uint64_t out = 0;
+  for (uint64_t s = sel; s && compact; s &= s - 1, compact >>= 1)
+    if (compact & 1ull) out |= s & (~s + 1ull);
+  return out;
+}
+
 // Next mask with the same popcount (Gosper's hack; reference: :240-245).
 __device__ __forceinline__ uint64_t rsed_gosper_next(uint64_t x) {
   uint64_t c = x & (~x + 1);

@@ -90,9 +90,12 @@ class Symmetry_Resolved_ED_Data:
 
 
 def build_ed_data(second_quantized_model, *, filling_fraction=Fraction(1, 2),
-                  symmetry_group: Finite_Symmetry_Group) -> Symmetry_Resolved_ED_Data:
+                  symmetry_group: Finite_Symmetry_Group,
+                  species: tuple[list[int], int] | None = None) -> Symmetry_Resolved_ED_Data:
     """``n_filled = filling * n_site`` (exact), irreps and the device catalog
-    (``symmetry_resolved_ed.py:2906-2963``)."""
+    (``symmetry_resolved_ed.py:2906-2963``).  ``species = (sites_b, n_b)``
+    additionally fixes ``n_b`` particles on the 1-based sites ``sites_b``
+    (e.g. the spin-down orbitals: fixed N_up and N_down)."""
     n_site = second_quantized_model.lattice.n_site
     if not isinstance(filling_fraction, Fraction):
         filling_fraction = Fraction(filling_fraction)
@@ -106,6 +109,7 @@ def build_ed_data(second_quantized_model, *, filling_fraction=Fraction(1, 2),
         n_filled=n_filled,
         symmetry_group=symmetry_group,
         particle_statistics=second_quantized_model.particle_statistics,
+        species=species,
     )
     return Symmetry_Resolved_ED_Data(second_quantized_model, n_filled, filling_fraction,
                                      symmetry_group, irreps, catalog, [0] * len(irreps))

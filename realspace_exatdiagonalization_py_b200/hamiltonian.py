@@ -112,7 +112,7 @@ class DeviceModel:
             _lib.ptr(self.term_begin), _lib.ptr(self.term_to), _lib.ptr(self.term_amp),
             _lib.ptr(self.term_jw), _lib.ptr(self.hdiag),
             _lib.ptr(pj.get("rowptr")), _lib.ptr(pj.get("cg")), _lib.ptr(pj.get("w64")),
-            _lib.ptr(pj.get("w32")),
+            _lib.ptr(pj.get("w32")), int(dg.species_b), int(dg.n_filled_b), 0,
         )
 
     def projection_bytes(self, precisions=(64, 32)) -> int:

@@ -278,6 +278,9 @@ def config_model(name: str) -> tuple[Any, int]:
       t'=0.6 exp(+-0.4 pi i), t''=0, V1=1.
     * ``checkerboard48``: checkerboard 4x6x2, 8 fermions, couplings of
       ``checkerboard24``.
+    * ``hubbard32``: spinful Fermi-Hubbard 4x4 (32 spin-orbitals), t=1, U=4,
+      10 electrons; with ``hubbard_spin_species`` the basis fixes
+      N_up = N_down = 5.
     """
     if name == "heisenberg16":
         return build_heisenberg_second_quantized_model(16, 1.0), 8
@@ -286,7 +289,18 @@ def config_model(name: str) -> tuple[Any, int]:
         p.update({"V1": 1.0, "V2": 0.0, "V3": 0.0})
         ss, nf = ([3, 4], 4) if name == "checkerboard24" else ([4, 6], 8)
         return build_zero_flux_fermionic_fci_second_quantized_model(sample_size=ss, params=p), nf
+    if name == "hubbard32":
+        return build_spinful_hubbard_second_quantized_model([4, 4], 1.0, 4.0), 10
     if name == "haldane32":
         p = {"t": 1.0, "t'": 0.6, "t''": 0.0, "phi_over_2pi": 0.2, "V1": 1.0, "V2": 0.0}
         return build_zero_flux_bosonic_fci_second_quantized_model(sample_size=[4, 4], params=p), 8
     raise ValueError(f"unknown workload {name!r}")
+
+
+def hubbard_spin_species(model, n_down: int) -> tuple[list[int], int]:
+    """``species`` argument fixing ``n_down`` electrons on the spin-down
+    orbitals of a model from :func:`build_spinful_hubbard_second_quantized_model`
+    (sublattice 2 of every cell)."""
+    idx = model.lattice.site_to_index_map
+    sites = sorted(i for (cell_sub, i) in idx.items() if cell_sub[1] == 2)
+    return sites, int(n_down)

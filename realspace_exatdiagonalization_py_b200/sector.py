@@ -177,9 +177,9 @@ def get_canonical(cmap: CanonicalMap, m: int) -> tuple[int, int, complex]:
     (``symmetry_resolved_ed.py:1595-1632``); other masks fall back to the
     O(|G|) scan as in the reference."""
     cat = cmap.catalog
-    if int(m).bit_count() != cat.n_filled or m >> cat.n_site:
+    if not cat.in_basis(m):
         return get_canonical_representative(m, cmap.symmetry_group, cmap.particle_statistics)
-    idx = rank_combination(m, cat.binom_table)
+    idx = cat.rank_of(m)
     e = cat.table[idx].cpu().numpy()
     rep = int(e[0])
     if rep < 0:

@@ -179,6 +179,25 @@ def rank_combination(m: Mask, binom_table: np.ndarray) -> int:
     return r
 
 
+def rank_two_species(m: Mask, species_b: int, binom_table: np.ndarray, c_b: int) -> int:
+    """Rank in a two-species basis: ``rank_A * C(|B|, k_B) + rank_B``, each
+    species ranked in colex order over its own sites (ascending)."""
+    ra = rb = 0
+    ja = jb = 1
+    while m:
+        low = m & -m
+        b = low.bit_length() - 1
+        below = (species_b & (low - 1)).bit_count()
+        if (species_b >> b) & 1:
+            rb += int(binom_table[below, jb])
+            jb += 1
+        else:
+            ra += int(binom_table[b - below, ja])
+            ja += 1
+        m ^= low
+    return ra * c_b + rb
+
+
 def unrank_combination(r: int, n_site: int, n_filled: int, binom_table: np.ndarray) -> Mask:
     """Inverse of :func:`rank_combination` (``:377-394`` for one rank)."""
     m = 0

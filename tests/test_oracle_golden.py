@@ -81,3 +81,46 @@ def test_rank_beyond_42_sites():
     r = np.array([0, 1, 17295, 17296 - 1], dtype=np.int64)
     m = port.unrank(r, n, k, bt)
     np.testing.assert_array_equal(port.rank(m, n, bt), r)
+
+
+def _spin_down_mask(n_site):
+    # spin-orbital index = 2 * cell + spin (1-based sites 2, 4, ... are spin down)
+    return sum(1 << i for i in range(1, n_site, 2))
+
+
+def test_two_species_spectra_union_is_total_n(golden):
+    """Per-spin (N_up, N_down) bases: the union of their sector spectra over
+    all N_down equals the reference's total-N sector spectrum (Hubbard 2x3,
+    6 electrons), and the lowest levels equal the reference's energies."""
+    g = golden("hubbard12")
+    n, k = int(g["n_site"]), int(g["n_filled"])
+    perm0 = (g["perm"] - 1).astype(np.uint8)
+    bil = [(int(i), int(j), t) for (i, j), t in zip(g["bil_ij"], g["bil_t"])]
+    den = [(int(i), int(j), v) for (i, j), v in zip(g["den_ij"], g["den_v"])]
+    sb = _spin_down_mask(n)
+    total = port.catalog(n, k, perm0, g["eta"], True)
+    per = {kb: port.catalog(n, k, perm0, g["eta"], True, species=(sb, kb))
+           for kb in range(0, k + 1) if k - kb <= n // 2 and kb <= n // 2}
+    assert sum(len(c["rep_rank"]) for c in per.values()) == len(total["rep_rank"])
+    for s in range(len(g["chi"])):
+        chi = g["chi"][s]
+        full = np.linalg.eigvalsh(port.csr_block(total, n, port.sector_orbits(total, chi), bil, den, chi,
+                                                 True).toarray())
+        parts = []
+        for c in per.values():
+            orb = port.sector_orbits(c, chi)
+            if len(orb):
+                parts.append(np.linalg.eigvalsh(port.csr_block(c, n, orb, bil, den, chi, True).toarray()))
+        union = np.sort(np.concatenate(parts))
+        np.testing.assert_allclose(union, full, atol=1e-10, rtol=0)
+        np.testing.assert_allclose(full[:4], g["eig_vals"][s][:4], atol=1e-9, rtol=0)
+
+
+def test_two_species_rank_roundtrip():
+    bt = port.binom_table(12, 6)
+    for kb in range(0, 7):
+        C, rk, ur = port.species_basis(12, 6, (_spin_down_mask(12), kb), bt)
+        r = np.arange(C)
+        m = ur(r)
+        assert np.array_equal(rk(m), r)
+        assert np.all(np.diff(r) > 0) and len(np.unique(m)) == C
