@@ -33,15 +33,12 @@ import numpy as np
 import torch
 
 from . import _lib
-from .batched import BatchedSectorSolver, SolverConfig, persistent_ok
+from .batched import PERSISTENT_MAX_ORBITS, BatchedSectorSolver, SolverConfig, persistent_ok
 from .hamiltonian import DeviceModel
 from .lanczos import LanczosParams, _auto_keep
 from .sector import SectorSet
 
 __all__ = ["Autotuner", "candidate_configs", "default_tuner"]
-
-# one cluster per sector only pays while a sector is a few hundred KB
-PERSISTENT_MAX_ORBITS = 1 << 16
 
 
 def _nev_fits(nev: int, b: int, n_slots: int) -> bool:

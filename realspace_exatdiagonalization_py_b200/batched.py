@@ -27,6 +27,8 @@ from .sector import SectorSet
 # rsed_apply_h variants: 0 = automatic (projection table when present),
 # 999 = automatic on-the-fly mapping
 APPLY_AUTO, APPLY_ON_THE_FLY = 0, 999
+# one thread-block cluster per sector only pays while a sector is a few hundred KB
+PERSISTENT_MAX_ORBITS = 1 << 16
 
 
 @dataclass(frozen=True)
@@ -70,14 +72,15 @@ class BatchedSectorSolver:
         self.precision = precision
         if config is None:
             bs = (p.block,) * len(self.sectors)
-            config = SolverConfig(bs, persistent if persistent_ok(bs) and persistent in (1, 2, 4, 8) else 0,
-                                  projection=model.proj is not None, n_slots=p.n_slots, poll=poll)
+            small = model.catalog.n_orbits <= PERSISTENT_MAX_ORBITS
+            config = SolverConfig(bs, persistent if small and persistent_ok(bs) and persistent in (1, 2, 4, 8)
+                                  else 0, projection=model.proj is not None, n_slots=p.n_slots, poll=poll)
         if len(config.block_sizes) != len(self.sectors):
             raise ValueError("config.block_sizes needs one entry per sector")
         if config.persistent and not persistent_ok(config.block_sizes):
             raise ValueError("the persistent path needs uniform blocks of 1, 2 or 4 columns")
         if config.projection and model.proj is None:
-            model.build_projection(sset.sqrt_stab, precisions=(64, 32) if precision == 32 else (64,))
+            model.build_projection(sset.sqrt_stab, precisions=projection_precisions(model, precision))
         p = LanczosParams(**{**p.__dict__, "n_slots": config.n_slots,
                              "apply_variant": APPLY_AUTO if config.projection else APPLY_ON_THE_FLY})
         self.config = config
@@ -132,6 +135,36 @@ class BatchedSectorSolver:
         b = self.batch
         tensors = [b.V, b.W, b.Xf, b.P, b.coef, b.partial, b.ritz_val, b.ritz_vec, b.resid, b.state]
         return int(sum(t.numel() * t.element_size() for t in tensors if t is not None))
+
+
+def projection_precisions(model: DeviceModel, precision: int, fraction: float = 0.25) -> tuple[int, ...]:
+    """Weights to build: an FP32 solve also streams FP64 weights in its
+    refinement when both fit in ``fraction`` of the free device memory;
+    otherwise the refinement's few FP64 products run on the fly."""
+    if precision == 64:
+        return (64,)
+    free, _ = torch.cuda.mem_get_info(model.hdiag.device)
+    return (64, 32) if model.projection_bytes((64, 32)) <= fraction * free else (32,)
+
+
+def plan_waves(n_orbits: int, block_sizes: list[int], budget: int, n_slots: int = 16,
+               precision: int = 32) -> list[list[int]]:
+    """Split instances (given by their block sizes, in order) into consecutive
+    waves whose Lanczos buffers fit ``budget`` bytes each."""
+    waves: list[list[int]] = []
+    cur: list[int] = []
+    cols = 0
+    for i, b in enumerate(block_sizes):
+        if cur and lanczos_footprint_bytes(n_orbits, cols + b, n_slots, precision) > budget:
+            waves.append(cur)
+            cur, cols = [], 0
+        if lanczos_footprint_bytes(n_orbits, b, n_slots, precision) > budget:
+            raise MemoryError(f"one instance of {b} columns over {n_orbits} orbits needs more than {budget} bytes")
+        cur.append(i)
+        cols += b
+    if cur:
+        waves.append(cur)
+    return waves
 
 
 def lanczos_footprint_bytes(n_orbits: int, n_cols: int, n_slots: int = 16, precision: int = 32) -> int:

@@ -18,6 +18,7 @@ from dataclasses import dataclass, field
 from fractions import Fraction
 
 import numpy as np
+import torch
 
 from .catalog import Symmetry_Orbit_Catalog, build_symmetry_orbit_catalog, update_orbit_stabilizer_phases
 from .hamiltonian import DeviceModel, MatrixFreeHamiltonian, build_ed_Hamiltonian_symmetry_block
@@ -208,21 +209,47 @@ def solve_sectors_batched(ed_data, sector_ids: list[int], *, nev: int = 5, preci
         else:
             big.append(s)
     if big:
-        if config is None and autotune:
+        from .batched import lanczos_footprint_bytes, plan_waves, projection_precisions
+
+        p = params or LanczosParams(precision=precision)
+        if dm.proj is None and (config is None or config.projection):
+            # the streaming matvec, when its table fits half the free memory
+            free, _ = torch.cuda.mem_get_info()
+            if dm.projection_bytes((precision,)) <= 0.5 * free:
+                dm.build_projection(sset.sqrt_stab, precisions=projection_precisions(dm, precision))
+        free, _ = torch.cuda.mem_get_info()
+        n_orb = ed_data.orbit_catalog.n_orbits
+        bs = list(config.block_sizes) if config is not None else [p.block] * len(big)
+        budget = int(0.7 * free)
+        if lanczos_footprint_bytes(n_orb, sum(bs), p.n_slots, precision) <= budget:
+            waves = [list(range(len(big)))]
+        else:
+            waves = plan_waves(n_orb, bs, budget, p.n_slots, precision)
+        if config is None and autotune and len(waves) == 1:
             from .autotune import default_tuner
 
             config = default_tuner().best(dm, sset, big, nev, precision, params)
-        key = (tuple(big), nev, precision, None if params is None else tuple(params.__dict__.items()), graph,
-               config)
         cache = ed_data.__dict__.setdefault("_solvers", {})
-        solver = cache.get(key)
-        if solver is None or solver.model is not dm:
-            solver = BatchedSectorSolver(dm, sset, big, nev, precision=precision, params=params, graph=graph,
-                                         config=config)
-            cache[key] = solver
-        vals, vecs = solver.solve(start_blocks, vectors=return_vectors)
-        for i, s in enumerate(big):
-            out[s] = (vals[i].copy(), vecs[i] if vecs is not None else None)
+        for wave in waves:
+            secs = [big[i] for i in wave]
+            cfg = config if len(waves) == 1 else (None if config is None else type(config)(
+                tuple(config.block_sizes[i] for i in wave), config.persistent, config.projection,
+                config.n_slots, config.poll))
+            key = (tuple(secs), nev, precision, None if params is None else tuple(params.__dict__.items()),
+                   graph, cfg)
+            solver = cache.get(key)
+            if solver is None or solver.model is not dm:
+                solver = BatchedSectorSolver(dm, sset, secs, nev, precision=precision, params=params,
+                                             graph=graph, config=cfg)
+                if len(waves) == 1:
+                    cache[key] = solver
+            blocks = None if start_blocks is None else [start_blocks[big.index(s)] for s in secs]
+            vals, vecs = solver.solve(blocks, vectors=return_vectors)
+            for i, s in enumerate(secs):
+                out[s] = (vals[i].copy(), vecs[i] if vecs is not None else None)
+            if len(waves) > 1:
+                del solver
+                torch.cuda.empty_cache()
     return out
 
 

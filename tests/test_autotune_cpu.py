@@ -49,3 +49,19 @@ def test_footprint_grows_with_columns():
     a = lanczos_footprint_bytes(10000, 8)
     b = lanczos_footprint_bytes(10000, 16)
     assert b > a > 10000 * 8 * 16 * 18
+
+
+def test_plan_waves_splits_by_footprint():
+    import pytest
+
+    from realspace_exatdiagonalization_py_b200.batched import plan_waves
+
+    n = 1_000_000
+    one = lanczos_footprint_bytes(n, 4)
+    waves = plan_waves(n, [4] * 10, budget=int(3.5 * one))
+    assert [i for w in waves for i in w] == list(range(10))
+    assert all(lanczos_footprint_bytes(n, 4 * len(w)) <= 3.5 * one for w in waves)
+    assert len(waves) == 4
+    assert plan_waves(n, [4] * 3, budget=10 * one) == [[0, 1, 2]]
+    with pytest.raises(MemoryError):
+        plan_waves(n, [8], budget=one)
