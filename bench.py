@@ -341,7 +341,7 @@ def serving_at_scale(ed, models, n_req=32, rate=20.0, block=2, plain_samples=2):
     # plain FP64 path on the first requests
     plain_t, dE = [], []
     for r in reqs[:plain_samples]:
-        ctx = ed.FluxContext(sm, sm.normalize_flux(r.flux), 64, projection=True)
+        ctx = ed.FluxContext(sm, sm.normalize_flux(r.flux), 64)
         p = ed.LanczosParams(block=1, n_slots=48, precision=64, check_every=1)
         b = ed.LanczosBatch(ctx.dm, ctx.sset, [r.sector], 4, p)
         torch.cuda.synchronize()
@@ -359,6 +359,33 @@ def serving_at_scale(ed, models, n_req=32, rate=20.0, block=2, plain_samples=2):
                 "served_over_plain": summ["throughput_per_s"] / plain_rate,
                 "max_abs_dE_served_vs_plain_fp64": max(dE)})
     return out
+
+
+def step_kernel_shares(step, top=10):
+    """Device time per kernel over one (untimed) step, from CUPTI through
+    torch.profiler: [{kernel, launches, total_us, share}] sorted by time."""
+    from torch.profiler import ProfilerActivity, profile
+
+    import torch
+
+    torch.cuda.synchronize()
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        step()
+        torch.cuda.synchronize()
+    agg = {}
+    for ev in prof.events():
+        if ev.device_type.name != "CUDA":
+            continue
+        name = ev.name.replace("(anonymous namespace)::", "").replace("<unnamed>::", "").replace("void ", "")
+        if "(" in name:
+            name = name.split("(")[0]
+        a = agg.setdefault(name, [0, 0.0])
+        a[0] += 1
+        a[1] += ev.device_time_total
+    tot = sum(v[1] for v in agg.values()) or 1.0
+    rows = sorted(agg.items(), key=lambda kv: -kv[1][1])[:top]
+    return [{"kernel": k, "launches": v[0], "total_us": round(v[1], 1), "share": round(v[1] / tot, 4)}
+            for k, v in rows]
 
 
 def run_b200(args):
@@ -442,6 +469,7 @@ def run_b200(args):
             if ref is not None:
                 v = vals.cpu().numpy()
                 max_de = max(max_de, max(float(np.max(np.abs(v[i] - ref[s][:nev]))) for i, s in enumerate(sectors)))
+    shares = step_kernel_shares(step) if rank == 0 else None
     t_step = float(np.sum(times))
     if ws > 1:
         import torch.distributed as dist
@@ -521,6 +549,7 @@ def run_b200(args):
         if fe is not None:
             extra["fp32_matvec_error_before_refinement"] = {"max": float(fe.max()), "median": float(np.median(fe))}
         extra["residual_norm_max"] = float(solver.residuals().max())
+        extra["step_kernel_shares"] = shares
         extra["autotune"] = {"chosen": config.describe(), "tune_s": tune_s,
                              "candidates": [{"config": r["config"], "solve_ms": None if r["time_s"] is None
                                              else 1e3 * r["time_s"], "ok": r["ok"]} for r in tune_table]}

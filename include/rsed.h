@@ -209,8 +209,9 @@ int rsed_apply_h(const rsed_model_t* model, const rsed_sectors_t* sec, const voi
  * so that column j of y = H^dagger x gets sum_hops w * chi_s(g) * x[c][j]
  * (s = sector of column j) plus conj(h_diag[r]) x[r][j].  Needs n_orbits <
  * 2^26 and |G| <= 64.  rsed_proj_count writes rowptr (n_orbits + 1) and the
- * number of hops; rsed_proj_fill writes cg and either weight array (NULL =
- * skip).  With the table set in the model, rsed_apply_h variant 3NN streams
+ * number of hops; rsed_proj_fill writes cg and either weight array (each
+ * NULL = skip: cg is the same for every amplitude update of one catalog, so
+ * tables of several flux points can share one cg and rowptr).  With the table set in the model, rsed_apply_h variant 3NN streams
  * it over column chunks of NN columns one chunk after another (the chunk of x
  * stays in L2 while the table streams from HBM), 4NN runs all chunks in one
  * launch; NN in {2,4,8,16,32} at precision 64 and {4,8,16,32,64} at 32.

@@ -69,7 +69,83 @@ __device__ __forceinline__ double2 cdotc(double2 a, double2 b) {
 // of an instance to finish (atomic ticket, no waiting) sums the partials in
 // chunk order, forms G' = G - C^H C, its Cholesky factor R and the
 // projected-matrix entries.
-constexpr int kRT = 256;  // threads of k_lz_reduce
+constexpr int kRT = 256;         // threads of k_lz_reduce
+constexpr int kTileRows = 256;  // rows of W staged in shared memory per tile
+
+// This chunk's Gram partials for one instance with block size BB: warp w owns
+// slots w, w+8, w+16, ... (slot nb = W itself) and keeps their sums in
+// registers across all row tiles; W's rows are staged tile by tile in shared
+// memory, so V and W are each read once, as whole row segments.  Lane sums
+// are combined in shared memory in a fixed order.
+template <int BB>
+__device__ void lz_gram_chunk(const double2* __restrict__ V, const double2* __restrict__ W, int64_t slot_stride,
+                              int64_t ld, int c0, int nb, int64_t r0, int64_t r1, double2* __restrict__ out,
+                              double2* buf) {
+  constexpr int SW = (kJacobiMax / BB + 1 + 7) / 8;  // most slots one warp owns
+  constexpr int RPW = 32 / BB;                       // rows per warp pass
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int rl = lane / BB, p = lane % BB;
+  const bool act = rl < RPW;
+  double2 acc[SW][BB];
+#pragma unroll
+  for (int j = 0; j < SW; ++j)
+#pragma unroll
+    for (int q = 0; q < BB; ++q) acc[j][q] = make_double2(0.0, 0.0);
+  double2* Wt = buf;  // [kTileRows][BB]
+  for (int64_t t0 = r0; t0 < r1; t0 += kTileRows) {
+    const int nr = (int)min((int64_t)kTileRows, r1 - t0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < nr * BB; i += kRT) {
+      const int rr = i / BB, q = i % BB;
+      Wt[rr * BB + q] = W[(t0 + rr) * ld + c0 + q];
+    }
+    __syncthreads();
+    if (act) {
+#pragma unroll
+      for (int j = 0; j < SW; ++j) {
+        const int sl = warp + 8 * j;
+        if (sl > nb) break;
+        if (sl < nb) {
+          const double2* Y = V + sl * slot_stride + c0 + p;
+#pragma unroll 4
+          for (int rr = rl; rr < nr; rr += RPW) {
+            const double2 y = Y[(t0 + rr) * ld];
+#pragma unroll
+            for (int q = 0; q < BB; ++q) acc[j][q] = cadd(acc[j][q], cdotc(y, Wt[rr * BB + q]));
+          }
+        } else {
+          for (int rr = rl; rr < nr; rr += RPW) {
+            const double2 y = Wt[rr * BB + p];
+#pragma unroll
+            for (int q = 0; q < BB; ++q) acc[j][q] = cadd(acc[j][q], cdotc(y, Wt[rr * BB + q]));
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+  double2(*red)[32][kBMax] = reinterpret_cast<double2(*)[32][kBMax]>(buf);  // reuses the tile
+#pragma unroll
+  for (int j = 0; j < SW; ++j) {
+    const int sl = warp + 8 * j;
+    if (sl > nb) break;
+    if (act) {
+#pragma unroll
+      for (int q = 0; q < BB; ++q) red[warp][lane][q] = acc[j][q];
+    }
+    __syncwarp();
+    if (lane < BB) {
+#pragma unroll
+      for (int q = 0; q < BB; ++q) {
+        double2 t = make_double2(0.0, 0.0);
+        for (int k = 0; k < RPW; ++k) t = cadd(t, red[warp][k * BB + lane][q]);
+        out[sl * kBMax * kBMax + lane * kBMax + q] = t;
+      }
+    }
+    __syncwarp();
+  }
+}
+
 __global__ void __launch_bounds__(kRT) k_lz_reduce(rsed_lanczos_t st, LzDims d, int pass) {
   const int chunk = blockIdx.x;
   const int inst = blockIdx.y;
@@ -101,36 +177,19 @@ __global__ void __launch_bounds__(kRT) k_lz_reduce(rsed_lanczos_t st, LzDims d, 
   double2* part = reinterpret_cast<double2*>(st.partial);
   const int64_t slot_stride = d.n_orb * d.ld;
   const int64_t pbase = ((int64_t)chunk * d.n_inst + inst) * (int64_t)d.pslots * kBMax * kBMax;
+  __shared__ double2 red_l[kRT / 32][32][kBMax];  // W tile, lane sums, then the finalisation's partials
   {
-    // threads = (row group, pair); the row groups split the chunk's rows and
-    // are summed through shared memory
-    __shared__ double2 red[kRT * kBMax];
-    const int groups = kRT / npairs;  // >= 3 since npairs <= kJacobiMax + kBMax
-    const int pair = threadIdx.x % npairs, rg = threadIdx.x / npairs;
-    if (rg < groups) {
-      const int sl = pair / b, p = pair % b;
-      const double2* Y = (sl < nb) ? V + sl * slot_stride : W;
-      double2 acc[kBMax];
-#pragma unroll
-      for (int q = 0; q < kBMax; ++q) acc[q] = make_double2(0.0, 0.0);
-#pragma unroll 4
-      for (int64_t r = r0 + rg; r < r1; r += groups) {
-        const double2 y = Y[r * d.ld + c0 + p];
-        const double2* wr = W + r * d.ld + c0;
-#pragma unroll
-        for (int q = 0; q < kBMax; ++q)
-          if (q < b) acc[q] = cadd(acc[q], cdotc(y, wr[q]));
-      }
-#pragma unroll
-      for (int q = 0; q < kBMax; ++q)
-        if (q < b) red[(rg * npairs + pair) * kBMax + q] = acc[q];
-    }
-    __syncthreads();
-    for (int e = threadIdx.x; e < npairs * b; e += kRT) {
-      const int pr = e / b, q = e % b, sl = pr / b, p = pr % b;
-      double2 a = make_double2(0.0, 0.0);
-      for (int g = 0; g < groups; ++g) a = cadd(a, red[(g * npairs + pr) * kBMax + q]);
-      part[pbase + sl * kBMax * kBMax + p * kBMax + q] = a;
+    double2* buf = &red_l[0][0][0];
+    double2* out = part + pbase;
+    switch (b) {
+      case 1: lz_gram_chunk<1>(V, W, slot_stride, d.ld, c0, nb, r0, r1, out, buf); break;
+      case 2: lz_gram_chunk<2>(V, W, slot_stride, d.ld, c0, nb, r0, r1, out, buf); break;
+      case 3: lz_gram_chunk<3>(V, W, slot_stride, d.ld, c0, nb, r0, r1, out, buf); break;
+      case 4: lz_gram_chunk<4>(V, W, slot_stride, d.ld, c0, nb, r0, r1, out, buf); break;
+      case 5: lz_gram_chunk<5>(V, W, slot_stride, d.ld, c0, nb, r0, r1, out, buf); break;
+      case 6: lz_gram_chunk<6>(V, W, slot_stride, d.ld, c0, nb, r0, r1, out, buf); break;
+      case 7: lz_gram_chunk<7>(V, W, slot_stride, d.ld, c0, nb, r0, r1, out, buf); break;
+      default: lz_gram_chunk<8>(V, W, slot_stride, d.ld, c0, nb, r0, r1, out, buf); break;
     }
   }
   __threadfence();
@@ -144,15 +203,29 @@ __global__ void __launch_bounds__(kRT) k_lz_reduce(rsed_lanczos_t st, LzDims d, 
   __threadfence();
   if (threadIdx.x == 0) stt[S_TICKET] = 0;
   // ---- finalisation (one block per instance) ----
+  // G threads per entry sum interleaved chunk subsets, then the G partial
+  // sums are added in order (deterministic for a given chunk count)
   const int nent = (nb + 1) * b * b;
-  for (int e = threadIdx.x; e < nent; e += blockDim.x) {
-    const int sl = e / (b * b), pq = e % (b * b), p = pq / b, q = pq % b;
-    double2 a = make_double2(0.0, 0.0);
+  const int G = max(1, kRT / nent);
+  {
+    double2* fin = &red_l[0][0][0];  // kRT * kBMax >= nent * G entries
     const int64_t cstride = (int64_t)d.n_inst * d.pslots * kBMax * kBMax;
-    const double2* src = part + (int64_t)inst * d.pslots * kBMax * kBMax + sl * kBMax * kBMax + p * kBMax + q;
+    for (int t = threadIdx.x; t < nent * G; t += kRT) {
+      const int e = t % nent, g = t / nent;
+      const int sl = e / (b * b), pq = e % (b * b), p = pq / b, q = pq % b;
+      const double2* src = part + (int64_t)inst * d.pslots * kBMax * kBMax + sl * kBMax * kBMax + p * kBMax + q;
+      double2 a = make_double2(0.0, 0.0);
 #pragma unroll 8
-    for (int c = 0; c < d.n_chunks; ++c) a = cadd(a, __ldcg(src + c * cstride));
-    sc[(sl * b + p) * kBMax + q] = a;  // row (sl*b + p), column q
+      for (int c = g; c < d.n_chunks; c += G) a = cadd(a, __ldcg(src + c * cstride));
+      fin[g * nent + e] = a;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < nent; e += kRT) {
+      const int sl = e / (b * b), pq = e % (b * b), p = pq / b, q = pq % b;
+      double2 a = make_double2(0.0, 0.0);
+      for (int g = 0; g < G; ++g) a = cadd(a, fin[g * nent + e]);
+      sc[(sl * b + p) * kBMax + q] = a;  // row (sl*b + p), column q
+    }
   }
   __syncthreads();
   // G' = G - C^H C, one thread per (p, q)
@@ -230,9 +303,9 @@ __global__ void __launch_bounds__(kRT) k_lz_reduce(rsed_lanczos_t st, LzDims d, 
 }
 
 // W <- (W - V C) R^-1 ; pass 2 writes the new basis block and the matvec input.
-// Block (row range, instance): the instance's coefficients are staged in
-// shared memory (read by every thread of the block as broadcasts), one row
-// per thread.
+// Block (row range, instance), the instance's coefficients staged in shared
+// memory; one thread per (row, column q) -- the b lanes of a row read the
+// row's segment together and solve with R across lanes by shuffles.
 __global__ void __launch_bounds__(256) k_lz_update(rsed_lanczos_t st, LzDims d, int pass) {
   const int inst = blockIdx.y;
   const int* stt = st.state + inst * kStateInts;
@@ -251,52 +324,136 @@ __global__ void __launch_bounds__(256) k_lz_update(rsed_lanczos_t st, LzDims d, 
   }
   for (int e = threadIdx.x; e < kBMax * kBMax; e += blockDim.x) Rs[e] = coef[(d.pslots - 1) * kBMax * kBMax + e];
   __syncthreads();
-  const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (row >= d.n_orb) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int rpw = 32 / b;
+  const int rl = lane / b, q = lane % b;
+  const int64_t row = ((int64_t)blockIdx.x * (blockDim.x >> 5) + warp) * rpw + rl;
+  const bool act = rl < rpw && row < d.n_orb;
   double2* V = reinterpret_cast<double2*>(st.V);
   double2* W = reinterpret_cast<double2*>(st.W);
   const int64_t slot_stride = d.n_orb * d.ld;
-  double2 w[kBMax];
-#pragma unroll
-  for (int q = 0; q < kBMax; ++q) w[q] = (q < b) ? W[row * d.ld + c0 + q] : make_double2(0.0, 0.0);
-#pragma unroll 2
-  for (int s = 0; s < nb; ++s) {
-    const double2* Vs = V + s * slot_stride + row * d.ld + c0;
-    double2 v[kBMax];
-#pragma unroll
-    for (int p = 0; p < kBMax; ++p) v[p] = (p < b) ? Vs[p] : make_double2(0.0, 0.0);
-#pragma unroll
-    for (int p = 0; p < kBMax; ++p) {
-      if (p >= b) break;
-#pragma unroll
-      for (int q = 0; q < kBMax; ++q)
-        if (q < b) w[q] = csub(w[q], cmul(v[p], cs[(s * b + p) * kBMax + q]));
+  double2 w = make_double2(0.0, 0.0);
+  if (act) {
+    w = W[row * d.ld + c0 + q];
+#pragma unroll 4
+    for (int s = 0; s < nb; ++s) {
+      const double2* Vs = V + s * slot_stride + row * d.ld + c0;
+      for (int p = 0; p < b; ++p) w = csub(w, cmul(Vs[p], cs[(s * b + p) * kBMax + q]));
     }
   }
-  double2 x[kBMax];
-#pragma unroll
-  for (int q = 0; q < kBMax; ++q) {
-    if (q >= b) break;
-    double2 v = w[q];
-    for (int p = 0; p < q; ++p) v = csub(v, cmul(x[p], Rs[p * kBMax + q]));
-    const double rr = Rs[q * kBMax + q].x;
-    x[q] = make_double2(v.x / rr, v.y / rr);
+  // x R = w: x_q = (w_q - sum_{p<q} x_p R[p][q]) / R[q][q], across the row's lanes
+  const int base = lane - q;
+  double2 acc = make_double2(0.0, 0.0), xq = make_double2(0.0, 0.0);
+  for (int pp = 0; pp < b; ++pp) {
+    if (q == pp) {
+      const double rr = Rs[pp * kBMax + pp].x;
+      xq = make_double2((w.x - acc.x) / rr, (w.y - acc.y) / rr);
+    }
+    const int src = min(base + pp, 31);
+    const double xpx = __shfl_sync(0xffffffffu, xq.x, src);
+    const double xpy = __shfl_sync(0xffffffffu, xq.y, src);
+    if (q > pp) acc = cadd(acc, cmul(make_double2(xpx, xpy), Rs[pp * kBMax + q]));
   }
+  if (!act) return;
   if (pass == 1) {
-#pragma unroll
-    for (int q = 0; q < kBMax; ++q)
-      if (q < b) W[row * d.ld + c0 + q] = x[q];
+    W[row * d.ld + c0 + q] = xq;
   } else {
-    double2* Vn = V + (int64_t)nb * slot_stride + row * d.ld + c0;
-    double2* X = V + (int64_t)(d.n_slots + 1) * slot_stride + row * d.ld + c0;
-#pragma unroll
-    for (int q = 0; q < kBMax; ++q) {
-      if (q >= b) break;
-      Vn[q] = x[q];
-      X[q] = x[q];
-      if (st.Xf) reinterpret_cast<float2*>(st.Xf)[row * d.ld + c0 + q] =
-          make_float2((float)x[q].x, (float)x[q].y);
+    V[(int64_t)nb * slot_stride + row * d.ld + c0 + q] = xq;
+    V[(int64_t)(d.n_slots + 1) * slot_stride + row * d.ld + c0 + q] = xq;
+    if (st.Xf) reinterpret_cast<float2*>(st.Xf)[row * d.ld + c0 + q] = make_float2((float)xq.x, (float)xq.y);
+  }
+}
+
+// The same update for all instances at once (batches of 2+ instances whose
+// coefficients fit in shared memory): a block holds every instance's
+// coefficients and walks groups of whole rows (thread = one column of one
+// row), so each slot is read as contiguous rows.  x R = w is solved per
+// thread by forward substitution over its instance's columns, from the row's
+// w values exchanged through shared memory.  Grid-stride over row groups.
+__global__ void __launch_bounds__(256) k_lz_update_rows(rsed_lanczos_t st, LzDims d, int pass, int cs_stride) {
+  extern __shared__ __align__(16) unsigned char smem_u[];
+  double2* cs = reinterpret_cast<double2*>(smem_u);                    // [inst][cs_stride]
+  double2* Rs = cs + (size_t)d.n_inst * cs_stride;                      // [inst][kBMax*kBMax]
+  double2* wsh = Rs + (size_t)d.n_inst * kBMax * kBMax;                 // [256] row-group w values
+  int* meta = reinterpret_cast<int*>(wsh + 256);                        // [ld]: inst of each column
+  for (int c = threadIdx.x; c < d.ld; c += blockDim.x) meta[c] = -1;
+  __syncthreads();
+  for (int inst = threadIdx.x; inst < d.n_inst; inst += blockDim.x) {
+    const int b = st.inst_b[inst], c0 = st.inst_col0[inst];
+    for (int q = 0; q < b; ++q) meta[c0 + q] = inst;
+  }
+  for (int inst = 0; inst < d.n_inst; ++inst) {
+    const int* stt = st.state + inst * kStateInts;
+    const int b = st.inst_b[inst];
+    const int nb = (pass == 2) ? stt[S_NEWSLOT] : stt[S_NB];
+    const double2* coef = reinterpret_cast<const double2*>(st.coef) +
+                          (int64_t)inst * 2 * d.pslots * kBMax * kBMax + (pass - 1) * d.pslots * kBMax * kBMax;
+    if (!stt[S_ACTIVE] || nb * b > kJacobiMax) continue;
+    for (int e = threadIdx.x; e < nb * b * b; e += blockDim.x) {
+      const int r = e / b, q = e % b;  // r = s * b + p
+      cs[(size_t)inst * cs_stride + r * b + q] = coef[(r / b) * kBMax * kBMax + (r % b) * kBMax + q];
     }
+    for (int e = threadIdx.x; e < kBMax * kBMax; e += blockDim.x)
+      Rs[inst * kBMax * kBMax + e] = coef[(d.pslots - 1) * kBMax * kBMax + e];
+  }
+  __syncthreads();
+  const int rows_pg = blockDim.x / d.ld;  // rows per group
+  const int rloc = threadIdx.x / d.ld, col = threadIdx.x % d.ld;
+  const bool lane_ok = rloc < rows_pg;
+  const int inst = lane_ok ? meta[col] : -1;
+  int b = 1, c0 = 0, nb = 0, q = 0;
+  bool act = false;
+  if (inst >= 0) {
+    const int* stt = st.state + inst * kStateInts;
+    b = st.inst_b[inst];
+    c0 = st.inst_col0[inst];
+    nb = (pass == 2) ? stt[S_NEWSLOT] : stt[S_NB];
+    q = col - c0;
+    act = stt[S_ACTIVE] && nb * b <= kJacobiMax;
+  }
+  const double2* csi = cs + (size_t)(inst < 0 ? 0 : inst) * cs_stride;
+  const double2* Ri = Rs + (inst < 0 ? 0 : inst) * kBMax * kBMax;
+  double2* V = reinterpret_cast<double2*>(st.V);
+  double2* W = reinterpret_cast<double2*>(st.W);
+  const int64_t slot_stride = d.n_orb * d.ld;
+  const int64_t n_groups = (d.n_orb + rows_pg - 1) / rows_pg;
+  for (int64_t grp = blockIdx.x; grp < n_groups; grp += gridDim.x) {
+    const int64_t row = grp * rows_pg + rloc;
+    const bool live = act && lane_ok && row < d.n_orb;
+    double2 w = make_double2(0.0, 0.0);
+    if (live) {
+      w = W[row * d.ld + col];
+#pragma unroll 4
+      for (int s = 0; s < nb; ++s) {
+        const double2* Vs = V + s * slot_stride + row * d.ld + c0;
+        for (int p = 0; p < b; ++p) w = csub(w, cmul(Vs[p], csi[(s * b + p) * b + q]));
+      }
+    }
+    wsh[threadIdx.x] = w;
+    __syncthreads();
+    if (live) {
+      // forward substitution over this instance's columns 0..q
+      const double2* wr = wsh + rloc * d.ld + c0;
+      double2 xs[kBMax];
+      double2 xq = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int pp = 0; pp < kBMax; ++pp) {
+        if (pp > q) break;
+        double2 v = wr[pp];
+        for (int k = 0; k < pp; ++k) v = csub(v, cmul(xs[k], Ri[k * kBMax + pp]));
+        const double rr = Ri[pp * kBMax + pp].x;
+        xs[pp] = make_double2(v.x / rr, v.y / rr);
+        xq = xs[pp];
+      }
+      if (pass == 1) {
+        W[row * d.ld + col] = xq;
+      } else {
+        V[(int64_t)nb * slot_stride + row * d.ld + col] = xq;
+        V[(int64_t)(d.n_slots + 1) * slot_stride + row * d.ld + col] = xq;
+        if (st.Xf) reinterpret_cast<float2*>(st.Xf)[row * d.ld + col] = make_float2((float)xq.x, (float)xq.y);
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -811,7 +968,9 @@ __global__ void __launch_bounds__(128) k_rr_gram(rsed_lanczos_t st, LzDims d) {
       for (int q = 0; q < kBMax; ++q)
         if (q < b) acc[q] = cadd(acc[q], cdotc(qv, Z[row * d.ld + q]));
     }
-    for (int q = 0; q < b; ++q) part[pbase + r * kRRMax + l2 * b + q] = acc[q];
+#pragma unroll
+    for (int q = 0; q < kBMax; ++q)
+      if (q < b) part[pbase + r * kRRMax + l2 * b + q] = acc[q];
   }
   __threadfence();
   __syncthreads();
@@ -827,12 +986,23 @@ __global__ void __launch_bounds__(128) k_rr_gram(rsed_lanczos_t st, LzDims d) {
     stt[S_RESTART_NB] = 0;
   }
   double2* P = reinterpret_cast<double2*>(st.P) + (int64_t)inst * d.pm * d.pm;
-  for (int e = threadIdx.x; e < M * M; e += blockDim.x) {
-    const int r = e / M, c = e % M;
+  // G threads per entry over interleaved chunk subsets, then in order
+  __shared__ double2 fin[kRRMax * kRRMax];
+  const int nent = M * M;
+  const int G = max(1, (int)blockDim.x / nent);
+  for (int t = threadIdx.x; t < nent * G; t += blockDim.x) {
+    const int e = t % nent, g = t / nent, r = e / M, c = e % M;
     double2 a = make_double2(0.0, 0.0);
-    for (int ch = 0; ch < d.n_chunks; ++ch)
+#pragma unroll 8
+    for (int ch = g; ch < d.n_chunks; ch += G)
       a = cadd(a, __ldcg(part + ((int64_t)ch * d.n_inst + inst) * (int64_t)kRRMax * kRRMax + r * kRRMax + c));
-    P[(int64_t)r * d.pm + c] = a;
+    fin[g * nent + e] = a;
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < nent; e += blockDim.x) {
+    double2 a = make_double2(0.0, 0.0);
+    for (int g = 0; g < G; ++g) a = cadd(a, fin[g * nent + e]);
+    P[(int64_t)(e / M) * d.pm + e % M] = a;
   }
 }
 
@@ -1440,7 +1610,30 @@ int launch_pass(const rsed_lanczos_t& st, const LzDims& d, int pass, cudaStream_
   dim3 g1(d.n_chunks, d.n_inst);
   k_lz_reduce<<<g1, kRT, 0, stream>>>(st, d, pass);
   RSED_CHECK_LAUNCH();
-  k_lz_update<<<dim3((unsigned)((d.n_orb + 255) / 256), d.n_inst), 256, 0, stream>>>(st, d, pass);
+  // all instances per block when their coefficients fit in shared memory
+  const int cs_stride = st.n_slots * st.bmax * st.bmax;
+  const size_t smem = sizeof(double2) * ((size_t)d.n_inst * (cs_stride + kBMax * kBMax) + 256) +
+                      sizeof(int) * (size_t)d.ld;
+  // (measured: above ~48 KB the lower occupancy costs more than whole-row reads save)
+  if (d.n_inst >= 2 && d.ld <= 256 && smem <= 48 * 1024) {
+    static bool attr_set = false;
+    if (!attr_set) {
+      RSED_TRY_CUDA(cudaFuncSetAttribute(k_lz_update_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+      attr_set = true;
+    }
+    const int rows_pg = 256 / d.ld;
+    const int64_t groups = (d.n_orb + rows_pg - 1) / rows_pg;
+    int dev = 0, n_sm = 148;
+    RSED_TRY_CUDA(cudaGetDevice(&dev));
+    RSED_TRY_CUDA(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
+    const int64_t grid = groups < (int64_t)n_sm * 8 ? groups : (int64_t)n_sm * 8;
+    k_lz_update_rows<<<(unsigned)grid, 256, smem, stream>>>(st, d, pass, cs_stride);
+  } else {
+    // rows per block: 8 warps x (32 / b) rows; sized for the largest block of the batch
+    const int64_t rows_per_block = 8 * (32 / st.bmax);
+    k_lz_update<<<dim3((unsigned)((d.n_orb + rows_per_block - 1) / rows_per_block), d.n_inst), 256, 0, stream>>>(
+        st, d, pass);
+  }
   RSED_CHECK_LAUNCH();
   return RSED_OK;
 }

@@ -80,7 +80,7 @@ __global__ void __launch_bounds__(256) k_proj_fill(rsed_model_t md, const double
       }
       const double ratio = sq[h] / sr;
       const double2 w = make_double2(ta.x * ratio, -ta.y * ratio);
-      cg[pos] = (uint32_t)e[h].rep | ((uint32_t)e[h].g << kOrbitBits);
+      if (cg) cg[pos] = (uint32_t)e[h].rep | ((uint32_t)e[h].g << kOrbitBits);
       if (w64) w64[pos] = w;
       if (w32) w32[pos] = make_float2((float)w.x, (float)w.y);
       ++pos;
@@ -443,7 +443,7 @@ extern "C" int rsed_proj_fill(const rsed_model_t* md, const double* sqrt_stab, c
                               uint32_t* cg, double* w64, float* w32, void* stream_) {
   int rc = check_proj_model(md);
   if (rc) return rc;
-  RSED_REQUIRE(sqrt_stab && rowptr && cg, RSED_EINVAL, "bad projection fill arguments");
+  RSED_REQUIRE(sqrt_stab && rowptr && (cg || w64 || w32), RSED_EINVAL, "bad projection fill arguments");
   cudaStream_t stream = as_stream(stream_);
   rsed_sectors_t none{};
   ApplySmemLayout lay = apply_layout(*md, none);

@@ -118,7 +118,9 @@ class DeviceModel:
     def projection_bytes(self, precisions=(64, 32)) -> int:
         """Device bytes of the projection table (exact hop count; one pass)."""
         if self.proj is not None:
-            return sum(int(t.numel() * t.element_size()) for k, t in self.proj.items() if torch.is_tensor(t))
+            skip = ("rowptr", "cg") if self.proj.get("shared") else ()
+            return sum(int(t.numel() * t.element_size()) for k, t in self.proj.items()
+                       if torch.is_tensor(t) and k not in skip)
         n = self.count_hops()
         return 8 * (self.catalog.n_orbits + 1) + n * (4 + (16 if 64 in precisions else 0)
                                                       + (8 if 32 in precisions else 0))
@@ -136,13 +138,30 @@ class DeviceModel:
         self._rowptr_cache = rowptr
         return int(n.value)
 
-    def build_projection(self, sqrt_stab: torch.Tensor, precisions=(64, 32), stream=None) -> None:
+    def build_projection(self, sqrt_stab: torch.Tensor, precisions=(64, 32), stream=None,
+                         share: dict | None = None) -> None:
         """Build the orbit-space projection table (K6b) for the current
-        catalog amplitudes; afterwards ``rsed_apply_h`` variant 0 streams it."""
+        catalog amplitudes; afterwards ``rsed_apply_h`` variant 0 streams it.
+
+        ``share``: the table of another amplitude state of the same catalog
+        (a copy moved to another flux point by ``update_orbit_stabilizer_phases``
+        keeps every target orbit and group element); its ``rowptr`` and ``cg``
+        are reused and only the weights are computed."""
         lib = _lib.lib()
         want = tuple(sorted(set(precisions)))
         if self.proj is not None and self.proj["table_version"] == self.catalog.version and \
                 set(want) <= set(self.proj["precisions"]):
+            return
+        if share is not None:
+            rowptr, cg, n = share["rowptr"], share["cg"], share["n_hops"]
+            dev = rowptr.device
+            w64 = torch.empty(max(n, 1), dtype=torch.complex128, device=dev) if 64 in want else None
+            w32 = torch.empty(max(n, 1), dtype=torch.complex64, device=dev) if 32 in want else None
+            _lib.check(lib.rsed_proj_fill(ctypes.byref(self.c), _lib.ptr(sqrt_stab), _lib.ptr(rowptr), None,
+                                          _lib.ptr(w64), _lib.ptr(w32), _lib.stream_ptr(stream)))
+            self.proj = {"rowptr": rowptr, "cg": cg, "w64": w64, "w32": w32, "n_hops": n, "precisions": want,
+                         "table_version": self.catalog.version, "shared": True}
+            self.refresh()
             return
         n = self.count_hops(stream)
         rowptr = self._rowptr_cache

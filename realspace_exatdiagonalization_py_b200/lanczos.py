@@ -122,9 +122,10 @@ class LanczosBatch:
         self.inst_b = torch.tensor(bs, dtype=torch.int32, device=dev)
         S = p.n_slots
         self.pm = (S + 1) * bmax
-        # reduction chunks: about 8 blocks per SM over all instances, >= 64 rows
+        # reduction chunks: about 8 blocks per SM over all instances, >= 64
+        # rows each and at most 256 per instance (the finalisation sums them)
         n_sm = torch.cuda.get_device_properties(dev).multi_processor_count if dev.type == "cuda" else 148
-        target = max(1, (8 * n_sm) // n_inst)
+        target = min(256, max(1, (8 * n_sm) // n_inst))
         self.chunk_rows = max(64, -(-n_orb // target))
         c128 = torch.complex128
         self.V = torch.zeros((S + 2, n_orb, self.ld), dtype=c128, device=dev)
@@ -169,8 +170,14 @@ class LanczosBatch:
             b = self.block_sizes[i]
             blk = blocks[i] if blocks is not None else None
             if blk is None:
+                # seeded blocks are deterministic: drawn on the host once per
+                # (sector, width, seed) and kept on the device for later solves
                 seed = 12345 if seeds is None else seeds[i]
-                blk = start_block(d, b, seed)
+                key = (s, d, b, seed)
+                cache = self.__dict__.setdefault("_start_cache", {})
+                if key not in cache:
+                    cache[key] = torch.from_numpy(start_block(d, b, seed)).to(self.dev)
+                blk = cache[key]
             if isinstance(blk, np.ndarray):
                 blk = torch.from_numpy(np.ascontiguousarray(blk, dtype=np.complex128))
             blk = blk.to(self.dev, non_blocking=True).reshape(d, -1)
@@ -246,10 +253,13 @@ class LanczosBatch:
             raise _lib.RsedError(code, f"instances {bad} did not converge (state {st[bad[0]].tolist()})")
         return st
 
-    def capture(self, n_iter: int):
+    def capture(self, n_iter: int, sync: bool = True):
         """CUDA graph of ``n_iter`` iterations (replayed by ``run(graph=True)``).
 
-        Runs one real iteration first, outside the graph, on the live state."""
+        Runs one real iteration first, outside the graph, on the live state.
+        ``sync=False`` captures without the device-wide synchronisation that
+        ``torch.cuda.graph`` performs first (work of other streams keeps
+        running; the capture only records this batch's launches)."""
         self.launches_per_graph = None
         s = torch.cuda.Stream()
         s.wait_stream(torch.cuda.current_stream())
@@ -258,8 +268,16 @@ class LanczosBatch:
         torch.cuda.current_stream().wait_stream(s)
         g = torch.cuda.CUDAGraph()
         n0 = _lib.load().rsed_launch_count()
-        with torch.cuda.graph(g, stream=s):
-            self.iterate(n_iter, s)
+        if sync:
+            with torch.cuda.graph(g, stream=s):
+                self.iterate(n_iter, s)
+        else:
+            with torch.cuda.stream(s):
+                g.capture_begin(capture_error_mode="thread_local")
+                try:
+                    self.iterate(n_iter, s)
+                finally:
+                    g.capture_end()
         self.launches_per_graph = int(_lib.load().rsed_launch_count() - n0)
         return g
 

@@ -1,26 +1,37 @@
 """Continuous-batching eigen-solve service.
 
 A request is one (lattice model, momentum sector, flux point) eigen-solve.
-The server keeps, per lattice model, the zero-flux orbit catalog, and per flux
-point a ``FluxContext``: a copy of that catalog whose amplitudes were moved to
-the flux point by ``update_orbit_stabilizer_phases`` (no rebuild), the twisted
-device model, the sector membership and the projection table.  Requests run in
-*lanes*: a lane is a resident ``LanczosBatch`` (Krylov basis, projected
-matrices, state) of 1..``max_width`` instances on its own CUDA stream, bound
-to one flux point and reused by later requests of that flux point.
+Per lattice model the server keeps the zero-flux orbit catalog and its
+orbit-space projection table; per flux point a ``FluxContext``: a copy of the
+catalog whose amplitudes were moved to the flux point by
+``update_orbit_stabilizer_phases`` (no rebuild), the twisted device model, the
+sector membership and the flux point's projection weights.  The projection
+table's structure (row offsets, target orbit and group element of every hop)
+does not change under the phase update, so every flux point of a model shares
+it and owns only its weights.
+
+Requests run in *lanes*.  A lane is a resident ``LanczosBatch`` (Krylov basis,
+projected matrices, state) of 1..``max_width`` instances on its own CUDA
+stream, plus the lane's own copy of one flux point's weights and sector
+membership.  A lane serves any flux point of its model: taking a request, it
+copies that flux point's weights and membership into its buffers (a device
+copy of a few hundred MB at most) and replays the Lanczos iterations from a
+CUDA graph captured once, when the lane was created -- its kernels only ever
+see the lane's own buffers.
 
 Scheduling (``step``), one host thread, no blocking waits on the device:
   * admission: pending requests are grouped by (model, flux); a group takes an
-    idle lane of its flux point or a new one, as many requests per lane as
-    arrived together (up to ``max_width``).  A new lane or flux context is
-    admitted only while the device bytes they need (measured for contexts,
-    computed for lanes) fit the budget; idle contexts and lanes are evicted
+    idle lane of its model (or a new one) with as many of its requests as the
+    lane is wide.  A new lane or flux context is admitted only while the device
+    bytes they need (measured for contexts, computed for lanes) fit the
+    budget; idle lanes and flux contexts no running lane uses are evicted
     (least recently used) to make room.  Requests that do not fit wait.
-  * progress: every running lane gets ``poll`` more Lanczos iterations on its
-    stream, followed by an asynchronous copy of its state into pinned host
-    memory and an event; lanes whose event completed and whose instances all
-    stopped move on to the FP64 Rayleigh-Ritz refinement (FP32 matvec) and
-    the asynchronous copy of their eigenvalues.  Lanes on different streams
+  * progress: every running lane gets ``poll`` more Lanczos iterations (one
+    graph replay) on its stream, followed by an asynchronous copy of its state
+    into pinned host memory and an event; lanes whose event completed and
+    whose instances all stopped move on to the FP64 Rayleigh-Ritz refinement
+    (FP32 matvec; run against the flux context's own model) and the
+    asynchronous copy of their eigenvalues.  Lanes on different streams
     overlap on the device; a request arriving while others run is admitted at
     the next step as soon as a lane and memory are free.
 
@@ -31,9 +42,10 @@ which other requests share the device or its lane.
 
 from __future__ import annotations
 
+import ctypes
 import time
 from collections import OrderedDict
-from dataclasses import dataclass, field
+from dataclasses import dataclass
 from fractions import Fraction
 
 import numpy as np
@@ -46,9 +58,10 @@ from .hamiltonian import DeviceModel
 from .lanczos import S_ACTIVE, S_ITERS, S_STATUS, LanczosBatch, LanczosParams
 from .lattice import generate_bilinear_terms
 from .sector import SectorSet
-from .symmetry import build_irrep_list, build_translation_group
+from .symmetry import build_irrep_list, build_translation_group, group_order
 
-__all__ = ["ServingModel", "FluxContext", "SolveRequest", "SolveResult", "SolveServer", "latency_summary"]
+__all__ = ["ServingModel", "FluxContext", "SolveRequest", "SolveResult", "SolveServer", "latency_summary",
+           "poisson_requests"]
 
 
 @dataclass
@@ -98,7 +111,8 @@ class ServingModel:
             symmetry_group=self.group0, particle_statistics=self.stats)
         self.n_orbits = self.catalog.n_orbits
         self.n_sectors = len(build_irrep_list(self.group0, self.lattice))
-        self.ctx_bytes: int | None = None  # measured device bytes of a flux point, once one was built
+        self.base: FluxContext | None = None  # zero-flux context: owns the shared table structure
+        self.ctx_bytes: int | None = None     # measured device bytes of a flux point, once one was built
 
     def normalize_flux(self, flux) -> tuple:
         f = tuple(float(x) for x in (flux or ()))
@@ -108,62 +122,120 @@ class ServingModel:
             raise ValueError(f"flux needs {self.lattice.dim} components")
         return f
 
+    def base_context(self, precision: int) -> "FluxContext":
+        if self.base is None:
+            self.base = FluxContext(self, (0.0,) * self.lattice.dim, precision)
+        return self.base
+
 
 class FluxContext:
     """Device state of one flux point of one model."""
 
-    def __init__(self, sm: ServingModel, flux: tuple, precision: int, projection: bool = True):
+    def __init__(self, sm: ServingModel, flux: tuple, precision: int):
         self.sm = sm
         self.flux = flux
+        # FP32 serving also keeps FP64 weights: the refinement's FP64 products
+        # then stream the table instead of re-deriving every hop
+        want = (32, 64) if precision == 32 else (64,)
         before = torch.cuda.memory_allocated()
-        if any(flux):
+        zero = not any(flux)
+        if zero:
+            terms, group, cat = sm.model.bilinear_terms, sm.group0, sm.catalog
+        else:
             terms = generate_bilinear_terms(sm.model.tb_model, twisted_phases_over_2π=list(flux))
             group = build_translation_group(sm.lattice, list(flux))
             cat = sm.catalog.clone()
             update_orbit_stabilizer_phases(cat, group, sm.stats)
-        else:
-            terms, group, cat = sm.model.bilinear_terms, sm.group0, sm.catalog
         self.catalog = cat
         self.irreps = build_irrep_list(group, sm.lattice)
         self.dm = DeviceModel(cat, terms, sm.model.density_density_terms)
         self.sset = SectorSet(cat, self.irreps)
-        if projection:
-            self.dm.build_projection(self.sset.sqrt_stab, precisions=(precision,))
-        torch.cuda.synchronize()
+        if zero:
+            self.dm.build_projection(self.sset.sqrt_stab, precisions=want)
+        else:
+            base = sm.base_context(precision)
+            if not torch.equal(self.sset.chi, base.sset.chi):
+                raise ValueError("the flux point changes the sector characters; lanes cannot share it")
+            self.dm.build_projection(self.sset.sqrt_stab, precisions=want, share=base.dm.proj)
+        # allocation accounting is host-side: no device synchronisation needed
         self.bytes = max(0, torch.cuda.memory_allocated() - before)
-        if any(flux):
+        if not zero:
             sm.ctx_bytes = max(sm.ctx_bytes or 0, self.bytes)
-        self.lanes: list[_Lane] = []
+        self.users = 0
         self.last_used = time.perf_counter()
 
-    def busy(self) -> bool:
-        return any(ln.state != "idle" for ln in self.lanes)
+    def weights(self, precision: int) -> torch.Tensor:
+        return self.dm.proj["w32" if precision == 32 else "w64"]
+
+
+class _LaneModel:
+    """Model view of a lane: the model's shared table structure with the
+    lane's own weight buffer (what ``LanczosBatch`` needs of a model)."""
+
+    def __init__(self, base: FluxContext, w: torch.Tensor, precision: int):
+        self.catalog = base.catalog
+        src = base.dm.c
+        self.c = _lib.RsedModel.from_buffer_copy(src)
+        self.c.proj_w32 = _lib.ptr(w) if precision == 32 else None
+        self.c.proj_w64 = _lib.ptr(w) if precision == 64 else None
+
+
+class _LaneSectors:
+    """Sector view of a lane: the lane's own membership buffer; row lists and
+    dimensions come from the flux context of the current request."""
+
+    def __init__(self, base: FluxContext, member: torch.Tensor):
+        self.base = base.sset
+        self.member = member
+        self.sqrt_stab = base.sset.sqrt_stab
+        self.chi = base.sset.chi
+        self.n_sectors = base.sset.n_sectors
+        self.current = base.sset
+
+    @property
+    def dims(self):
+        return self.current.dims
+
+    def rows(self, s: int, stream=None):
+        return self.current.rows(s, stream)
+
+    def sectors_struct(self, col_sector: torch.Tensor, n_cols: int, ld: int) -> _lib.RsedSectors:
+        return _lib.RsedSectors(self.n_sectors, n_cols, ld, group_order(self.base.catalog.symmetry_group),
+                                _lib.ptr(self.member), _lib.ptr(self.sqrt_stab), _lib.ptr(self.chi),
+                                _lib.ptr(col_sector))
 
 
 class _Lane:
     _ids = 0
 
-    def __init__(self, ctx: FluxContext, width: int, nev: int, params: LanczosParams, poll: int,
-                 graph: bool):
+    def __init__(self, sm: ServingModel, width: int, nev: int, params: LanczosParams, poll: int):
         _Lane._ids += 1
         self.id = _Lane._ids
-        self.ctx = ctx
+        self.sm = sm
         self.width = width
         self.nev = nev
         self.params = params
         self.poll = poll
-        self.use_graph = graph
         self.stream = torch.cuda.Stream()
+        base = sm.base_context(params.precision)
+        if base.weights(params.precision) is None:
+            raise ValueError(f"model {sm.name!r} was first served at another precision")
+        wdt = torch.complex64 if params.precision == 32 else torch.complex128
+        self.w = torch.empty_like(base.weights(params.precision), dtype=wdt)
+        self.member = torch.empty_like(base.sset.member)
+        self.model = _LaneModel(base, self.w, params.precision)
+        self.sectors = _LaneSectors(base, self.member)
         self.batch: LanczosBatch | None = None
         self.graph = None
         self.state = "idle"
+        self.ctx: FluxContext | None = None
         self.reqs: list[SolveRequest] = []
         self.admitted = 0.0
+        self.last_used = time.perf_counter()
         self.event = torch.cuda.Event()
-        self.h_state = None
-        self.h_vals = self.h_res = self.h_fp32 = None
-        self.bytes = lanczos_footprint_bytes(ctx.sset.catalog.n_orbits, width * params.block, params.n_slots,
-                                             params.precision)
+        self.h_state = self.h_vals = self.h_res = self.h_fp32 = None
+        self.bytes = (lanczos_footprint_bytes(sm.n_orbits, width * params.block, params.n_slots, params.precision)
+                      + self.w.numel() * self.w.element_size() + self.member.numel() * 8)
 
     # -- device work (all on the lane's stream) ----------------------------
     def _start_blocks(self):
@@ -176,14 +248,22 @@ class _Lane:
             out.append(blk / torch.linalg.vector_norm(blk, dim=0, keepdim=True))
         return out
 
-    def begin(self, reqs: list[SolveRequest], now: float) -> None:
+    def begin(self, reqs: list[SolveRequest], ctx: FluxContext, now: float) -> None:
         assert len(reqs) == self.width and self.state == "idle"
         self.reqs = list(reqs)
+        self.ctx = ctx
+        ctx.users += 1
         self.admitted = now
         sectors = [r.sector for r in reqs]
+        self.sectors.current = ctx.sset
+        # the flux context was built on the admitting stream: order the lane after it
+        self.stream.wait_stream(torch.cuda.current_stream())
         with torch.cuda.stream(self.stream):
+            # the flux point's weights and membership into the lane's buffers
+            self.w.copy_(ctx.weights(self.params.precision), non_blocking=True)
+            self.member.copy_(ctx.sset.member, non_blocking=True)
             if self.batch is None:
-                self.batch = LanczosBatch(self.ctx.dm, self.ctx.sset, sectors, self.nev, self.params,
+                self.batch = LanczosBatch(self.model, self.sectors, sectors, self.nev, self.params,
                                           block_sizes=[self.params.block] * self.width)
                 self.h_state = torch.empty(self.batch.state.shape, dtype=torch.int32).pin_memory()
                 self.h_vals = torch.empty((self.width, self.nev), dtype=torch.float64).pin_memory()
@@ -196,18 +276,14 @@ class _Lane:
                 b.col_sector.copy_(torch.from_numpy(cs), non_blocking=False)
             self.batch.load_start(self._start_blocks())
             self.batch.start()
-            if self.use_graph and self.graph is None:
-                self.graph = self.batch.capture(self.poll)
+            if self.graph is None:
+                self.graph = self.batch.capture(self.poll, sync=False)
             self._advance()
         self.state = "running"
-        self.ctx.last_used = time.perf_counter()
 
     def _advance(self) -> None:
         b = self.batch
-        if self.graph is not None:
-            self.graph.replay()
-        else:
-            b.iterate(self.poll)
+        self.graph.replay()
         self.h_state.copy_(b.state, non_blocking=True)
         self.event.record(self.stream)
 
@@ -215,12 +291,25 @@ class _Lane:
         b = self.batch
         if self.params.precision == 32:
             fp32 = b.ritz_val[:, : self.nev].clone()
-            b.rayleigh_ritz()
+            # FP64 products against the flux point's own model and membership
+            sc = self.ctx.sset.sectors_struct(b.col_sector, b.n_cols, b.ld)
+            _lib.check(_lib.lib().rsed_lanczos_rayleigh_ritz(
+                ctypes.byref(self.ctx.dm.c), ctypes.byref(sc), ctypes.byref(b.c), APPLY_AUTO,
+                _lib.stream_ptr(self.stream)))
             self.h_fp32.copy_((fp32 - b.ritz_val[:, : self.nev]).abs(), non_blocking=True)
         self.h_vals.copy_(b.ritz_val[:, : self.nev], non_blocking=True)
         self.h_res.copy_(b.resid[:, : self.nev], non_blocking=True)
         self.h_state.copy_(b.state, non_blocking=True)
         self.event.record(self.stream)
+
+    def _release(self) -> None:
+        if self.ctx is not None:
+            self.ctx.users -= 1
+            self.ctx.last_used = time.perf_counter()
+        self.ctx = None
+        self.reqs = []
+        self.state = "idle"
+        self.last_used = time.perf_counter()
 
     def poll_once(self, now: float, max_iter: int) -> list[SolveResult] | None:
         """Advance the lane if its last work completed; results when done."""
@@ -235,9 +324,9 @@ class _Lane:
                 bad = [i for i in range(self.width) if st[i, S_STATUS] != 1]
                 if bad:
                     code = int(st[bad[0], S_STATUS]) or _lib.RSED_ENOTCONV
-                    self.state = "idle"
-                    raise _lib.RsedError(code, f"lane {self.id}: requests {[self.reqs[i].rid for i in bad]} "
-                                               f"did not converge")
+                    rids = [self.reqs[i].rid for i in bad]
+                    self._release()
+                    raise _lib.RsedError(code, f"lane {self.id}: requests {rids} did not converge")
                 self._finish()
                 self.state = "finishing"
                 return None
@@ -250,9 +339,7 @@ class _Lane:
                 fp32_error=self.h_fp32[i].numpy().copy() if self.params.precision == 32 else None,
                 iterations=int(st[i, S_ITERS]), dim=int(self.ctx.sset.dims[r.sector]), arrival=r.arrival,
                 admitted=self.admitted, finished=now, lane=self.id, lane_width=self.width))
-        self.state = "idle"
-        self.reqs = []
-        self.ctx.last_used = time.perf_counter()
+        self._release()
         return out
 
 
@@ -261,8 +348,7 @@ class SolveServer:
 
     def __init__(self, models: dict[str, ServingModel] | ServingModel, *, nev: int = 4, precision: int = 32,
                  block: int = 4, n_slots: int = 16, poll: int = 16, max_width: int = 4,
-                 memory_budget: int | None = None, projection: bool = True, graph: bool | None = None,
-                 max_iter: int = 4000):
+                 memory_budget: int | None = None, max_iter: int = 4000, creations_per_step: int = 1):
         if isinstance(models, ServingModel):
             models = {models.name: models}
         self.models = dict(models)
@@ -272,14 +358,16 @@ class SolveServer:
                                     apply_variant=APPLY_AUTO)
         self.poll = poll
         self.max_width = max_width
-        self.projection = projection
-        self.graph = graph
         self.max_iter = max_iter
+        # new flux contexts and lanes cost milliseconds of host work; making at
+        # most this many per step keeps the running lanes fed in between
+        self.creations_per_step = creations_per_step
         if memory_budget is None:
             free, _ = torch.cuda.mem_get_info()
             memory_budget = int(0.8 * free)
         self.budget = memory_budget
         self.contexts: OrderedDict[tuple, FluxContext] = OrderedDict()
+        self.lanes: list[_Lane] = []
         self.pending: list[SolveRequest] = []
         self.t0 = time.perf_counter()
         self.peak_running = 0
@@ -287,35 +375,36 @@ class SolveServer:
 
     # -- memory ------------------------------------------------------------
     def used_bytes(self) -> int:
-        return sum(c.bytes + sum(ln.bytes for ln in c.lanes) for c in self.contexts.values())
+        base = sum(sm.base.bytes for sm in self.models.values() if sm.base is not None)
+        return base + sum(c.bytes for c in self.contexts.values()) + sum(ln.bytes for ln in self.lanes)
 
     def _ctx_estimate(self, sm: ServingModel) -> int:
         if sm.ctx_bytes:
             return sm.ctx_bytes
         n = sm.n_orbits
-        return int(sm.catalog.n_states * 16 + n * 64 + n * 74 * (4 + 8 * (self.precision // 32)))
-
-    def _evict(self, need: int) -> bool:
-        """Drop idle lanes, then idle contexts, least recently used first,
-        until ``need`` more bytes fit; False if they cannot."""
-        if self.used_bytes() + need <= self.budget:
-            return True
-        for key, c in sorted(self.contexts.items(), key=lambda kv: kv[1].last_used):
-            for ln in [ln for ln in c.lanes if ln.state == "idle"]:
-                c.lanes.remove(ln)
-                if self.used_bytes() + need <= self.budget:
-                    torch.cuda.empty_cache()
-                    return True
-            if not c.lanes and not c.busy():
-                del self.contexts[key]
-                if self.used_bytes() + need <= self.budget:
-                    torch.cuda.empty_cache()
-                    return True
-        torch.cuda.empty_cache()
-        return self.used_bytes() + need <= self.budget
+        return int(sm.catalog.n_states * 16 + n * 64 + n * 74 * (16 + (8 if self.precision == 32 else 0)))
 
     def _lane_bytes(self, sm: ServingModel, width: int) -> int:
-        return lanczos_footprint_bytes(sm.n_orbits, width * self.params.block, self.params.n_slots, self.precision)
+        n = sm.n_orbits
+        return (lanczos_footprint_bytes(n, width * self.params.block, self.params.n_slots, self.precision)
+                + n * 74 * 8 * (self.precision // 32) + n * 8)
+
+    def _evict(self, need: int) -> bool:
+        """Drop idle lanes and flux contexts no running lane uses, least
+        recently used first, until ``need`` more bytes fit."""
+        if self.used_bytes() + need <= self.budget:
+            return True
+        victims = [("ctx", k, c.last_used) for k, c in self.contexts.items() if c.users == 0]
+        victims += [("lane", ln, ln.last_used) for ln in self.lanes if ln.state == "idle"]
+        for kind, obj, _ in sorted(victims, key=lambda v: v[2]):
+            if kind == "ctx":
+                del self.contexts[obj]
+            else:
+                self.lanes.remove(obj)
+            if self.used_bytes() + need <= self.budget:
+                break
+        torch.cuda.empty_cache()
+        return self.used_bytes() + need <= self.budget
 
     # -- API -----------------------------------------------------------------
     def now(self) -> float:
@@ -329,35 +418,78 @@ class SolveServer:
         self.pending.append(req)
 
     def running(self) -> int:
-        return sum(1 for c in self.contexts.values() for ln in c.lanes if ln.state != "idle")
+        return sum(1 for ln in self.lanes if ln.state != "idle")
+
+    def _context(self, sm: ServingModel, flux: tuple) -> FluxContext | None:
+        if not any(flux):
+            if sm.base is None and not self._evict(self._ctx_estimate(sm)):
+                return None
+            return sm.base_context(self.precision)
+        key = (sm.name, flux)
+        ctx = self.contexts.get(key)
+        if ctx is None:
+            if sm.base is None and not self._evict(2 * self._ctx_estimate(sm)):
+                return None
+            sm.base_context(self.precision)
+            if not self._evict(self._ctx_estimate(sm)):
+                return None
+            ctx = FluxContext(sm, flux, self.precision)
+            self.contexts[key] = ctx
+        self.contexts.move_to_end(key)
+        return ctx
+
+    def warm(self, n_lanes: int, width: int = 1, model: str | None = None) -> None:
+        """Create ``n_lanes`` idle lanes (buffers and captured graphs) ahead of
+        the requests, as a server does at start-up."""
+        for name, sm in self.models.items():
+            if model is not None and name != model:
+                continue
+            base = sm.base_context(self.precision)
+            for _ in range(n_lanes):
+                if not self._evict(self._lane_bytes(sm, width)):
+                    break
+                ln = _Lane(sm, width, self.nev, self.params, self.poll)
+                # one throw-away solve on the zero-flux context captures the graph
+                ln.begin([SolveRequest(-1, 0, (0.0,) * sm.lattice.dim, name)] * width, base, 0.0)
+                self.lanes.append(ln)
+            while any(ln.state != "idle" for ln in self.lanes):
+                for ln in self.lanes:
+                    ln.poll_once(0.0, self.max_iter)
 
     def _admit(self, now: float) -> None:
         groups: OrderedDict[tuple, list[SolveRequest]] = OrderedDict()
         for r in self.pending:
             groups.setdefault((r.model, r.flux), []).append(r)
         admitted: set[int] = set()
+        created = 0
         for key, reqs in groups.items():
             sm = self.models[key[0]]
             while reqs:
-                ctx = self.contexts.get(key)
-                if ctx is not None:
-                    idle = [ln for ln in ctx.lanes if ln.state == "idle" and ln.width <= len(reqs)]
-                    lane = max(idle, key=lambda ln: ln.width) if idle else None
-                else:
-                    lane = None
+                idle = [ln for ln in self.lanes if ln.sm is sm and ln.state == "idle" and ln.width <= len(reqs)]
+                lane = max(idle, key=lambda ln: ln.width) if idle else None
+                have_ctx = (sm.base is not None) if not any(key[1]) else key in self.contexts
+                cost = (0 if have_ctx else 1) + (0 if lane is not None else 1)
+                if cost and created >= self.creations_per_step:
+                    break
+                created += cost
+                if lane is not None:
+                    lane.state = "reserved"  # not evictable while the context is made
+                ctx = self._context(sm, key[1])
+                if lane is not None:
+                    lane.state = "idle"
+                if ctx is None:
+                    break
                 if lane is None:
                     width = min(len(reqs), self.max_width)
-                    need = self._lane_bytes(sm, width) + (0 if ctx is not None else self._ctx_estimate(sm))
-                    if not self._evict(need):
+                    ctx.users += 1  # pinned while the lane is made
+                    ok = self._evict(self._lane_bytes(sm, width))
+                    ctx.users -= 1
+                    if not ok:
                         break
-                    if ctx is None:
-                        ctx = FluxContext(sm, key[1], self.precision, self.projection)
-                        self.contexts[key] = ctx
-                    use_graph = self.graph if self.graph is not None else sm.n_orbits < 65536
-                    lane = _Lane(ctx, width, self.nev, self.params, self.poll, use_graph)
-                    ctx.lanes.append(lane)
+                    lane = _Lane(sm, width, self.nev, self.params, self.poll)
+                    self.lanes.append(lane)
                 take, reqs[:] = reqs[: lane.width], reqs[lane.width:]
-                lane.begin(take, now)
+                lane.begin(take, ctx, now)
                 self.admissions += 1
                 admitted.update(r.rid for r in take)
         if admitted:
@@ -367,11 +499,10 @@ class SolveServer:
         """One scheduling round; returns the requests that finished in it."""
         now = self.now()
         done: list[SolveResult] = []
-        for c in list(self.contexts.values()):
-            for ln in c.lanes:
-                res = ln.poll_once(now, self.max_iter)
-                if res:
-                    done.extend(res)
+        for ln in list(self.lanes):
+            res = ln.poll_once(now, self.max_iter)
+            if res:
+                done.extend(res)
         if self.pending:
             self._admit(self.now())
         self.peak_running = max(self.peak_running, self.running())

@@ -82,12 +82,12 @@ def test_admission_respects_memory_budget(golden):
     probe = ed.SolveServer({"haldane24": sm}, nev=4, precision=32, max_width=1)
     probe.run([ed.SolveRequest(99, 0, (0.5, 0.5), "haldane24")], realtime=False)  # measures a flux point
     ctx_bytes = probe._ctx_estimate(sm)
-    assert ctx_bytes == sm.ctx_bytes > 0
+    assert ctx_bytes == sm.ctx_bytes > 0 and sm.base is not None
     lane_bytes = probe._lane_bytes(sm, 1)
     del probe
-    # room for one flux point and its lane, not for a second flux point
+    # room for the shared zero-flux table, one flux point and its lane, not for a second flux point
     server = ed.SolveServer({"haldane24": sm}, nev=4, precision=32, max_width=1,
-                            memory_budget=int(ctx_bytes + 1.5 * lane_bytes))
+                            memory_budget=int(sm.base.bytes + ctx_bytes + 1.5 * lane_bytes))
     # four flux points: a second one never fits next to a running first one
     reqs = [ed.SolveRequest(i, s, f, "haldane24") for i, (s, f) in
             enumerate([(0, theta), (1, (0.5, 0.0)), (2, (0.25, 0.75)), (3, (0.0, 0.25))])]
