@@ -325,8 +325,8 @@ def serving_at_scale(ed, models, n_req=32, rate=20.0, block=2, plain_samples=2):
     model, nf = models.config_model("haldane32")
     sm = ed.ServingModel(model, nf, name="haldane32")
     reqs = poisson_requests(n_req, rate=rate, n_sectors=sm.n_sectors, flux_grid=16, model="haldane32", seed=0)
-    srv = ed.SolveServer(sm, nev=4, precision=32, block=block, poll=8)
-    srv.run([ed.SolveRequest(10 ** 6, 0, (0.5, 0.5), "haldane32")], realtime=False)  # warm-up
+    srv = ed.SolveServer(sm, nev=4, precision=32, block=block, poll=16)
+    srv.warm(48)  # start-up: lane buffers and captured graphs, before the stream begins
     res = srv.run([ed.SolveRequest(r.rid, r.sector, r.flux, r.model, r.arrival) for r in reqs], realtime=True)
     summ = ed.latency_summary(res)
     by_id = {r.rid: r for r in res}

@@ -70,6 +70,11 @@ def candidate_configs(dims: list[int], nev: int, n_orbits: int, *, projection_ok
         slots = 16 if max(bs) < 8 else 8
         for proj in mats:
             out.append(SolverConfig(bs, 0, proj, slots))
+        # the projected eigen-solve at a restart grows as (n_slots * b)^2..3
+        # while restarts come every ~n_slots/2 steps: a second basis length
+        alt = {2: 24, 4: 12}.get(max(bs))
+        if alt and projection_ok and _nev_fits(nev, max(bs), alt):
+            out.append(SolverConfig(bs, 0, True, alt))
         if persistent_ok(bs) and n_orbits <= PERSISTENT_MAX_ORBITS:
             for cs in (2, 4, 8):
                 out.append(SolverConfig(bs, cs, False, slots))

@@ -528,17 +528,23 @@ __device__ void herm_lowest(double2* A, int M, int Kp, double* theta, double2* S
     __syncthreads();
     const double2 t = tau[k];
     if (t.x == 0.0 && t.y == 0.0) continue;
-    // phase B: p = tau * A22 v, one thread per row (odd stride: no bank conflicts)
-    if (tid < M - k - 1) {
-      const int i = k + 1 + tid;
+    // phase B: p = tau * A22 v, four lanes per row (odd stride: no bank conflicts)
+    {
+      const int i = k + 1 + (tid >> 2), sub = tid & 3;
       double sx = 0.0, sy = 0.0;
-      const double2* Ar = A + i * lda;
-      for (int j = k + 1; j < M; ++j) {
-        const double2 a = Ar[j], v = vv[j];
-        sx += a.x * v.x - a.y * v.y;
-        sy += a.x * v.y + a.y * v.x;
+      if (i < M) {
+        const double2* Ar = A + i * lda;
+        for (int j = k + 1 + sub; j < M; j += 4) {
+          const double2 a = Ar[j], v = vv[j];
+          sx += a.x * v.x - a.y * v.y;
+          sy += a.x * v.y + a.y * v.x;
+        }
       }
-      pw[i] = cmul(t, make_double2(sx, sy));
+      sx += __shfl_xor_sync(0xffffffffu, sx, 1);
+      sy += __shfl_xor_sync(0xffffffffu, sy, 1);
+      sx += __shfl_xor_sync(0xffffffffu, sx, 2);
+      sy += __shfl_xor_sync(0xffffffffu, sy, 2);
+      if (i < M && sub == 0) pw[i] = cmul(t, make_double2(sx, sy));
     }
     __syncthreads();
     // p^H v (warp 0) into red[0..1]
@@ -645,6 +651,7 @@ __device__ void herm_lowest(double2* A, int M, int Kp, double* theta, double2* S
       }
     }
     if (dg[M - 1] == 0.0) dg[M - 1] = tiny;
+    for (int i = 0; i < M; ++i) dg[i] = 1.0 / dg[i];  // reciprocal pivots: the solves multiply
     unsigned h = 2166136261u ^ (unsigned)(j * 16777619u);
     for (int i = 0; i < M; ++i) {
       h = h * 1664525u + 1013904223u;
@@ -660,9 +667,9 @@ __device__ void herm_lowest(double2* A, int M, int Kp, double* theta, double2* S
           z[i + 1] = tmp - dl[i] * z[i];
         }
       }
-      z[M - 1] /= dg[M - 1];
-      if (M > 1) z[M - 2] = (z[M - 2] - du[M - 2] * z[M - 1]) / dg[M - 2];
-      for (int i = M - 3; i >= 0; --i) z[i] = (z[i] - du[i] * z[i + 1] - du2[i] * z[i + 2]) / dg[i];
+      z[M - 1] *= dg[M - 1];
+      if (M > 1) z[M - 2] = (z[M - 2] - du[M - 2] * z[M - 1]) * dg[M - 2];
+      for (int i = M - 3; i >= 0; --i) z[i] = (z[i] - du[i] * z[i + 1] - du2[i] * z[i + 2]) * dg[i];
       double nrm = 0.0;
       for (int i = 0; i < M; ++i) nrm = fmax(nrm, fabs(z[i]));
       const double inv = nrm > 0.0 ? 1.0 / nrm : 1.0;
@@ -674,39 +681,57 @@ __device__ void herm_lowest(double2* A, int M, int Kp, double* theta, double2* S
     for (int i = 0; i < M; ++i) Z[i * Kp + j] = z[i] * inv;
   }
   __syncthreads();
-  // modified Gram-Schmidt in ascending order (one warp)
-  if (warp == 0) {
-    for (int j = 0; j < Kp; ++j) {
-      for (int i = 0; i < j; ++i) {
+  // Gram-Schmidt in ascending order (orthonormal bases of degenerate
+  // clusters): for vector j, all dots with 0..j-1 at once (one warp each),
+  // one update by all threads, twice; then the normalisation
+  for (int j = 0; j < Kp; ++j) {
+    for (int pass = 0; pass < 2 && j > 0; ++pass) {
+      for (int i = warp; i < j; i += nwarp) {
         double dt = 0.0;
         for (int r = lane; r < M; r += 32) dt += Z[r * Kp + i] * Z[r * Kp + j];
         dt = warp_sum(dt);
-        for (int r = lane; r < M; r += 32) Z[r * Kp + j] -= dt * Z[r * Kp + i];
-        __syncwarp();
+        if (lane == 0) red[i] = dt;
       }
+      __syncthreads();
+      for (int r = tid; r < M; r += nt) {
+        double v = Z[r * Kp + j];
+        for (int i = 0; i < j; ++i) v -= red[i] * Z[r * Kp + i];
+        Z[r * Kp + j] = v;
+      }
+      __syncthreads();
+    }
+    if (warp == 0) {
       double n2 = 0.0;
       for (int r = lane; r < M; r += 32) n2 += Z[r * Kp + j] * Z[r * Kp + j];
       n2 = warp_sum(n2);
-      const double inv = 1.0 / sqrt(n2);
-      for (int r = lane; r < M; r += 32) Z[r * Kp + j] *= inv;
-      __syncwarp();
+      if (lane == 0) red[kKeepMax] = 1.0 / sqrt(n2);
     }
+    __syncthreads();
+    const double inv = red[kKeepMax];
+    for (int r = tid; r < M; r += nt) Z[r * Kp + j] *= inv;
+    __syncthreads();
   }
-  __syncthreads();
   // ---- 4. back-transformation: s = H_0 (H_1 (... H_{M-2} z)), all vectors at once ----
   for (int i = tid; i < M * Kp; i += nt) S[i] = make_double2(Z[i], 0.0);
   __syncthreads();
   for (int k = M - 2; k >= 0; --k) {
     const double2 t = tau[k];
     if (t.x == 0.0 && t.y == 0.0) continue;
-    if (tid < Kp) {  // f_j = tau (v^H s_j)
+    {  // f_j = tau (v^H s_j), 16 lanes per vector
+      const int j = tid >> 4, sub = tid & 15;
       double sx = 0.0, sy = 0.0;
-      for (int r = k + 1; r < M; ++r) {
-        const double2 c = cdotc(A[r * lda + k], S[r * Kp + tid]);
-        sx += c.x;
-        sy += c.y;
+      if (j < Kp) {
+        for (int r = k + 1 + sub; r < M; r += 16) {
+          const double2 c = cdotc(A[r * lda + k], S[r * Kp + j]);
+          sx += c.x;
+          sy += c.y;
+        }
       }
-      pw[tid] = cmul(t, make_double2(sx, sy));
+      for (int o = 1; o < 16; o <<= 1) {
+        sx += __shfl_xor_sync(0xffffffffu, sx, o);
+        sy += __shfl_xor_sync(0xffffffffu, sy, o);
+      }
+      if (j < Kp && sub == 0) pw[j] = cmul(t, make_double2(sx, sy));
     }
     __syncthreads();
     for (int i = tid; i < (M - k - 1) * Kp; i += nt) {
