@@ -55,7 +55,7 @@ def _dist():
 # ---------------------------------------------------------------------------
 
 
-def cpu_sector_solves(model, n_filled, G, irreps, nev, budget_s=20.0, min_sectors=3):
+def cpu_sector_solves(model, n_filled, G, irreps, nev, budget_s=20.0, min_sectors=3, cat=None):
     """Time the reference algorithm (projection table + CSR + ARPACK per
     sector, catalog built outside the timing as in the reference benchmark)
     on a bounded sample of sectors; returns (solves/s, n_timed, eigvals)."""
@@ -63,11 +63,14 @@ def cpu_sector_solves(model, n_filled, G, irreps, nev, budget_s=20.0, min_sector
 
     n = G.n_site
     fermion = model.particle_statistics.name == "FERMIONIC"
-    perm0, eta = port.group_arrays(G)
-    cat = port.catalog(n, n_filled, perm0, eta, fermion)
+    if cat is None:
+        perm0, eta = port.group_arrays(G)
+        cat = port.catalog(n, n_filled, perm0, eta, fermion)
+    # sectors in order, cycling through the workload again until the budget
+    # is spent (a bounded sample of about budget_s seconds of host work)
     t_all, done, vals = 0.0, 0, {}
     s = 0
-    while s < len(irreps) and (t_all < budget_s or done < min_sectors):
+    while t_all < budget_s or done < min_sectors:
         chi = np.asarray(irreps[s].values, dtype=np.complex128)
         t0 = time.perf_counter()
         orbits = port.sector_orbits(cat, chi)
@@ -76,7 +79,7 @@ def cpu_sector_solves(model, n_filled, G, irreps, nev, budget_s=20.0, min_sector
         t_all += time.perf_counter() - t0
         vals[s] = w
         done += 1
-        s += 1
+        s = (s + 1) % len(irreps)
     return done / t_all, done, vals, t_all
 
 
@@ -107,9 +110,14 @@ def run_reference(args):
     model, nf = models.config_model(args.workload)
     G = sym.build_translation_group(model.lattice)
     irreps = sym.build_irrep_list(G, model.lattice)
+    from oracle import port
+
+    perm0, eta = port.group_arrays(G)
+    cat = port.catalog(G.n_site, nf, perm0, eta, model.particle_statistics.name == "FERMIONIC")
     per_step = []
     for it in range(args.warmup + args.steps):
-        rate, n_done, _, t = cpu_sector_solves(model, nf, G, irreps, wl["nev"], budget_s=8.0, min_sectors=2)
+        rate, n_done, _, t = cpu_sector_solves(model, nf, G, irreps, wl["nev"], budget_s=4.0, min_sectors=2,
+                                               cat=cat)
         if it >= args.warmup:
             per_step.append((n_done, t))
     tot_n = sum(n for n, _ in per_step)
@@ -594,8 +602,9 @@ def run_b200(args):
                     "api": "solve_sectors_batched(start_blocks=pinned host) -> numpy eigenpairs"},
             "roofline": roof,
             "cpu_baseline": {"value": cpu_rate, "unit": "sector-solves/s", "cores": _NCPU, "kind": "port",
-                             "sample": f"{cpu_n} sectors of the same workload in {cpu_t:.1f} s "
-                                       "(projection table + CSR + ARPACK; catalog untimed)"},
+                             "sample": f"{cpu_n} sector solves of the same workload (its 12 sectors, "
+                                       f"cycled) in {cpu_t:.1f} s: projection table + CSR + ARPACK per "
+                                       "sector, catalog untimed"},
             "clocks": clk.summary(),
             "gpu_launches": launches,
             "extra": extra,
@@ -617,7 +626,7 @@ def main():
     ap.add_argument("--workload", default="checkerboard24", choices=sorted(WORKLOADS))
     ap.add_argument("--precision", type=int, default=32, choices=[32, 64])
     ap.add_argument("--plain-sectors", type=int, default=12)
-    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--skip-scale", action="store_true")
     ap.add_argument("--matvec-only", action="store_true",
                     help="only the 32-site matvec at scale (for kernel profiling)")
