@@ -435,7 +435,12 @@ def run_b200(args):
     params = ed.LanczosParams(precision=args.precision)
     tuner = ed.Autotuner(trials=2)
     t0 = time.perf_counter()
-    config, tune_table = tuner.tune(dm, sset, sectors, nev, precision=args.precision, params=params)
+    if args.solver == "auto":
+        config, tune_table = tuner.tune(dm, sset, sectors, nev, precision=args.precision, params=params)
+    else:  # "graph:<block>:<proj|otf>:<n_slots>" fixes the configuration (e.g. for profiling runs)
+        _, bb, mv, ns = args.solver.split(":")
+        config = ed.SolverConfig((int(bb),) * n_sec, 0, mv == "proj", int(ns))
+        tune_table = []
     tune_s = time.perf_counter() - t0
     solver = BatchedSectorSolver(dm, sset, sectors, nev, precision=args.precision, params=params, config=config)
     b = solver.batch
@@ -535,7 +540,8 @@ def run_b200(args):
             "batched_over_plain": value / ws / plain_rate,
         })
         # FP64-matvec batched variant (its own tuned configuration)
-        cfg64, _ = tuner.tune(dm, sset, sectors, nev, precision=64, params=ed.LanczosParams(precision=64))
+        cfg64 = config if args.solver != "auto" else tuner.tune(
+            dm, sset, sectors, nev, precision=64, params=ed.LanczosParams(precision=64))[0]
         extra["fp64_batched_config"] = cfg64.describe()
         s64 = BatchedSectorSolver(dm, sset, sectors, nev, precision=64,
                                   params=ed.LanczosParams(precision=64), config=cfg64)
@@ -628,12 +634,34 @@ def main():
     ap.add_argument("--plain-sectors", type=int, default=12)
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--skip-scale", action="store_true")
+    ap.add_argument("--solver", default="auto",
+                    help='"auto" (measured by the autotuner) or "graph:<block>:<proj|otf>:<n_slots>"')
     ap.add_argument("--matvec-only", action="store_true",
                     help="only the 32-site matvec at scale (for kernel profiling)")
     ap.add_argument("--matvec-launches", type=int, default=20)
+    ap.add_argument("--solve-scale", type=int, default=0,
+                    help="only a batched solve of this many 32-site Haldane sectors (for kernel profiling)")
     ap.add_argument("--matvec-precision", type=int, default=0, choices=[0, 32, 64])
     ap.add_argument("--matvec-no-otf", action="store_true")
     args = ap.parse_args()
+    if args.solve_scale:
+        import realspace_exatdiagonalization_py_b200 as ed
+        import torch
+        from realspace_exatdiagonalization_py_b200 import models
+
+        model, nf = models.config_model("haldane32")
+        G = ed.build_translation_group(model.lattice)
+        data = ed.build_ed_data(model, filling_fraction=Fraction(nf, model.lattice.n_site), symmetry_group=G)
+        secs = list(range(args.solve_scale))
+        cfg = ed.SolverConfig((2,) * len(secs), 0, True, 16)
+        res = ed.solve_sectors_batched(data, secs, nev=4, precision=32, config=cfg, return_vectors=False)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = ed.solve_sectors_batched(data, secs, nev=4, precision=32, config=cfg, return_vectors=False)
+        torch.cuda.synchronize()
+        print(json.dumps({"workload": f"haldane32: {len(secs)} sectors, FP32 + FP64 refinement, b=2, nev 4",
+                          "solve_s": time.perf_counter() - t0, "E0": [float(res[s][0][0]) for s in secs]}))
+        return
     if args.matvec_only:
         import realspace_exatdiagonalization_py_b200 as ed
         from realspace_exatdiagonalization_py_b200 import models
