@@ -146,6 +146,113 @@ __device__ void lz_gram_chunk(const double2* __restrict__ V, const double2* __re
   }
 }
 
+// Finalisation of one instance's Gram partials (one block of kRT threads):
+// sum the chunk partials (G threads per entry over interleaved chunk subsets,
+// then in order: deterministic for a given chunk count), form
+// G' = G - C^H C, its Cholesky factor R and the projected-matrix entries.
+__device__ void lz_finalize(const rsed_lanczos_t& st, const LzDims& d, int inst, int pass, int b, int nb, int* stt,
+                            double2* sc, double2* sR, double2* sG, int* s_ok, double2* fin) {
+  const double2* part = reinterpret_cast<const double2*>(st.partial);
+  // ---- finalisation (one block per instance) ----
+  // G threads per entry sum interleaved chunk subsets, then the G partial
+  // sums are added in order (deterministic for a given chunk count)
+  const int nent = (nb + 1) * b * b;
+  const int G = max(1, kRT / nent);
+  {
+    // fin: kRT * kBMax >= nent * G entries
+    const int64_t cstride = (int64_t)d.n_inst * d.pslots * kBMax * kBMax;
+    for (int t = threadIdx.x; t < nent * G; t += kRT) {
+      const int e = t % nent, g = t / nent;
+      const int sl = e / (b * b), pq = e % (b * b), p = pq / b, q = pq % b;
+      const double2* src = part + (int64_t)inst * d.pslots * kBMax * kBMax + sl * kBMax * kBMax + p * kBMax + q;
+      double2 a = make_double2(0.0, 0.0);
+#pragma unroll 8
+      for (int c = g; c < d.n_chunks; c += G) a = cadd(a, __ldcg(src + c * cstride));
+      fin[g * nent + e] = a;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < nent; e += kRT) {
+      const int sl = e / (b * b), pq = e % (b * b), p = pq / b, q = pq % b;
+      double2 a = make_double2(0.0, 0.0);
+      for (int g = 0; g < G; ++g) a = cadd(a, fin[g * nent + e]);
+      sc[(sl * b + p) * kBMax + q] = a;  // row (sl*b + p), column q
+    }
+  }
+  __syncthreads();
+  // G' = G - C^H C, one thread per (p, q)
+  for (int e = threadIdx.x; e < b * b; e += blockDim.x) {
+    const int p = e / b, q = e % b;
+    double2 g = sc[(nb * b + p) * kBMax + q];
+    for (int r = 0; r < nb * b; ++r) g = csub(g, cdotc(sc[r * kBMax + p], sc[r * kBMax + q]));
+    sG[p * kBMax + q] = g;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double gmax = 0.0;
+    for (int p = 0; p < b; ++p) gmax = fmax(gmax, sc[(nb * b + p) * kBMax + p].x);
+    for (int i = 0; i < kBMax * kBMax; ++i) sR[i] = make_double2(0.0, 0.0);
+    bool ok = gmax > 0.0;
+    for (int j = 0; j < b && ok; ++j) {
+      double sdiag = sG[j * kBMax + j].x;
+      for (int k = 0; k < j; ++k) sdiag -= sR[k * kBMax + j].x * sR[k * kBMax + j].x + sR[k * kBMax + j].y * sR[k * kBMax + j].y;
+      if (!(sdiag > 1e-26 * gmax)) {
+        ok = false;
+        break;
+      }
+      const double rjj = sqrt(sdiag);
+      sR[j * kBMax + j] = make_double2(rjj, 0.0);
+      for (int q = j + 1; q < b; ++q) {
+        double2 t = sG[j * kBMax + q];
+        for (int k = 0; k < j; ++k) t = csub(t, cdotc(sR[k * kBMax + j], sR[k * kBMax + q]));
+        sR[j * kBMax + q] = make_double2(t.x / rjj, t.y / rjj);
+      }
+    }
+    *s_ok = ok;
+    if (!ok) {
+      stt[S_STATUS] = RSED_EBREAKDOWN;
+      stt[S_ACTIVE] = 0;
+    }
+  }
+  __syncthreads();
+  if (!*s_ok) return;
+  double2* coefp = reinterpret_cast<double2*>(st.coef) + (int64_t)inst * 2 * d.pslots * kBMax * kBMax;
+  double2* cp = coefp + (pass - 1) * d.pslots * kBMax * kBMax;
+  for (int e = threadIdx.x; e < nb * b * b; e += blockDim.x) {
+    const int r = e / b, q = e % b;  // C[s r'][q] stored slot-major as before
+    cp[(r / b) * kBMax * kBMax + (r % b) * kBMax + q] = sc[r * kBMax + q];
+  }
+  double2* Rout = cp + (d.pslots - 1) * kBMax * kBMax;
+  for (int e = threadIdx.x; e < kBMax * kBMax; e += blockDim.x) Rout[e] = sR[e];
+  if (pass == 2) {
+    const int nb_old = nb;
+    if (nb_old >= 1) {
+      // combine passes: C = C1 + C2 R1, Rtot = R2 R1 ; column block cb = nb_old-1
+      const double2* c1 = coefp;
+      const double2* R1 = coefp + (d.pslots - 1) * kBMax * kBMax;
+      double2* P = reinterpret_cast<double2*>(st.P) + (int64_t)inst * d.pm * d.pm;
+      const int cb = nb_old - 1;
+      for (int e = threadIdx.x; e < nb_old * b * b; e += blockDim.x) {
+        const int r = e / b, q = e % b, sl = r / b, p = r % b;
+        double2 v = c1[sl * kBMax * kBMax + p * kBMax + q];
+        for (int k = 0; k < b; ++k) v = cadd(v, cmul(sc[r * kBMax + k], R1[k * kBMax + q]));
+        P[(int64_t)r * d.pm + cb * b + q] = v;
+      }
+      for (int e = threadIdx.x; e < b * b; e += blockDim.x) {
+        const int p = e / b, q = e % b;
+        double2 v = make_double2(0.0, 0.0);
+        for (int k = 0; k < b; ++k) v = cadd(v, cmul(sR[p * kBMax + k], R1[k * kBMax + q]));
+        P[(int64_t)(nb_old * b + p) * d.pm + cb * b + q] = v;
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      stt[S_NEWSLOT] = nb_old;
+      stt[S_NB] = nb_old + 1;
+      stt[S_ITERS] += 1;
+    }
+  }
+}
+
 __global__ void __launch_bounds__(kRT) k_lz_reduce(rsed_lanczos_t st, LzDims d, int pass) {
   const int chunk = blockIdx.x;
   const int inst = blockIdx.y;
@@ -202,104 +309,7 @@ __global__ void __launch_bounds__(kRT) k_lz_reduce(rsed_lanczos_t st, LzDims d, 
   if (!s_last) return;
   __threadfence();
   if (threadIdx.x == 0) stt[S_TICKET] = 0;
-  // ---- finalisation (one block per instance) ----
-  // G threads per entry sum interleaved chunk subsets, then the G partial
-  // sums are added in order (deterministic for a given chunk count)
-  const int nent = (nb + 1) * b * b;
-  const int G = max(1, kRT / nent);
-  {
-    double2* fin = &red_l[0][0][0];  // kRT * kBMax >= nent * G entries
-    const int64_t cstride = (int64_t)d.n_inst * d.pslots * kBMax * kBMax;
-    for (int t = threadIdx.x; t < nent * G; t += kRT) {
-      const int e = t % nent, g = t / nent;
-      const int sl = e / (b * b), pq = e % (b * b), p = pq / b, q = pq % b;
-      const double2* src = part + (int64_t)inst * d.pslots * kBMax * kBMax + sl * kBMax * kBMax + p * kBMax + q;
-      double2 a = make_double2(0.0, 0.0);
-#pragma unroll 8
-      for (int c = g; c < d.n_chunks; c += G) a = cadd(a, __ldcg(src + c * cstride));
-      fin[g * nent + e] = a;
-    }
-    __syncthreads();
-    for (int e = threadIdx.x; e < nent; e += kRT) {
-      const int sl = e / (b * b), pq = e % (b * b), p = pq / b, q = pq % b;
-      double2 a = make_double2(0.0, 0.0);
-      for (int g = 0; g < G; ++g) a = cadd(a, fin[g * nent + e]);
-      sc[(sl * b + p) * kBMax + q] = a;  // row (sl*b + p), column q
-    }
-  }
-  __syncthreads();
-  // G' = G - C^H C, one thread per (p, q)
-  for (int e = threadIdx.x; e < b * b; e += blockDim.x) {
-    const int p = e / b, q = e % b;
-    double2 g = sc[(nb * b + p) * kBMax + q];
-    for (int r = 0; r < nb * b; ++r) g = csub(g, cdotc(sc[r * kBMax + p], sc[r * kBMax + q]));
-    sG[p * kBMax + q] = g;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double gmax = 0.0;
-    for (int p = 0; p < b; ++p) gmax = fmax(gmax, sc[(nb * b + p) * kBMax + p].x);
-    for (int i = 0; i < kBMax * kBMax; ++i) sR[i] = make_double2(0.0, 0.0);
-    bool ok = gmax > 0.0;
-    for (int j = 0; j < b && ok; ++j) {
-      double sdiag = sG[j * kBMax + j].x;
-      for (int k = 0; k < j; ++k) sdiag -= sR[k * kBMax + j].x * sR[k * kBMax + j].x + sR[k * kBMax + j].y * sR[k * kBMax + j].y;
-      if (!(sdiag > 1e-26 * gmax)) {
-        ok = false;
-        break;
-      }
-      const double rjj = sqrt(sdiag);
-      sR[j * kBMax + j] = make_double2(rjj, 0.0);
-      for (int q = j + 1; q < b; ++q) {
-        double2 t = sG[j * kBMax + q];
-        for (int k = 0; k < j; ++k) t = csub(t, cdotc(sR[k * kBMax + j], sR[k * kBMax + q]));
-        sR[j * kBMax + q] = make_double2(t.x / rjj, t.y / rjj);
-      }
-    }
-    s_ok = ok;
-    if (!ok) {
-      stt[S_STATUS] = RSED_EBREAKDOWN;
-      stt[S_ACTIVE] = 0;
-    }
-  }
-  __syncthreads();
-  if (!s_ok) return;
-  double2* coef = reinterpret_cast<double2*>(st.coef) + (int64_t)inst * 2 * d.pslots * kBMax * kBMax;
-  double2* cp = coef + (pass - 1) * d.pslots * kBMax * kBMax;
-  for (int e = threadIdx.x; e < nb * b * b; e += blockDim.x) {
-    const int r = e / b, q = e % b;  // C[s r'][q] stored slot-major as before
-    cp[(r / b) * kBMax * kBMax + (r % b) * kBMax + q] = sc[r * kBMax + q];
-  }
-  double2* Rout = cp + (d.pslots - 1) * kBMax * kBMax;
-  for (int e = threadIdx.x; e < kBMax * kBMax; e += blockDim.x) Rout[e] = sR[e];
-  if (pass == 2) {
-    const int nb_old = nb;
-    if (nb_old >= 1) {
-      // combine passes: C = C1 + C2 R1, Rtot = R2 R1 ; column block cb = nb_old-1
-      const double2* c1 = coef;
-      const double2* R1 = coef + (d.pslots - 1) * kBMax * kBMax;
-      double2* P = reinterpret_cast<double2*>(st.P) + (int64_t)inst * d.pm * d.pm;
-      const int cb = nb_old - 1;
-      for (int e = threadIdx.x; e < nb_old * b * b; e += blockDim.x) {
-        const int r = e / b, q = e % b, sl = r / b, p = r % b;
-        double2 v = c1[sl * kBMax * kBMax + p * kBMax + q];
-        for (int k = 0; k < b; ++k) v = cadd(v, cmul(sc[r * kBMax + k], R1[k * kBMax + q]));
-        P[(int64_t)r * d.pm + cb * b + q] = v;
-      }
-      for (int e = threadIdx.x; e < b * b; e += blockDim.x) {
-        const int p = e / b, q = e % b;
-        double2 v = make_double2(0.0, 0.0);
-        for (int k = 0; k < b; ++k) v = cadd(v, cmul(sR[p * kBMax + k], R1[k * kBMax + q]));
-        P[(int64_t)(nb_old * b + p) * d.pm + cb * b + q] = v;
-      }
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      stt[S_NEWSLOT] = nb_old;
-      stt[S_NB] = nb_old + 1;
-      stt[S_ITERS] += 1;
-    }
-  }
+  lz_finalize(st, d, inst, pass, b, nb, stt, sc, sR, sG, &s_ok, &red_l[0][0][0]);
 }
 
 // W <- (W - V C) R^-1 ; pass 2 writes the new basis block and the matvec input.
