@@ -754,7 +754,9 @@ __device__ void herm_lowest(double2* A, int M, int Kp, double* theta, double2* S
 }
 
 // Ritz step: per instance, when due.  Dynamic smem: 2 * kJacobiMax^2 double2.
-__global__ void k_lz_ritz(rsed_lanczos_t st, LzDims d, int check_every, int force, int rr) {
+constexpr int kRitzThreads = 256;  // one CTA per instance (512 measured no faster: serial FP64 chains)
+__global__ void __launch_bounds__(kRitzThreads) k_lz_ritz(rsed_lanczos_t st, LzDims d, int check_every, int force,
+                                                         int rr) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int inst = blockIdx.x;
   int* stt = st.state + inst * kStateInts;
@@ -1765,7 +1767,7 @@ extern "C" int rsed_lanczos_iterate(const rsed_model_t* md, const rsed_sectors_t
     if (rc) return rc;
     rc = launch_pass(*st, d, 2, stream);
     if (rc) return rc;
-    k_lz_ritz<<<d.n_inst, 256, kRitzSmem, stream>>>(*st, d, check_every, 0, 0);
+    k_lz_ritz<<<d.n_inst, kRitzThreads, kRitzSmem, stream>>>(*st, d, check_every, 0, 0);
     RSED_CHECK_LAUNCH();
     k_lz_restart<<<dim3((unsigned)((d.n_orb + 255) / 256), d.n_inst), 256, 0, stream>>>(*st, d);
     RSED_CHECK_LAUNCH();
@@ -1796,7 +1798,7 @@ extern "C" int rsed_lanczos_rayleigh_ritz(const rsed_model_t* md, const rsed_sec
   dim3 g(d.n_chunks, d.n_inst);
   k_rr_gram<<<g, 128, 0, stream>>>(*st, d);
   RSED_CHECK_LAUNCH();
-  k_lz_ritz<<<d.n_inst, 256, kRitzSmem, stream>>>(*st, d, 1, 1, 1);
+  k_lz_ritz<<<d.n_inst, kRitzThreads, kRitzSmem, stream>>>(*st, d, 1, 1, 1);
   RSED_CHECK_LAUNCH();
   k_rr_resid<<<g, 128, 0, stream>>>(*st, d);
   RSED_CHECK_LAUNCH();
