@@ -246,6 +246,23 @@ int rsed_triplets_fill(const rsed_model_t* model, int64_t n_rows, const int32_t*
 int rsed_csr_spmv(int64_t n_rows, const int64_t* row_ptr, const int32_t* col_idx,
                   const double* vals, int32_t n_vec, const double* x, double* y, void* stream);
 
+/* ---- K9: sector state -> Fock amplitudes ------------------------------------
+ * Replaces _expand_sector_state_to_fock_amplitudes
+ * (observables/entanglement_spectrum.py:82-145).  x_orbit holds the sector
+ * vector in orbit layout (complex128 per orbit, zero outside the sector), chi
+ * the sector's |G| characters.  For every basis state (table rank r) amp[r] =
+ * sum over g with g(s) = mask(r), ascending, of
+ * x[s] / sqrt(|G| |Stab(s)|) * conj(chi(g)) * phase_g(s) (product form),
+ * representatives with |x| <= atol skipped, amplitudes <= atol set to 0, then
+ * the whole vector scaled to unit norm; masks[r] (optional, NULL = skip) gets
+ * the state's mask.  *norm2_out receives the norm before scaling (the call
+ * synchronises the stream); RSED_EINVAL if it is <= atol. */
+size_t rsed_fock_scratch_bytes(int64_t n_states);
+int rsed_fock_expand(const rsed_group_t* grp, const rsed_entry_t* table, int64_t n_orbits,
+                     const uint64_t* repr_masks, const uint64_t* stab_mask, const double* x_orbit,
+                     const double* chi, double atol, double* amp, uint64_t* masks, double* norm2_out,
+                     void* scratch, size_t scratch_bytes, void* stream);
+
 /* ---- K8: batched thick-restart block Lanczos -------------------------------
  * Replaces diagonalize_block_matrixfree / diagonalize_block_arpack
  * (symmetry_resolved_ed.py:2214-2299, ARPACK eigs(which="SR", tol=1e-10))

@@ -13,6 +13,8 @@ import this module.  It restates, in vectorised numpy, the algorithm of
 * the sector filter (SRE:1484-1546),
 * the per-term vectorised triplet builder (SRE:595-693) and the CSR operator
   (SRE:1913-1976),
+* the sector-state -> Fock amplitude expansion
+  (``observables/entanglement_spectrum.py:82-145``),
 * the eigen-solves: dense ``eigh(UPLO="U")`` for n <= 500 and ARPACK
   ``eigs(k=nev, which="SR", tol=1e-10)`` with the seeded ``v0`` otherwise
   (SRE:2180-2299).
@@ -361,3 +363,28 @@ def scan(model, n_filled: int, G, irreps, nev: int, sectors=None):
         w, _ = solve(H, nev)
         out[s] = (w, len(orbits))
     return out
+
+
+def fock_expand(cat: dict, orbits: np.ndarray, c: np.ndarray, chi: np.ndarray, perm0: np.ndarray,
+                eta: np.ndarray, fermion: bool, atol: float = 1e-12) -> dict:
+    """Sector vector -> normalised Fock amplitudes {mask: amplitude}
+    (observables/entanglement_spectrum.py:82-145): every representative with
+    |c| > atol adds c / sqrt(|G| |Stab|) * conj(chi(g)) * U_g|s> for all g;
+    amplitudes <= atol are dropped and the rest renormalised."""
+    ng = perm0.shape[0]
+    amps: dict = {}
+    for col, o in enumerate(orbits):
+        coeff = c[col]
+        if abs(coeff) <= atol:
+            continue
+        pref = coeff / np.sqrt(ng * len(cat["stab_g"][o]))
+        m = int(cat["reprs"][o])
+        for g in range(ng):
+            img, ph = apply_product(m, perm0[g], eta[g], fermion)
+            amps[img] = amps.get(img, 0j) + pref * np.conj(chi[g]) * ph
+    amps = {k: v for k, v in amps.items() if abs(v) > atol}
+    norm2 = sum(abs(v) ** 2 for v in amps.values())
+    if norm2 <= atol:
+        raise ValueError("Expanded state has near-zero norm.")
+    inv = 1.0 / np.sqrt(norm2)
+    return {k: v * inv for k, v in amps.items()}

@@ -168,6 +168,9 @@ SIGNATURES = {
         c_int,
         [POINTER(RsedModel), POINTER(RsedSectors), c_void_p, c_void_p, c_int32, c_int32, c_void_p],
     ),
+    "rsed_fock_scratch_bytes": (c_size_t, [c_int64]),
+    "rsed_fock_expand": (c_int, [POINTER(RsedGroup), c_void_p, c_int64, c_void_p, c_void_p, c_void_p, c_void_p,
+                                 c_double, c_void_p, c_void_p, POINTER(c_double), c_void_p, c_size_t, c_void_p]),
     "rsed_proj_scratch_bytes": (c_size_t, [c_int64]),
     "rsed_proj_count": (c_int, [POINTER(RsedModel), c_void_p, POINTER(c_int64), c_void_p, c_size_t, c_void_p]),
     "rsed_proj_fill": (c_int, [POINTER(RsedModel), c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),

@@ -276,7 +276,6 @@ __global__ void __launch_bounds__(kRT) k_lz_reduce(rsed_lanczos_t st, LzDims d, 
     }
     return;
   }
-  const int npairs = (nb + 1) * b;
   const int64_t r0 = (int64_t)chunk * d.chunk_rows;
   const int64_t r1 = min(r0 + d.chunk_rows, d.n_orb);
   const double2* V = reinterpret_cast<const double2*>(st.V);

@@ -124,3 +124,22 @@ def test_two_species_rank_roundtrip():
         m = ur(r)
         assert np.array_equal(rk(m), r)
         assert np.all(np.diff(r) > 0) and len(np.unique(m)) == C
+
+
+@pytest.mark.parametrize("case", ["haldane12_flux", "checkerboard12_flux", "hubbard12"])
+def test_fock_expansion_matches_reference(golden, case):
+    """The oracle's sector -> Fock expansion against the reference's own
+    function (tests/golden/make_fock_golden.py)."""
+    import os
+
+    g = golden(case)
+    f = np.load(os.path.join(os.path.dirname(__file__), "golden", f"fock_{case}.npz"))
+    n, k = int(g["n_site"]), int(g["n_filled"])
+    perm0 = (g["perm"] - 1).astype(np.uint8)
+    cat = port.catalog(n, k, perm0, g["eta"], bool(g["fermionic"]))
+    for s in f["sectors"]:
+        orbits = port.sector_orbits(cat, g["chi"][s])
+        amps = port.fock_expand(cat, orbits, f[f"c_{s}"], g["chi"][s], perm0, g["eta"], bool(g["fermionic"]))
+        keys = np.array(sorted(amps), dtype=np.uint64)
+        np.testing.assert_array_equal(keys, f[f"masks_{s}"])
+        np.testing.assert_allclose(np.array([amps[int(x)] for x in keys]), f[f"amps_{s}"], atol=1e-14, rtol=0)
