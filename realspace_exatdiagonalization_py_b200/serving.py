@@ -111,6 +111,10 @@ class ServingModel:
             symmetry_group=self.group0, particle_statistics=self.stats)
         self.n_orbits = self.catalog.n_orbits
         self.n_sectors = len(build_irrep_list(self.group0, self.lattice))
+        # sector dimensions at zero flux (flux points differ only for orbits
+        # with nontrivial stabilizers): decides dense vs Lanczos admission
+        self.dims_hint: list[int] | None = SectorSet(self.catalog, build_irrep_list(self.group0,
+                                                                                    self.lattice)).dims
         self.base: FluxContext | None = None  # zero-flux context: owns the shared table structure
         self.ctx_bytes: int | None = None     # measured device bytes of a flux point, once one was built
 
@@ -348,7 +352,8 @@ class SolveServer:
 
     def __init__(self, models: dict[str, ServingModel] | ServingModel, *, nev: int = 4, precision: int = 32,
                  block: int = 4, n_slots: int = 16, poll: int = 16, max_width: int = 4,
-                 memory_budget: int | None = None, max_iter: int = 4000, creations_per_step: int = 1):
+                 memory_budget: int | None = None, max_iter: int = 4000, creations_per_step: int = 1,
+                 dense_max: int = 500):
         if isinstance(models, ServingModel):
             models = {models.name: models}
         self.models = dict(models)
@@ -362,6 +367,10 @@ class SolveServer:
         # new flux contexts and lanes cost milliseconds of host work; making at
         # most this many per step keeps the running lanes fed in between
         self.creations_per_step = creations_per_step
+        # sectors up to this dimension are solved densely at admission (as the
+        # reference does below 500), not in a Lanczos lane
+        self.dense_max = dense_max
+        self._ready: list[SolveResult] = []
         if memory_budget is None:
             free, _ = torch.cuda.mem_get_info()
             memory_budget = int(0.8 * free)
@@ -456,6 +465,23 @@ class SolveServer:
                 for ln in self.lanes:
                     ln.poll_once(0.0, self.max_iter)
 
+    def _dense(self, req: SolveRequest, ctx: FluxContext, now: float) -> SolveResult:
+        from .hamiltonian import MatrixFreeHamiltonian
+        from .lanczos import diagonalize_block_matrixfree
+        from .sector import Symmetry_Sector_Basis
+
+        basis = Symmetry_Sector_Basis(ctx.irreps[req.sector], ctx.catalog, ctx.sset, req.sector)
+        if basis.dim == 0:
+            vals = np.zeros(0)
+        else:
+            H = MatrixFreeHamiltonian(basis, ctx.dm.bilinear_terms, ctx.dm.density_terms, None, model=ctx.dm)
+            vals, _ = diagonalize_block_matrixfree(H, basis.dim, nev=self.nev)
+        k = len(vals)
+        return SolveResult(rid=req.rid, sector=req.sector, flux=req.flux, model=req.model,
+                           eigenvalues=np.asarray(vals, dtype=np.float64), residuals=np.zeros(k), fp32_error=None,
+                           iterations=0, dim=basis.dim, arrival=req.arrival, admitted=now, finished=self.now(),
+                           lane=0, lane_width=1)
+
     def _admit(self, now: float) -> None:
         groups: OrderedDict[tuple, list[SolveRequest]] = OrderedDict()
         for r in self.pending:
@@ -464,6 +490,20 @@ class SolveServer:
         created = 0
         for key, reqs in groups.items():
             sm = self.models[key[0]]
+            small = [r for r in reqs if sm.dims_hint is not None and sm.dims_hint[r.sector] <= self.dense_max]
+            if small:
+                have_ctx = (sm.base is not None) if not any(key[1]) else key in self.contexts
+                if not have_ctx and created >= self.creations_per_step:
+                    continue
+                ctx = self._context(sm, key[1])
+                if ctx is None:
+                    continue
+                created += 0 if have_ctx else 1
+                for r in small:
+                    if ctx.sset.dims[r.sector] <= self.dense_max:
+                        self._ready.append(self._dense(r, ctx, now))
+                        admitted.add(r.rid)
+                reqs = [r for r in reqs if r.rid not in admitted]
             while reqs:
                 idle = [ln for ln in self.lanes if ln.sm is sm and ln.state == "idle" and ln.width <= len(reqs)]
                 lane = max(idle, key=lambda ln: ln.width) if idle else None
@@ -498,7 +538,8 @@ class SolveServer:
     def step(self) -> list[SolveResult]:
         """One scheduling round; returns the requests that finished in it."""
         now = self.now()
-        done: list[SolveResult] = []
+        done: list[SolveResult] = self._ready
+        self._ready = []
         for ln in list(self.lanes):
             res = ln.poll_once(now, self.max_iter)
             if res:
