@@ -263,6 +263,19 @@ int rsed_fock_expand(const rsed_group_t* grp, const rsed_entry_t* table, int64_t
                      const double* chi, double atol, double* amp, uint64_t* masks, double* norm2_out,
                      void* scratch, size_t scratch_bytes, void* stream);
 
+/* Overlap matrices of dense Fock-amplitude states, for the Berry links of
+ * many_body_chern_number (replaces _fock_amplitude_overlap and
+ * _subspace_overlap_matrix, observables/many_body_chern_number.py:141-182).
+ * states: device complex128 [n_slots][n_m][n_states], each level a dense
+ * rank-indexed vector as rsed_fock_expand writes it.  pairs: HOST int32
+ * [n_pairs][2] slot indices (a, b), each in [0, n_slots).  out: device
+ * complex128 [n_pairs][n_m][n_m], out[p][i][j] = sum_r conj(a_i[r]) b_j[r],
+ * the same sum order on every run.  Asynchronous on `stream`. */
+size_t rsed_fock_overlap_scratch_bytes(int64_t n_states, int32_t n_m, int32_t n_pairs);
+int rsed_fock_overlaps(const double* states, int64_t n_states, int32_t n_m, int32_t n_slots,
+                       const int32_t* pairs, int32_t n_pairs, double* out, void* scratch,
+                       size_t scratch_bytes, void* stream);
+
 /* ---- K8: batched thick-restart block Lanczos -------------------------------
  * Replaces diagonalize_block_matrixfree / diagonalize_block_arpack
  * (symmetry_resolved_ed.py:2214-2299, ARPACK eigs(which="SR", tol=1e-10))

@@ -15,6 +15,9 @@ import this module.  It restates, in vectorised numpy, the algorithm of
   (SRE:1913-1976),
 * the sector-state -> Fock amplitude expansion
   (``observables/entanglement_spectrum.py:82-145``),
+* the many-body Chern number on the flux torus: dictionary overlaps,
+  determinant links and plaquette phases
+  (``observables/many_body_chern_number.py:141-207, 341-438``),
 * the eigen-solves: dense ``eigh(UPLO="U")`` for n <= 500 and ARPACK
   ``eigs(k=nev, which="SR", tol=1e-10)`` with the seeded ``v0`` otherwise
   (SRE:2180-2299).
@@ -388,3 +391,68 @@ def fock_expand(cat: dict, orbits: np.ndarray, c: np.ndarray, chi: np.ndarray, p
         raise ValueError("Expanded state has near-zero norm.")
     inv = 1.0 / np.sqrt(norm2)
     return {k: v * inv for k, v in amps.items()}
+
+
+def fock_overlap(a: dict, b: dict) -> complex:
+    """<a|b> of two {mask: amplitude} maps (many_body_chern_number.py:141-160)."""
+    if len(a) <= len(b):
+        return sum((np.conj(v) * b.get(k, 0j) for k, v in a.items()), 0j)
+    return sum((np.conj(a.get(k, 0j)) * v for k, v in b.items()), 0j)
+
+
+def chern(model, n_filled: int, labels, grid, nev: int, flux_setup, det_atol: float = 1e-10):
+    """Many-body Chern number (many_body_chern_number.py:341-438) on the CPU.
+
+    ``flux_setup(flux)`` moves ``model`` to the flux point and returns
+    ``(G, irreps)``; ``labels`` is ``["identity"]`` or momentum tuples.  Each
+    sector is solved in matrix mode (``solve(..., seeded_v0=False)``), its
+    lowest ``nev`` states expanded with ``fock_expand``.  Returns a dict with
+    ``chern_number``, ``berry_curvature``, ``link_det_abs_x/y``,
+    ``energies[nx, ny, n]`` and ``n_singular`` (links replaced by 1)."""
+    nx, ny = grid
+    n = model.lattice.n_site
+    fermion = model.particle_statistics.name == "FERMIONIC"
+    states = [[None] * ny for _ in range(nx)]
+    energies = np.zeros((nx, ny, len(labels) * nev))
+    for ix in range(nx):
+        for iy in range(ny):
+            G, irreps = flux_setup([ix / nx, iy / ny])
+            perm0, eta = group_arrays(G)
+            cat = catalog(n, n_filled, perm0, eta, fermion)
+            pts = []
+            for label in labels:
+                s = 0 if label == "identity" else next(i for i, ir in enumerate(irreps) if ir.label == label)
+                chi = np.asarray(irreps[s].values, dtype=np.complex128)
+                orbits = sector_orbits(cat, chi)
+                H = csr_block(cat, n, orbits, model.bilinear_terms, model.density_density_terms, chi, fermion)
+                w, v = solve(H, nev, seeded_v0=False)
+                for lev in range(nev):
+                    energies[ix, iy, len(pts)] = w[lev]
+                    pts.append(fock_expand(cat, orbits, v[:, lev], chi, perm0, eta, fermion))
+            states[ix][iy] = pts
+    n_sing = 0
+
+    def link(a, b):
+        nonlocal n_sing
+        M = np.array([[fock_overlap(x, y) for y in b] for x in a], dtype=np.complex128)
+        z = np.linalg.det(M)
+        if abs(z) <= det_atol:
+            n_sing += 1
+            return 1.0 + 0.0j, abs(z)
+        return z / abs(z), abs(z)
+
+    Ux = np.empty((nx, ny), dtype=np.complex128)
+    Uy = np.empty((nx, ny), dtype=np.complex128)
+    dx = np.empty((nx, ny))
+    dy = np.empty((nx, ny))
+    for ix in range(nx):
+        for iy in range(ny):
+            Ux[ix, iy], dx[ix, iy] = link(states[ix][iy], states[(ix + 1) % nx][iy])
+            Uy[ix, iy], dy[ix, iy] = link(states[ix][iy], states[ix][(iy + 1) % ny])
+    F = np.empty((nx, ny))
+    for ix in range(nx):
+        for iy in range(ny):
+            ixp, iyp = (ix + 1) % nx, (iy + 1) % ny
+            F[ix, iy] = np.angle(Ux[ix, iy] * Uy[ixp, iy] * np.conj(Ux[ix, iyp]) * np.conj(Uy[ix, iy]))
+    return {"chern_number": float(F.sum()) / (2 * np.pi), "berry_curvature": F, "link_det_abs_x": dx,
+            "link_det_abs_y": dy, "energies": energies, "n_singular": n_sing}

@@ -12,6 +12,20 @@ returned as a ``SimpleNamespace`` with the reference's fields.  Two engines:
   ``SolveServer`` -- the zero-flux catalog is built once and moved to each flux
   point by ``update_orbit_stabilizer_phases``, solves of different flux points
   overlap on the device; no checkpoints (``checkpoint_paths`` is ``None``).
+
+``many_body_chern_number`` keeps the contract of the reference's driver
+(``observables/many_body_chern_number.py:341-458``): the Chern number of the
+manifold spanned by the lowest ``nev_per_sector`` states of the given sectors
+on an ``nx x ny`` twisted-boundary flux torus, from U(1) links (phases of the
+determinants of overlap matrices between neighbouring flux points) and
+plaquette phases summed over 2 pi.  Each flux point is solved like the
+reference's (one ED scan of the listed sectors with a checkpoint per point,
+reused unless ``overwrite``), on a phase-updated copy of the zero-flux
+catalog; its manifold states are expanded into dense rank-indexed Fock
+vectors on the device, and the overlap matrices of each row of links are one
+device launch (``rsed_fock_overlaps``).  Only the zero-flux row and the two
+most recent rows stay resident, so device memory is
+``3 * ny * n_manifold * n_states * 16`` bytes, not the whole grid.
 """
 
 from __future__ import annotations
@@ -22,7 +36,7 @@ from types import SimpleNamespace
 
 import numpy as np
 
-__all__ = ["flux_spectrum_flow"]
+__all__ = ["flux_spectrum_flow", "many_body_chern_number"]
 
 
 def _labels(sector_labels):
@@ -111,3 +125,209 @@ def flux_spectrum_flow(model, sector_labels, *, filling_fraction, flux_direction
     return SimpleNamespace(twisted_phases_over_2π_list=thetas, energies=energies, sector_labels=labels,
                            flux_direction=flux_direction, nev=nev, is_identity=is_identity, fig_path=fig_path,
                            checkpoint_paths=checkpoint_paths)
+
+
+# ---- many-body Chern number ----------------------------------------------------
+
+
+def _normalize_flux_grid_size(flux_grid_size) -> tuple[int, int]:
+    """``(nx, ny)`` from an int (square grid) or a pair; each at least 2
+    (``many_body_chern_number.py:37-56``)."""
+    if isinstance(flux_grid_size, int):
+        nx = ny = int(flux_grid_size)
+    else:
+        nx, ny = int(flux_grid_size[0]), int(flux_grid_size[1])
+    if min(nx, ny) < 2:
+        raise ValueError("flux_grid_size must be at least 2 in both directions.")
+    return nx, ny
+
+
+def _chern_sector_labels(sector_labels) -> list:
+    """``["identity"]`` or the momentum labels as int tuples (``:59-72``)."""
+    if isinstance(sector_labels, str) and sector_labels == "identity":
+        return ["identity"]
+    return [tuple(int(x) for x in lab) for lab in sector_labels]
+
+
+def _chern_params_digest(params: dict) -> str:
+    """64-bit FNV-1a of the UTF-8 ``repr`` of the parameter pairs sorted by key
+    name, in hex: the checkpoint-name tag of the reference (``:75-94``), kept
+    byte-compatible so checkpoints of either implementation are found."""
+    data = repr(sorted(params.items(), key=lambda kv: str(kv[0]))).encode("utf-8")
+    h = 0xCBF29CE484222325
+    for byte in data:
+        h = ((h ^ byte) * 0x100000001B3) % (1 << 64)
+    return f"{h:x}"
+
+
+def _chern_flux_tag(flux) -> str:
+    """``0.250000_0.500000`` style tag with ``.`` -> ``p`` and ``-`` -> ``m`` (``:97-108``)."""
+    return "_".join(f"{float(t):.6f}".replace(".", "p").replace("-", "m") for t in flux)
+
+
+def _chern_checkpoint_path(model, filling_fraction: Fraction, flux, checkpoint_dir: str) -> str:
+    """Checkpoint file of one flux point of the Chern scan, named as the
+    reference names it (``:111-138``)."""
+    sample = "x".join(str(n) for n in model.lattice.sample_size)
+    name = (f"many_body_chern_{model.tb_model.model_name}_{sample}_nu={filling_fraction.numerator}_"
+            f"{filling_fraction.denominator}_theta={_chern_flux_tag(flux)}_p={_chern_params_digest(model.params)}.pkl")
+    return os.path.join(checkpoint_dir, name)
+
+
+def _unit_det_link(M: np.ndarray, *, det_atol: float = 1e-10):
+    """``(z / |z|, |z|)`` for ``z = det(M)``; a near-singular ``|z| <= det_atol``
+    gives the link 1 and a warning (``:185-207``)."""
+    import warnings
+
+    z = complex(np.linalg.det(M))
+    if abs(z) <= det_atol:
+        warnings.warn("Near-singular Berry link; selected manifold may not be isolated.", stacklevel=2)
+        return 1.0 + 0.0j, abs(z)
+    return z / abs(z), abs(z)
+
+
+def _chern_point(model, labels, base, filling_fraction, flux, nev_per_sector, mode, checkpoint_dir, overwrite,
+                 out):
+    """Solve one flux point and expand its manifold states into ``out``
+    (``[n_manifold, n_states]`` device rows) -- the reference's
+    ``_flux_point_states_for_chern`` (``:210-307``) with dense device states."""
+    from .catalog import update_orbit_stabilizer_phases
+    from .ed import Symmetry_Resolved_ED_Data, _ed_scan_sectors
+    from .fock import expand_sector_state_to_fock_dense
+    from .second_quantized_model import update_second_quantized_model_with_twisted_phases
+    from .sector import Symmetry_Sector_Basis, build_symmetry_sector_basis
+    from .symmetry import build_irrep_list, build_translation_group
+
+    update_second_quantized_model_with_twisted_phases(model, twisted_phases_over_2π=list(flux))
+    identity = labels == ["identity"]
+    if identity:
+        group, cat = base.symmetry_group, base.orbit_catalog
+    else:
+        group = build_translation_group(model.lattice, list(flux))
+        cat = base.orbit_catalog.clone()
+        update_orbit_stabilizer_phases(cat, group, model.particle_statistics)
+    irreps = build_irrep_list(group, model.lattice)
+    data = Symmetry_Resolved_ED_Data(model, base.n_filled, filling_fraction, group, irreps, cat, [0] * len(irreps))
+    path = _chern_checkpoint_path(model, filling_fraction, flux, checkpoint_dir)
+    _ed_scan_sectors(data, nev=nev_per_sector, mode=mode, scanned_sectors=None if identity else list(labels),
+                     checkpoint_path=path, overwrite=overwrite)
+    _, sset = data._device()
+    energies, level_labels = [], []
+    row = 0
+    for label in labels:
+        if identity:
+            idx = 0
+        else:
+            idx = next((i for i, ir in enumerate(irreps) if ir.label == label), None)
+            if idx is None:
+                raise ValueError(f"Sector {label!r} not found at flux {list(flux)}.")
+        if idx not in data.ed_scan_res:
+            raise ValueError(f"Sector {label!r} was not scanned at flux {list(flux)}.")
+        vals, vecs = data.ed_scan_res[idx]
+        n_take = min(nev_per_sector, vecs.shape[1])
+        if n_take != nev_per_sector:
+            raise ValueError(f"Requested {nev_per_sector} states in sector {label!r}, only found {n_take}.")
+        basis = (Symmetry_Sector_Basis(irreps[idx], cat, sset, idx) if sset is not None
+                 else build_symmetry_sector_basis(cat, irreps[idx]))
+        for level in range(n_take):
+            expand_sector_state_to_fock_dense(vecs[:, level], basis, out=out[row])
+            energies.append(float(vals[level]))
+            level_labels.append((label, level + 1))
+            row += 1
+    return energies, level_labels, path
+
+
+def _plot_many_body_chern_curvature(result, *, fig_path: str | None = None):
+    import matplotlib.pyplot as plt  # optional, as in the reference
+
+    fig, ax = plt.subplots(figsize=(6.5, 5.4))
+    ax.set_xlabel("θ_x / 2π")
+    ax.set_ylabel("θ_y / 2π")
+    ax.set_title(f"Flux-torus Berry curvature, C={result.chern_number:.6f}")
+    mesh = ax.pcolormesh(result.flux_x, result.flux_y, result.berry_curvature.T, shading="auto", cmap="RdBu")
+    fig.colorbar(mesh, ax=ax, label="plaquette phase")
+    if fig_path is not None:
+        os.makedirs(os.path.dirname(os.path.abspath(fig_path)), exist_ok=True)
+        fig.savefig(fig_path)
+    return fig, ax
+
+
+def many_body_chern_number(model, sector_labels, *, filling_fraction, flux_grid_size=(5, 5), nev_per_sector: int = 1,
+                           mode: str = "matrix", checkpoint_dir: str = "checkpoints", overwrite: bool = False,
+                           fig_path: str | None = None, det_atol: float = 1e-10):
+    """Chern number of the many-body manifold on the flux torus; returns the
+    reference's fields (``chern_number``, ``rounded_chern``,
+    ``berry_curvature[ix, iy]``, ``flux_x``, ``flux_y``, ``sector_labels``,
+    ``nev_per_sector``, ``flux_grid_size``, ``energies[ix][iy]``,
+    ``min_link_det``, ``link_det_abs_x``, ``link_det_abs_y``,
+    ``checkpoint_paths[ix][iy]``, ``fig_path``)."""
+    import torch
+
+    from .ed import build_ed_data
+    from .fock import fock_overlaps
+    from .second_quantized_model import update_second_quantized_model_with_twisted_phases
+    from .symmetry import build_identity_group, build_translation_group
+
+    filling_fraction = Fraction(filling_fraction)
+    if model.lattice.dim != 2:
+        raise ValueError("many_body_chern_number currently expects a 2D lattice.")
+    nx, ny = _normalize_flux_grid_size(flux_grid_size)
+    labels = _chern_sector_labels(sector_labels)
+    if mode not in ("matrix", "matrixfree"):
+        raise ValueError(f"Unknown ED scan mode: {mode}. Use 'matrix' or 'matrixfree'.")
+    flux_x = np.arange(nx) / nx
+    flux_y = np.arange(ny) / ny
+    os.makedirs(checkpoint_dir, exist_ok=True)
+
+    # the zero-flux catalog, moved to every flux point by a phase update
+    update_second_quantized_model_with_twisted_phases(model, twisted_phases_over_2π=[0.0, 0.0])
+    group0 = (build_identity_group(model.lattice.n_site) if labels == ["identity"]
+              else build_translation_group(model.lattice, [0.0, 0.0]))
+    base = build_ed_data(model, filling_fraction=filling_fraction, symmetry_group=group0)
+    cat = base.orbit_catalog
+    n_m = len(labels) * int(nev_per_sector)
+    rows_kept = min(nx, 3)
+    states = torch.zeros((rows_kept * ny, n_m, cat.n_states), dtype=torch.complex128, device=cat.table.device)
+
+    def slot(ix, iy):  # row 0 stays; later rows alternate between two row buffers
+        return iy if ix == 0 else ny * (1 + (ix - 1) % 2) + iy
+
+    Ux = np.empty((nx, ny), dtype=np.complex128)
+    Uy = np.empty((nx, ny), dtype=np.complex128)
+    det_abs_x = np.empty((nx, ny))
+    det_abs_y = np.empty((nx, ny))
+
+    def row_links(ix, ixp):
+        pairs = [(slot(ix, iy), slot(ixp, iy)) for iy in range(ny)]
+        pairs += [(slot(ix, iy), slot(ix, (iy + 1) % ny)) for iy in range(ny)]
+        M = fock_overlaps(states, pairs)
+        for iy in range(ny):
+            Ux[ix, iy], det_abs_x[ix, iy] = _unit_det_link(M[iy], det_atol=det_atol)
+            Uy[ix, iy], det_abs_y[ix, iy] = _unit_det_link(M[ny + iy], det_atol=det_atol)
+
+    energies = [[None] * ny for _ in range(nx)]
+    checkpoint_paths = [[None] * ny for _ in range(nx)]
+    for ix in range(nx):
+        for iy in range(ny):
+            flux = (float(flux_x[ix]), float(flux_y[iy]))
+            energies[ix][iy], _, checkpoint_paths[ix][iy] = _chern_point(
+                model, labels, base, filling_fraction, flux, nev_per_sector, mode, checkpoint_dir, overwrite,
+                states[slot(ix, iy)])
+        if ix >= 1:
+            row_links(ix - 1, ix)
+    row_links(nx - 1, 0)
+
+    ixp = (np.arange(nx) + 1) % nx
+    iyp = (np.arange(ny) + 1) % ny
+    plaquette = Ux * Uy[ixp, :] * np.conj(Ux[:, iyp]) * np.conj(Uy)
+    berry_curvature = np.angle(plaquette).astype(np.float64)
+    chern_number = float(np.sum(berry_curvature)) / (2 * np.pi)
+    res = SimpleNamespace(chern_number=chern_number, rounded_chern=round(chern_number),
+                          berry_curvature=berry_curvature, flux_x=flux_x, flux_y=flux_y, sector_labels=labels,
+                          nev_per_sector=nev_per_sector, flux_grid_size=(nx, ny), energies=energies,
+                          min_link_det=min(float(det_abs_x.min()), float(det_abs_y.min())),
+                          link_det_abs_x=det_abs_x, link_det_abs_y=det_abs_y, checkpoint_paths=checkpoint_paths,
+                          fig_path=fig_path)
+    if fig_path is not None:
+        _plot_many_body_chern_curvature(res, fig_path=fig_path)
+    return res

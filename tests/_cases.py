@@ -55,3 +55,26 @@ def oracle_block(g, s):
     chi = g["chi"][s]
     orbits = port.sector_orbits(cat, chi)
     return port.csr_block(cat, int(g["n_site"]), orbits, bil, den, chi, bool(g["fermionic"])), orbits
+
+
+CHERN_CASES = ["haldane12", "haldane16", "haldane16_singular", "checkerboard12", "haldane12_identity"]
+
+
+def chern_case(name):
+    """(model at zero flux, n_particles, labels, nev, grid, fixture) of one
+    chern_*.npz fixture (tests/golden/make_chern_golden.py)."""
+    import os
+
+    import numpy as np
+
+    from realspace_exatdiagonalization_py_b200 import models
+
+    f = dict(np.load(os.path.join(os.path.dirname(__file__), "golden", f"chern_{name}.npz")))
+    sample = [int(x) for x in f["sample"]]
+    if str(f["kind"]) == "bosonic":
+        m = models.build_zero_flux_bosonic_fci_second_quantized_model(sample_size=sample, params=models.params_DNSheng)
+    else:
+        m = models.build_zero_flux_fermionic_fci_second_quantized_model(
+            sample_size=sample, params=dict(models.params_Sun_Gu_Katsura_Sarma))
+    labels = "identity" if f["labels"].dtype.kind == "U" else [tuple(int(x) for x in lab) for lab in f["labels"]]
+    return m, int(f["n_particles"]), labels, int(f["nev"]), tuple(int(x) for x in f["grid"]), f

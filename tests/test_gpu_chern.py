@@ -1,0 +1,97 @@
+"""Many-body Chern number (observables/many_body_chern_number.py:341-458) on
+the device against the reference's own driver (tests/golden/make_chern_golden.py),
+and the device overlap kernel behind its links against numpy."""
+
+import os
+import warnings
+from fractions import Fraction
+
+import numpy as np
+import pytest
+import torch
+
+from _cases import CHERN_CASES, chern_case
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("n_m,n_states,n_slots", [(1, 1, 2), (1, 70001, 3), (3, 4099, 4), (5, 20000, 3),
+                                                  (9, 3001, 2)])
+def test_fock_overlaps_match_numpy(n_m, n_states, n_slots):
+    import realspace_exatdiagonalization_py_b200 as ed
+
+    g = torch.Generator().manual_seed(n_m * 7 + n_slots)
+    s = torch.complex(torch.randn(n_slots, n_m, n_states, generator=g, dtype=torch.float64),
+                      torch.randn(n_slots, n_m, n_states, generator=g, dtype=torch.float64))
+    pairs = [(a, b) for a in range(n_slots) for b in range(n_slots)]
+    M = ed.fock_overlaps(s.cuda().contiguous(), pairs)
+    host = s.numpy()
+    for p, (a, b) in enumerate(pairs):
+        ref = host[a].conj() @ host[b].T
+        np.testing.assert_allclose(M[p], ref, rtol=0, atol=1e-11 * max(1.0, np.abs(ref).max()))
+    again = ed.fock_overlaps(s.cuda().contiguous(), pairs)
+    assert np.array_equal(M.view(np.float64), again.view(np.float64))  # fixed summation order
+
+
+def test_fock_overlaps_reject_bad_pairs():
+    import realspace_exatdiagonalization_py_b200 as ed
+
+    s = torch.zeros((2, 1, 16), dtype=torch.complex128, device="cuda")
+    with pytest.raises(Exception):
+        ed.fock_overlaps(s, [(0, 2)])
+    with pytest.raises(Exception):
+        ed.fock_overlaps(s, [(-1, 0)])
+
+
+def _run(case, tmp, mode="matrix", overwrite=False):
+    import realspace_exatdiagonalization_py_b200 as ed
+
+    model, n_part, labels, nev, grid, f = chern_case(case)
+    with warnings.catch_warnings(record=True) as caught:
+        warnings.simplefilter("always")
+        res = ed.many_body_chern_number(model, labels, filling_fraction=Fraction(n_part, model.lattice.n_site),
+                                        flux_grid_size=grid, nev_per_sector=nev, mode=mode,
+                                        checkpoint_dir=str(tmp), overwrite=overwrite)
+    n_warn = sum("Near-singular Berry link" in str(w.message) for w in caught)
+    return res, n_warn, f
+
+
+def _check(res, n_warn, f):
+    nx, ny = res.flux_grid_size
+    assert (nx, ny) == tuple(int(x) for x in f["grid"])
+    E = np.array([[res.energies[ix][iy] for iy in range(ny)] for ix in range(nx)])
+    np.testing.assert_allclose(E, f["energies"], atol=1e-9, rtol=0)
+    np.testing.assert_allclose(res.berry_curvature, f["berry_curvature"], atol=1e-8, rtol=0)
+    assert abs(res.chern_number - float(f["chern_number"])) < 1e-8
+    assert res.rounded_chern == int(f["rounded_chern"])
+    for k in ("link_det_abs_x", "link_det_abs_y"):
+        got, want = getattr(res, k), f[k]
+        big = want > 1e-8
+        np.testing.assert_allclose(got[big], want[big], atol=1e-8, rtol=0)
+        assert np.all(got[~big] <= 1e-10)
+    if float(f["min_link_det"]) > 1e-8:
+        assert abs(res.min_link_det - float(f["min_link_det"])) < 1e-8
+    assert n_warn == int(f["n_singular_warnings"])
+    np.testing.assert_array_equal(res.flux_x, np.arange(nx) / nx)
+    np.testing.assert_array_equal(res.flux_y, np.arange(ny) / ny)
+
+
+@pytest.mark.parametrize("case", CHERN_CASES)
+def test_chern_matches_reference(tmp_path, case):
+    res, n_warn, f = _run(case, tmp_path)
+    _check(res, n_warn, f)
+    assert os.path.basename(res.checkpoint_paths[0][0]) == str(f["checkpoint_00"])
+    assert os.path.basename(res.checkpoint_paths[1][1]) == str(f["checkpoint_11"])
+
+
+def test_chern_checkpoints_reused_and_matrixfree(tmp_path):
+    res, n_warn, f = _run("haldane16", tmp_path, mode="matrixfree")
+    _check(res, n_warn, f)
+    paths = [p for row in res.checkpoint_paths for p in row]
+    assert all(os.path.isfile(p) for p in paths)
+    stamp = [os.path.getmtime(p) for p in paths]
+    again, n2, _ = _run("haldane16", tmp_path, mode="matrixfree")
+    assert [os.path.getmtime(p) for p in paths] == stamp  # loaded, not recomputed
+    np.testing.assert_array_equal(again.berry_curvature, res.berry_curvature)
+    fresh, n3, _ = _run("haldane16", tmp_path, mode="matrixfree", overwrite=True)
+    _check(fresh, n3, f)

@@ -143,3 +143,55 @@ def test_fock_expansion_matches_reference(golden, case):
         keys = np.array(sorted(amps), dtype=np.uint64)
         np.testing.assert_array_equal(keys, f[f"masks_{s}"])
         np.testing.assert_allclose(np.array([amps[int(x)] for x in keys]), f[f"amps_{s}"], atol=1e-14, rtol=0)
+
+
+@pytest.mark.parametrize("case", ["haldane12", "haldane16", "haldane16_singular", "checkerboard12",
+                                  "haldane12_identity"])
+def test_chern_oracle_matches_reference(case):
+    """The oracle's flux-torus Chern number against the reference's driver
+    (tests/golden/make_chern_golden.py): gauge-invariant plaquette phases,
+    |det| of every link, energies and the near-singular count."""
+    from _cases import chern_case
+
+    import realspace_exatdiagonalization_py_b200 as ed
+
+    model, n_part, labels, nev, grid, f = chern_case(case)
+    ident = labels == "identity"
+
+    def flux_setup(flux):
+        ed.update_second_quantized_model_with_twisted_phases(model, twisted_phases_over_2π=flux)
+        G = ed.build_identity_group(model.lattice.n_site) if ident else ed.build_translation_group(model.lattice, flux)
+        return G, ed.build_irrep_list(G, model.lattice)
+
+    r = port.chern(model, n_part, ["identity"] if ident else labels, grid, nev, flux_setup)
+    np.testing.assert_allclose(r["energies"], f["energies"], atol=1e-10, rtol=0)
+    np.testing.assert_allclose(r["berry_curvature"], f["berry_curvature"], atol=1e-9, rtol=0)
+    assert abs(r["chern_number"] - float(f["chern_number"])) < 1e-9
+    for k in ("link_det_abs_x", "link_det_abs_y"):
+        big = f[k] > 1e-8
+        np.testing.assert_allclose(r[k][big], f[k][big], atol=1e-9, rtol=0)
+        assert np.all(r[k][~big] <= 1e-10)
+    assert r["n_singular"] == int(f["n_singular_warnings"])
+
+
+def test_chern_checkpoint_names():
+    """Checkpoint file names of the Chern scan, including the FNV-1a digest of
+    the parameters, are the reference's (many_body_chern_number.py:75-138)."""
+    from fractions import Fraction
+
+    from _cases import chern_case
+
+    from realspace_exatdiagonalization_py_b200 import observables as obs
+
+    for case in ("haldane12", "checkerboard12", "haldane16"):
+        model, n_part, labels, nev, grid, f = chern_case(case)
+        ff = Fraction(n_part, model.lattice.n_site)
+        nx, ny = grid
+        assert obs._chern_checkpoint_path(model, ff, [0.0, 0.0], "d") == "d/" + str(f["checkpoint_00"])
+        assert obs._chern_checkpoint_path(model, ff, [1 / nx, 1 / ny], "d") == "d/" + str(f["checkpoint_11"])
+    assert obs._normalize_flux_grid_size(4) == (4, 4) and obs._normalize_flux_grid_size([3, 2]) == (3, 2)
+    with pytest.raises(ValueError):
+        obs._normalize_flux_grid_size((1, 3))
+    assert obs._chern_sector_labels("identity") == ["identity"]
+    assert obs._chern_sector_labels([[1, 0]]) == [(1, 0)]
+    assert obs._chern_flux_tag([0.25, -0.5]) == "0p250000_m0p500000"
