@@ -369,6 +369,123 @@ def serving_at_scale(ed, models, n_req=32, rate=20.0, block=2, plain_samples=2):
     return out
 
 
+def _laughlin_manifold(ed, model, nf, n=2):
+    """The ``n`` lowest zero-flux states over all momentum sectors (the
+    nu = 1/2 Laughlin pair), from one batched FP64 solve with two levels per
+    sector, as ``(labels, nev_per_sector, energies)``: two sectors with one
+    level each, or one sector with two."""
+    G = ed.build_translation_group(model.lattice, [0.0, 0.0])
+    data = ed.build_ed_data(model, filling_fraction=Fraction(nf, model.lattice.n_site), symmetry_group=G)
+    res = ed.solve_sectors_batched(data, list(range(len(data.irrep_list))), nev=n, return_vectors=False)
+    low = sorted((float(res[s][0][k]), s) for s in res for k in range(min(n, len(res[s][0]))))[:n]
+    secs = sorted({s for _, s in low}, key=lambda s: min(e for e, t in low if t == s))
+    per = n // len(secs) if n % len(secs) == 0 else 1
+    if per * len(secs) != n:
+        raise RuntimeError(f"lowest states {low} do not split evenly over their sectors")
+    return [data.irrep_list[s].label for s in secs], per, [e for e, _ in low]
+
+
+def _time_chern(ed, model, nf, labels, grid, nev=1, mode="matrixfree", engine="scan"):
+    import shutil
+    import tempfile
+
+    import torch
+
+    d = tempfile.mkdtemp(prefix="chern_")
+    try:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = ed.many_body_chern_number(model, labels, filling_fraction=Fraction(nf, model.lattice.n_site),
+                                      flux_grid_size=grid, nev_per_sector=nev, mode=mode, checkpoint_dir=d,
+                                      engine=engine)
+        torch.cuda.synchronize()
+        return r, time.perf_counter() - t0
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+
+
+def chern_at_scale(ed, models, grid=4, peak_gbs=6650.0, cpu_grid=2, scan_grid=4):
+    """The many-body Chern number of the two lowest zero-flux states of the
+    32-site Haldane bosons on a grid x grid flux torus, end to end through
+    ``many_body_chern_number`` with the served engine (every (flux point,
+    sector) FP64 solve a request) and, on scan_grid x scan_grid, with the scan
+    engine (the reference's route: flux point after flux point, checkpoints in
+    a temporary directory); the overlap launch of one row of links timed alone
+    against the HBM peak; and, like for like, the scan engine and the CPU
+    oracle's restatement of the reference's driver on the 24-site model
+    (cpu_grid x cpu_grid points)."""
+    import warnings
+
+    import torch
+
+    from oracle import port
+
+    model, nf = models.config_model("haldane32")
+    labels, nev, e0 = _laughlin_manifold(ed, model, nf)
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        _time_chern(ed, model, nf, labels, (2, 2), nev)  # warm-up: library, allocator, tuner cache
+        _time_chern(ed, model, nf, labels, (2, 2), nev, engine="served")
+        r, total = _time_chern(ed, model, nf, labels, (grid, grid), nev, engine="served")
+        rs, ts = _time_chern(ed, model, nf, labels, (scan_grid, scan_grid), nev)
+    C = int(model_basis_size(model, nf))
+    n_m = len(labels) * nev
+    out = {"workload": f"haldane32: 32 sites, 8 bosons, C={C:,}, sectors {labels} x {nev} level(s), "
+                       f"{grid}x{grid} flux grid, FP64 solves",
+           "chern_number": r.chern_number, "min_link_det": r.min_link_det, "zero_flux_E0": e0,
+           "served": {"grid": [grid, grid], "total_s": total, "s_per_flux_point": total / (grid * grid)},
+           "scan": {"grid": [scan_grid, scan_grid], "total_s": ts, "s_per_flux_point": ts / (scan_grid * scan_grid),
+                    "chern_number": rs.chern_number}}
+    # one row of links alone: 2*grid pairs of n_m-state Fock vectors
+    g = torch.Generator(device="cuda").manual_seed(0)
+    states = torch.randn((2 * grid, n_m, C), dtype=torch.complex128, device="cuda", generator=g)
+    pairs = [(iy, grid + iy) for iy in range(grid)] + [(iy, (iy + 1) % grid) for iy in range(grid)]
+    for _ in range(2):
+        ed.fock_overlaps(states, pairs)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 5
+    torch.cuda.synchronize()
+    ev0.record()
+    for _ in range(reps):
+        ed.fock_overlaps(states, pairs)
+    ev1.record()
+    torch.cuda.synchronize()
+    t = ev0.elapsed_time(ev1) / 1e3 / reps
+    algo = len(pairs) * 2 * n_m * C * 16
+    out["overlap_row"] = {"pairs": len(pairs), "n_m": n_m, "s": t, "algorithmic_bytes": algo,
+                          "achieved_GBs": algo / t / 1e9, "frac_of_measured_hbm": algo / t / 1e9 / peak_gbs}
+    del states
+    torch.cuda.empty_cache()
+    # like for like on the 24-site model: the device driver and the oracle
+    m24, nf24 = models.config_model("haldane24")
+    lab24, nev24, _ = _laughlin_manifold(ed, m24, nf24)
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        r24, t24 = _time_chern(ed, m24, nf24, lab24, (cpu_grid, cpu_grid), nev24)
+    def flux_setup(flux):
+        ed.update_second_quantized_model_with_twisted_phases(m24, twisted_phases_over_2π=flux)
+        G = ed.build_translation_group(m24.lattice, flux)
+        return G, ed.build_irrep_list(G, m24.lattice)
+
+    t0 = time.perf_counter()
+    o24 = port.chern(m24, nf24, lab24, (cpu_grid, cpu_grid), nev24, flux_setup)
+    tc = time.perf_counter() - t0
+    npts = cpu_grid * cpu_grid
+    out["haldane24_like_for_like"] = {
+        "grid": [cpu_grid, cpu_grid], "sectors": lab24, "nev_per_sector": nev24,
+        "device_scan_s_per_flux_point": t24 / npts,
+        "oracle_s_per_flux_point": tc / npts, "device_chern": r24.chern_number, "oracle_chern": o24["chern_number"],
+        "max_abs_curvature_diff": float(np.max(np.abs(r24.berry_curvature - o24["berry_curvature"]))),
+        "oracle_threads": _NCPU, "oracle_kind": "port"}
+    return out
+
+
+def model_basis_size(model, nf):
+    import math
+
+    return math.comb(model.lattice.n_site, nf)
+
+
 def step_kernel_shares(step, top=10):
     """Device time per kernel over one (untimed) step, from CUPTI through
     torch.profiler: [{kernel, launches, total_us, share}] sorted by time."""
@@ -643,6 +760,8 @@ def main():
                     help="only a batched solve of this many 32-site Haldane sectors (for kernel profiling)")
     ap.add_argument("--matvec-precision", type=int, default=0, choices=[0, 32, 64])
     ap.add_argument("--matvec-no-otf", action="store_true")
+    ap.add_argument("--chern", type=int, default=0,
+                    help="only the many-body Chern number of the 32-site Haldane pair on this flux grid")
     args = ap.parse_args()
     if args.solve_scale:
         import realspace_exatdiagonalization_py_b200 as ed
@@ -661,6 +780,15 @@ def main():
         torch.cuda.synchronize()
         print(json.dumps({"workload": f"haldane32: {len(secs)} sectors, FP32 + FP64 refinement, b=2, nev 4",
                           "solve_s": time.perf_counter() - t0, "E0": [float(res[s][0][0]) for s in secs]}))
+        return
+    if args.chern:
+        import realspace_exatdiagonalization_py_b200 as ed
+        from realspace_exatdiagonalization_py_b200 import models
+
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+            os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+        print(json.dumps(chern_at_scale(ed, models, grid=args.chern, peak_gbs=float(peaks.get("hbm_gbs", 6650.0)))),
+              flush=True)
         return
     if args.matvec_only:
         import realspace_exatdiagonalization_py_b200 as ed

@@ -276,6 +276,7 @@ def config_model(name: str) -> tuple[Any, int]:
       hoppings (band-flipped), V1=1, V2=V3=0.
     * ``haldane32``: Haldane honeycomb 4x4x2, 8 hard-core bosons, t=1,
       t'=0.6 exp(+-0.4 pi i), t''=0, V1=1.
+    * ``haldane24``: the same couplings on 3x4x2, 6 bosons (also nu = 1/2).
     * ``checkerboard48``: checkerboard 4x6x2, 8 fermions, couplings of
       ``checkerboard24``.
     * ``hubbard32``: spinful Fermi-Hubbard 4x4 (32 spin-orbitals), t=1, U=4,
@@ -291,9 +292,10 @@ def config_model(name: str) -> tuple[Any, int]:
         return build_zero_flux_fermionic_fci_second_quantized_model(sample_size=ss, params=p), nf
     if name == "hubbard32":
         return build_spinful_hubbard_second_quantized_model([4, 4], 1.0, 4.0), 10
-    if name == "haldane32":
+    if name in ("haldane32", "haldane24"):
         p = {"t": 1.0, "t'": 0.6, "t''": 0.0, "phi_over_2pi": 0.2, "V1": 1.0, "V2": 0.0}
-        return build_zero_flux_bosonic_fci_second_quantized_model(sample_size=[4, 4], params=p), 8
+        ss, nf = ([4, 4], 8) if name == "haldane32" else ([3, 4], 6)
+        return build_zero_flux_bosonic_fci_second_quantized_model(sample_size=ss, params=p), nf
     raise ValueError(f"unknown workload {name!r}")
 
 

@@ -25,7 +25,11 @@ catalog; its manifold states are expanded into dense rank-indexed Fock
 vectors on the device, and the overlap matrices of each row of links are one
 device launch (``rsed_fock_overlaps``).  Only the zero-flux row and the two
 most recent rows stay resident, so device memory is
-``3 * ny * n_manifold * n_states * 16`` bytes, not the whole grid.
+``3 * ny * n_manifold * n_states * 16`` bytes, not the whole grid.  With
+``engine="served"`` every (flux point, sector) solve of the grid is instead a
+request to a ``SolveServer`` that returns its eigenvectors; solves of
+different flux points overlap on the device, and the sector eigenvectors
+(not the Fock states) of the whole grid wait on the device for the links.
 """
 
 from __future__ import annotations
@@ -252,15 +256,71 @@ def _plot_many_body_chern_curvature(result, *, fig_path: str | None = None):
     return fig, ax
 
 
+def _chern_served(model, labels, n_filled, flux_x, flux_y, nev_per_sector):
+    """Every (flux point, sector) solve of the grid as one request to a
+    ``SolveServer`` (FP64, eigenvectors kept on the device); returns the
+    results by ``(ix, iy, label)`` and a function that expands one flux
+    point's manifold into dense Fock rows."""
+    from .catalog import update_orbit_stabilizer_phases
+    from .fock import expand_sector_state_to_fock_dense
+    from .sector import SectorSet, Symmetry_Sector_Basis
+    from .serving import ServingModel, SolveRequest, SolveServer
+    from .symmetry import build_irrep_list, build_translation_group
+
+    sm = ServingModel(model, n_filled, name="chern")
+    irr = [ir.label for ir in build_irrep_list(sm.group0, model.lattice)]
+    for lab in labels:
+        if lab not in irr:
+            raise ValueError(f"Sector {lab!r} not found at flux [0.0, 0.0].")
+    reqs, where = [], {}
+    for ix, fx in enumerate(flux_x):
+        for iy, fy in enumerate(flux_y):
+            for lab in labels:
+                where[len(reqs)] = (ix, iy, lab)
+                reqs.append(SolveRequest(len(reqs), irr.index(lab), (float(fx), float(fy)), "chern", vectors=True))
+    server = SolveServer(sm, nev=nev_per_sector, precision=64, block=2)
+    solved = {where[r.rid]: r for r in server.run(reqs, realtime=False, timeout=24 * 3600.0)}
+    del server
+
+    def fill(ix, iy, out):
+        flux = [float(flux_x[ix]), float(flux_y[iy])]
+        group = build_translation_group(model.lattice, flux)
+        cat = sm.catalog.clone()
+        update_orbit_stabilizer_phases(cat, group, sm.stats)
+        irreps = build_irrep_list(group, model.lattice)
+        sset = SectorSet(cat, irreps)
+        energies, row = [], 0
+        for lab in labels:
+            res = solved.pop((ix, iy, lab))
+            idx = irr.index(lab)
+            if len(res.eigenvalues) < nev_per_sector:
+                raise ValueError(f"Requested {nev_per_sector} states in sector {lab!r}, "
+                                 f"only found {len(res.eigenvalues)}.")
+            basis = Symmetry_Sector_Basis(irreps[idx], cat, sset, idx)
+            for level in range(nev_per_sector):
+                expand_sector_state_to_fock_dense(res.eigenvectors[:, level], basis, out=out[row])
+                energies.append(float(res.eigenvalues[level]))
+                row += 1
+        return energies, None
+
+    return sm.catalog, fill
+
+
 def many_body_chern_number(model, sector_labels, *, filling_fraction, flux_grid_size=(5, 5), nev_per_sector: int = 1,
                            mode: str = "matrix", checkpoint_dir: str = "checkpoints", overwrite: bool = False,
-                           fig_path: str | None = None, det_atol: float = 1e-10):
+                           fig_path: str | None = None, det_atol: float = 1e-10, engine: str = "scan"):
     """Chern number of the many-body manifold on the flux torus; returns the
     reference's fields (``chern_number``, ``rounded_chern``,
     ``berry_curvature[ix, iy]``, ``flux_x``, ``flux_y``, ``sector_labels``,
     ``nev_per_sector``, ``flux_grid_size``, ``energies[ix][iy]``,
     ``min_link_det``, ``link_det_abs_x``, ``link_det_abs_y``,
-    ``checkpoint_paths[ix][iy]``, ``fig_path``)."""
+    ``checkpoint_paths[ix][iy]``, ``fig_path``).
+
+    ``engine="scan"`` solves flux point after flux point with the
+    reference's per-point checkpoints; ``engine="served"`` submits every
+    (flux point, sector) solve to a ``SolveServer`` at once (FP64, solves of
+    different flux points overlapping on the device; momentum sectors only,
+    no checkpoints: ``checkpoint_paths`` entries are ``None``)."""
     import torch
 
     from .ed import build_ed_data
@@ -275,16 +335,31 @@ def many_body_chern_number(model, sector_labels, *, filling_fraction, flux_grid_
     labels = _chern_sector_labels(sector_labels)
     if mode not in ("matrix", "matrixfree"):
         raise ValueError(f"Unknown ED scan mode: {mode}. Use 'matrix' or 'matrixfree'.")
+    if engine not in ("scan", "served"):
+        raise ValueError(f"unknown engine {engine!r}")
     flux_x = np.arange(nx) / nx
     flux_y = np.arange(ny) / ny
-    os.makedirs(checkpoint_dir, exist_ok=True)
 
     # the zero-flux catalog, moved to every flux point by a phase update
     update_second_quantized_model_with_twisted_phases(model, twisted_phases_over_2π=[0.0, 0.0])
-    group0 = (build_identity_group(model.lattice.n_site) if labels == ["identity"]
-              else build_translation_group(model.lattice, [0.0, 0.0]))
-    base = build_ed_data(model, filling_fraction=filling_fraction, symmetry_group=group0)
-    cat = base.orbit_catalog
+    if engine == "scan":
+        os.makedirs(checkpoint_dir, exist_ok=True)
+        group0 = (build_identity_group(model.lattice.n_site) if labels == ["identity"]
+                  else build_translation_group(model.lattice, [0.0, 0.0]))
+        base = build_ed_data(model, filling_fraction=filling_fraction, symmetry_group=group0)
+        cat = base.orbit_catalog
+
+        def fill(ix, iy, out):
+            e, _, path = _chern_point(model, labels, base, filling_fraction, (float(flux_x[ix]), float(flux_y[iy])),
+                                      nev_per_sector, mode, checkpoint_dir, overwrite, out)
+            return e, path
+    else:
+        if labels == ["identity"]:
+            raise ValueError("the served engine solves momentum sectors; use engine='scan' for 'identity'")
+        n_filled = filling_fraction * model.lattice.n_site
+        if n_filled.denominator != 1:
+            raise ValueError("filling_fraction * n_site must be an integer (particle number).")
+        cat, fill = _chern_served(model, labels, int(n_filled), flux_x, flux_y, int(nev_per_sector))
     n_m = len(labels) * int(nev_per_sector)
     rows_kept = min(nx, 3)
     states = torch.zeros((rows_kept * ny, n_m, cat.n_states), dtype=torch.complex128, device=cat.table.device)
@@ -309,10 +384,7 @@ def many_body_chern_number(model, sector_labels, *, filling_fraction, flux_grid_
     checkpoint_paths = [[None] * ny for _ in range(nx)]
     for ix in range(nx):
         for iy in range(ny):
-            flux = (float(flux_x[ix]), float(flux_y[iy]))
-            energies[ix][iy], _, checkpoint_paths[ix][iy] = _chern_point(
-                model, labels, base, filling_fraction, flux, nev_per_sector, mode, checkpoint_dir, overwrite,
-                states[slot(ix, iy)])
+            energies[ix][iy], checkpoint_paths[ix][iy] = fill(ix, iy, states[slot(ix, iy)])
         if ix >= 1:
             row_links(ix - 1, ix)
     row_links(nx - 1, 0)

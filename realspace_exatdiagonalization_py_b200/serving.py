@@ -72,6 +72,7 @@ class SolveRequest:
     model: str = "default"
     arrival: float = 0.0             # seconds after the start of the run
     seed: int | None = None          # start-block seed offset (default: rid)
+    vectors: bool = False            # also return the eigenvectors (device tensor in the result)
 
 
 @dataclass
@@ -90,6 +91,9 @@ class SolveResult:
     finished: float
     lane: int
     lane_width: int
+    # [dim, nev] complex128 CUDA tensor in the sector's basis order at the
+    # request's flux point, when the request asked for vectors
+    eigenvectors: torch.Tensor | None = None
 
     @property
     def latency(self) -> float:
@@ -238,6 +242,7 @@ class _Lane:
         self.last_used = time.perf_counter()
         self.event = torch.cuda.Event()
         self.h_state = self.h_vals = self.h_res = self.h_fp32 = None
+        self.vecs: list[torch.Tensor] | None = None
         self.bytes = (lanczos_footprint_bytes(sm.n_orbits, width * params.block, params.n_slots, params.precision)
                       + self.w.numel() * self.w.element_size() + self.member.numel() * 8)
 
@@ -301,6 +306,7 @@ class _Lane:
                 ctypes.byref(self.ctx.dm.c), ctypes.byref(sc), ctypes.byref(b.c), APPLY_AUTO,
                 _lib.stream_ptr(self.stream)))
             self.h_fp32.copy_((fp32 - b.ritz_val[:, : self.nev]).abs(), non_blocking=True)
+        self.vecs = b.eigenvectors(stream=self.stream) if any(r.vectors for r in self.reqs) else None
         self.h_vals.copy_(b.ritz_val[:, : self.nev], non_blocking=True)
         self.h_res.copy_(b.resid[:, : self.nev], non_blocking=True)
         self.h_state.copy_(b.state, non_blocking=True)
@@ -334,15 +340,20 @@ class _Lane:
                 self._finish()
                 self.state = "finishing"
                 return None
-        # finishing: results are in pinned memory
+        # finishing: results are in pinned memory (vectors on the device)
         out = []
+        vecs = self.vecs or [None] * self.width
+        self.vecs = None
         for i, r in enumerate(self.reqs):
+            v = vecs[i] if r.vectors else None
+            if v is not None:  # the caller reads it on its own stream
+                v.record_stream(torch.cuda.current_stream())
             out.append(SolveResult(
                 rid=r.rid, sector=r.sector, flux=r.flux, model=r.model,
                 eigenvalues=self.h_vals[i].numpy().copy(), residuals=self.h_res[i].numpy().copy(),
                 fp32_error=self.h_fp32[i].numpy().copy() if self.params.precision == 32 else None,
                 iterations=int(st[i, S_ITERS]), dim=int(self.ctx.sset.dims[r.sector]), arrival=r.arrival,
-                admitted=self.admitted, finished=now, lane=self.id, lane_width=self.width))
+                admitted=self.admitted, finished=now, lane=self.id, lane_width=self.width, eigenvectors=v))
         self._release()
         return out
 
@@ -471,16 +482,20 @@ class SolveServer:
         from .sector import Symmetry_Sector_Basis
 
         basis = Symmetry_Sector_Basis(ctx.irreps[req.sector], ctx.catalog, ctx.sset, req.sector)
+        vecs = None
         if basis.dim == 0:
             vals = np.zeros(0)
         else:
             H = MatrixFreeHamiltonian(basis, ctx.dm.bilinear_terms, ctx.dm.density_terms, None, model=ctx.dm)
-            vals, _ = diagonalize_block_matrixfree(H, basis.dim, nev=self.nev)
+            vals, vecs = diagonalize_block_matrixfree(H, basis.dim, nev=self.nev)
         k = len(vals)
+        if req.vectors:
+            vecs = (torch.zeros((0, 0), dtype=torch.complex128, device=ctx.catalog.table.device) if vecs is None
+                    else torch.as_tensor(np.asarray(vecs)).to(ctx.catalog.table.device, torch.complex128))
         return SolveResult(rid=req.rid, sector=req.sector, flux=req.flux, model=req.model,
                            eigenvalues=np.asarray(vals, dtype=np.float64), residuals=np.zeros(k), fp32_error=None,
                            iterations=0, dim=basis.dim, arrival=req.arrival, admitted=now, finished=self.now(),
-                           lane=0, lane_width=1)
+                           lane=0, lane_width=1, eigenvectors=vecs if req.vectors else None)
 
     def _admit(self, now: float) -> None:
         groups: OrderedDict[tuple, list[SolveRequest]] = OrderedDict()

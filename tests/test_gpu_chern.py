@@ -95,3 +95,66 @@ def test_chern_checkpoints_reused_and_matrixfree(tmp_path):
     np.testing.assert_array_equal(again.berry_curvature, res.berry_curvature)
     fresh, n3, _ = _run("haldane16", tmp_path, mode="matrixfree", overwrite=True)
     _check(fresh, n3, f)
+
+
+@pytest.mark.parametrize("case", ["haldane12", "haldane16", "checkerboard12"])
+def test_chern_served_engine_matches_reference(tmp_path, case):
+    import realspace_exatdiagonalization_py_b200 as ed
+
+    model, n_part, labels, nev, grid, f = chern_case(case)
+    with warnings.catch_warnings(record=True) as caught:
+        warnings.simplefilter("always")
+        res = ed.many_body_chern_number(model, labels, filling_fraction=Fraction(n_part, model.lattice.n_site),
+                                        flux_grid_size=grid, nev_per_sector=nev, engine="served")
+    _check(res, sum("Near-singular Berry link" in str(w.message) for w in caught), f)
+    assert all(p is None for row in res.checkpoint_paths for p in row)
+
+
+def test_chern_served_lanes_match_scan():
+    """Sectors above the dense limit (24-site Haldane bosons, ~11k orbits per
+    sector): eigenvectors out of the server's Lanczos lanes give the scan
+    engine's links and curvature."""
+    import realspace_exatdiagonalization_py_b200 as ed
+    from realspace_exatdiagonalization_py_b200 import models
+
+    model, nf = models.config_model("haldane24")
+    ff = Fraction(nf, model.lattice.n_site)
+    labels = [(0, 0), (0, 1)]
+    kw = dict(filling_fraction=ff, flux_grid_size=(2, 3), nev_per_sector=1)
+    served = ed.many_body_chern_number(model, labels, engine="served", **kw)
+    import tempfile
+
+    with tempfile.TemporaryDirectory() as d:
+        scan = ed.many_body_chern_number(model, labels, mode="matrixfree", checkpoint_dir=d, **kw)
+    np.testing.assert_allclose(np.array(served.energies), np.array(scan.energies), atol=1e-9, rtol=0)
+    np.testing.assert_allclose(served.berry_curvature, scan.berry_curvature, atol=1e-8, rtol=0)
+    np.testing.assert_allclose(served.link_det_abs_x, scan.link_det_abs_x, atol=1e-8, rtol=0)
+    np.testing.assert_allclose(served.link_det_abs_y, scan.link_det_abs_y, atol=1e-8, rtol=0)
+    assert abs(served.chern_number - scan.chern_number) < 1e-8
+
+
+def test_served_request_vectors_are_eigenvectors():
+    """A request with ``vectors=True`` gets unit eigenvectors in its sector's
+    basis order at its flux point: H v = E v through the device operator."""
+    import realspace_exatdiagonalization_py_b200 as ed
+    from realspace_exatdiagonalization_py_b200 import models
+
+    model, nf = models.config_model("haldane24")
+    sm = ed.ServingModel(model, nf, name="h24")
+    srv = ed.SolveServer(sm, nev=2, precision=64, block=2)
+    reqs = [ed.SolveRequest(i, s, (0.25, 0.5), "h24", vectors=True) for i, s in enumerate((0, 3))]
+    reqs.append(ed.SolveRequest(2, 1, (0.25, 0.5), "h24"))
+    res = {r.rid: r for r in srv.run(reqs, realtime=False)}
+    assert res[2].eigenvectors is None
+    ctx = ed.FluxContext(sm, (0.25, 0.5), 64)
+    for rid, s in ((0, 0), (1, 3)):
+        v = res[rid].eigenvectors
+        assert v.shape == (res[rid].dim, 2) and v.is_cuda
+        basis = ed.Symmetry_Sector_Basis(ctx.irreps[s], ctx.catalog, ctx.sset, s)
+        H = ed.MatrixFreeHamiltonian(basis, ctx.dm.bilinear_terms, ctx.dm.density_terms, None, model=ctx.dm)
+        Hv = H.matvec_device(v.contiguous(), 2)
+        # the operator applies H^dagger = H
+        for j in range(2):
+            r = torch.linalg.vector_norm(Hv[:, j] - res[rid].eigenvalues[j] * v[:, j]).item()
+            assert r < 1e-8, r
+            assert abs(torch.linalg.vector_norm(v[:, j]).item() - 1.0) < 1e-12
