@@ -436,26 +436,7 @@ def chern_at_scale(ed, models, grid=4, peak_gbs=6650.0, cpu_grid=2, scan_grid=4)
            "served": {"grid": [grid, grid], "total_s": total, "s_per_flux_point": total / (grid * grid)},
            "scan": {"grid": [scan_grid, scan_grid], "total_s": ts, "s_per_flux_point": ts / (scan_grid * scan_grid),
                     "chern_number": rs.chern_number}}
-    # one row of links alone: 2*grid pairs of n_m-state Fock vectors
-    g = torch.Generator(device="cuda").manual_seed(0)
-    states = torch.randn((2 * grid, n_m, C), dtype=torch.complex128, device="cuda", generator=g)
-    pairs = [(iy, grid + iy) for iy in range(grid)] + [(iy, (iy + 1) % grid) for iy in range(grid)]
-    for _ in range(2):
-        ed.fock_overlaps(states, pairs)
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    reps = 5
-    torch.cuda.synchronize()
-    ev0.record()
-    for _ in range(reps):
-        ed.fock_overlaps(states, pairs)
-    ev1.record()
-    torch.cuda.synchronize()
-    t = ev0.elapsed_time(ev1) / 1e3 / reps
-    algo = len(pairs) * 2 * n_m * C * 16
-    out["overlap_row"] = {"pairs": len(pairs), "n_m": n_m, "s": t, "algorithmic_bytes": algo,
-                          "achieved_GBs": algo / t / 1e9, "frac_of_measured_hbm": algo / t / 1e9 / peak_gbs}
-    del states
-    torch.cuda.empty_cache()
+    out["overlap_row"] = overlap_row(ed, C, n_m, grid, peak_gbs)
     # like for like on the 24-site model: the device driver and the oracle
     m24, nf24 = models.config_model("haldane24")
     lab24, nev24, _ = _laughlin_manifold(ed, m24, nf24)
@@ -478,6 +459,36 @@ def chern_at_scale(ed, models, grid=4, peak_gbs=6650.0, cpu_grid=2, scan_grid=4)
         "max_abs_curvature_diff": float(np.max(np.abs(r24.berry_curvature - o24["berry_curvature"]))),
         "oracle_threads": _NCPU, "oracle_kind": "port"}
     return out
+
+
+def overlap_row(ed, C, n_m, grid, peak_gbs, reps=5):
+    """One row of Chern links alone: ``rsed_fock_overlaps`` over the 2*grid
+    slot pairs (x links to the next row, y links within the row) of random
+    dense Fock states (complex128, ``2*grid`` slots of ``n_m`` states of ``C``
+    amplitudes), CUDA-event time per call against the HBM peak.  Algorithmic
+    bytes = every distinct slot once (2*grid * n_m * C * 16); each slot enters
+    up to four pairs, and ``pair_bytes`` counts it once per pair."""
+    import torch
+
+    g = torch.Generator(device="cuda").manual_seed(0)
+    states = torch.randn((2 * grid, n_m, C), dtype=torch.complex128, device="cuda", generator=g)
+    pairs = [(iy, grid + iy) for iy in range(grid)] + [(iy, (iy + 1) % grid) for iy in range(grid)]
+    for _ in range(3):
+        ed.fock_overlaps(states, pairs)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record()
+    for _ in range(reps):
+        ed.fock_overlaps(states, pairs)
+    ev1.record()
+    torch.cuda.synchronize()
+    t = ev0.elapsed_time(ev1) / 1e3 / reps
+    algo = len({x for pr in pairs for x in pr}) * n_m * C * 16
+    del states
+    torch.cuda.empty_cache()
+    return {"pairs": len(pairs), "n_m": n_m, "n_states": C, "s": t, "algorithmic_bytes": algo,
+            "pair_bytes": len(pairs) * 2 * n_m * C * 16, "achieved_GBs": algo / t / 1e9,
+            "frac_of_measured_hbm": algo / t / 1e9 / peak_gbs}
 
 
 def model_basis_size(model, nf):
@@ -760,6 +771,8 @@ def main():
                     help="only a batched solve of this many 32-site Haldane sectors (for kernel profiling)")
     ap.add_argument("--matvec-precision", type=int, default=0, choices=[0, 32, 64])
     ap.add_argument("--matvec-no-otf", action="store_true")
+    ap.add_argument("--overlap-only", type=int, default=0,
+                    help="only the Chern link overlaps of one row of this flux grid (for kernel profiling)")
     ap.add_argument("--chern", type=int, default=0,
                     help="only the many-body Chern number of the 32-site Haldane pair on this flux grid")
     args = ap.parse_args()
@@ -780,6 +793,16 @@ def main():
         torch.cuda.synchronize()
         print(json.dumps({"workload": f"haldane32: {len(secs)} sectors, FP32 + FP64 refinement, b=2, nev 4",
                           "solve_s": time.perf_counter() - t0, "E0": [float(res[s][0][0]) for s in secs]}))
+        return
+    if args.overlap_only:
+        import realspace_exatdiagonalization_py_b200 as ed
+
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+            os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+        print(json.dumps({"workload": f"one row of Chern links: {args.overlap_only}x{args.overlap_only} grid, "
+                                      "2 states per flux point, 10,518,300 amplitudes per state (32-site Haldane)",
+                          **overlap_row(ed, 10_518_300, 2, args.overlap_only,
+                                        float(peaks.get("hbm_gbs", 6650.0)))}), flush=True)
         return
     if args.chern:
         import realspace_exatdiagonalization_py_b200 as ed

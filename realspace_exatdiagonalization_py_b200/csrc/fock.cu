@@ -125,104 +125,155 @@ extern "C" int rsed_fock_expand(const rsed_group_t* grp, const rsed_entry_t* tab
 //
 // states: complex128 [slot][level][rank], n_m levels of n_states amplitudes per
 // slot.  For every pair p = (a, b) of slots, out[p][i][j] = sum_r
-// conj(states[a][i][r]) * states[b][j][r].  Each block streams one chunk of
-// ranks for one pair and one 4x4 tile of (i, j), coalesced 16-byte loads of
-// up to 8 vectors, and writes its 16 partial sums; a second pass adds the
-// chunks in order, so the result does not depend on scheduling.
+// conj(states[a][i][r]) * states[b][j][r].
+//
+// Work unit = (chunk of kOvChunk ranks, pair, T x T tile of (i, j)), T =
+// min(n_m, 4), so a one- or two-state manifold keeps few registers and many
+// warps in flight.  Units are numbered chunk-major, and one wave of blocks
+// (occupancy x SMs) walks them with a grid stride, so the blocks in flight
+// work on the same few chunks for every pair: a slot that several pairs share
+// (each state of a Chern row enters up to four links) is read from DRAM once
+// and from L2 after that.  Per unit a block streams the chunk with coalesced
+// 16-byte loads (two ranks per thread and step for T <= 2), reduces, and
+// writes the unit's T*T partial sums.  A second pass (one warp per output)
+// adds the chunk partials in a fixed order.  The chunking does not depend on
+// the device or the grid, so the result is the same on every run.
 namespace {
 
 constexpr int kOvT = 256;
-constexpr int kOvTile = 4;
-constexpr int kOvTargetBlocks = 148 * 8;
+constexpr int kOvMaxTile = 4;
+constexpr int64_t kOvChunk = 4096;
 
 struct OvShape {
-  int64_t chunk_rows;
-  int n_chunks, n_tiles;
+  int64_t n_chunks;
+  int n_tiles, tile;
+  int64_t n_units;
 };
 
 OvShape ov_shape(int64_t n_states, int n_m, int n_pairs) {
   OvShape s;
-  s.n_tiles = (n_m + kOvTile - 1) / kOvTile;
-  const int64_t per_chunk = (int64_t)n_pairs * s.n_tiles * s.n_tiles;
-  int64_t want = (kOvTargetBlocks + per_chunk - 1) / per_chunk;
-  const int64_t most = (n_states + 4 * kOvT - 1) / (4 * kOvT);
-  if (want > most) want = most;
-  if (want < 1) want = 1;
-  s.chunk_rows = (n_states + want - 1) / want;
-  s.n_chunks = (int)((n_states + s.chunk_rows - 1) / s.chunk_rows);
+  s.tile = n_m < kOvMaxTile ? n_m : kOvMaxTile;
+  s.n_tiles = (n_m + s.tile - 1) / s.tile;
+  s.n_chunks = (n_states + kOvChunk - 1) / kOvChunk;
+  s.n_units = s.n_chunks * n_pairs * s.n_tiles * s.n_tiles;
   return s;
 }
 
 size_t ov_pairs_bytes(int n_pairs) { return ((size_t)n_pairs * 2 * sizeof(int32_t) + 255) / 256 * 256; }
 
-__global__ void __launch_bounds__(kOvT) k_fock_overlap_part(const double2* __restrict__ states, int64_t n_states,
-                                                            int n_m, const int32_t* __restrict__ pairs,
-                                                            int n_tiles, int64_t chunk_rows, int n_chunks,
-                                                            double2* __restrict__ part) {
-  __shared__ double2 red[kOvT / 32][kOvTile * kOvTile];
-  const int chunk = blockIdx.x, p = blockIdx.y, t = blockIdx.z;
-  const int ti0 = (t / n_tiles) * kOvTile, tj0 = (t % n_tiles) * kOvTile;
-  const int ni = min(kOvTile, n_m - ti0), nj = min(kOvTile, n_m - tj0);
-  const int64_t slot = (int64_t)n_m * n_states;
-  const double2* A = states + (int64_t)pairs[2 * p] * slot + (int64_t)ti0 * n_states;
-  const double2* B = states + (int64_t)pairs[2 * p + 1] * slot + (int64_t)tj0 * n_states;
-  double acc_re[kOvTile][kOvTile], acc_im[kOvTile][kOvTile];
+template <int T>
+__device__ __forceinline__ void ov_accumulate(const double2* __restrict__ A, const double2* __restrict__ B,
+                                              int64_t n_states, int64_t r, int ni, int nj, double (&re)[T][T],
+                                              double (&im)[T][T]) {
+  double2 a[T], b[T];
 #pragma unroll
-  for (int i = 0; i < kOvTile; ++i)
+  for (int i = 0; i < T; ++i) a[i] = i < ni ? __ldg(A + (int64_t)i * n_states + r) : make_double2(0.0, 0.0);
 #pragma unroll
-    for (int j = 0; j < kOvTile; ++j) acc_re[i][j] = acc_im[i][j] = 0.0;
-  const int64_t r0 = (int64_t)chunk * chunk_rows;
-  const int64_t r1 = min(n_states, r0 + chunk_rows);
-  for (int64_t r = r0 + threadIdx.x; r < r1; r += kOvT) {
-    double2 a[kOvTile], b[kOvTile];
+  for (int j = 0; j < T; ++j) b[j] = j < nj ? __ldg(B + (int64_t)j * n_states + r) : make_double2(0.0, 0.0);
 #pragma unroll
-    for (int i = 0; i < kOvTile; ++i) a[i] = i < ni ? __ldg(A + (int64_t)i * n_states + r) : make_double2(0.0, 0.0);
+  for (int i = 0; i < T; ++i)
 #pragma unroll
-    for (int j = 0; j < kOvTile; ++j) b[j] = j < nj ? __ldg(B + (int64_t)j * n_states + r) : make_double2(0.0, 0.0);
-#pragma unroll
-    for (int i = 0; i < kOvTile; ++i)
-#pragma unroll
-      for (int j = 0; j < kOvTile; ++j) {
-        acc_re[i][j] = fma(a[i].x, b[j].x, fma(a[i].y, b[j].y, acc_re[i][j]));
-        acc_im[i][j] = fma(a[i].x, b[j].y, fma(-a[i].y, b[j].x, acc_im[i][j]));
-      }
-  }
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for (int i = 0; i < kOvTile; ++i)
-#pragma unroll
-    for (int j = 0; j < kOvTile; ++j) {
-      double re = acc_re[i][j], im = acc_im[i][j];
-      for (int o = 16; o > 0; o >>= 1) {
-        re += __shfl_xor_sync(0xffffffffu, re, o);
-        im += __shfl_xor_sync(0xffffffffu, im, o);
-      }
-      if (lane == 0) red[warp][i * kOvTile + j] = make_double2(re, im);
+    for (int j = 0; j < T; ++j) {
+      re[i][j] = fma(a[i].x, b[j].x, fma(a[i].y, b[j].y, re[i][j]));
+      im[i][j] = fma(a[i].x, b[j].y, fma(-a[i].y, b[j].x, im[i][j]));
     }
-  __syncthreads();
-  if (threadIdx.x < kOvTile * kOvTile) {
-    double2 s = make_double2(0.0, 0.0);
-    for (int w = 0; w < kOvT / 32; ++w) s = make_double2(s.x + red[w][threadIdx.x].x, s.y + red[w][threadIdx.x].y);
-    part[(((int64_t)p * n_tiles * n_tiles + t) * n_chunks + chunk) * (kOvTile * kOvTile) + threadIdx.x] = s;
+}
+
+template <int T>
+__global__ void __launch_bounds__(kOvT, T <= 2 ? 4 : 2) k_fock_overlap_part(const double2* __restrict__ states, int64_t n_states,
+                                                            int n_m, const int32_t* __restrict__ pairs,
+                                                            int n_tiles, int64_t n_chunks, int64_t n_units,
+                                                            double2* __restrict__ part) {
+  __shared__ double2 red[kOvT / 32][T * T];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t slot = (int64_t)n_m * n_states;
+  const int tt2 = n_tiles * n_tiles;
+  const int64_t per_chunk = n_units / n_chunks;  // pairs x tiles
+  for (int64_t u = blockIdx.x; u < n_units; u += gridDim.x) {
+    // unit u = chunk * (n_pairs * n_tiles^2) + p * n_tiles^2 + t
+    const int64_t chunk = u / per_chunk;
+    const int64_t p = (u % per_chunk) / tt2;
+    const int t = (int)(u % tt2);
+    const int ti0 = (t / n_tiles) * T, tj0 = (t % n_tiles) * T;
+    const int ni = min(T, n_m - ti0), nj = min(T, n_m - tj0);
+    const double2* A = states + (int64_t)pairs[2 * p] * slot + (int64_t)ti0 * n_states;
+    const double2* B = states + (int64_t)pairs[2 * p + 1] * slot + (int64_t)tj0 * n_states;
+    double re[T][T], im[T][T];
+#pragma unroll
+    for (int i = 0; i < T; ++i)
+#pragma unroll
+      for (int j = 0; j < T; ++j) re[i][j] = im[i][j] = 0.0;
+    const int64_t r0 = chunk * kOvChunk;
+    const int64_t r1 = min(n_states, r0 + kOvChunk);
+    int64_t r = r0 + threadIdx.x;
+    if (T <= 2) {
+      for (; r + kOvT < r1; r += 2 * kOvT) {
+        ov_accumulate<T>(A, B, n_states, r, ni, nj, re, im);
+        ov_accumulate<T>(A, B, n_states, r + kOvT, ni, nj, re, im);
+      }
+    }
+    for (; r < r1; r += kOvT) ov_accumulate<T>(A, B, n_states, r, ni, nj, re, im);
+#pragma unroll
+    for (int i = 0; i < T; ++i)
+#pragma unroll
+      for (int j = 0; j < T; ++j) {
+        double x = re[i][j], y = im[i][j];
+        for (int o = 16; o > 0; o >>= 1) {
+          x += __shfl_xor_sync(0xffffffffu, x, o);
+          y += __shfl_xor_sync(0xffffffffu, y, o);
+        }
+        if (lane == 0) red[warp][i * T + j] = make_double2(x, y);
+      }
+    __syncthreads();
+    if (threadIdx.x < T * T) {
+      double2 s = make_double2(0.0, 0.0);
+      for (int w = 0; w < kOvT / 32; ++w) s = make_double2(s.x + red[w][threadIdx.x].x, s.y + red[w][threadIdx.x].y);
+      part[u * (T * T) + threadIdx.x] = s;
+    }
+    __syncthreads();  // red is rewritten by the next unit
   }
 }
 
-__global__ void k_fock_overlap_final(const double2* __restrict__ part, int n_m, int n_tiles, int n_chunks,
-                                     int64_t n_out, double2* __restrict__ out) {
-  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= n_out) return;
+// One warp per output: lane l adds the partials of chunks l, l + 32, ... in
+// order, then a fixed butterfly combines the lanes.
+__global__ void k_fock_overlap_final(const double2* __restrict__ part, int n_m, int tile, int n_tiles,
+                                     int64_t n_chunks, int64_t per_chunk, int64_t n_out, double2* __restrict__ out) {
+  const int64_t idx = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (idx >= n_out) return;  // whole warps leave together
   const int64_t mm = (int64_t)n_m * n_m;
   const int64_t p = idx / mm;
   const int i = (int)((idx % mm) / n_m), j = (int)(idx % n_m);
-  const int t = (i / kOvTile) * n_tiles + j / kOvTile;
-  const int k = (i % kOvTile) * kOvTile + j % kOvTile;
-  const double2* src = part + ((p * n_tiles * n_tiles + t) * n_chunks) * (kOvTile * kOvTile) + k;
-  double2 s = make_double2(0.0, 0.0);
-  for (int c = 0; c < n_chunks; ++c) {
-    const double2 v = src[(int64_t)c * (kOvTile * kOvTile)];
-    s = make_double2(s.x + v.x, s.y + v.y);
+  const int t = (i / tile) * n_tiles + j / tile;
+  const int tt = tile * tile;
+  const int k = (i % tile) * tile + j % tile;
+  const double2* src = part + (p * n_tiles * n_tiles + t) * tt + k;
+  double x = 0.0, y = 0.0;
+  for (int64_t c = lane; c < n_chunks; c += 32) {
+    const double2 v = src[c * per_chunk * tt];
+    x += v.x;
+    y += v.y;
   }
-  out[idx] = s;
+  for (int o = 16; o > 0; o >>= 1) {
+    x += __shfl_xor_sync(0xffffffffu, x, o);
+    y += __shfl_xor_sync(0xffffffffu, y, o);
+  }
+  if (lane == 0) out[idx] = make_double2(x, y);
+}
+
+template <int T>
+int ov_launch(const double2* st, int64_t n_states, int n_m, const int32_t* dpairs, const OvShape& s, double2* part,
+              cudaStream_t stream) {
+  int dev = 0, n_sm = 0, per_sm = 0;
+  RSED_TRY_CUDA(cudaGetDevice(&dev));
+  RSED_TRY_CUDA(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
+  RSED_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fock_overlap_part<T>, kOvT, 0));
+  int64_t grid = (int64_t)n_sm * (per_sm > 0 ? per_sm : 1);
+  if (grid > s.n_units) grid = s.n_units;
+  k_fock_overlap_part<T><<<(unsigned)grid, kOvT, 0, stream>>>(st, n_states, n_m, dpairs, s.n_tiles, s.n_chunks,
+                                                              s.n_units, part);
+  RSED_CHECK_LAUNCH();
+  return RSED_OK;
 }
 
 }  // namespace
@@ -230,16 +281,15 @@ __global__ void k_fock_overlap_final(const double2* __restrict__ part, int n_m, 
 extern "C" size_t rsed_fock_overlap_scratch_bytes(int64_t n_states, int32_t n_m, int32_t n_pairs) {
   if (n_states < 1 || n_m < 1 || n_pairs < 1) return 0;
   const OvShape s = ov_shape(n_states, n_m, n_pairs);
-  return ov_pairs_bytes(n_pairs) +
-         sizeof(double2) * kOvTile * kOvTile * (size_t)n_pairs * s.n_tiles * s.n_tiles * (size_t)s.n_chunks;
+  return ov_pairs_bytes(n_pairs) + sizeof(double2) * (size_t)s.tile * s.tile * (size_t)s.n_units;
 }
 
 extern "C" int rsed_fock_overlaps(const double* states, int64_t n_states, int32_t n_m, int32_t n_slots,
                                   const int32_t* pairs, int32_t n_pairs, double* out, void* scratch,
                                   size_t scratch_bytes, void* stream_) {
   RSED_REQUIRE(states && pairs && out && scratch, RSED_EINVAL, "null Fock overlap argument");
-  RSED_REQUIRE(n_states >= 1 && n_m >= 1 && n_m <= 512 && n_slots >= 1 && n_pairs >= 1 && n_pairs <= 65535,
-               RSED_EINVAL, "Fock overlap sizes out of range");
+  RSED_REQUIRE(n_states >= 1 && n_m >= 1 && n_m <= 512 && n_slots >= 1 && n_pairs >= 1, RSED_EINVAL,
+               "Fock overlap sizes out of range");
   for (int32_t p = 0; p < 2 * n_pairs; ++p)
     RSED_REQUIRE(pairs[p] >= 0 && pairs[p] < n_slots, RSED_EINVAL, "Fock overlap pair names a slot out of range");
   RSED_REQUIRE(scratch_bytes >= rsed_fock_overlap_scratch_bytes(n_states, n_m, n_pairs), RSED_ESCRATCH,
@@ -250,13 +300,18 @@ extern "C" int rsed_fock_overlaps(const double* states, int64_t n_states, int32_
   double2* part = reinterpret_cast<double2*>(reinterpret_cast<char*>(scratch) + ov_pairs_bytes(n_pairs));
   RSED_TRY_CUDA(cudaMemcpyAsync(dpairs, pairs, sizeof(int32_t) * 2 * (size_t)n_pairs, cudaMemcpyHostToDevice,
                                 stream));
-  k_fock_overlap_part<<<dim3((unsigned)s.n_chunks, (unsigned)n_pairs, (unsigned)(s.n_tiles * s.n_tiles)), kOvT, 0,
-                        stream>>>(reinterpret_cast<const double2*>(states), n_states, n_m, dpairs, s.n_tiles,
-                                  s.chunk_rows, s.n_chunks, part);
-  RSED_CHECK_LAUNCH();
+  const double2* st = reinterpret_cast<const double2*>(states);
+  int rc;
+  switch (s.tile) {
+    case 1: rc = ov_launch<1>(st, n_states, n_m, dpairs, s, part, stream); break;
+    case 2: rc = ov_launch<2>(st, n_states, n_m, dpairs, s, part, stream); break;
+    case 3: rc = ov_launch<3>(st, n_states, n_m, dpairs, s, part, stream); break;
+    default: rc = ov_launch<4>(st, n_states, n_m, dpairs, s, part, stream);
+  }
+  if (rc) return rc;
   const int64_t n_out = (int64_t)n_pairs * n_m * n_m;
-  k_fock_overlap_final<<<(unsigned)((n_out + 127) / 128), 128, 0, stream>>>(part, n_m, s.n_tiles, s.n_chunks,
-                                                                            n_out, reinterpret_cast<double2*>(out));
+  k_fock_overlap_final<<<(unsigned)((n_out + 3) / 4), 128, 0, stream>>>(
+      part, n_m, s.tile, s.n_tiles, s.n_chunks, s.n_units / s.n_chunks, n_out, reinterpret_cast<double2*>(out));
   RSED_CHECK_LAUNCH();
   return RSED_OK;
 }
