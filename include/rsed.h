@@ -276,6 +276,24 @@ int rsed_fock_overlaps(const double* states, int64_t n_states, int32_t n_m, int3
                        const int32_t* pairs, int32_t n_pairs, double* out, void* scratch,
                        size_t scratch_bytes, void* stream);
 
+/* Resta's periodic position operator exp(2 pi i X / L) projected between two
+ * symmetry sectors, for flux_charge_pump (replaces _position_operator_matrix
+ * and the manifold products P[row, col], observables/charge_pump.py:102-161,
+ * :465-486).  Per orbit o (representative s = repr_masks[o]):
+ *   elem(o) = (1/|G|) sum_g chi_to[g] conj(chi_from[g]) z(g(s)),
+ *   z(m) = product over the occupied sites j of m, ascending, of site_phase[j],
+ * |elem| <= 1e-13 dropped (the reference's form: diagonal in the orbit, no
+ * stabilizer terms).  x_to / x_from: device complex128 [k][n_orbits] sector
+ * vectors in orbit layout (zero outside their sectors); out: device
+ * complex128 [k_to][k_from], out[i][j] = sum_o conj(x_to[i][o]) elem(o)
+ * x_from[j][o], the same sum order on every run.  chi_to, chi_from (|G|) and
+ * site_phase (N) are device complex128 arrays.  Asynchronous on `stream`. */
+size_t rsed_position_scratch_bytes(int64_t n_orbits, int32_t k_to, int32_t k_from);
+int rsed_position_overlaps(const rsed_group_t* grp, int64_t n_orbits, const uint64_t* repr_masks,
+                           const double* chi_to, const double* chi_from, const double* site_phase,
+                           const double* x_to, int32_t k_to, const double* x_from, int32_t k_from,
+                           double* out, void* scratch, size_t scratch_bytes, void* stream);
+
 /* ---- K8: batched thick-restart block Lanczos -------------------------------
  * Replaces diagonalize_block_matrixfree / diagonalize_block_arpack
  * (symmetry_resolved_ed.py:2214-2299, ARPACK eigs(which="SR", tol=1e-10))

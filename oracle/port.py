@@ -18,6 +18,9 @@ import this module.  It restates, in vectorised numpy, the algorithm of
 * the many-body Chern number on the flux torus: dictionary overlaps,
   determinant links and plaquette phases
   (``observables/many_body_chern_number.py:141-207, 341-438``),
+* the charge pump: the orbit-diagonal position operator between sectors,
+  manifold eigenvalues and phase-branch tracking
+  (``observables/charge_pump.py:41-240, 325-505``),
 * the eigen-solves: dense ``eigh(UPLO="U")`` for n <= 500 and ARPACK
   ``eigs(k=nev, which="SR", tol=1e-10)`` with the seeded ``v0`` otherwise
   (SRE:2180-2299).
@@ -456,3 +459,92 @@ def chern(model, n_filled: int, labels, grid, nev: int, flux_setup, det_atol: fl
             F[ix, iy] = np.angle(Ux[ix, iy] * Uy[ixp, iy] * np.conj(Ux[ix, iyp]) * np.conj(Uy[ix, iy]))
     return {"chern_number": float(F.sum()) / (2 * np.pi), "berry_curvature": F, "link_det_abs_x": dx,
             "link_det_abs_y": dy, "energies": energies, "n_singular": n_sing}
+
+
+def position_element(m: int, perm0: np.ndarray, w: np.ndarray, site_phase: np.ndarray) -> complex:
+    """(1/|G|) sum_g w_g z(g(m)), z = product of site phases over the occupied
+    sites in ascending order; |elem| <= 1e-13 -> 0 (charge_pump.py:102-161)."""
+    ng = perm0.shape[0]
+    e = 0j
+    for g in range(ng):
+        img = 0
+        for i in range(perm0.shape[1]):
+            if (m >> i) & 1:
+                img |= 1 << int(perm0[g, i])
+        z = 1 + 0j
+        for j in range(perm0.shape[1]):
+            if (img >> j) & 1:
+                z *= site_phase[j]
+        e += w[g] * z
+    e *= 1.0 / ng
+    return e if abs(e) > 1e-13 else 0j
+
+
+def _track(raw: np.ndarray) -> np.ndarray:
+    """Branch tracking (charge_pump.py:180-240): exhaustive assignment with the
+    least summed squared wrapped jump, first in lexicographic order."""
+    import itertools
+
+    out = np.empty_like(raw)
+    out[0] = np.sort(raw[0])
+    for t in range(1, raw.shape[0]):
+        prev = out[t - 1]
+        best, best_cost = None, np.inf
+        for perm in itertools.permutations(range(raw.shape[1])):
+            c = 0.0
+            for d, j in enumerate(perm):
+                x = raw[t, j] - prev[d]
+                c += (x - round(x)) ** 2
+            if c < best_cost:
+                best, best_cost = perm, c
+        for b, j in enumerate(best):
+            out[t, b] = raw[t, j] + round(prev[b] - raw[t, j])
+    return out
+
+
+def charge_pump(model, n_filled: int, specs, thetas, flux_direction: int, site_phase: np.ndarray, flux_setup):
+    """Charge pump (charge_pump.py:325-505) on the CPU.  ``specs`` = list of
+    (sector label, 1-based level); ``flux_setup(flux)`` moves ``model`` to the
+    flux point and returns ``(G, irreps)``.  Sectors solved in matrix mode
+    with ``max(max level, 2)`` levels.  Returns ``(polarization_eigenvalues,
+    polarizations, pumped_charges, energies)``."""
+    n = model.lattice.n_site
+    dim = model.lattice.dim
+    fermion = model.particle_statistics.name == "FERMIONIC"
+    labels = list(dict.fromkeys(lab for lab, _ in specs))
+    need = {lab: max(lev for l2, lev in specs if l2 == lab) for lab in labels}
+    nev = max(max(need.values()), 2)
+    ev_all = np.zeros((len(thetas), len(specs)), dtype=np.complex128)
+    energies = np.full((len(thetas), len(labels), max(need.values())), np.nan)
+    for it, th in enumerate(thetas):
+        flux = [0.0] * dim
+        flux[flux_direction - 1] = float(th)
+        G, irreps = flux_setup(flux)
+        perm0, eta = group_arrays(G)
+        cat = catalog(n, n_filled, perm0, eta, fermion)
+        vecs, orbs, chis = {}, {}, {}
+        for il, lab in enumerate(labels):
+            s = next(i for i, ir in enumerate(irreps) if ir.label == lab)
+            chi = np.asarray(irreps[s].values, dtype=np.complex128)
+            o = sector_orbits(cat, chi)
+            H = csr_block(cat, n, o, model.bilinear_terms, model.density_density_terms, chi, fermion)
+            w, v = solve(H, nev, seeded_v0=False)
+            energies[it, il, : need[lab]] = w[: need[lab]]
+            vecs[lab], orbs[lab], chis[lab] = v, o, chi
+        P = np.zeros((len(specs), len(specs)), dtype=np.complex128)
+        for r, (lt, vt) in enumerate(specs):
+            for c, (lf, vf) in enumerate(specs):
+                w = chis[lt] * np.conj(chis[lf])
+                pos_t = {int(o): k for k, o in enumerate(orbs[lt])}
+                acc = 0j
+                for k, o in enumerate(orbs[lf]):
+                    kt = pos_t.get(int(o))
+                    if kt is None:
+                        continue
+                    e = position_element(int(cat["reprs"][o]), perm0, w, site_phase)
+                    acc += np.conj(vecs[lt][kt, vt - 1]) * e * vecs[lf][k, vf - 1]
+                P[r, c] = acc
+        ev = np.linalg.eigvals(P)
+        ev_all[it] = ev[np.argsort(np.angle(ev))]
+    pol = _track(np.angle(ev_all) / (2 * np.pi))
+    return ev_all, pol, pol[-1] - pol[0], energies

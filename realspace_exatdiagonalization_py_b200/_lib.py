@@ -174,6 +174,10 @@ SIGNATURES = {
     "rsed_fock_overlap_scratch_bytes": (c_size_t, [c_int64, c_int32, c_int32]),
     "rsed_fock_overlaps": (c_int, [c_void_p, c_int64, c_int32, c_int32, c_void_p, c_int32, c_void_p, c_void_p,
                                    c_size_t, c_void_p]),
+    "rsed_position_scratch_bytes": (c_size_t, [c_int64, c_int32, c_int32]),
+    "rsed_position_overlaps": (c_int, [POINTER(RsedGroup), c_int64, c_void_p, c_void_p, c_void_p, c_void_p,
+                                       c_void_p, c_int32, c_void_p, c_int32, c_void_p, c_void_p, c_size_t,
+                                       c_void_p]),
     "rsed_proj_scratch_bytes": (c_size_t, [c_int64]),
     "rsed_proj_count": (c_int, [POINTER(RsedModel), c_void_p, POINTER(c_int64), c_void_p, c_size_t, c_void_p]),
     "rsed_proj_fill": (c_int, [POINTER(RsedModel), c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),

@@ -315,3 +315,204 @@ extern "C" int rsed_fock_overlaps(const double* states, int64_t n_states, int32_
   RSED_CHECK_LAUNCH();
   return RSED_OK;
 }
+
+// ---- Resta position operator projected into a manifold (charge pump) -------------
+//
+// For orbit o with representative s the projected operator is diagonal:
+// elem(o) = (1/|G|) sum_g chi_to(g) conj(chi_from(g)) z(g(s)), z(m) = the
+// product over the occupied sites j of m (ascending) of site_phase[j]; an
+// element with |elem| <= 1e-13 is dropped.  out[i][j] = sum_o
+// conj(x_to[i][o]) elem(o) x_from[j][o] over the orbit-layout vectors.  Units
+// = (chunk of kOvChunk orbits, T x T tile of (i, j)); elem is recomputed per
+// tile (|G| permutations per orbit, cheap against the vector stream).
+namespace {
+
+__device__ __forceinline__ double2 pos_elem(uint64_t s, const rsed_group_t& grp, const double2* __restrict__ w,
+                                            const double2* __restrict__ site_phase, double inv_ng) {
+  double2 e = make_double2(0.0, 0.0);
+  for (int g = 0; g < grp.n_group; ++g) {
+    uint64_t m = rsed_permute(s, grp.perm + (int64_t)g * grp.n_site);
+    double2 z = make_double2(1.0, 0.0);
+    while (m) {
+      const int j = __ffsll((long long)m) - 1;
+      z = rsed_cmul_exact(z, site_phase[j]);
+      m &= m - 1;
+    }
+    const double2 t = rsed_cmul_exact(w[g], z);
+    e = make_double2(e.x + t.x, e.y + t.y);
+  }
+  e = make_double2(e.x * inv_ng, e.y * inv_ng);
+  if (sqrt(e.x * e.x + e.y * e.y) <= 1e-13) e = make_double2(0.0, 0.0);
+  return e;
+}
+
+template <int T>
+__global__ void __launch_bounds__(kOvT, 2) k_position_part(rsed_group_t grp, int64_t n_orbits,
+                                                           const uint64_t* __restrict__ repr_masks,
+                                                           const double2* __restrict__ chi_to,
+                                                           const double2* __restrict__ chi_from,
+                                                           const double2* __restrict__ site_phase, double inv_ng,
+                                                           const double2* __restrict__ x_to, int k_to,
+                                                           const double2* __restrict__ x_from, int k_from,
+                                                           int n_tiles, int64_t n_chunks, int64_t n_units,
+                                                           double2* __restrict__ part) {
+  __shared__ double2 red[kOvT / 32][T * T];
+  __shared__ double2 sw[64];
+  __shared__ double2 sph[64];
+  // chi_to(g) * conj(chi_from(g)), the reference's product order
+  for (int g = threadIdx.x; g < grp.n_group; g += kOvT)
+    sw[g] = rsed_cmul_exact(chi_to[g], make_double2(chi_from[g].x, -chi_from[g].y));
+  for (int j = threadIdx.x; j < grp.n_site; j += kOvT) sph[j] = site_phase[j];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int tt2 = n_tiles * n_tiles;
+  for (int64_t u = blockIdx.x; u < n_units; u += gridDim.x) {
+    const int64_t chunk = u / tt2;
+    const int t = (int)(u % tt2);
+    const int ti0 = (t / n_tiles) * T, tj0 = (t % n_tiles) * T;
+    const int ni = min(T, k_to - ti0), nj = min(T, k_from - tj0);
+    const double2* A = x_to + (int64_t)ti0 * n_orbits;
+    const double2* B = x_from + (int64_t)tj0 * n_orbits;
+    double re[T][T], im[T][T];
+#pragma unroll
+    for (int i = 0; i < T; ++i)
+#pragma unroll
+      for (int j = 0; j < T; ++j) re[i][j] = im[i][j] = 0.0;
+    const int64_t r1 = min(n_orbits, (chunk + 1) * kOvChunk);
+    for (int64_t o = chunk * kOvChunk + threadIdx.x; o < r1; o += kOvT) {
+      double2 a[T], b[T];
+      bool any = false;
+#pragma unroll
+      for (int i = 0; i < T; ++i) {
+        a[i] = i < ni ? __ldg(A + (int64_t)i * n_orbits + o) : make_double2(0.0, 0.0);
+        any |= (a[i].x != 0.0) | (a[i].y != 0.0);
+      }
+      if (!any) continue;  // orbit outside the target sector (or a zero row)
+      bool anyb = false;
+#pragma unroll
+      for (int j = 0; j < T; ++j) {
+        b[j] = j < nj ? __ldg(B + (int64_t)j * n_orbits + o) : make_double2(0.0, 0.0);
+        anyb |= (b[j].x != 0.0) | (b[j].y != 0.0);
+      }
+      if (!anyb) continue;
+      const double2 e = pos_elem(__ldg(repr_masks + o), grp, sw, sph, inv_ng);
+#pragma unroll
+      for (int j = 0; j < T; ++j) b[j] = rsed_cmul_exact(e, b[j]);
+#pragma unroll
+      for (int i = 0; i < T; ++i)
+#pragma unroll
+        for (int j = 0; j < T; ++j) {
+          re[i][j] = fma(a[i].x, b[j].x, fma(a[i].y, b[j].y, re[i][j]));
+          im[i][j] = fma(a[i].x, b[j].y, fma(-a[i].y, b[j].x, im[i][j]));
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < T; ++i)
+#pragma unroll
+      for (int j = 0; j < T; ++j) {
+        double x = re[i][j], y = im[i][j];
+        for (int o = 16; o > 0; o >>= 1) {
+          x += __shfl_xor_sync(0xffffffffu, x, o);
+          y += __shfl_xor_sync(0xffffffffu, y, o);
+        }
+        if (lane == 0) red[warp][i * T + j] = make_double2(x, y);
+      }
+    __syncthreads();
+    if (threadIdx.x < T * T) {
+      double2 s = make_double2(0.0, 0.0);
+      for (int wq = 0; wq < kOvT / 32; ++wq)
+        s = make_double2(s.x + red[wq][threadIdx.x].x, s.y + red[wq][threadIdx.x].y);
+      part[u * (T * T) + threadIdx.x] = s;
+    }
+    __syncthreads();
+  }
+}
+
+// out[i][j] from the chunk partials, one warp per output (fixed order).
+__global__ void k_position_final(const double2* __restrict__ part, int k_to, int k_from, int tile, int n_tiles,
+                                 int64_t n_chunks, double2* __restrict__ out) {
+  const int64_t idx = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (idx >= (int64_t)k_to * k_from) return;
+  const int i = (int)(idx / k_from), j = (int)(idx % k_from);
+  const int t = (i / tile) * n_tiles + j / tile;
+  const int tt = tile * tile;
+  const int64_t per_chunk = (int64_t)n_tiles * n_tiles;
+  const double2* src = part + (int64_t)t * tt + (i % tile) * tile + j % tile;
+  double x = 0.0, y = 0.0;
+  for (int64_t c = lane; c < n_chunks; c += 32) {
+    const double2 v = src[c * per_chunk * tt];
+    x += v.x;
+    y += v.y;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    x += __shfl_xor_sync(0xffffffffu, x, o);
+    y += __shfl_xor_sync(0xffffffffu, y, o);
+  }
+  if (lane == 0) out[idx] = make_double2(x, y);
+}
+
+template <int T>
+int pos_launch(const rsed_group_t& grp, int64_t n_orbits, const uint64_t* repr_masks, const double2* cto,
+               const double2* cfrom, const double2* ph, double inv_ng, const double2* x_to, int k_to,
+               const double2* x_from, int k_from, const OvShape& s, double2* part, cudaStream_t stream) {
+  int dev = 0, n_sm = 0, per_sm = 0;
+  RSED_TRY_CUDA(cudaGetDevice(&dev));
+  RSED_TRY_CUDA(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
+  RSED_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_position_part<T>, kOvT, 0));
+  int64_t grid = (int64_t)n_sm * (per_sm > 0 ? per_sm : 1);
+  if (grid > s.n_units) grid = s.n_units;
+  k_position_part<T><<<(unsigned)grid, kOvT, 0, stream>>>(grp, n_orbits, repr_masks, cto, cfrom, ph, inv_ng, x_to,
+                                                          k_to, x_from, k_from, s.n_tiles, s.n_chunks, s.n_units,
+                                                          part);
+  RSED_CHECK_LAUNCH();
+  return RSED_OK;
+}
+
+OvShape pos_shape(int64_t n_orbits, int k_to, int k_from) {
+  const int k = k_to > k_from ? k_to : k_from;
+  return ov_shape(n_orbits, k, 1);
+}
+
+}  // namespace
+
+extern "C" size_t rsed_position_scratch_bytes(int64_t n_orbits, int32_t k_to, int32_t k_from) {
+  if (n_orbits < 1 || k_to < 1 || k_from < 1) return 0;
+  const OvShape s = pos_shape(n_orbits, k_to, k_from);
+  return sizeof(double2) * (size_t)s.tile * s.tile * (size_t)s.n_units;
+}
+
+extern "C" int rsed_position_overlaps(const rsed_group_t* grp, int64_t n_orbits, const uint64_t* repr_masks,
+                                      const double* chi_to, const double* chi_from, const double* site_phase,
+                                      const double* x_to, int32_t k_to, const double* x_from, int32_t k_from,
+                                      double* out, void* scratch, size_t scratch_bytes, void* stream_) {
+  int rc = check_group(grp);
+  if (rc) return rc;
+  RSED_REQUIRE(repr_masks && chi_to && chi_from && site_phase && x_to && x_from && out && scratch, RSED_EINVAL,
+               "null position-operator argument");
+  RSED_REQUIRE(n_orbits >= 1 && k_to >= 1 && k_from >= 1 && k_to <= 512 && k_from <= 512, RSED_EINVAL,
+               "position-operator sizes out of range");
+  RSED_REQUIRE(scratch_bytes >= rsed_position_scratch_bytes(n_orbits, k_to, k_from), RSED_ESCRATCH,
+               "position-operator scratch too small");
+  cudaStream_t stream = as_stream(stream_);
+  const OvShape s = pos_shape(n_orbits, k_to, k_from);
+  double2* part = reinterpret_cast<double2*>(scratch);
+  const double inv_ng = 1.0 / (double)grp->n_group;
+  const double2* ct = reinterpret_cast<const double2*>(chi_to);
+  const double2* cf = reinterpret_cast<const double2*>(chi_from);
+  const double2* ph = reinterpret_cast<const double2*>(site_phase);
+  const double2* xt = reinterpret_cast<const double2*>(x_to);
+  const double2* xf = reinterpret_cast<const double2*>(x_from);
+  switch (s.tile) {
+    case 1: rc = pos_launch<1>(*grp, n_orbits, repr_masks, ct, cf, ph, inv_ng, xt, k_to, xf, k_from, s, part, stream); break;
+    case 2: rc = pos_launch<2>(*grp, n_orbits, repr_masks, ct, cf, ph, inv_ng, xt, k_to, xf, k_from, s, part, stream); break;
+    case 3: rc = pos_launch<3>(*grp, n_orbits, repr_masks, ct, cf, ph, inv_ng, xt, k_to, xf, k_from, s, part, stream); break;
+    default: rc = pos_launch<4>(*grp, n_orbits, repr_masks, ct, cf, ph, inv_ng, xt, k_to, xf, k_from, s, part, stream);
+  }
+  if (rc) return rc;
+  const int64_t n_out = (int64_t)k_to * k_from;
+  k_position_final<<<(unsigned)((n_out + 3) / 4), 128, 0, stream>>>(part, k_to, k_from, s.tile, s.n_tiles,
+                                                                   s.n_chunks, reinterpret_cast<double2*>(out));
+  RSED_CHECK_LAUNCH();
+  return RSED_OK;
+}

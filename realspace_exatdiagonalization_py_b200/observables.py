@@ -30,6 +30,15 @@ most recent rows stay resident, so device memory is
 request to a ``SolveServer`` that returns its eigenvectors; solves of
 different flux points overlap on the device, and the sector eigenvectors
 (not the Fock states) of the whole grid wait on the device for the links.
+
+``flux_charge_pump`` keeps the contract of the reference's driver
+(``observables/charge_pump.py:325-558``): along a flux scan (the flux-scan
+checkpoints shared with ``flux_spectrum_flow``) Resta's periodic position
+operator in the transverse direction is projected into the manifold of
+(sector, level) states, one device launch per pair of sectors
+(``rsed_position_overlaps``: the orbit-diagonal element and the products with
+every pair of levels in one stream over the orbit-layout vectors); its
+eigenvalue phases are tracked branch by branch into pumped charges.
 """
 
 from __future__ import annotations
@@ -40,7 +49,7 @@ from types import SimpleNamespace
 
 import numpy as np
 
-__all__ = ["flux_spectrum_flow", "many_body_chern_number"]
+__all__ = ["flux_spectrum_flow", "many_body_chern_number", "flux_charge_pump", "many_body_position_phases"]
 
 
 def _labels(sector_labels):
@@ -403,3 +412,260 @@ def many_body_chern_number(model, sector_labels, *, filling_fraction, flux_grid_
     if fig_path is not None:
         _plot_many_body_chern_curvature(res, fig_path=fig_path)
     return res
+
+
+# ---- charge pump -----------------------------------------------------------------
+
+
+def many_body_position_phases(lattice, direction: int, *, include_sublattice: bool = True) -> np.ndarray:
+    """``exp(2 pi i x_j / L)`` per site (0-based), ``x_j`` the crystal
+    coordinate of site ``j`` along the 1-based ``direction`` (cell index plus,
+    optionally, the sub-lattice offset) and ``L`` the sample size there
+    (``charge_pump.py:41-78``)."""
+    import cmath
+    import math
+
+    if not 1 <= direction <= lattice.dim:
+        raise ValueError(f"direction must be in 1..{lattice.dim}.")
+    L = float(lattice.sample_size[direction - 1])
+    out = np.zeros(lattice.n_site, dtype=np.complex128)
+    for i, (cell, sub) in enumerate(lattice.site_list):
+        x = float(cell[direction - 1])
+        if include_sublattice:
+            x += float(lattice.sub_crys_list[sub - 1][direction - 1])
+        out[i] = cmath.exp(2j * math.pi * x / L)
+    return out
+
+
+def _default_polarization_direction(dim: int, flux_direction: int) -> int:
+    """The next direction after the flux direction (1-based, cyclic); the flux
+    direction itself in 1-D (``charge_pump.py:164-177``)."""
+    return flux_direction if dim == 1 else flux_direction % dim + 1
+
+
+def _best_phase_permutation(raw: np.ndarray, prev: np.ndarray) -> np.ndarray:
+    """The assignment of current branches to previous ones with the least
+    sum of squared wrapped phase jumps; among equal costs the lexicographically
+    first, each cost summed in branch order (``charge_pump.py:180-216``)."""
+    import itertools
+
+    n = len(prev)
+    best, best_cost = tuple(range(n)), float("inf")
+    for perm in itertools.permutations(range(n)):
+        cost = 0.0
+        for depth, j in enumerate(perm):
+            d = raw[j] - prev[depth]
+            d -= round(d)
+            cost = cost + d ** 2
+            if cost >= best_cost:
+                break
+        else:
+            best, best_cost = perm, cost
+    return np.asarray(best, dtype=np.int64)
+
+
+def _tracked_phase_branches(raw_phases: np.ndarray) -> np.ndarray:
+    """Branches sorted at the first flux value, then matched step by step
+    (``_best_phase_permutation``) and shifted by whole windings to stay
+    continuous (``charge_pump.py:219-240``)."""
+    n_t, _ = raw_phases.shape
+    tracked = np.empty_like(raw_phases)
+    tracked[0] = raw_phases[0, np.argsort(raw_phases[0])]
+    for it in range(1, n_t):
+        perm = _best_phase_permutation(raw_phases[it], tracked[it - 1])
+        for b, j in enumerate(perm):
+            phi = raw_phases[it, j]
+            tracked[it, b] = phi + round(tracked[it - 1, b] - phi)
+    return tracked
+
+
+class _ManifoldState:
+    """One manifold state: a sector label and a 1-based level."""
+
+    __slots__ = ("sector", "level")
+
+    def __init__(self, sector, level):
+        self.sector, self.level = sector, level
+
+    def __eq__(self, other):
+        return isinstance(other, _ManifoldState) and (self.sector, self.level) == (other.sector, other.level)
+
+    def __repr__(self):
+        return f"_ManifoldState(sector={self.sector!r}, level={self.level})"
+
+
+def _normalize_manifold_state_specs(sector_labels, nev_per_sector: int, manifold_states):
+    """``(labels, specs, required_levels, is_identity)`` from the legacy
+    ``nev_per_sector`` form or explicit ``(sector, level)`` states, with the
+    reference's validation (``charge_pump.py:256-322``)."""
+    if nev_per_sector <= 0:
+        raise ValueError("nev_per_sector must be positive.")
+    is_identity = isinstance(sector_labels, str) and sector_labels == "identity"
+    if is_identity:
+        base = ["identity"]
+    elif isinstance(sector_labels, tuple):
+        base = [tuple(int(x) for x in sector_labels)]
+    else:
+        base = [tuple(int(x) for x in lab) for lab in sector_labels]
+    if manifold_states is None:
+        specs = [_ManifoldState(lab, lev) for lab in base for lev in range(1, nev_per_sector + 1)]
+    else:
+        if is_identity:
+            raise ValueError("Explicit manifold_states are only supported for symmetry-sector ED.")
+        specs = []
+        for st in manifold_states:
+            if hasattr(st, "sector"):
+                sec, lev = st.sector, st.level
+            elif isinstance(st, dict):
+                sec, lev = st["sector"], st["level"]
+            else:
+                sec, lev = st[0], st[1]
+            sec, lev = tuple(int(x) for x in sec), int(lev)
+            if lev <= 0:
+                raise ValueError(f"Manifold levels must be positive; got {lev} in sector {sec}.")
+            if sec not in base:
+                raise ValueError(f"Manifold state ({sec}, level {lev}) is absent from sector_labels={base}.")
+            specs.append(_ManifoldState(sec, lev))
+        if not specs:
+            raise ValueError("manifold_states must not be empty.")
+        if len({(x.sector, x.level) for x in specs}) != len(specs):
+            raise ValueError("manifold_states contains duplicate (sector, level) entries.")
+    labels = list(dict.fromkeys(x.sector for x in specs))
+    required: dict = {}
+    for x in specs:
+        required[x.sector] = max(required.get(x.sector, 0), x.level)
+    return labels, specs, required, is_identity
+
+
+def _position_block(cat, chi_to, chi_from, x_to, x_from, site_phase, stream=None) -> np.ndarray:
+    """``[k_to, k_from]`` position-operator products of orbit-layout vectors
+    ``x_to [k_to, n_orbits]`` and ``x_from [k_from, n_orbits]`` on the device."""
+    import ctypes
+
+    import torch
+
+    from . import _lib
+
+    lib = _lib.lib()
+    k_to, k_from = int(x_to.shape[0]), int(x_from.shape[0])
+    n_orb = cat.n_orbits
+    out = torch.empty((k_to, k_from), dtype=torch.complex128, device=x_to.device)
+    scratch = torch.empty(int(lib.rsed_position_scratch_bytes(n_orb, k_to, k_from)), dtype=torch.uint8,
+                          device=x_to.device)
+    _lib.check(lib.rsed_position_overlaps(ctypes.byref(cat.dgroup.c), n_orb, _lib.ptr(cat.repr_masks),
+                                          _lib.ptr(chi_to), _lib.ptr(chi_from), _lib.ptr(site_phase), _lib.ptr(x_to),
+                                          k_to, _lib.ptr(x_from), k_from, _lib.ptr(out), _lib.ptr(scratch),
+                                          scratch.numel(), _lib.stream_ptr(stream)))
+    return out.cpu().numpy()
+
+
+def flux_charge_pump(model, sector_labels, *, filling_fraction, flux_direction: int = 1,
+                     polarization_direction: int | None = None, twisted_phases_over_2π_list=None,
+                     nev_per_sector: int = 1, manifold_states=None, include_sublattice: bool = True,
+                     checkpoint_dir: str = "checkpoints", fig_path: str | None = None, overwrite: bool = False):
+    """Many-body charge pump under flux insertion; returns the reference's
+    fields (``twisted_phases_over_2π_list``, ``energies[θ, sector, level]``,
+    ``sector_labels``, ``flux_direction``, ``polarization_direction``,
+    ``nev_per_sector``, ``manifold_states``, ``polarization_eigenvalues``,
+    ``polarizations``, ``pumped_charge_trajectories``, ``pumped_charges``,
+    ``include_sublattice``, ``is_identity``, ``fig_path``,
+    ``checkpoint_paths``).  The identity sector is rejected: the flux scan
+    holds translation sectors only."""
+    import math
+
+    import torch
+
+    from .catalog import update_orbit_stabilizer_phases
+    from .ed import build_ed_data, ed_scan, load_checkpoint
+    from .second_quantized_model import update_second_quantized_model_with_twisted_phases
+    from .sector import SectorSet
+    from .symmetry import build_translation_group
+
+    if twisted_phases_over_2π_list is None:
+        twisted_phases_over_2π_list = list(np.linspace(0.0, 1.0, 9))
+    labels, specs, required, is_identity = _normalize_manifold_state_specs(sector_labels, nev_per_sector,
+                                                                            manifold_states)
+    if is_identity:
+        raise ValueError("flux_charge_pump reads translation-sector flux-scan checkpoints; "
+                         "the 'identity' sector is not among them.")
+    dim = model.lattice.dim
+    if not 1 <= flux_direction <= dim:
+        raise ValueError(f"flux_direction must be in 1..{dim}.")
+    if polarization_direction is None:
+        polarization_direction = _default_polarization_direction(dim, flux_direction)
+    if not 1 <= polarization_direction <= dim:
+        raise ValueError(f"polarization_direction must be in 1..{dim}.")
+    thetas = list(twisted_phases_over_2π_list)
+    n_states = len(specs)
+    max_level = max(required.values())
+    energies = np.full((len(thetas), len(labels), max_level), np.nan)
+    pol_ev = np.zeros((len(thetas), n_states), dtype=np.complex128)
+
+    flux0 = [0.0] * dim
+    update_second_quantized_model_with_twisted_phases(model, twisted_phases_over_2π=flux0)
+    init = build_ed_data(model, filling_fraction=filling_fraction,
+                         symmetry_group=build_translation_group(model.lattice, flux0))
+    paths = ed_scan(init, nev=max(max_level, 2), mode="matrix", twisted_phases_over_2π_list=thetas,
+                    flux_direction=flux_direction, checkpoint_dir=checkpoint_dir, overwrite=overwrite,
+                    scanned_sectors=labels)
+    base = init.orbit_catalog
+    dev = base.table.device
+    site_phase = torch.as_tensor(many_body_position_phases(model.lattice, polarization_direction,
+                                                           include_sublattice=include_sublattice)).to(dev)
+    for it, path in enumerate(paths):
+        data = load_checkpoint(path)
+        cat = base.clone()
+        update_orbit_stabilizer_phases(cat, data.symmetry_group, model.particle_statistics)
+        sset = SectorSet(cat, data.irrep_list)
+        X, chi = {}, {}
+        for il, lab in enumerate(labels):
+            idx = next((i for i, ir in enumerate(data.irrep_list) if ir.label == lab), None)
+            if idx is None or idx not in data.ed_scan_res:
+                raise ValueError(f"sector {lab} not found in checkpoint {path}")
+            vals, vecs = data.ed_scan_res[idx]
+            nv = required[lab]
+            if vecs.shape[1] < nv:
+                raise ValueError(f"Sector {lab} in {path} has {vecs.shape[1]} eigenvectors; need {nv}.")
+            if len(vals) < nv:
+                raise ValueError(f"Sector {lab} in {path} has {len(vals)} eigenvalues; need {nv}.")
+            energies[it, il, :nv] = vals[:nv]
+            rows = sset.rows(idx)[0].long()
+            x = torch.zeros((nv, cat.n_orbits), dtype=torch.complex128, device=dev)
+            x[:, rows] = torch.as_tensor(np.ascontiguousarray(np.asarray(vecs)[:, :nv].T)).to(dev)
+            X[lab], chi[lab] = x, sset.chi[idx].contiguous()
+        blocks: dict = {}
+        P = np.zeros((n_states, n_states), dtype=np.complex128)
+        for r, st in enumerate(specs):
+            for c, sf in enumerate(specs):
+                key = (st.sector, sf.sector)
+                if key not in blocks:
+                    blocks[key] = _position_block(cat, chi[st.sector], chi[sf.sector], X[st.sector], X[sf.sector],
+                                                  site_phase)
+                P[r, c] = blocks[key][st.level - 1, sf.level - 1]
+        ev = np.linalg.eigvals(P)
+        pol_ev[it] = ev[np.argsort(np.angle(ev))]
+    raw = np.angle(pol_ev) / (2 * math.pi)
+    polarizations = _tracked_phase_branches(raw)
+    trajectories = polarizations - polarizations[0:1, :]
+    pumped = trajectories[-1, :]
+    if fig_path is not None:
+        import matplotlib.pyplot as plt  # optional, as in the reference
+
+        os.makedirs(os.path.dirname(os.path.abspath(fig_path)), exist_ok=True)
+        fig, ax = plt.subplots(figsize=(8.0, 6.0))
+        ax.set_xlabel(f"Inserted Flux [2π] along Direction-{flux_direction}")
+        ax.set_ylabel("Pumped Charge ΔQ")
+        ax.set_title(f"{model.lattice.sample_size}-sample Charge Pump — sectors: "
+                     + ", ".join(repr(lab) for lab in labels))
+        for b, st in enumerate(specs):
+            ax.plot(thetas, trajectories[:, b], linewidth=2, label=f"sector {st.sector!r}, level {st.level}")
+            ax.scatter(thetas, trajectories[:, b], s=12)
+        ax.legend(loc="best")
+        fig.tight_layout()
+        fig.savefig(fig_path)
+    return SimpleNamespace(twisted_phases_over_2π_list=thetas, energies=energies, sector_labels=labels,
+                           flux_direction=flux_direction, polarization_direction=polarization_direction,
+                           nev_per_sector=max_level, manifold_states=specs, polarization_eigenvalues=pol_ev,
+                           polarizations=polarizations, pumped_charge_trajectories=trajectories,
+                           pumped_charges=pumped, include_sublattice=include_sublattice, is_identity=is_identity,
+                           fig_path=fig_path, checkpoint_paths=paths)

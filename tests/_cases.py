@@ -78,3 +78,33 @@ def chern_case(name):
             sample_size=sample, params=dict(models.params_Sun_Gu_Katsura_Sarma))
     labels = "identity" if f["labels"].dtype.kind == "U" else [tuple(int(x) for x in lab) for lab in f["labels"]]
     return m, int(f["n_particles"]), labels, int(f["nev"]), tuple(int(x) for x in f["grid"]), f
+
+
+PUMP_CASES = ["haldane12", "checkerboard12", "haldane16"]
+
+
+def pump_case(name):
+    """(model at zero flux, fixture) of one pump_*.npz fixture
+    (tests/golden/make_pump_golden.py)."""
+    import os
+
+    import numpy as np
+
+    from realspace_exatdiagonalization_py_b200 import models
+
+    f = dict(np.load(os.path.join(os.path.dirname(__file__), "golden", f"pump_{name}.npz")))
+    sample = [int(x) for x in f["sample"]]
+    if str(f["kind"]) == "bosonic":
+        m = models.build_zero_flux_bosonic_fci_second_quantized_model(sample_size=sample, params=models.params_DNSheng)
+    else:
+        m = models.build_zero_flux_fermionic_fci_second_quantized_model(
+            sample_size=sample, params=dict(models.params_Sun_Gu_Katsura_Sarma))
+    return m, f
+
+
+def pump_specs(f):
+    """The (sector, level) manifold of a pump fixture."""
+    labels = [tuple(int(x) for x in lab) for lab in f["labels"]]
+    if len(f["states"]):
+        return [((int(a), int(b)), int(lev)) for a, b, lev in f["states"]]
+    return [(lab, lev) for lab in labels for lev in range(1, int(f["nev"]) + 1)]

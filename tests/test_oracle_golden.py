@@ -195,3 +195,72 @@ def test_chern_checkpoint_names():
     assert obs._chern_sector_labels("identity") == ["identity"]
     assert obs._chern_sector_labels([[1, 0]]) == [(1, 0)]
     assert obs._chern_flux_tag([0.25, -0.5]) == "0p250000_m0p500000"
+
+
+@pytest.mark.parametrize("case", ["haldane12", "checkerboard12", "haldane16"])
+def test_charge_pump_oracle_matches_reference(case):
+    """The oracle's charge pump against the reference's driver
+    (tests/golden/make_pump_golden.py): polarization eigenvalues (invariant
+    under the gauge of the manifold states), tracked polarizations, pumped
+    charges and energies."""
+    from _cases import pump_case, pump_specs
+
+    import realspace_exatdiagonalization_py_b200 as ed
+
+    model, f = pump_case(case)
+
+    def flux_setup(flux):
+        ed.update_second_quantized_model_with_twisted_phases(model, twisted_phases_over_2π=flux)
+        G = ed.build_translation_group(model.lattice, flux)
+        return G, ed.build_irrep_list(G, model.lattice)
+
+    phases = ed.many_body_position_phases(model.lattice, int(f["polarization_direction"]),
+                                          include_sublattice=bool(f["include_sublattice"]))
+    ev, pol, pumped, E = port.charge_pump(model, int(f["n_particles"]), pump_specs(f), list(f["thetas"]),
+                                          int(f["flux_direction"]), phases, flux_setup)
+    np.testing.assert_allclose(E, f["energies"], atol=1e-10, rtol=0)
+    np.testing.assert_allclose(ev, f["polarization_eigenvalues"], atol=1e-9, rtol=0)
+    np.testing.assert_allclose(pol, f["polarizations"], atol=1e-9, rtol=0)
+    np.testing.assert_allclose(pumped, f["pumped_charges"], atol=1e-9, rtol=0)
+
+
+def test_charge_pump_host_helpers():
+    """Position phases, default direction, manifold specs and branch tracking
+    (charge_pump.py:41-322) on fixed inputs."""
+    from realspace_exatdiagonalization_py_b200 import models
+    from realspace_exatdiagonalization_py_b200 import observables as obs
+
+    m = models.build_zero_flux_bosonic_fci_second_quantized_model(sample_size=[2, 3], params=models.params_DNSheng)
+    ph = obs.many_body_position_phases(m.lattice, 2)
+    for i, (cell, sub) in enumerate(m.lattice.site_list):
+        x = cell[1] + m.lattice.sub_crys_list[sub - 1][1]
+        assert abs(ph[i] - np.exp(2j * np.pi * x / 3)) < 1e-15
+    with pytest.raises(ValueError):
+        obs.many_body_position_phases(m.lattice, 3)
+    assert obs._default_polarization_direction(2, 1) == 2 and obs._default_polarization_direction(2, 2) == 1
+    assert obs._default_polarization_direction(1, 1) == 1
+    labels, specs, req, ident = obs._normalize_manifold_state_specs([(0, 0), (1, 0)], 2, None)
+    assert labels == [(0, 0), (1, 0)] and len(specs) == 4 and req == {(0, 0): 2, (1, 0): 2} and not ident
+    labels, specs, req, _ = obs._normalize_manifold_state_specs([(0, 0)], 1, [((0, 0), 2), {"sector": (0, 0),
+                                                                                             "level": 1}])
+    assert [(s.sector, s.level) for s in specs] == [((0, 0), 2), ((0, 0), 1)] and req == {(0, 0): 2}
+    for bad in ([((1, 1), 1)], [((0, 0), 0)], [((0, 0), 1), ((0, 0), 1)], []):
+        with pytest.raises(ValueError):
+            obs._normalize_manifold_state_specs([(0, 0)], 1, bad)
+    with pytest.raises(ValueError):
+        obs._normalize_manifold_state_specs([(0, 0)], 0, None)
+    raw = np.array([[0.1, -0.2, 0.4], [0.45, 0.15, -0.1], [-0.45, 0.2, -0.05]])
+    np.testing.assert_array_equal(obs._tracked_phase_branches(raw), port._track(raw))
+
+
+def test_charge_pump_rejects_identity_before_any_work():
+    from fractions import Fraction
+
+    from realspace_exatdiagonalization_py_b200 import models
+    from realspace_exatdiagonalization_py_b200 import observables as obs
+
+    m = models.build_zero_flux_bosonic_fci_second_quantized_model(sample_size=[2, 3], params=models.params_DNSheng)
+    with pytest.raises(ValueError, match="identity"):
+        obs.flux_charge_pump(m, "identity", filling_fraction=Fraction(3, 12))
+    with pytest.raises(ValueError, match="flux_direction"):
+        obs.flux_charge_pump(m, [(0, 0)], filling_fraction=Fraction(3, 12), flux_direction=3)
