@@ -44,7 +44,8 @@ from .lanczos import (
     diagonalize_block_matrixfree,
     refine,
 )
-from .serving import FluxContext, ServingModel, SolveRequest, SolveResult, SolveServer, latency_summary
+from .serving import (FluxContext, ServedCheckpoints, ServingModel, SolveRequest, SolveResult, SolveServer,
+                      latency_summary)
 from .second_quantized_model import (
     Real_Space_Second_Quantized_Model,
     update_second_quantized_model_with_twisted_phases,

@@ -11,7 +11,10 @@ returned as a ``SimpleNamespace`` with the reference's fields.  Two engines:
 * ``engine="served"``: every (flux value, sector) solve is a request to a
   ``SolveServer`` -- the zero-flux catalog is built once and moved to each flux
   point by ``update_orbit_stabilizer_phases``, solves of different flux points
-  overlap on the device; no checkpoints (``checkpoint_paths`` is ``None``).
+  overlap on the device; the results are written (and, unless ``overwrite``,
+  read back) as the same per-flux-point checkpoints the scan engine uses
+  (``ServedCheckpoints``: asynchronous device-to-host copies, a writer
+  thread).
 
 ``many_body_chern_number`` keeps the contract of the reference's driver
 (``observables/many_body_chern_number.py:341-458``): the Chern number of the
@@ -99,7 +102,7 @@ def flux_spectrum_flow(model, sector_labels, *, filling_fraction, flux_direction
                     nv = min(len(vals), nev)
                     energies[it, isec, :nv] = vals[:nv]
     elif engine == "served":
-        from .serving import ServingModel, SolveRequest, SolveServer
+        from .serving import ServedCheckpoints, ServingModel, SolveRequest, SolveServer
 
         n_filled = int(filling_fraction * model.lattice.n_site)
         sm = ServingModel(model, n_filled, name="flow")
@@ -114,11 +117,18 @@ def flux_spectrum_flow(model, sector_labels, *, filling_fraction, flux_direction
                 rid = len(reqs)
                 reqs.append(SolveRequest(rid, irr.index(lab), tuple(flux), "flow"))
                 where[rid] = (it, isec)
-        server = SolveServer(sm, nev=nev, precision=precision, block=2)
+        ck = ServedCheckpoints(checkpoint_dir, overwrite=overwrite)
+        server = SolveServer(sm, nev=nev, precision=precision, block=2, checkpoints=ck)
         for res in server.run(reqs, realtime=False):
             it, isec = where[res.rid]
             nv = min(len(res.eigenvalues), nev)
             energies[it, isec, :nv] = res.eigenvalues[:nv]
+        ck.close()
+        checkpoint_paths = []
+        for th in thetas:
+            flux = [0.0] * dim
+            flux[flux_direction - 1] = th
+            checkpoint_paths.append(ck.path_of(sm, tuple(flux)))
     else:
         raise ValueError(f"unknown engine {engine!r}")
     if fig_path is not None:
@@ -265,18 +275,23 @@ def _plot_many_body_chern_curvature(result, *, fig_path: str | None = None):
     return fig, ax
 
 
-def _chern_served(model, labels, n_filled, flux_x, flux_y, nev_per_sector):
+def _chern_served(model, labels, n_filled, flux_x, flux_y, nev_per_sector, checkpoint_dir, overwrite):
     """Every (flux point, sector) solve of the grid as one request to a
-    ``SolveServer`` (FP64, eigenvectors kept on the device); returns the
-    results by ``(ix, iy, label)`` and a function that expands one flux
-    point's manifold into dense Fock rows."""
+    ``SolveServer`` (FP64, eigenvectors kept on the device, results written
+    to -- and, unless ``overwrite``, answered from -- the Chern scan's
+    per-point checkpoints); returns the catalog, a function that expands one
+    flux point's manifold into dense Fock rows, and the checkpoint path of a
+    flux point."""
     from .catalog import update_orbit_stabilizer_phases
     from .fock import expand_sector_state_to_fock_dense
     from .sector import SectorSet, Symmetry_Sector_Basis
-    from .serving import ServingModel, SolveRequest, SolveServer
+    from .serving import ServedCheckpoints, ServingModel, SolveRequest, SolveServer
     from .symmetry import build_irrep_list, build_translation_group
 
     sm = ServingModel(model, n_filled, name="chern")
+    ff = Fraction(n_filled, model.lattice.n_site)
+    ck = ServedCheckpoints(checkpoint_dir, overwrite=overwrite,
+                           path_of=lambda sm_, flux: _chern_checkpoint_path(model, ff, list(flux), checkpoint_dir))
     irr = [ir.label for ir in build_irrep_list(sm.group0, model.lattice)]
     for lab in labels:
         if lab not in irr:
@@ -287,9 +302,10 @@ def _chern_served(model, labels, n_filled, flux_x, flux_y, nev_per_sector):
             for lab in labels:
                 where[len(reqs)] = (ix, iy, lab)
                 reqs.append(SolveRequest(len(reqs), irr.index(lab), (float(fx), float(fy)), "chern", vectors=True))
-    server = SolveServer(sm, nev=nev_per_sector, precision=64, block=2)
+    server = SolveServer(sm, nev=nev_per_sector, precision=64, block=2, checkpoints=ck)
     solved = {where[r.rid]: r for r in server.run(reqs, realtime=False, timeout=24 * 3600.0)}
     del server
+    ck.close()
 
     def fill(ix, iy, out):
         flux = [float(flux_x[ix]), float(flux_y[iy])]
@@ -310,7 +326,7 @@ def _chern_served(model, labels, n_filled, flux_x, flux_y, nev_per_sector):
                 expand_sector_state_to_fock_dense(res.eigenvectors[:, level], basis, out=out[row])
                 energies.append(float(res.eigenvalues[level]))
                 row += 1
-        return energies, None
+        return energies, ck.path_of(sm, tuple(flux))
 
     return sm.catalog, fill
 
@@ -328,8 +344,8 @@ def many_body_chern_number(model, sector_labels, *, filling_fraction, flux_grid_
     ``engine="scan"`` solves flux point after flux point with the
     reference's per-point checkpoints; ``engine="served"`` submits every
     (flux point, sector) solve to a ``SolveServer`` at once (FP64, solves of
-    different flux points overlapping on the device; momentum sectors only,
-    no checkpoints: ``checkpoint_paths`` entries are ``None``)."""
+    different flux points overlapping on the device; momentum sectors only)
+    and keeps the same per-point checkpoints through ``ServedCheckpoints``."""
     import torch
 
     from .ed import build_ed_data
@@ -368,7 +384,9 @@ def many_body_chern_number(model, sector_labels, *, filling_fraction, flux_grid_
         n_filled = filling_fraction * model.lattice.n_site
         if n_filled.denominator != 1:
             raise ValueError("filling_fraction * n_site must be an integer (particle number).")
-        cat, fill = _chern_served(model, labels, int(n_filled), flux_x, flux_y, int(nev_per_sector))
+        os.makedirs(checkpoint_dir, exist_ok=True)
+        cat, fill = _chern_served(model, labels, int(n_filled), flux_x, flux_y, int(nev_per_sector), checkpoint_dir,
+                                  overwrite)
     n_m = len(labels) * int(nev_per_sector)
     rows_kept = min(nx, 3)
     states = torch.zeros((rows_kept * ny, n_m, cat.n_states), dtype=torch.complex128, device=cat.table.device)

@@ -42,7 +42,12 @@ which other requests share the device or its lane.
 
 from __future__ import annotations
 
+import copy
 import ctypes
+import dataclasses
+import os
+import queue
+import threading
 import time
 from collections import OrderedDict
 from dataclasses import dataclass
@@ -60,8 +65,8 @@ from .lattice import generate_bilinear_terms
 from .sector import SectorSet
 from .symmetry import build_irrep_list, build_translation_group, group_order
 
-__all__ = ["ServingModel", "FluxContext", "SolveRequest", "SolveResult", "SolveServer", "latency_summary",
-           "poisson_requests"]
+__all__ = ["ServingModel", "FluxContext", "SolveRequest", "SolveResult", "SolveServer", "ServedCheckpoints",
+           "latency_summary", "poisson_requests"]
 
 
 @dataclass
@@ -243,6 +248,7 @@ class _Lane:
         self.event = torch.cuda.Event()
         self.h_state = self.h_vals = self.h_res = self.h_fp32 = None
         self.vecs: list[torch.Tensor] | None = None
+        self.keep_vectors = False  # set by a server that checkpoints its results
         self.bytes = (lanczos_footprint_bytes(sm.n_orbits, width * params.block, params.n_slots, params.precision)
                       + self.w.numel() * self.w.element_size() + self.member.numel() * 8)
 
@@ -306,7 +312,8 @@ class _Lane:
                 ctypes.byref(self.ctx.dm.c), ctypes.byref(sc), ctypes.byref(b.c), APPLY_AUTO,
                 _lib.stream_ptr(self.stream)))
             self.h_fp32.copy_((fp32 - b.ritz_val[:, : self.nev]).abs(), non_blocking=True)
-        self.vecs = b.eigenvectors(stream=self.stream) if any(r.vectors for r in self.reqs) else None
+        want = self.keep_vectors or any(r.vectors for r in self.reqs)
+        self.vecs = b.eigenvectors(stream=self.stream) if want else None
         self.h_vals.copy_(b.ritz_val[:, : self.nev], non_blocking=True)
         self.h_res.copy_(b.resid[:, : self.nev], non_blocking=True)
         self.h_state.copy_(b.state, non_blocking=True)
@@ -345,7 +352,7 @@ class _Lane:
         vecs = self.vecs or [None] * self.width
         self.vecs = None
         for i, r in enumerate(self.reqs):
-            v = vecs[i] if r.vectors else None
+            v = vecs[i] if (r.vectors or self.keep_vectors) else None
             if v is not None:  # the caller reads it on its own stream
                 v.record_stream(torch.cuda.current_stream())
             out.append(SolveResult(
@@ -358,13 +365,148 @@ class _Lane:
         return out
 
 
+class ServedCheckpoints:
+    """Served results written as the flux scan's checkpoints: one pickled
+    ``Symmetry_Resolved_ED_Data`` per (model, flux point) holding
+    ``ed_scan_res[sector] = (eigenvalues, eigenvectors)`` (the reference's
+    format, ``symmetry_resolved_ed.py:2530-2600``), so a served run resumes
+    from, and leaves behind, what the scan path reads and writes.
+
+    A finished result is copied device -> pinned host on the current stream
+    (asynchronous, ordered by an event) and handed to a writer thread, which
+    merges all queued results of a file and replaces the file atomically; the
+    scheduling loop never waits on the disk or the copy.  ``path_of(sm,
+    flux)`` names the file (default: the flux scan's canonical name in
+    ``checkpoint_dir``); with ``overwrite`` existing files are neither read
+    nor kept.
+    """
+
+    def __init__(self, checkpoint_dir: str, *, path_of=None, overwrite: bool = False):
+        from .ed import ed_scan_checkpoint_filename
+
+        os.makedirs(checkpoint_dir, exist_ok=True)
+        self.dir = checkpoint_dir
+        self.overwrite = overwrite
+        self.path_of = path_of or (lambda sm, flux: os.path.join(
+            checkpoint_dir, ed_scan_checkpoint_filename(sm.model, list(flux), Fraction(sm.n_filled, sm.lattice.n_site))))
+        self._data: dict[str, object] = {}      # path -> ED data written (or read) so far
+        self._fresh: set[str] = set()           # paths started anew under overwrite
+        self._q: queue.Queue = queue.Queue()
+        self._lock = threading.Lock()
+        self._error: BaseException | None = None
+        self._thread = threading.Thread(target=self._loop, name="rsed-checkpoints", daemon=True)
+        self._thread.start()
+        self.written: set[str] = set()
+
+    # -- reading -------------------------------------------------------------
+    def _load(self, path: str):
+        with self._lock:
+            if path in self._data:
+                return self._data[path]
+        if self.overwrite or not os.path.isfile(path):
+            return None
+        from .ed import load_checkpoint
+
+        data = load_checkpoint(path)
+        with self._lock:
+            self._data.setdefault(path, data)
+            return self._data[path]
+
+    def lookup(self, sm: "ServingModel", flux: tuple, sector: int, nev: int):
+        """``(eigenvalues, eigenvectors)`` of a finished solve with at least
+        ``nev`` levels, or ``None``."""
+        data = self._load(self.path_of(sm, flux))
+        if data is None:
+            return None
+        res = data.ed_scan_res.get(sector)
+        if res is None or len(res[0]) < nev or res[1] is None:
+            return None
+        return res
+
+    # -- writing -------------------------------------------------------------
+    def put(self, sm: "ServingModel", flux: tuple, sector: int, eigenvalues: np.ndarray,
+            eigenvectors: torch.Tensor, dim: int) -> None:
+        host = torch.empty(eigenvectors.shape, dtype=eigenvectors.dtype, pin_memory=True)
+        host.copy_(eigenvectors, non_blocking=True)
+        ev = torch.cuda.Event()
+        ev.record()
+        self._q.put((self.path_of(sm, flux), sm, tuple(flux), int(sector), np.array(eigenvalues), host, ev, dim))
+
+    def _skeleton(self, sm: "ServingModel", flux: tuple):
+        from .ed import Symmetry_Resolved_ED_Data
+
+        lat = copy.copy(sm.lattice)
+        lat.twisted_phases_over_2π = list(flux)
+        model = dataclasses.replace(sm.model, lattice=lat, bilinear_terms=generate_bilinear_terms(
+            sm.model.tb_model, twisted_phases_over_2π=list(flux)))
+        group = build_translation_group(lat, list(flux))
+        irreps = build_irrep_list(group, lat)
+        return Symmetry_Resolved_ED_Data(model, sm.n_filled, Fraction(sm.n_filled, lat.n_site), group, irreps,
+                                         None, [0] * len(irreps))
+
+    def _loop(self) -> None:
+        from .ed import save_checkpoint
+
+        while True:
+            item = self._q.get()
+            if item is None:
+                self._q.task_done()
+                return
+            batch = [item]
+            while True:  # everything queued meanwhile: one write per file
+                try:
+                    nxt = self._q.get_nowait()
+                except queue.Empty:
+                    break
+                if nxt is None:
+                    self._q.put(None)
+                    self._q.task_done()
+                    break
+                batch.append(nxt)
+            try:
+                by_path: dict[str, list] = {}
+                for it in batch:
+                    by_path.setdefault(it[0], []).append(it)
+                for path, items in by_path.items():
+                    data = self._load(path) if path not in self._fresh else self._data.get(path)
+                    if data is None:
+                        data = self._skeleton(items[0][1], items[0][2])
+                        if self.overwrite:
+                            self._fresh.add(path)
+                    for _, _, _, sector, vals, host, ev, dim in items:
+                        ev.synchronize()
+                        data.ed_scan_res[sector] = (vals, host.numpy().copy())
+                        data.sector_dims[sector] = dim
+                    with self._lock:
+                        self._data[path] = data
+                    save_checkpoint(data, path)
+                    self.written.add(path)
+            except BaseException as e:  # reported by flush()
+                self._error = e
+            finally:
+                for _ in batch:
+                    self._q.task_done()
+
+    def flush(self) -> None:
+        """Wait until every queued result is on disk."""
+        self._q.join()
+        if self._error is not None:
+            err, self._error = self._error, None
+            raise RuntimeError("writing a checkpoint failed") from err
+
+    def close(self) -> None:
+        self.flush()
+        self._q.put(None)
+        self._thread.join()
+
+
 class SolveServer:
     """Continuous-batching server over one or more ``ServingModel``s."""
 
     def __init__(self, models: dict[str, ServingModel] | ServingModel, *, nev: int = 4, precision: int = 32,
                  block: int = 4, n_slots: int = 16, poll: int = 16, max_width: int = 4,
                  memory_budget: int | None = None, max_iter: int = 4000, creations_per_step: int = 1,
-                 dense_max: int = 500):
+                 dense_max: int = 500, checkpoints: ServedCheckpoints | None = None):
         if isinstance(models, ServingModel):
             models = {models.name: models}
         self.models = dict(models)
@@ -381,6 +523,10 @@ class SolveServer:
         # sectors up to this dimension are solved densely at admission (as the
         # reference does below 500), not in a Lanczos lane
         self.dense_max = dense_max
+        # finished results also go to per-flux-point checkpoints, and requests
+        # already there are answered from them
+        self.checkpoints = checkpoints
+        self._wants_vectors: dict[int, bool] = {}
         self._ready: list[SolveResult] = []
         if memory_budget is None:
             free, _ = torch.cuda.mem_get_info()
@@ -435,7 +581,37 @@ class SolveServer:
         req.flux = sm.normalize_flux(req.flux)
         if not 0 <= req.sector < sm.n_sectors:
             raise ValueError(f"request {req.rid}: no sector {req.sector}")
+        if self.checkpoints is not None:
+            hit = self.checkpoints.lookup(sm, req.flux, req.sector, self.nev)
+            if hit is not None:
+                vals, vecs = hit
+                now = self.now()
+                v = None
+                if req.vectors:
+                    v = torch.as_tensor(np.ascontiguousarray(np.asarray(vecs)[:, : self.nev])).to(
+                        sm.catalog.table.device, torch.complex128)
+                self._ready.append(SolveResult(
+                    rid=req.rid, sector=req.sector, flux=req.flux, model=req.model,
+                    eigenvalues=np.asarray(vals[: self.nev], dtype=np.float64), residuals=np.zeros(self.nev),
+                    fp32_error=None, iterations=0, dim=int(np.asarray(vecs).shape[0]), arrival=req.arrival,
+                    admitted=now, finished=now, lane=-1, lane_width=0, eigenvectors=v))
+                return
+        self._wants_vectors[req.rid] = req.vectors
         self.pending.append(req)
+
+    def _record(self, results: list[SolveResult]) -> list[SolveResult]:
+        # checkpoint finished solves; keep vectors only where they were asked for
+        if self.checkpoints is None:
+            return results
+        for r in results:
+            if r.lane == -1:
+                continue
+            sm = self.models[r.model]
+            if r.eigenvectors is not None:
+                self.checkpoints.put(sm, r.flux, r.sector, r.eigenvalues, r.eigenvectors, r.dim)
+            if not self._wants_vectors.pop(r.rid, False):
+                r.eigenvectors = None
+        return results
 
     def running(self) -> int:
         return sum(1 for ln in self.lanes if ln.state != "idle")
@@ -489,13 +665,14 @@ class SolveServer:
             H = MatrixFreeHamiltonian(basis, ctx.dm.bilinear_terms, ctx.dm.density_terms, None, model=ctx.dm)
             vals, vecs = diagonalize_block_matrixfree(H, basis.dim, nev=self.nev)
         k = len(vals)
-        if req.vectors:
+        keep = req.vectors or self.checkpoints is not None
+        if keep:
             vecs = (torch.zeros((0, 0), dtype=torch.complex128, device=ctx.catalog.table.device) if vecs is None
                     else torch.as_tensor(np.asarray(vecs)).to(ctx.catalog.table.device, torch.complex128))
         return SolveResult(rid=req.rid, sector=req.sector, flux=req.flux, model=req.model,
                            eigenvalues=np.asarray(vals, dtype=np.float64), residuals=np.zeros(k), fp32_error=None,
                            iterations=0, dim=basis.dim, arrival=req.arrival, admitted=now, finished=self.now(),
-                           lane=0, lane_width=1, eigenvectors=vecs if req.vectors else None)
+                           lane=0, lane_width=1, eigenvectors=vecs if keep else None)
 
     def _admit(self, now: float) -> None:
         groups: OrderedDict[tuple, list[SolveRequest]] = OrderedDict()
@@ -544,6 +721,7 @@ class SolveServer:
                     lane = _Lane(sm, width, self.nev, self.params, self.poll)
                     self.lanes.append(lane)
                 take, reqs[:] = reqs[: lane.width], reqs[lane.width:]
+                lane.keep_vectors = self.checkpoints is not None
                 lane.begin(take, ctx, now)
                 self.admissions += 1
                 admitted.update(r.rid for r in take)
@@ -562,7 +740,7 @@ class SolveServer:
         if self.pending:
             self._admit(self.now())
         self.peak_running = max(self.peak_running, self.running())
-        return done
+        return self._record(done)
 
     def run(self, requests: list[SolveRequest], *, realtime: bool = True, timeout: float = 600.0
             ) -> list[SolveResult]:

@@ -102,12 +102,25 @@ def test_chern_served_engine_matches_reference(tmp_path, case):
     import realspace_exatdiagonalization_py_b200 as ed
 
     model, n_part, labels, nev, grid, f = chern_case(case)
+    kw = dict(filling_fraction=Fraction(n_part, model.lattice.n_site), flux_grid_size=grid, nev_per_sector=nev,
+              engine="served", checkpoint_dir=str(tmp_path))
     with warnings.catch_warnings(record=True) as caught:
         warnings.simplefilter("always")
-        res = ed.many_body_chern_number(model, labels, filling_fraction=Fraction(n_part, model.lattice.n_site),
-                                        flux_grid_size=grid, nev_per_sector=nev, engine="served")
+        res = ed.many_body_chern_number(model, labels, **kw)
     _check(res, sum("Near-singular Berry link" in str(w.message) for w in caught), f)
-    assert all(p is None for row in res.checkpoint_paths for p in row)
+    # the served engine leaves the scan engine's per-point checkpoints behind
+    assert os.path.basename(res.checkpoint_paths[0][0]) == str(f["checkpoint_00"])
+    paths = [p for row in res.checkpoint_paths for p in row]
+    assert all(os.path.isfile(p) for p in paths)
+    stamp = [os.path.getmtime(p) for p in paths]
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        scan = ed.many_body_chern_number(model, labels, filling_fraction=kw["filling_fraction"], flux_grid_size=grid,
+                                         nev_per_sector=nev, checkpoint_dir=str(tmp_path))
+        again = ed.many_body_chern_number(model, labels, **kw)
+    assert [os.path.getmtime(p) for p in paths] == stamp  # both read them back, neither recomputed
+    np.testing.assert_allclose(scan.berry_curvature, res.berry_curvature, atol=1e-12, rtol=0)
+    np.testing.assert_allclose(again.berry_curvature, res.berry_curvature, atol=1e-12, rtol=0)
 
 
 def test_chern_served_lanes_match_scan():
@@ -121,9 +134,10 @@ def test_chern_served_lanes_match_scan():
     ff = Fraction(nf, model.lattice.n_site)
     labels = [(0, 0), (0, 1)]
     kw = dict(filling_fraction=ff, flux_grid_size=(2, 3), nev_per_sector=1)
-    served = ed.many_body_chern_number(model, labels, engine="served", **kw)
     import tempfile
 
+    with tempfile.TemporaryDirectory() as d:
+        served = ed.many_body_chern_number(model, labels, engine="served", checkpoint_dir=d, **kw)
     with tempfile.TemporaryDirectory() as d:
         scan = ed.many_body_chern_number(model, labels, mode="matrixfree", checkpoint_dir=d, **kw)
     np.testing.assert_allclose(np.array(served.energies), np.array(scan.energies), atol=1e-9, rtol=0)

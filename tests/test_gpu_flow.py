@@ -36,4 +36,11 @@ def test_flux_spectrum_flow_matches_reference(tmp_path, engine):
         assert [os.path.getmtime(p) for p in again.checkpoint_paths] == stamp  # reused, not recomputed
         np.testing.assert_array_equal(again.energies, res.energies)
     else:
-        assert res.checkpoint_paths is None
+        # the served results are the scan engine's checkpoints: a scan run reads them, recomputes nothing
+        assert len(res.checkpoint_paths) == len(thetas) and all(os.path.isfile(p) for p in res.checkpoint_paths)
+        stamp = [os.path.getmtime(p) for p in res.checkpoint_paths]
+        scan = ed.flux_spectrum_flow(model, labels, filling_fraction=Fraction(3, 12), flux_direction=1,
+                                     twisted_phases_over_2π_list=thetas, checkpoint_dir=str(tmp_path), nev=3)
+        assert scan.checkpoint_paths == res.checkpoint_paths
+        assert [os.path.getmtime(p) for p in res.checkpoint_paths] == stamp
+        np.testing.assert_array_equal(scan.energies, res.energies)

@@ -109,3 +109,55 @@ def test_poisson_stream_latency_summary(golden):
     summ = ed.latency_summary(res)
     assert summ["requests"] == 12 and summ["p99_ms"] >= summ["p50_ms"] > 0
     assert all(r.finished >= r.admitted >= r.arrival - 1e-3 for r in res)
+
+
+def test_checkpointed_server_writes_and_resumes(golden, tmp_path):
+    """Served results land in the flux scan's per-flux-point checkpoint files
+    (loadable by ``load_checkpoint``, eigenvectors included); a second server
+    over the same directory answers those requests from disk, with the same
+    eigenvalues and vectors; ``overwrite`` solves again."""
+    import os
+
+    import torch
+
+    import realspace_exatdiagonalization_py_b200 as ed
+
+    models, g, gh = _models(golden)
+    sm = models["haldane24"]
+    reqs = [ed.SolveRequest(0, 0, (0.25, 0.5), "haldane24", vectors=True),
+            ed.SolveRequest(1, 4, (0.25, 0.5), "haldane24"),
+            ed.SolveRequest(2, 2, (0.0, 0.0), "haldane24", vectors=True)]
+    ck = ed.ServedCheckpoints(str(tmp_path))
+    first = {r.rid: r for r in ed.SolveServer(sm, nev=3, precision=64, block=2, checkpoints=ck).run(
+        [ed.SolveRequest(r.rid, r.sector, r.flux, r.model, vectors=r.vectors) for r in reqs], realtime=False)}
+    ck.close()
+    assert first[1].eigenvectors is None and first[0].eigenvectors is not None
+    paths = sorted(ck.written)
+    assert len(paths) == 2 and all(os.path.isfile(p) for p in paths)
+    assert ck.path_of(sm, (0.25, 0.5)) == os.path.join(str(tmp_path), ed.ed_scan_checkpoint_filename(
+        sm.model, [0.25, 0.5], Fraction(sm.n_filled, sm.lattice.n_site)))
+    data = ed.load_checkpoint(ck.path_of(sm, (0.25, 0.5)))
+    assert sorted(data.ed_scan_res) == [0, 4] and data.symmetry_group.name == "translations"
+    vals, vecs = data.ed_scan_res[0]
+    np.testing.assert_array_equal(vals, first[0].eigenvalues)
+    np.testing.assert_array_equal(vecs, first[0].eigenvectors.cpu().numpy())
+    assert data.sector_dims[0] == first[0].dim
+    # resume: answered from disk
+    ck2 = ed.ServedCheckpoints(str(tmp_path))
+    stamp = [os.path.getmtime(p) for p in paths]
+    second = {r.rid: r for r in ed.SolveServer(sm, nev=3, precision=64, block=2, checkpoints=ck2).run(
+        [ed.SolveRequest(r.rid, r.sector, r.flux, r.model, vectors=r.vectors) for r in reqs], realtime=False)}
+    ck2.close()
+    assert all(r.lane == -1 and r.iterations == 0 for r in second.values())
+    assert [os.path.getmtime(p) for p in paths] == stamp
+    for rid in first:
+        np.testing.assert_array_equal(second[rid].eigenvalues, first[rid].eigenvalues)
+    assert torch.equal(second[2].eigenvectors, first[2].eigenvectors)
+    # overwrite: solved again, files rewritten
+    ck3 = ed.ServedCheckpoints(str(tmp_path), overwrite=True)
+    third = ed.SolveServer(sm, nev=3, precision=64, block=2, checkpoints=ck3).run(
+        [ed.SolveRequest(0, 0, (0.25, 0.5), "haldane24")], realtime=False)
+    ck3.close()
+    assert third[0].lane != -1
+    np.testing.assert_allclose(third[0].eigenvalues, first[0].eigenvalues, atol=1e-10, rtol=0)
+    assert sorted(ed.load_checkpoint(ck.path_of(sm, (0.25, 0.5))).ed_scan_res) == [0]
