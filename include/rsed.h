@@ -294,6 +294,30 @@ int rsed_position_overlaps(const rsed_group_t* grp, int64_t n_orbits, const uint
                            const double* x_to, int32_t k_to, const double* x_from, int32_t k_from,
                            double* out, void* scratch, size_t scratch_bytes, void* stream);
 
+/* ---- correlators of one sector state ---------------------------------------
+ * One-body density matrix rho[i][j] = <psi| a_i^dagger a_j |psi> (replaces the
+ * orbit loops of off_diagonal_long_range_order,
+ * observables/off_diagonal_long_range_order.py:77-140): x_orbit is the sector
+ * vector in orbit layout (complex128, zero outside the sector), member/sector
+ * the sector's membership bit per orbit, chi its |G| characters; rho is
+ * device complex128 [N][N] (row i, column j, 0-based sites).  A hop between
+ * the two species of a two-species basis contributes zero.  Asynchronous on
+ * `stream`; the sums run in a fixed order for a given device. */
+size_t rsed_obdm_scratch_bytes(int32_t n_site);
+int rsed_one_body_density(const rsed_group_t* grp, const rsed_entry_t* table, int64_t n_orbits,
+                          const uint64_t* repr_masks, const uint64_t* stab_mask, const uint64_t* member,
+                          int32_t sector, const double* chi, const double* x_orbit, double* rho,
+                          void* scratch, size_t scratch_bytes, void* stream);
+
+/* Density pairs of one sector state over the representatives (the orbit sum
+ * of _build_density_correlation_matrix, observables/static_structure_factor.py:
+ * 54-149, before the sum over the group): pairs[a][b] = sum_o |x_o|^2
+ * n_a(s_o) n_b(s_o), device float64 [N][N].  The caller forms
+ * <n_i n_j> = (1/|G|) sum_g pairs[a][b] at i = g(a), j = g(b). */
+size_t rsed_density_pairs_scratch_bytes(int32_t n_site);
+int rsed_density_pairs(int32_t n_site, int64_t n_orbits, const uint64_t* repr_masks, const double* x_orbit,
+                       double* pairs, void* scratch, size_t scratch_bytes, void* stream);
+
 /* ---- K8: batched thick-restart block Lanczos -------------------------------
  * Replaces diagonalize_block_matrixfree / diagonalize_block_arpack
  * (symmetry_resolved_ed.py:2214-2299, ARPACK eigs(which="SR", tol=1e-10))

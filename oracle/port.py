@@ -21,6 +21,12 @@ import this module.  It restates, in vectorised numpy, the algorithm of
 * the charge pump: the orbit-diagonal position operator between sectors,
   manifold eigenvalues and phase-branch tracking
   (``observables/charge_pump.py:41-240, 325-505``),
+* the one-body density matrix orbit by orbit as the reference computes it
+  (``observables/off_diagonal_long_range_order.py:77-140``), and <a_i^dagger
+  a_j>, <n_i n_j> as exact expectation values over the Fock amplitudes (the
+  reference's <n_i n_j>, ``static_structure_factor.py:54-149``, is exactly
+  that; its one-body density matrix equals it where alpha' conj(chi(g')) of
+  every projected hop is real),
 * the eigen-solves: dense ``eigh(UPLO="U")`` for n <= 500 and ARPACK
   ``eigs(k=nev, which="SR", tol=1e-10)`` with the seeded ``v0`` otherwise
   (SRE:2180-2299).
@@ -548,3 +554,78 @@ def charge_pump(model, n_filled: int, specs, thetas, flux_direction: int, site_p
         ev_all[it] = ev[np.argsort(np.angle(ev))]
     pol = _track(np.angle(ev_all) / (2 * np.pi))
     return ev_all, pol, pol[-1] - pol[0], energies
+
+
+def fock_correlators(amps: dict, n: int, fermion: bool):
+    """``(rho, nn)`` of a normalised {mask: amplitude} state: rho[i, j] =
+    <a_i^dagger a_j> (sign (-1)^(occupied sites strictly between i and j) for
+    fermions) and nn[i, j] = <n_i n_j>, 0-based sites."""
+    rho = np.zeros((n, n), dtype=np.complex128)
+    nn = np.zeros((n, n))
+    for m, a in amps.items():
+        w = abs(a) ** 2
+        occ = [i for i in range(n) if (m >> i) & 1]
+        for i in occ:
+            for j in occ:
+                nn[i, j] += w
+        for j in occ:
+            rho[j, j] += w
+            for i in range(n):
+                if (m >> i) & 1:
+                    continue
+                m2 = m ^ (1 << j) ^ (1 << i)
+                b = amps.get(m2)
+                if b is None:
+                    continue
+                sign = 1.0
+                if fermion:
+                    lo, hi = min(i, j), max(i, j)
+                    between = ((1 << (hi - lo - 1)) - 1) << (lo + 1) if hi - lo > 1 else 0
+                    if bin(m & between).count("1") & 1:
+                        sign = -1.0
+                rho[i, j] += np.conj(b) * a * sign
+    return rho, nn
+
+
+def obdm_orbitwise(cat: dict, orbits: np.ndarray, c: np.ndarray, chi: np.ndarray, perm0: np.ndarray,
+                   eta: np.ndarray, fermion: bool, n: int, k: int) -> np.ndarray:
+    """rho[i, j] as off_diagonal_long_range_order.py:77-140 accumulates it:
+    per representative and group element the ket c / sqrt(|G| |Stab|) *
+    conj(chi(g)) * phase_g; |c|^2/|G| on the diagonal of every occupied site;
+    for a hop j -> i onto an orbit of the sector the bra c_row *
+    sqrt(|Stab_row| / |G|) * conj(alpha' conj(chi(g'))) from the catalog entry
+    of the hopped mask, times the Jordan-Wigner sign of the hop."""
+    bt = binom_table(n, k)
+    pos = {int(o): t for t, o in enumerate(orbits)}
+    ng = perm0.shape[0]
+    rho = np.zeros((n, n), dtype=np.complex128)
+    for t, o in enumerate(orbits):
+        if c[t] == 0:
+            continue
+        s_mask = int(cat["reprs"][o])
+        S = len(cat["stab_g"][o])
+        for g in range(ng):
+            km, ph = apply_product(s_mask, perm0[g], eta[g], fermion)
+            ket = c[t] * ((1 / np.sqrt(ng) / np.sqrt(S)) * np.conj(chi[g]) * ph)
+            for j in range(n):
+                if not (km >> j) & 1:
+                    continue
+                rho[j, j] += abs(c[t]) ** 2 / ng
+                for i in range(n):
+                    if i == j or (km >> i) & 1:
+                        continue
+                    nm = km ^ (1 << j) ^ (1 << i)
+                    r = int(rank(np.array([nm], dtype=np.uint64), n, bt)[0])
+                    ro = int(cat["rep_rank"][r])
+                    if ro not in pos:
+                        continue
+                    p = complex(cat["rep_amp"][r]) * np.conj(chi[int(cat["rep_sym"][r])])
+                    bra = c[pos[ro]] * (np.sqrt(len(cat["stab_g"][ro])) / np.sqrt(ng) * np.conj(p))
+                    sign = 1.0
+                    if fermion:
+                        lo, hi = min(i, j), max(i, j)
+                        between = ((1 << (hi - lo - 1)) - 1) << (lo + 1) if hi - lo > 1 else 0
+                        if bin(km & between).count("1") & 1:
+                            sign = -1.0
+                    rho[i, j] += np.conj(bra) * ket * sign
+    return rho

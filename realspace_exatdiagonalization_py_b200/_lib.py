@@ -178,6 +178,12 @@ SIGNATURES = {
     "rsed_position_overlaps": (c_int, [POINTER(RsedGroup), c_int64, c_void_p, c_void_p, c_void_p, c_void_p,
                                        c_void_p, c_int32, c_void_p, c_int32, c_void_p, c_void_p, c_size_t,
                                        c_void_p]),
+    "rsed_obdm_scratch_bytes": (c_size_t, [c_int32]),
+    "rsed_one_body_density": (c_int, [POINTER(RsedGroup), c_void_p, c_int64, c_void_p, c_void_p, c_void_p,
+                                      c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p]),
+    "rsed_density_pairs_scratch_bytes": (c_size_t, [c_int32]),
+    "rsed_density_pairs": (c_int, [c_int32, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_size_t,
+                                   c_void_p]),
     "rsed_proj_scratch_bytes": (c_size_t, [c_int64]),
     "rsed_proj_count": (c_int, [POINTER(RsedModel), c_void_p, POINTER(c_int64), c_void_p, c_size_t, c_void_p]),
     "rsed_proj_fill": (c_int, [POINTER(RsedModel), c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),

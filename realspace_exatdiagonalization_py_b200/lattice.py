@@ -50,6 +50,8 @@ __all__ = [
     "initialize_real_space_tightbinding_model",
     "add_hopping_term",
     "generate_bilinear_terms",
+    "Uniform_Grids",
+    "initialize_uniform_grids_from_lattice",
 ]
 
 
@@ -77,6 +79,39 @@ class Real_Space_Lattice:
 
     def cell_list(self) -> list[tuple[int, ...]]:
         return list(itertools.product(*[range(L) for L in self.sample_size]))
+
+    @property
+    def site_cart_list(self) -> list[list[float]]:
+        """Cartesian position of every site: sum over d of (cell_d + sub_d) a_d,
+        the sub-lattice offset given in crystal coordinates."""
+        out = []
+        for cell, sub in self.site_list:
+            crys = [float(c) + float(x) for c, x in zip(cell, self.sub_crys_list[sub - 1])]
+            out.append([sum(crys[d] * self.brav_vec_list[d][k] for d in range(self.dim)) for k in range(self.dim)])
+        return out
+
+
+@dataclass
+class Uniform_Grids:
+    """The finite-torus momentum mesh of a lattice: ``site_cart_list`` holds
+    q = sum_d (n_d / L_d) b_d for every n in range(L_1) x ... x range(L_dim)
+    (last index fastest), ``b_d`` the reciprocal vectors (a_d . b_e = 2 pi
+    delta_de); ``nsite`` = the number of q points."""
+
+    site_cart_list: list[list[float]]
+    nsite: int
+
+
+def initialize_uniform_grids_from_lattice(lattice: Real_Space_Lattice) -> Uniform_Grids:
+    A = [[lattice.brav_vec_list[d][k] for d in range(lattice.dim)] for k in range(lattice.dim)]  # columns a_d
+    import numpy as np
+
+    B = 2 * math.pi * np.linalg.inv(np.array(A, dtype=np.float64)).T  # columns b_d
+    pts = []
+    for n in itertools.product(*[range(L) for L in lattice.sample_size]):
+        q = sum((n[d] / lattice.sample_size[d]) * B[:, d] for d in range(lattice.dim))
+        pts.append([float(v) for v in q])
+    return Uniform_Grids(site_cart_list=pts, nsite=len(pts))
 
 
 def initialize_real_space_lattice(

@@ -108,3 +108,27 @@ def pump_specs(f):
     if len(f["states"]):
         return [((int(a), int(b)), int(lev)) for a, b, lev in f["states"]]
     return [(lab, lev) for lab in labels for lev in range(1, int(f["nev"]) + 1)]
+
+
+CORR_CASES = ["haldane12", "checkerboard12", "haldane12_identity", "haldane16"]
+
+
+def corr_case(name):
+    """(model at zero flux, sector label, level, flavour_a filter, fixture) of
+    one corr_*.npz fixture (tests/golden/make_corr_golden.py)."""
+    import os
+
+    import numpy as np
+
+    from realspace_exatdiagonalization_py_b200 import models
+
+    f = dict(np.load(os.path.join(os.path.dirname(__file__), "golden", f"corr_{name}.npz")))
+    sample = [int(x) for x in f["sample"]]
+    if str(f["kind"]) == "bosonic":
+        m = models.build_zero_flux_bosonic_fci_second_quantized_model(sample_size=sample, params=models.params_DNSheng)
+    else:
+        m = models.build_zero_flux_fermionic_fci_second_quantized_model(
+            sample_size=sample, params=dict(models.params_Sun_Gu_Katsura_Sarma))
+    label = "identity" if f["label"].dtype.kind == "U" else tuple(int(x) for x in f["label"])
+    fa = (lambda i: True) if str(f["flavor_a"]) == "all" else (lambda i: i % 2 == 1)
+    return m, label, int(f["level"]), fa, f

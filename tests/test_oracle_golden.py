@@ -264,3 +264,64 @@ def test_charge_pump_rejects_identity_before_any_work():
         obs.flux_charge_pump(m, "identity", filling_fraction=Fraction(3, 12))
     with pytest.raises(ValueError, match="flux_direction"):
         obs.flux_charge_pump(m, [(0, 0)], filling_fraction=Fraction(3, 12), flux_direction=3)
+
+
+@pytest.mark.parametrize("case", ["haldane12", "checkerboard12", "haldane12_identity", "haldane16"])
+def test_correlators_oracle_matches_reference(case):
+    """The oracle's one-body density matrix (the reference's orbit-by-orbit
+    accumulation) and connected <n_i n_j> (exact sums over the state's Fock
+    amplitudes) against the reference's functions
+    (tests/golden/make_corr_golden.py)."""
+    from _cases import corr_case
+
+    import realspace_exatdiagonalization_py_b200 as ed
+
+    model, label, level, fa, f = corr_case(case)
+    n = model.lattice.n_site
+    nf = int(f["n_particles"])
+    G = ed.build_identity_group(n) if label == "identity" else ed.build_translation_group(model.lattice)
+    irreps = ed.build_irrep_list(G, model.lattice)
+    s = 0 if label == "identity" else next(i for i, ir in enumerate(irreps) if ir.label == label)
+    perm0, eta = port.group_arrays(G)
+    fermion = model.particle_statistics.name == "FERMIONIC"
+    cat = port.catalog(n, nf, perm0, eta, fermion)
+    chi = np.asarray(irreps[s].values, dtype=np.complex128)
+    orbits = port.sector_orbits(cat, chi)
+    H = port.csr_block(cat, n, orbits, model.bilinear_terms, model.density_density_terms, chi, fermion)
+    _, v = port.solve(H, max(level, 2), seeded_v0=False)
+    rho = port.obdm_orbitwise(cat, orbits, v[:, level - 1], chi, perm0, eta, fermion, n, nf)
+    np.testing.assert_allclose(rho, f["odlro"], atol=1e-11, rtol=0)
+    amps = port.fock_expand(cat, orbits, v[:, level - 1], chi, perm0, eta, fermion)
+    rho_fock, nn = port.fock_correlators(amps, n, fermion)
+    if case in ("haldane12", "haldane12_identity"):
+        # real projection coefficients (zero flux, real characters): the
+        # reference's matrix is the exact <a_i^dagger a_j>
+        np.testing.assert_allclose(rho_fock, f["odlro"], atol=1e-11, rtol=0)
+    a = np.array([fa(i + 1) for i in range(n)])
+    dens = np.diag(nn)
+    da = np.where(a, dens, 0.0)
+    C = np.where(a[:, None], nn, 0.0) - np.outer(da, dens)
+    np.testing.assert_allclose(da, f["density_a"], atol=1e-11, rtol=0)
+    np.testing.assert_allclose(dens, f["density_b"], atol=1e-11, rtol=0)
+    np.testing.assert_allclose(C, f["C"], atol=1e-11, rtol=0)
+
+
+def test_uniform_grid_and_positions():
+    """The momentum mesh q = sum_d (n_d / L_d) b_d and the site positions of
+    the lattice restatement: a_d . b_e = 2 pi delta_de, L_1 L_2 points, and
+    exp(i q . R) = 1 for q on the mesh and R a torus period."""
+    from realspace_exatdiagonalization_py_b200 import lattice as tb
+    from realspace_exatdiagonalization_py_b200 import models
+
+    m = models.build_zero_flux_bosonic_fci_second_quantized_model(sample_size=[2, 3], params=models.params_DNSheng)
+    lat = m.lattice
+    grid = tb.initialize_uniform_grids_from_lattice(lat)
+    assert grid.nsite == 6 and len(grid.site_cart_list) == 6
+    a = np.array(lat.brav_vec_list)
+    for q in grid.site_cart_list:
+        for d, L in enumerate(lat.sample_size):
+            assert abs(np.exp(1j * np.dot(q, L * a[d])) - 1) < 1e-12
+    pos = np.array(lat.site_cart_list)
+    cell, sub = lat.site_list[5]
+    want = sum((cell[d] + lat.sub_crys_list[sub - 1][d]) * a[d] for d in range(2))
+    np.testing.assert_allclose(pos[5], want, atol=1e-15)
