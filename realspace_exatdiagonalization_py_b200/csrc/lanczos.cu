@@ -36,9 +36,11 @@ constexpr int kKeepMax = 16;    // largest thick-restart basis (columns)
 constexpr int kJacobiMax = 64;  // largest projected matrix
 constexpr int kRRMax = kKeepMax + kBMax;  // Rayleigh-Ritz basis (restart basis + residual block)
 constexpr int kStateInts = 16;
-// dynamic shared memory of k_lz_ritz: padded A (M x (M+1)), S (M x 16 complex), Z (M x 16 real)
+// dynamic shared memory of k_lz_ritz: padded A (M x (M+1)), S (M x 16 complex), Z (M x 16 real),
+// then the eigensolver's work area for the inverse iteration
 constexpr size_t kRitzSmem = sizeof(double2) * (kJacobiMax * (kJacobiMax + 1) + kJacobiMax * kKeepMax) +
-                             sizeof(double) * kJacobiMax * kKeepMax;
+                             sizeof(double) * kJacobiMax * kKeepMax + sizeof(double) * 5 * kJacobiMax * kKeepMax +
+                             kJacobiMax * kKeepMax;
 // state fields
 constexpr int S_NB = 0, S_STATUS = 1, S_RESTARTS = 2, S_ITERS = 3, S_ACTIVE = 4, S_RESTART_NB = 5,
               S_NEWSLOT = 6, S_NCONV = 7, S_TICKET = 8, S_RR = 9;
@@ -496,57 +498,78 @@ __device__ int sturm_count(const double* dd, const double* ee, int M, double x, 
   return c;
 }
 
+// Householder reflector of column c (rows c+1..M-1) by one warp: v (v[c+1] =
+// 1) into A's column c and into vb, tau[c], the off-diagonal ee[c].
+__device__ __forceinline__ void herm_reflector(double2* A, int lda, int M, int c, double2* vb, double2* tau,
+                                               double* ee, int lane) {
+  double sq = 0.0;
+  for (int i = c + 2 + lane; i < M; i += 32) {
+    const double2 v = A[i * lda + c];
+    sq += v.x * v.x + v.y * v.y;
+  }
+  sq = warp_sum(sq);
+  const double2 al = A[(c + 1) * lda + c];
+  double2 t = make_double2(0.0, 0.0), scl = make_double2(0.0, 0.0);
+  double beta = al.x;
+  if (sq != 0.0 || al.y != 0.0) {
+    beta = -copysign(sqrt(al.x * al.x + al.y * al.y + sq), al.x);
+    const double ib = 1.0 / beta;
+    t = make_double2((beta - al.x) * ib, -al.y * ib);
+    const double2 den = make_double2(al.x - beta, al.y);
+    const double idn = 1.0 / (den.x * den.x + den.y * den.y);
+    scl = make_double2(den.x * idn, -den.y * idn);
+  }
+  for (int i = c + 2 + lane; i < M; i += 32) {
+    const double2 v = cmul(A[i * lda + c], scl);
+    A[i * lda + c] = v;
+    vb[i] = v;
+  }
+  if (lane == 0) {
+    vb[c + 1] = make_double2(1.0, 0.0);
+    A[(c + 1) * lda + c] = make_double2(1.0, 0.0);
+    tau[c] = t;
+    ee[c] = beta;
+  }
+  __syncwarp();
+}
+
+// iwork: optional shared-memory work area of kHermWork bytes for the inverse
+// iteration (NULL: thread-local arrays).
+constexpr size_t kHermWork = sizeof(double) * 5 * kJacobiMax * kKeepMax + kJacobiMax * kKeepMax;
 __device__ void herm_lowest(double2* A, int M, int Kp, double* theta, double2* S, double* Z, double2* tau,
-                            double* dd, double* ee, double* red, double2* vv, double2* pw) {
+                            double* dd, double* ee, double* red, double2* vv, double2* pw, double* iwork) {
   // A is M x M with row stride lda = M + 1 (odd, so column walks hit distinct banks)
   const int lda = M + 1;
   const int tid = threadIdx.x, nt = blockDim.x;
   const int lane = tid & 31, warp = tid >> 5, nwarp = nt >> 5;
-  // ---- 1. tridiagonalisation: three barriers per column ----
+  // ---- 1. tridiagonalisation: two barriers per column ----
+  // Warp 0 updates column k+1 itself during step k's rank-2 update and forms
+  // the next reflector at once (look-ahead), while the other warps update the
+  // rest of the trailing matrix; the reflector vectors alternate between two
+  // buffers (vv and the still unused S), so the next one never overwrites the
+  // one being applied.  p^H v is formed redundantly by every warp.
+  double2* vbuf[2] = {vv, S};
+  if (M >= 2 && warp == 0) herm_reflector(A, lda, M, 0, vbuf[0], tau, ee, lane);
+  __syncthreads();
   for (int k = 0; k < M - 1; ++k) {
-    // phase A (warp 0): reflector of column k, scaled v into vv and back into A
-    if (warp == 0) {
-      double sq = 0.0;
-      for (int i = k + 2 + lane; i < M; i += 32) {
-        const double2 v = A[i * lda + k];
-        sq += v.x * v.x + v.y * v.y;
-      }
-      sq = warp_sum(sq);
-      const double2 al = A[(k + 1) * lda + k];
-      double2 t = make_double2(0.0, 0.0), scl = make_double2(0.0, 0.0);
-      double beta = al.x;
-      if (sq != 0.0 || al.y != 0.0) {
-        beta = -copysign(sqrt(al.x * al.x + al.y * al.y + sq), al.x);
-        t = make_double2((beta - al.x) / beta, -al.y / beta);
-        const double2 den = make_double2(al.x - beta, al.y);
-        const double dn = den.x * den.x + den.y * den.y;
-        scl = make_double2(den.x / dn, -den.y / dn);
-      }
-      for (int i = k + 2 + lane; i < M; i += 32) {
-        const double2 v = cmul(A[i * lda + k], scl);
-        A[i * lda + k] = v;
-        vv[i] = v;
-      }
-      if (lane == 0) {
-        vv[k + 1] = make_double2(1.0, 0.0);
-        A[(k + 1) * lda + k] = make_double2(1.0, 0.0);
-        tau[k] = t;
-        ee[k] = beta;
-      }
-    }
-    __syncthreads();
+    const double2* v = vbuf[k & 1];
     const double2 t = tau[k];
-    if (t.x == 0.0 && t.y == 0.0) continue;
-    // phase B: p = tau * A22 v, four lanes per row (odd stride: no bank conflicts)
+    const bool next = k + 1 < M - 1;
+    if (t.x == 0.0 && t.y == 0.0) {  // H_k = I: nothing to update
+      if (next && warp == 0) herm_reflector(A, lda, M, k + 1, vbuf[(k + 1) & 1], tau, ee, lane);
+      __syncthreads();
+      continue;
+    }
+    // p = tau * A22 v, four lanes per row
     {
       const int i = k + 1 + (tid >> 2), sub = tid & 3;
       double sx = 0.0, sy = 0.0;
       if (i < M) {
         const double2* Ar = A + i * lda;
         for (int j = k + 1 + sub; j < M; j += 4) {
-          const double2 a = Ar[j], v = vv[j];
-          sx += a.x * v.x - a.y * v.y;
-          sy += a.x * v.y + a.y * v.x;
+          const double2 a = Ar[j], vj = v[j];
+          sx += a.x * vj.x - a.y * vj.y;
+          sy += a.x * vj.y + a.y * vj.x;
         }
       }
       sx += __shfl_xor_sync(0xffffffffu, sx, 1);
@@ -556,35 +579,46 @@ __device__ void herm_lowest(double2* A, int M, int Kp, double* theta, double2* S
       if (i < M && sub == 0) pw[i] = cmul(t, make_double2(sx, sy));
     }
     __syncthreads();
-    // p^H v (warp 0) into red[0..1]
-    if (warp == 0) {
+    // p^H v in every warp; alpha = -1/2 tau (p^H v); w = p + alpha v
+    double2 alpha;
+    {
       double sx = 0.0, sy = 0.0;
       for (int i = k + 1 + lane; i < M; i += 32) {
-        const double2 c = cdotc(pw[i], vv[i]);
+        const double2 c = cdotc(pw[i], v[i]);
         sx += c.x;
         sy += c.y;
       }
-      sx = warp_sum(sx);
-      sy = warp_sum(sy);
-      if (lane == 0) {
-        red[0] = sx;
-        red[1] = sy;
-      }
+      const double2 ta = cmul(t, make_double2(warp_sum(sx), warp_sum(sy)));
+      alpha = make_double2(-0.5 * ta.x, -0.5 * ta.y);
     }
-    __syncthreads();
-    // phase C: alpha = -1/2 tau (p^H v); A22 -= v w^H + w v^H with w = p + alpha v
-    const double2 pv = make_double2(red[0], red[1]);
-    const double2 ta = cmul(t, pv);
-    const double2 alpha = make_double2(-0.5 * ta.x, -0.5 * ta.y);
-    for (int i = k + 1 + warp; i < M; i += nwarp) {
-      const double2 vi = vv[i];
-      const double2 wi = cadd(pw[i], cmul(alpha, vi));
-      for (int j = k + 1 + lane; j < M; j += 32) {
-        const double2 vj = vv[j];
-        const double2 wj = cadd(pw[j], cmul(alpha, vj));
-        const double2 u = cadd(make_double2(vi.x * wj.x + vi.y * wj.y, vi.y * wj.x - vi.x * wj.y),
-                               make_double2(wi.x * vj.x + wi.y * vj.y, wi.y * vj.x - wi.x * vj.y));
-        A[i * lda + j] = csub(A[i * lda + j], u);
+    // A22 -= v w^H + w v^H: column k+1 by warp 0 (then the next reflector),
+    // columns k+2.. of every row by the other warps (all warps if there is one)
+    const int c1 = k + 1;
+    const double2 v1 = v[c1];
+    const double2 w1 = cadd(pw[c1], cmul(alpha, v1));
+    if (warp == 0) {
+      for (int i = c1 + lane; i < M; i += 32) {
+        const double2 vi = v[i];
+        const double2 wi = cadd(pw[i], cmul(alpha, vi));
+        const double2 u = cadd(make_double2(vi.x * w1.x + vi.y * w1.y, vi.y * w1.x - vi.x * w1.y),
+                               make_double2(wi.x * v1.x + wi.y * v1.y, wi.y * v1.x - wi.x * v1.y));
+        A[i * lda + c1] = csub(A[i * lda + c1], u);
+      }
+      __syncwarp();
+      if (next) herm_reflector(A, lda, M, c1, vbuf[c1 & 1], tau, ee, lane);
+    }
+    const int w0 = nwarp > 1 ? 1 : 0, nw = nwarp > 1 ? nwarp - 1 : 1;
+    if (warp >= w0) {
+      for (int i = c1 + (warp - w0); i < M; i += nw) {
+        const double2 vi = v[i];
+        const double2 wi = cadd(pw[i], cmul(alpha, vi));
+        for (int j = c1 + 1 + lane; j < M; j += 32) {
+          const double2 vj = v[j];
+          const double2 wj = cadd(pw[j], cmul(alpha, vj));
+          const double2 u = cadd(make_double2(vi.x * wj.x + vi.y * wj.y, vi.y * wj.x - vi.x * wj.y),
+                                 make_double2(wi.x * vj.x + wi.y * vj.y, wi.y * vj.x - wi.x * vj.y));
+          A[i * lda + j] = csub(A[i * lda + j], u);
+        }
       }
     }
     __syncthreads();
@@ -606,8 +640,10 @@ __device__ void herm_lowest(double2* A, int M, int Kp, double* theta, double2* S
     const int j = tid >> 4, sub = tid & 15;  // eigenvalue j, sample point sub
     double a = lo - 1e-12 * tnorm - 1e-300, bnd = hi + 1e-12 * tnorm + 1e-300;
     // 16 rounds shrink the Gershgorin interval by 16^16 ~ 1.8e19: below one ulp.
-    // No early exit, so every lane of the warp stays in the ballot.
+    // A warp stops early once both its brackets are down to rounding level
+    // (decided by __all_sync, so every lane of the warp stays in the ballot).
     for (int round = 0; round < 16; ++round) {
+      if (__all_sync(0xffffffffu, bnd - a <= 4e-16 * fmax(fabs(a), fabs(bnd)) + pivmin)) break;
       const double w = (bnd - a) * (1.0 / 16.0);
       const double x = a + w * (sub + 1);
       const int c = (j < Kp && sub < 15) ? sturm_count(dd, ee, M, x, pivmin) : 1 << 30;
@@ -629,73 +665,102 @@ __device__ void herm_lowest(double2* A, int M, int Kp, double* theta, double2* S
     const double sep = 1e-14 * fmax(tnorm, 1e-300);
     for (int i = 0; i < j; ++i)  // separate shifts of (nearly) equal eigenvalues
       if (fabs(lam - theta[i]) < sep) lam = theta[i] + sep * (j - i + 1);
-    double dl[kJacobiMax], dg[kJacobiMax], du[kJacobiMax], du2[kJacobiMax], z[kJacobiMax];
-    unsigned char piv[kJacobiMax];
+    // the vector's work arrays: in the shared work area, element i of vector
+    // j at i * Kp + j (the Kp threads touch consecutive words), else local
+    double ldl[kJacobiMax], ldg[kJacobiMax], ldu[kJacobiMax], ldu2[kJacobiMax], lz[kJacobiMax];
+    unsigned char lpiv[kJacobiMax];
+    const int sw = iwork ? Kp : 1;
+    const int mk = kJacobiMax * kKeepMax;
+    double* dlp = iwork ? iwork + j : ldl;
+    double* dgp = iwork ? iwork + mk + j : ldg;
+    double* dup = iwork ? iwork + 2 * mk + j : ldu;
+    double* du2p = iwork ? iwork + 3 * mk + j : ldu2;
+    double* zp = iwork ? iwork + 4 * mk + j : lz;
+    unsigned char* pivp = iwork ? reinterpret_cast<unsigned char*>(iwork + 5 * mk) + j : lpiv;
+#define dl(i) dlp[(i) * sw]
+#define dg(i) dgp[(i) * sw]
+#define du(i) dup[(i) * sw]
+#define du2(i) du2p[(i) * sw]
+#define z(i) zp[(i) * sw]
+#define piv(i) pivp[(i) * sw]
     for (int i = 0; i < M; ++i) {
-      dg[i] = dd[i] - lam;
-      dl[i] = (i < M - 1) ? ee[i] : 0.0;
-      du[i] = (i < M - 1) ? ee[i] : 0.0;
-      du2[i] = 0.0;
+      dg(i) = dd[i] - lam;
+      dl(i) = (i < M - 1) ? ee[i] : 0.0;
+      du(i) = (i < M - 1) ? ee[i] : 0.0;
+      du2(i) = 0.0;
     }
     const double tiny = 1e-15 * fmax(tnorm, 1e-300);
     for (int i = 0; i < M - 1; ++i) {
-      if (fabs(dg[i]) >= fabs(dl[i])) {
-        piv[i] = 0;
-        if (dg[i] == 0.0) dg[i] = tiny;
-        const double f = dl[i] / dg[i];
-        dl[i] = f;
-        dg[i + 1] -= f * du[i];
+      if (fabs(dg(i)) >= fabs(dl(i))) {
+        piv(i) = 0;
+        if (dg(i) == 0.0) dg(i) = tiny;
+        const double f = dl(i) / dg(i);
+        dl(i) = f;
+        dg(i + 1) -= f * du(i);
       } else {
-        piv[i] = 1;
-        const double f = dg[i] / dl[i];
-        dg[i] = dl[i];
-        dl[i] = f;
-        const double tmp = du[i];
-        du[i] = dg[i + 1];
-        dg[i + 1] = tmp - f * dg[i + 1];
+        piv(i) = 1;
+        const double f = dg(i) / dl(i);
+        dg(i) = dl(i);
+        dl(i) = f;
+        const double tmp = du(i);
+        du(i) = dg(i + 1);
+        dg(i + 1) = tmp - f * dg(i + 1);
         if (i < M - 2) {
-          du2[i] = du[i + 1];
-          du[i + 1] = -f * du[i + 1];
+          du2(i) = du(i + 1);
+          du(i + 1) = -f * du(i + 1);
         }
       }
     }
-    if (dg[M - 1] == 0.0) dg[M - 1] = tiny;
-    for (int i = 0; i < M; ++i) dg[i] = 1.0 / dg[i];  // reciprocal pivots: the solves multiply
+    if (dg(M - 1) == 0.0) dg(M - 1) = tiny;
+    for (int i = 0; i < M; ++i) dg(i) = 1.0 / dg(i);  // reciprocal pivots: the solves multiply
     unsigned h = 2166136261u ^ (unsigned)(j * 16777619u);
     for (int i = 0; i < M; ++i) {
       h = h * 1664525u + 1013904223u;
-      z[i] = ((h >> 8) * (1.0 / 16777216.0)) - 0.5;
+      z(i) = ((h >> 8) * (1.0 / 16777216.0)) - 0.5;
     }
     for (int rep = 0; rep < 3; ++rep) {
       for (int i = 0; i < M - 1; ++i) {
-        if (piv[i] == 0) {
-          z[i + 1] -= dl[i] * z[i];
+        if (piv(i) == 0) {
+          z(i + 1) -= dl(i) * z(i);
         } else {
-          const double tmp = z[i];
-          z[i] = z[i + 1];
-          z[i + 1] = tmp - dl[i] * z[i];
+          const double tmp = z(i);
+          z(i) = z(i + 1);
+          z(i + 1) = tmp - dl(i) * z(i);
         }
       }
-      z[M - 1] *= dg[M - 1];
-      if (M > 1) z[M - 2] = (z[M - 2] - du[M - 2] * z[M - 1]) * dg[M - 2];
-      for (int i = M - 3; i >= 0; --i) z[i] = (z[i] - du[i] * z[i + 1] - du2[i] * z[i + 2]) * dg[i];
+      z(M - 1) *= dg(M - 1);
+      if (M > 1) z(M - 2) = (z(M - 2) - du(M - 2) * z(M - 1)) * dg(M - 2);
+      for (int i = M - 3; i >= 0; --i) z(i) = (z(i) - du(i) * z(i + 1) - du2(i) * z(i + 2)) * dg(i);
       double nrm = 0.0;
-      for (int i = 0; i < M; ++i) nrm = fmax(nrm, fabs(z[i]));
+      for (int i = 0; i < M; ++i) nrm = fmax(nrm, fabs(z(i)));
       const double inv = nrm > 0.0 ? 1.0 / nrm : 1.0;
-      for (int i = 0; i < M; ++i) z[i] *= inv;
+      for (int i = 0; i < M; ++i) z(i) *= inv;
     }
     double n2 = 0.0;
-    for (int i = 0; i < M; ++i) n2 += z[i] * z[i];
+    for (int i = 0; i < M; ++i) n2 += z(i) * z(i);
     const double inv = 1.0 / sqrt(n2);
-    for (int i = 0; i < M; ++i) Z[i * Kp + j] = z[i] * inv;
+    for (int i = 0; i < M; ++i) Z[i * Kp + j] = z(i) * inv;
+#undef dl
+#undef dg
+#undef du
+#undef du2
+#undef z
+#undef piv
   }
   __syncthreads();
-  // Gram-Schmidt in ascending order (orthonormal bases of degenerate
-  // clusters): for vector j, all dots with 0..j-1 at once (one warp each),
-  // one update by all threads, twice; then the normalisation
+  // Gram-Schmidt inside clusters only (as LAPACK's inverse iteration does):
+  // eigenvalues closer than 1e-3 |T| to their neighbour form a cluster, and
+  // a vector is orthogonalised, twice, against the earlier vectors of its
+  // cluster, then normalised.  Vectors of separated eigenvalues are already
+  // orthogonal to ~eps |T| / gap.  Every thread derives the same clusters
+  // from theta, so the barriers below are uniform.
+  const double ortol = 1e-3 * fmax(tnorm, 1e-300);
+  int cs = 0;  // first vector of the current cluster
   for (int j = 0; j < Kp; ++j) {
-    for (int pass = 0; pass < 2 && j > 0; ++pass) {
-      for (int i = warp; i < j; i += nwarp) {
+    if (j > 0 && theta[j] - theta[j - 1] > ortol) cs = j;
+    if (cs == j) continue;
+    for (int pass = 0; pass < 2; ++pass) {
+      for (int i = cs + warp; i < j; i += nwarp) {
         double dt = 0.0;
         for (int r = lane; r < M; r += 32) dt += Z[r * Kp + i] * Z[r * Kp + j];
         dt = warp_sum(dt);
@@ -703,9 +768,9 @@ __device__ void herm_lowest(double2* A, int M, int Kp, double* theta, double2* S
       }
       __syncthreads();
       for (int r = tid; r < M; r += nt) {
-        double v = Z[r * Kp + j];
-        for (int i = 0; i < j; ++i) v -= red[i] * Z[r * Kp + i];
-        Z[r * Kp + j] = v;
+        double vz = Z[r * Kp + j];
+        for (int i = cs; i < j; ++i) vz -= red[i] * Z[r * Kp + i];
+        Z[r * Kp + j] = vz;
       }
       __syncthreads();
     }
@@ -720,32 +785,66 @@ __device__ void herm_lowest(double2* A, int M, int Kp, double* theta, double2* S
     for (int r = tid; r < M; r += nt) Z[r * Kp + j] *= inv;
     __syncthreads();
   }
-  // ---- 4. back-transformation: s = H_0 (H_1 (... H_{M-2} z)), all vectors at once ----
+  // ---- 4. back-transformation: S = H_0 H_1 ... H_{M-2} Z ----
+  // Reflectors in blocks of nbw, the last block first.  A block's product is
+  // H_k0 ... H_k1-1 = I - V T V^H with T^-1 = diag(1/tau) + strict_upper(V^H V)
+  // (the "UT transform" of compact WY), so S <- S - V T (V^H S) needs only the
+  // block's Gram matrix G = V^H V: Y = V^H S, then T Y by back-substitution,
+  // Y'_c = tau_c (Y_c - sum_{b > c} G_cb Y'_b) (tau_c = 0 gives 0, as it must),
+  // then S -= V Y'.  G and Y live in Z's space (kJacobiMax x kKeepMax doubles
+  // in every caller), free once S holds Z; nbw is the largest block (<= 16)
+  // that fits there.
   for (int i = tid; i < M * Kp; i += nt) S[i] = make_double2(Z[i], 0.0);
   __syncthreads();
-  for (int k = M - 2; k >= 0; --k) {
-    const double2 t = tau[k];
-    if (t.x == 0.0 && t.y == 0.0) continue;
-    {  // f_j = tau (v^H s_j), 16 lanes per vector
-      const int j = tid >> 4, sub = tid & 15;
-      double sx = 0.0, sy = 0.0;
-      if (j < Kp) {
-        for (int r = k + 1 + sub; r < M; r += 16) {
-          const double2 c = cdotc(A[r * lda + k], S[r * Kp + j]);
-          sx += c.x;
-          sy += c.y;
-        }
+  int nbw = 16;
+  while (nbw > 1 && 2 * nbw * (nbw + Kp) > kJacobiMax * kKeepMax) --nbw;
+  double2* Gv = reinterpret_cast<double2*>(Z);  // nbw x nbw, strict upper part
+  double2* Yv = Gv + nbw * nbw;                 // nbw x Kp
+  for (int k1 = M - 1; k1 > 0; k1 -= nbw) {     // reflectors k0 .. k1-1
+    const int k0 = max(0, k1 - nbw);
+    const int nb = k1 - k0;
+    // v_c (reflector k = k0 + c) at row r: 0 for r <= k, 1 at r = k + 1, A[r][k] below.
+    // One thread per output entry, a serial dot over the rows: G[a][c] =
+    // v_a^H v_c (a < c) for the first nb*nb entries, Y[c][j] = v_c^H s_j after
+    for (int e = tid; e < nb * nb + nb * Kp; e += nt) {
+      double2 acc = make_double2(0.0, 0.0);
+      if (e < nb * nb) {
+        const int ga = e / nb, gc = e % nb;
+        if (ga >= gc) continue;
+        const int ka = k0 + ga, kc = k0 + gc;
+        acc = cconj(A[(kc + 1) * lda + ka]);  // v_c's unit entry; v_a there and below is A[r][ka]
+        for (int r = kc + 2; r < M; ++r) acc = cadd(acc, cdotc(A[r * lda + ka], A[r * lda + kc]));
+        Gv[ga * nbw + gc] = acc;
+      } else {
+        const int f = e - nb * nb;
+        const int c = f / Kp, j = f % Kp;
+        const int k = k0 + c;
+        acc = S[(k + 1) * Kp + j];
+        for (int r = k + 2; r < M; ++r) acc = cadd(acc, cdotc(A[r * lda + k], S[r * Kp + j]));
+        Yv[f] = acc;
       }
-      for (int o = 1; o < 16; o <<= 1) {
-        sx += __shfl_xor_sync(0xffffffffu, sx, o);
-        sy += __shfl_xor_sync(0xffffffffu, sy, o);
-      }
-      if (j < Kp && sub == 0) pw[j] = cmul(t, make_double2(sx, sy));
     }
     __syncthreads();
-    for (int i = tid; i < (M - k - 1) * Kp; i += nt) {
-      const int r = k + 1 + i / Kp, j = i % Kp;
-      S[r * Kp + j] = csub(S[r * Kp + j], cmul(A[r * lda + k], pw[j]));
+    // Y <- T Y by back-substitution, one thread per column j (rows descending)
+    for (int j = tid; j < Kp; j += nt) {
+      for (int c = nb - 1; c >= 0; --c) {
+        double2 acc = Yv[c * Kp + j];
+        for (int bb = c + 1; bb < nb; ++bb) acc = csub(acc, cmul(Gv[c * nbw + bb], Yv[bb * Kp + j]));
+        Yv[c * Kp + j] = cmul(tau[k0 + c], acc);
+      }
+    }
+    __syncthreads();
+    // S -= V Y on rows k0+1 .. M-1
+    for (int e = tid; e < (M - k0 - 1) * Kp; e += nt) {
+      const int r = k0 + 1 + e / Kp, j = e % Kp;
+      double2 acc = make_double2(0.0, 0.0);
+      for (int c = 0; c < nb; ++c) {
+        const int k = k0 + c;
+        if (r <= k) break;
+        const double2 vr = (r == k + 1) ? make_double2(1.0, 0.0) : A[r * lda + k];
+        acc = cadd(acc, cmul(vr, Yv[c * Kp + j]));
+      }
+      S[r * Kp + j] = csub(S[r * Kp + j], acc);
     }
     __syncthreads();
   }
@@ -794,7 +893,8 @@ __global__ void __launch_bounds__(kRitzThreads) k_lz_ritz(rsed_lanczos_t st, LzD
     A[r * (M + 1) + c] = make_double2(0.5 * (a.x + bt.x), 0.5 * (a.y - bt.y));
   }
   __syncthreads();
-  herm_lowest(A, M, Kp, theta, Sv, Z, tau, dd, ee, red, vv, pw);
+  herm_lowest(A, M, Kp, theta, Sv, Z, tau, dd, ee, red, vv, pw,
+              reinterpret_cast<double*>(Z + kJacobiMax * kKeepMax));
   double* rv = st.ritz_val + (int64_t)inst * d.pm;
   double2* rvec = reinterpret_cast<double2*>(st.ritz_vec) + (int64_t)inst * d.pm * d.pm;
   double* res = st.resid + (int64_t)inst * d.pm;
@@ -1404,7 +1504,7 @@ k_lz_persist(rsed_model_t md, rsed_sectors_t sc, rsed_lanczos_t st, LzDims d, rs
               A[r * (M + 1) + c] = make_double2(0.5 * (a.x + bt.x), 0.5 * (a.y - bt.y));
             }
             __syncthreads();
-            herm_lowest(A, M, Kp, theta, Sv, Zs, tau, dd, ee, red, vv, pw);
+            herm_lowest(A, M, Kp, theta, Sv, Zs, tau, dd, ee, red, vv, pw, nullptr);
             double* rv = st.ritz_val + (int64_t)inst * d.pm;
             double2* rvec = reinterpret_cast<double2*>(st.ritz_vec) + (int64_t)inst * d.pm * d.pm;
             double* res = st.resid + (int64_t)inst * d.pm;
