@@ -503,6 +503,70 @@ def overlap_row(ed, C, n_m, grid, peak_gbs, reps=5):
             "frac_of_measured_hbm": algo / t / 1e9 / peak_gbs}
 
 
+def correlators_at_scale(ed, models):
+    """The one-body density matrix and the density pairs of the lowest state
+    of sector (0, 0) of the 32-site Haldane bosons (657,756 orbits, |G| = 16,
+    8 bosons: 16 x 8 x 24 hops per orbit projected back into the sector), timed
+    on the device with CUDA events; and, like for like on the 16-site model
+    (sector (0, 1), lowest state), the device kernel against the CPU oracle's
+    restatement of the reference's orbit-by-orbit loop."""
+    import torch
+
+    from oracle import port
+    from realspace_exatdiagonalization_py_b200 import correlators as cr
+
+    out = {}
+    model, nf = models.config_model("haldane32")
+    G = ed.build_translation_group(model.lattice, [0.0, 0.0])
+    data = ed.build_ed_data(model, filling_fraction=Fraction(nf, model.lattice.n_site), symmetry_group=G)
+    res = ed.solve_sectors_batched(data, [0], nev=1, precision=64)
+    _, sset = data._device()
+    basis = ed.Symmetry_Sector_Basis(data.irrep_list[0], data.orbit_catalog, sset, 0)
+    c = res[0][1][:, 0]
+    cr.one_body_density_matrix(basis, c)  # warm-up (occupancy query, allocator)
+    cr.density_pairs(basis, c)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    torch.cuda.synchronize()
+    ev[0].record()
+    rho = cr.one_body_density_matrix(basis, c)
+    ev[1].record()
+    D = cr.density_pairs(basis, c)
+    ev[2].record()
+    torch.cuda.synchronize()
+    n, k = model.lattice.n_site, nf
+    hops = basis.dim * 16 * k * (n - k)
+    out["haldane32"] = {"sector": [0, 0], "dim": basis.dim, "E0": float(res[0][0][0]),
+                        "obdm_ms": ev[0].elapsed_time(ev[1]), "pairs_ms": ev[1].elapsed_time(ev[2]),
+                        "hops_projected": hops, "trace_rho": float(np.trace(rho).real),
+                        "sum_pairs_diag": float(np.trace(D))}
+    # like for like: 16-site model, device vs oracle
+    m16 = models.build_zero_flux_bosonic_fci_second_quantized_model(sample_size=[2, 4],
+                                                                    params=models.params_DNSheng)
+    G16 = ed.build_translation_group(m16.lattice, [0.0, 0.0])
+    d16 = ed.build_ed_data(m16, filling_fraction=Fraction(4, 16), symmetry_group=G16)
+    s = next(i for i, ir in enumerate(d16.irrep_list) if ir.label == (0, 1))
+    r16 = ed.solve_sectors_batched(d16, [s], nev=1, precision=64)
+    _, ss16 = d16._device()
+    b16 = ed.Symmetry_Sector_Basis(d16.irrep_list[s], d16.orbit_catalog, ss16, s)
+    c16 = r16[s][1][:, 0]
+    cr.one_body_density_matrix(b16, c16)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    rho16 = cr.one_body_density_matrix(b16, c16)
+    t_dev = time.perf_counter() - t0
+    perm0, eta = port.group_arrays(G16)
+    cat = port.catalog(16, 4, perm0, eta, False)
+    chi = np.asarray(d16.irrep_list[s].values, dtype=np.complex128)
+    orbits = port.sector_orbits(cat, chi)
+    t0 = time.perf_counter()
+    rho_o = port.obdm_orbitwise(cat, orbits, np.asarray(c16), chi, perm0, eta, False, 16, 4)
+    t_cpu = time.perf_counter() - t0
+    out["haldane16_like_for_like"] = {"sector": [0, 1], "dim": b16.dim, "device_ms": t_dev * 1e3,
+                                      "oracle_ms": t_cpu * 1e3, "oracle_threads": 1,
+                                      "max_abs_diff": float(np.abs(rho16 - rho_o).max())}
+    return out
+
+
 def model_basis_size(model, nf):
     import math
 
@@ -784,6 +848,7 @@ def main():
     ap.add_argument("--matvec-precision", type=int, default=0, choices=[0, 32, 64])
     ap.add_argument("--matvec-no-otf", action="store_true")
     ap.add_argument("--serving-only", action="store_true", help="only the 32-site served request stream")
+    ap.add_argument("--corr", action="store_true", help="only the correlators of the 32-site Haldane ground state")
     ap.add_argument("--overlap-only", type=int, default=0,
                     help="only the Chern link overlaps of one row of this flux grid (for kernel profiling)")
     ap.add_argument("--chern", type=int, default=0,
@@ -806,6 +871,12 @@ def main():
         torch.cuda.synchronize()
         print(json.dumps({"workload": f"haldane32: {len(secs)} sectors, FP32 + FP64 refinement, b=2, nev 4",
                           "solve_s": time.perf_counter() - t0, "E0": [float(res[s][0][0]) for s in secs]}))
+        return
+    if args.corr:
+        import realspace_exatdiagonalization_py_b200 as ed
+        from realspace_exatdiagonalization_py_b200 import models
+
+        print(json.dumps(correlators_at_scale(ed, models)), flush=True)
         return
     if args.serving_only:
         import realspace_exatdiagonalization_py_b200 as ed
