@@ -325,3 +325,34 @@ def test_uniform_grid_and_positions():
     cell, sub = lat.site_list[5]
     want = sum((cell[d] + lat.sub_crys_list[sub - 1][d]) * a[d] for d in range(2))
     np.testing.assert_allclose(pos[5], want, atol=1e-15)
+
+
+@pytest.mark.parametrize("model,label", [("Heisenberg", "N=18"), ("Haldane_Boson", "2×3"), ("Haldane_Boson", "2×4"),
+                                         ("Haldane_Boson", "2×5"), ("Hubbard_Fermion", "2×2"),
+                                         ("Hubbard_Fermion", "2×3"), ("Hubbard_Fermion", "2×4")])
+def test_oracle_matches_reference_benchmark(model, label):
+    """The oracle's sector-0 dimension and lowest energy against the
+    reference's own benchmark results (tests/golden/make_benchmark_golden.py)
+    on the sizes the CPU restatement finishes in seconds."""
+    import os
+    from fractions import Fraction
+
+    import realspace_exatdiagonalization_py_b200 as ed
+    from realspace_exatdiagonalization_py_b200 import models
+
+    f = dict(np.load(os.path.join(os.path.dirname(__file__), "golden", "reference_benchmark.npz")))
+    i = next(k for k in range(len(f["model"])) if str(f["model"][k]) == model and str(f["label"][k]) == label)
+    n_site, n_filled = int(f["n_site"][i]), int(f["n_filled"][i])
+    if model == "Heisenberg":
+        m = models.build_heisenberg_second_quantized_model(n_site, 1.0)
+    elif model == "Haldane_Boson":
+        m = models.build_zero_flux_bosonic_fci_second_quantized_model(
+            sample_size=[int(x) for x in label.split("×")], params=models.params_DNSheng)
+    else:
+        m = models.build_spinful_hubbard_second_quantized_model([int(x) for x in label.split("×")], 1.0, 8.0)
+    G = ed.build_translation_group(m.lattice)
+    irreps = ed.build_irrep_list(G, m.lattice)
+    out = port.scan(m, n_filled, G, irreps, 1, sectors=[0])
+    vals, dim = out[0]
+    assert dim == int(f["sector_dim"][i])
+    assert abs(float(vals[0]) - float(f["energy"][i])) < 1e-9
