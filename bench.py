@@ -857,6 +857,11 @@ def run_b200(args):
                 extra["serving_at_scale"] = serving_at_scale(ed, models)
             except Exception as exc:  # noqa: BLE001 - reported, not fatal
                 extra["serving_at_scale"] = {"error": repr(exc)}
+            torch.cuda.empty_cache()
+            try:
+                extra["reference_benchmark"] = reference_benchmark(ed, models)
+            except Exception as exc:  # noqa: BLE001 - reported, not fatal
+                extra["reference_benchmark"] = {"error": repr(exc)}
         # CPU baseline: the oracle (reference algorithm) on the host cores, N = 1 only
         cpu_base = None
         if ws == 1:
