@@ -36,11 +36,13 @@ constexpr int kKeepMax = 16;    // largest thick-restart basis (columns)
 constexpr int kJacobiMax = 64;  // largest projected matrix
 constexpr int kRRMax = kKeepMax + kBMax;  // Rayleigh-Ritz basis (restart basis + residual block)
 constexpr int kStateInts = 16;
+// the eigensolver's shared work area for the inverse iteration: five double
+// arrays and the pivot flags of kKeepMax vectors of up to kJacobiMax entries
+constexpr size_t kHermWork = sizeof(double) * 5 * kJacobiMax * kKeepMax + kJacobiMax * kKeepMax;
 // dynamic shared memory of k_lz_ritz: padded A (M x (M+1)), S (M x 16 complex), Z (M x 16 real),
-// then the eigensolver's work area for the inverse iteration
+// then the eigensolver's work area
 constexpr size_t kRitzSmem = sizeof(double2) * (kJacobiMax * (kJacobiMax + 1) + kJacobiMax * kKeepMax) +
-                             sizeof(double) * kJacobiMax * kKeepMax + sizeof(double) * 5 * kJacobiMax * kKeepMax +
-                             kJacobiMax * kKeepMax;
+                             sizeof(double) * kJacobiMax * kKeepMax + kHermWork;
 // state fields
 constexpr int S_NB = 0, S_STATUS = 1, S_RESTARTS = 2, S_ITERS = 3, S_ACTIVE = 4, S_RESTART_NB = 5,
               S_NEWSLOT = 6, S_NCONV = 7, S_TICKET = 8, S_RR = 9;
@@ -535,7 +537,6 @@ __device__ __forceinline__ void herm_reflector(double2* A, int lda, int M, int c
 
 // iwork: optional shared-memory work area of kHermWork bytes for the inverse
 // iteration (NULL: thread-local arrays).
-constexpr size_t kHermWork = sizeof(double) * 5 * kJacobiMax * kKeepMax + kJacobiMax * kKeepMax;
 __device__ void herm_lowest(double2* A, int M, int Kp, double* theta, double2* S, double* Z, double2* tau,
                             double* dd, double* ee, double* red, double2* vv, double2* pw, double* iwork) {
   // A is M x M with row stride lda = M + 1 (odd, so column walks hit distinct banks)
