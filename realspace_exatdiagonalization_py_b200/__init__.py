@@ -11,8 +11,10 @@ beside the plain API.
 
 from .autotune import Autotuner, candidate_configs, default_tuner
 from .batched import BatchedSectorSolver, SolverConfig
-from .correlators import (compute_odlro_map, compute_structure_factor_map, off_diagonal_long_range_order,
-                          static_structure_factor)
+from .correlators import (compute_odlro_map, compute_structure_factor_manifold_average_map,
+                          compute_structure_factor_map, off_diagonal_long_range_order, static_structure_factor,
+                          static_structure_factor_manifold_average, structure_factor_allowed_momenta,
+                          structure_factor_manifold_allowed_momenta)
 from .catalog import Symmetry_Orbit_Catalog, build_symmetry_orbit_catalog, update_orbit_stabilizer_phases
 from .fock import expand_sector_state_to_fock_amplitudes, expand_sector_state_to_fock_dense, fock_overlaps
 from .observables import flux_charge_pump, flux_spectrum_flow, many_body_chern_number, many_body_position_phases

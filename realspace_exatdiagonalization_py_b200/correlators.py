@@ -14,6 +14,11 @@ sector's orbits run on the GPU:
   the group sum that turns it into <n_i n_j> and the densities is a |G| x N^2
   scatter on the host, followed by the flavour filters and the Fourier sums.
 
+Manifold averages (an incoherent mixture of (sector, level) states) combine
+the per-state correlation matrices with normalised weights before the
+connected part is taken; the allowed-momenta variants fold the mesh into the
+first Brillouin zone (the nearest of the 25 shifts by n_1 b_1 + n_2 b_2).
+
 The momentum mesh of ``static_structure_factor`` comes from
 ``lattice.initialize_uniform_grids_from_lattice`` (the q = sum_d (n_d/L_d) b_d
 grid of the ``tightbinding_py`` dependency, which the reference imports).
@@ -31,7 +36,9 @@ import torch
 from . import _lib
 
 __all__ = ["off_diagonal_long_range_order", "compute_odlro_map", "static_structure_factor",
-           "compute_structure_factor_map"]
+           "compute_structure_factor_map", "static_structure_factor_manifold_average",
+           "compute_structure_factor_manifold_average_map", "structure_factor_allowed_momenta",
+           "structure_factor_manifold_allowed_momenta"]
 
 
 def _bootstrap_ed_sector(model, sector_label, filling_fraction, target_eigval_idx: int, ed_mode: str, ed_data):
@@ -226,3 +233,180 @@ def compute_structure_factor_map(model, sector_label, *, target_eigval_idx: int 
     flat = np.zeros(len(q))
     _fourier_transform(flat, phases, C, lattice.n_site)
     return kx, ky, flat.reshape(k_resolution, k_resolution, order="F")
+
+
+# ---- manifold averages and the first Brillouin zone ----------------------------
+
+
+def _manifold_state_components(state):
+    """``(sector, level)`` of a manifold state given as an object with
+    ``sector``/``level``, a dict, or a pair (``static_structure_factor.py:530-550``)."""
+    if hasattr(state, "sector") and hasattr(state, "level"):
+        return tuple(int(x) for x in state.sector), int(state.level)
+    if isinstance(state, dict) and "sector" in state and "level" in state:
+        return tuple(int(x) for x in state["sector"]), int(state["level"])
+    if isinstance(state, tuple) and len(state) == 2:
+        return tuple(int(x) for x in state[0]), int(state[1])
+    raise ValueError(f"A manifold state must provide `(sector, level)`; got {state!r}.")
+
+
+def _manifold_connected_density_correlation(model, manifold_states, *, weights=None, filling_fraction,
+                                            flavor_a=None, flavor_b=None, ed_mode: str = "matrix",
+                                            ed_data=None) -> np.ndarray:
+    """Connected <n_i n_j> of rho = sum_a w_a |psi_a><psi_a| (weights
+    normalised to one; uniform by default): the weighted per-state
+    correlations and densities, then the disconnected part of the mixture
+    (``static_structure_factor.py:551-632``)."""
+    if not manifold_states:
+        raise ValueError("The manifold-state list must not be empty.")
+    if weights is None:
+        w = [1.0 / len(manifold_states)] * len(manifold_states)
+    else:
+        if len(weights) != len(manifold_states):
+            raise ValueError(f"Received {len(weights)} weights for {len(manifold_states)} states.")
+        if any(x < 0 for x in weights):
+            raise ValueError("Manifold weights must be nonnegative.")
+        total = sum(weights)
+        if total <= 0:
+            raise ValueError("At least one manifold weight must be positive.")
+        w = [float(x) / total for x in weights]
+    flavor_a = flavor_a or (lambda i: True)
+    flavor_b = flavor_b or (lambda i: True)
+    n = model.lattice.n_site
+    C = np.zeros((n, n))
+    da = np.zeros(n)
+    db = np.zeros(n)
+    for state, wt in zip(manifold_states, w):
+        sector, level = _manifold_state_components(state)
+        _, basis, vec = _bootstrap_ed_sector(model, sector, filling_fraction, level, ed_mode, ed_data)
+        Cs, das, dbs = np.zeros((n, n)), np.zeros(n), np.zeros(n)
+        _build_density_correlation_matrix(Cs, das, dbs, vec, basis, n, flavor_a, flavor_b,
+                                          model.particle_statistics, subtract_disconnected=False)
+        C += wt * Cs
+        da += wt * das
+        db += wt * dbs
+    C -= np.outer(da, db)
+    return C
+
+
+def static_structure_factor_manifold_average(model, manifold_states, *, weights=None, filling_fraction,
+                                             flavor_a=None, flavor_b=None, ed_mode: str = "matrix", ed_data=None):
+    """``(q_points, S_q)`` of the manifold mixture on the lattice's momentum
+    mesh (``static_structure_factor.py:635-683``)."""
+    from .lattice import initialize_uniform_grids_from_lattice
+
+    C = _manifold_connected_density_correlation(model, manifold_states, weights=weights,
+                                                filling_fraction=filling_fraction, flavor_a=flavor_a,
+                                                flavor_b=flavor_b, ed_mode=ed_mode, ed_data=ed_data)
+    kgrid = initialize_uniform_grids_from_lattice(model.lattice)
+    phases = _precompute_phases(kgrid.site_cart_list, model.lattice.site_cart_list)
+    S_q = np.zeros(kgrid.nsite)
+    _fourier_transform(S_q, phases, C, model.lattice.n_site)
+    return list(kgrid.site_cart_list), S_q
+
+
+def compute_structure_factor_manifold_average_map(model, manifold_states, *, weights=None, filling_fraction,
+                                                  flavor_a=None, flavor_b=None, k_resolution: int = 61,
+                                                  ed_mode: str = "matrix", ed_data=None):
+    """``(kx, ky, S_map)`` of the manifold mixture over ``[-1.5 pi, 1.5 pi]^2``
+    (``static_structure_factor.py:853-905``)."""
+    C = _manifold_connected_density_correlation(model, manifold_states, weights=weights,
+                                                filling_fraction=filling_fraction, flavor_a=flavor_a,
+                                                flavor_b=flavor_b, ed_mode=ed_mode, ed_data=ed_data)
+    kx, ky, q = _dense_grid(k_resolution)
+    phases = _precompute_phases(q, model.lattice.site_cart_list)
+    flat = np.zeros(len(q))
+    _fourier_transform(flat, phases, C, model.lattice.n_site)
+    return kx, ky, flat.reshape(k_resolution, k_resolution, order="F")
+
+
+def _reciprocal_basis_vectors(lattice):
+    """``[b1, b2]`` with a_i . b_j = 2 pi delta_ij (2-D lattices)."""
+    if lattice.dim != 2:
+        raise ValueError("BZ boundary plotting is implemented only for 2D lattices.")
+    A = np.array([[lattice.brav_vec_list[0][0], lattice.brav_vec_list[1][0]],
+                  [lattice.brav_vec_list[0][1], lattice.brav_vec_list[1][1]]], dtype=np.float64)
+    B = 2 * np.pi * np.linalg.inv(A).T
+    return [B[:, 0], B[:, 1]]
+
+
+def _clip_polygon_by_halfplane(poly, normal, offset, *, atol: float = 1e-12):
+    """The part of polygon ``poly`` with normal . p <= offset (Sutherland-Hodgman
+    step against one half-plane)."""
+    if not poly:
+        return poly
+    normal = np.asarray(normal, dtype=np.float64)
+    out = []
+    for idx in range(len(poly)):
+        p = np.asarray(poly[idx], dtype=np.float64)
+        q = np.asarray(poly[(idx + 1) % len(poly)], dtype=np.float64)
+        fp, fq = float(np.dot(normal, p) - offset), float(np.dot(normal, q) - offset)
+        if fp <= atol and fq <= atol:
+            out.append(q)
+        elif fp <= atol or fq <= atol:
+            t = fp / (fp - fq)
+            out.append(p + t * (q - p))
+            if fq <= atol:
+                out.append(q)
+    return out
+
+
+def _first_bz_polygon(lattice):
+    """First Brillouin zone: a large square clipped by the bisecting
+    half-planes of the reciprocal vectors n1 b1 + n2 b2 (|n| <= 2), shortest
+    first."""
+    b1, b2 = _reciprocal_basis_vectors(lattice)
+    ext = 2.5 * max(float(np.linalg.norm(b1)), float(np.linalg.norm(b2)))
+    poly = [np.array([-ext, -ext]), np.array([ext, -ext]), np.array([ext, ext]), np.array([-ext, ext])]
+    Gs = [n1 * b1 + n2 * b2 for n1 in range(-2, 3) for n2 in range(-2, 3) if (n1, n2) != (0, 0)]
+    Gs.sort(key=lambda g: float(np.linalg.norm(g)))
+    for G in Gs:
+        poly = _clip_polygon_by_halfplane(poly, G, float(np.dot(G, G)) / 2)
+        if not poly:
+            break
+    return poly
+
+
+def _fold_momentum_to_first_bz(q, lattice):
+    """The shortest of q - n1 b1 - n2 b2, n1, n2 in -2..2 (the first strictly
+    shorter one in that order); q itself for lattices that are not 2-D."""
+    q = np.asarray(q, dtype=np.float64)
+    if lattice.dim != 2:
+        return q.copy()
+    b1, b2 = _reciprocal_basis_vectors(lattice)
+    best, best_n = q.copy(), float(np.dot(q, q))
+    for n1 in range(-2, 3):
+        for n2 in range(-2, 3):
+            f = q - n1 * b1 - n2 * b2
+            fn = float(np.dot(f, f))
+            if fn < best_n:
+                best, best_n = f, fn
+    return best
+
+
+def _fold_momenta_to_first_bz(q_points, lattice):
+    return [_fold_momentum_to_first_bz(np.asarray(q, dtype=np.float64), lattice) for q in q_points]
+
+
+def structure_factor_allowed_momenta(model, sector_label, *, target_eigval_idx: int = 1, filling_fraction,
+                                     flavor_a=None, flavor_b=None, ed_mode: str = "matrix", ed_data=None,
+                                     fold_to_first_bz: bool = True):
+    """``(qx, qy, S_q)`` on the mesh, momenta folded into the first Brillouin
+    zone (``static_structure_factor.py:734-780``)."""
+    q, S = static_structure_factor(model, sector_label, target_eigval_idx=target_eigval_idx,
+                                   filling_fraction=filling_fraction, flavor_a=flavor_a, flavor_b=flavor_b,
+                                   ed_mode=ed_mode, ed_data=ed_data)
+    pts = _fold_momenta_to_first_bz(q, model.lattice) if fold_to_first_bz else q
+    return [p[0] for p in pts], [p[1] for p in pts], S
+
+
+def structure_factor_manifold_allowed_momenta(model, manifold_states, *, weights=None, filling_fraction,
+                                              flavor_a=None, flavor_b=None, ed_mode: str = "matrix", ed_data=None,
+                                              fold_to_first_bz: bool = True):
+    """``(qx, qy, S_q)`` of the manifold mixture, folded as above
+    (``static_structure_factor.py:686-731``)."""
+    q, S = static_structure_factor_manifold_average(model, manifold_states, weights=weights,
+                                                    filling_fraction=filling_fraction, flavor_a=flavor_a,
+                                                    flavor_b=flavor_b, ed_mode=ed_mode, ed_data=ed_data)
+    pts = _fold_momenta_to_first_bz(q, model.lattice) if fold_to_first_bz else q
+    return [p[0] for p in pts], [p[1] for p in pts], S

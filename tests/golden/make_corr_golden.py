@@ -19,6 +19,13 @@ Cases (model, particles, sector, 1-based level, flavour filter a):
 
 Stored per case: the ODLRO matrix, the connected correlation matrix C and the
 densities, S(q) on the mesh and both 5 x 5 maps.
+
+corr_manifold_haldane12.npz: the manifold functions on the 2x3 Haldane bosons
+for the states ((0,0), 1), ((1,0), 1) -- static_structure_factor_manifold_average
+(uniform and 2:1 weights), structure_factor_manifold_allowed_momenta,
+compute_structure_factor_manifold_average_map (5 x 5),
+structure_factor_allowed_momenta of ((0,0), 1) and the first-Brillouin-zone
+polygon.
 """
 
 from __future__ import annotations
@@ -95,5 +102,27 @@ def main():
         print(f"corr_{name}: trace rho = {np.trace(rho).real:.6f}, max S = {S.max():.6f} -> {os.path.getsize(path)} B")
 
 
+def manifold_case(R, ssf):
+    with contextlib.redirect_stdout(io.StringIO()):
+        model = build_model(R, "bosonic", [2, 3])
+        ff = Fraction(3, 12)
+        states = [((0, 0), 1), ((1, 0), 1)]
+        q, S_u = ssf.static_structure_factor_manifold_average(model, states, filling_fraction=ff)
+        _, S_w = ssf.static_structure_factor_manifold_average(model, states, weights=[2.0, 1.0], filling_fraction=ff)
+        mx, my, mS = ssf.structure_factor_manifold_allowed_momenta(model, states, filling_fraction=ff)
+        _, _, mmap = ssf.compute_structure_factor_manifold_average_map(model, states, filling_fraction=ff,
+                                                                      k_resolution=5)
+        ax, ay, aS = ssf.structure_factor_allowed_momenta(model, (0, 0), filling_fraction=ff)
+        poly = ssf._first_bz_polygon(model.lattice)
+    out = dict(q_points=np.array(q), S_uniform=S_u, S_weighted=S_w, manifold_qx=np.array(mx),
+               manifold_qy=np.array(my), manifold_S=mS, manifold_map=mmap, allowed_qx=np.array(ax),
+               allowed_qy=np.array(ay), allowed_S=aS, bz_polygon=np.array([np.asarray(p) for p in poly]))
+    path = os.path.join(HERE, "corr_manifold_haldane12.npz")
+    np.savez_compressed(path, **out)
+    print(f"corr_manifold_haldane12: {len(poly)}-gon zone -> {os.path.getsize(path)} B")
+
+
 if __name__ == "__main__":
     main()
+    _R = ref_shim.load()
+    manifold_case(_R, importlib.import_module(ref_shim.PKG + ".observables.static_structure_factor"))

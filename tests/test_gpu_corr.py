@@ -76,3 +76,36 @@ def test_one_body_density_two_species_blocks():
     b[[s - 1 for s in sites_b]] = True
     assert np.abs(rho[np.ix_(b, ~b)]).max() == 0 and np.abs(rho[np.ix_(~b, b)]).max() == 0
     assert abs(np.trace(rho[np.ix_(b, b)]) - nb) < 1e-10
+
+
+def test_manifold_structure_factor_matches_reference():
+    """Manifold averages (uniform and 2:1 weights), their allowed-momenta and
+    map forms, and the single-state allowed momenta against the reference
+    (tests/golden/make_corr_golden.py)."""
+    import os
+
+    import realspace_exatdiagonalization_py_b200 as ed
+    from realspace_exatdiagonalization_py_b200 import models
+
+    f = dict(np.load(os.path.join(os.path.dirname(__file__), "golden", "corr_manifold_haldane12.npz")))
+    m = models.build_zero_flux_bosonic_fci_second_quantized_model(sample_size=[2, 3], params=models.params_DNSheng)
+    ff = Fraction(3, 12)
+    states = [((0, 0), 1), ((1, 0), 1)]
+    q, S = ed.static_structure_factor_manifold_average(m, states, filling_fraction=ff)
+    np.testing.assert_allclose(np.array(q), f["q_points"], atol=1e-14, rtol=0)
+    np.testing.assert_allclose(S, f["S_uniform"], atol=1e-11, rtol=0)
+    _, Sw = ed.static_structure_factor_manifold_average(m, states, weights=[2.0, 1.0], filling_fraction=ff)
+    np.testing.assert_allclose(Sw, f["S_weighted"], atol=1e-11, rtol=0)
+    mx, my, mS = ed.structure_factor_manifold_allowed_momenta(m, states, filling_fraction=ff)
+    np.testing.assert_allclose(mx, f["manifold_qx"], atol=1e-12, rtol=0)
+    np.testing.assert_allclose(my, f["manifold_qy"], atol=1e-12, rtol=0)
+    np.testing.assert_allclose(mS, f["manifold_S"], atol=1e-11, rtol=0)
+    _, _, mmap = ed.compute_structure_factor_manifold_average_map(m, states, filling_fraction=ff, k_resolution=5)
+    np.testing.assert_allclose(mmap, f["manifold_map"], atol=1e-11, rtol=0)
+    ax, ay, aS = ed.structure_factor_allowed_momenta(m, (0, 0), filling_fraction=ff)
+    np.testing.assert_allclose(aS, f["allowed_S"], atol=1e-11, rtol=0)
+    np.testing.assert_allclose(ax, f["allowed_qx"], atol=1e-12, rtol=0)
+    with pytest.raises(ValueError):
+        ed.static_structure_factor_manifold_average(m, states, weights=[1.0], filling_fraction=ff)
+    with pytest.raises(ValueError):
+        ed.static_structure_factor_manifold_average(m, [], filling_fraction=ff)

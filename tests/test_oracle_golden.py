@@ -356,3 +356,21 @@ def test_oracle_matches_reference_benchmark(model, label):
     vals, dim = out[0]
     assert dim == int(f["sector_dim"][i])
     assert abs(float(vals[0]) - float(f["energy"][i])) < 1e-9
+
+
+def test_brillouin_zone_helpers_match_reference():
+    """First-Brillouin-zone polygon and folded mesh momenta of the 2x3
+    honeycomb lattice against the reference (static_structure_factor.py:210-377,
+    tests/golden/make_corr_golden.py)."""
+    import os
+
+    from realspace_exatdiagonalization_py_b200 import correlators as cr
+    from realspace_exatdiagonalization_py_b200 import models
+
+    f = dict(np.load(os.path.join(os.path.dirname(__file__), "golden", "corr_manifold_haldane12.npz")))
+    m = models.build_zero_flux_bosonic_fci_second_quantized_model(sample_size=[2, 3], params=models.params_DNSheng)
+    poly = np.array([np.asarray(p) for p in cr._first_bz_polygon(m.lattice)])
+    np.testing.assert_allclose(poly, f["bz_polygon"], atol=1e-12, rtol=0)
+    folded = cr._fold_momenta_to_first_bz(list(f["q_points"]), m.lattice)
+    np.testing.assert_allclose([p[0] for p in folded], f["allowed_qx"], atol=1e-12, rtol=0)
+    np.testing.assert_allclose([p[1] for p in folded], f["allowed_qy"], atol=1e-12, rtol=0)
