@@ -748,7 +748,7 @@ def run_b200(args):
             flush.zero_()
             torch.cuda.synchronize()
             n0 = lib.rsed_launch_count()
-            r0 = b.replays
+            r0 = b.replayed_launches
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
             vals, _ = step()
@@ -756,7 +756,7 @@ def run_b200(args):
             torch.cuda.synchronize()
             times.append(e0.elapsed_time(e1) * 1e-3)
             launches += int(lib.rsed_launch_count() - n0)
-            launches += (b.replays - r0) * (b.launches_per_graph or 0)
+            launches += b.replayed_launches - r0
             if ref is not None:
                 v = vals.cpu().numpy()
                 max_de = max(max_de, max(float(np.max(np.abs(v[i] - ref[s][:nev]))) for i, s in enumerate(sectors)))

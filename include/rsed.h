@@ -366,6 +366,17 @@ int rsed_lanczos_start(const rsed_model_t* model, const rsed_sectors_t* sec, rse
                        void* stream);
 int rsed_lanczos_iterate(const rsed_model_t* model, const rsed_sectors_t* sec, rsed_lanczos_t* st,
                          int32_t n_iter, int32_t check_every, int32_t apply_variant, void* stream);
+/* n_iter block steps that launch the Ritz check and the restart only after
+ * the last step (ritz_last != 0) or not at all.  Same state as
+ * rsed_lanczos_iterate with the same n_iter when neither a restart (the
+ * basis reaching n_slots + 1 blocks) nor a periodic check falls due before
+ * the last step -- the active instances all advance one block per step, so
+ * restarts come n_slots steps after rsed_lanczos_start and every
+ * n_slots - keep_blocks steps after that.  A restart that falls due inside
+ * the span stops its instance with RSED_EINVAL at the next Gram pass. */
+int rsed_lanczos_iterate_span(const rsed_model_t* model, const rsed_sectors_t* sec, rsed_lanczos_t* st,
+                              int32_t n_iter, int32_t ritz_last, int32_t check_every,
+                              int32_t apply_variant, void* stream);
 /* FP64 Rayleigh-Ritz refinement of converged instances (typically after an
  * FP32-matvec solve): the thick-restart basis (keep_blocks*b Ritz vectors
  * plus the residual block) is re-projected with the FP64 operator, the

@@ -217,6 +217,11 @@ SIGNATURES = {
         [POINTER(RsedModel), POINTER(RsedSectors), POINTER(RsedLanczos), c_int32, c_int32, c_int32,
          c_void_p],
     ),
+    "rsed_lanczos_iterate_span": (
+        c_int,
+        [POINTER(RsedModel), POINTER(RsedSectors), POINTER(RsedLanczos), c_int32, c_int32, c_int32,
+         c_int32, c_void_p],
+    ),
     "rsed_lanczos_rayleigh_ritz": (
         c_int,
         [POINTER(RsedModel), POINTER(RsedSectors), POINTER(RsedLanczos), c_int32, c_void_p],

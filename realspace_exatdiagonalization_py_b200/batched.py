@@ -95,8 +95,10 @@ class BatchedSectorSolver:
         b.start()
         if self.persistent:
             b.run_persistent(self.persistent)
+        elif self.graph:
+            b.run_aligned(poll=poll)
         else:
-            b.run(poll=poll, graph=self.graph)
+            b.run(poll=poll, graph=False)
 
     def solve(self, start_blocks=None, *, vectors: bool = True, host: bool = True):
         """Solve every sector; ``start_blocks`` as in ``LanczosBatch.load_start``.

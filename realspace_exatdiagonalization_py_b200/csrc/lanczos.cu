@@ -1848,14 +1848,17 @@ extern "C" int rsed_lanczos_start(const rsed_model_t* md, const rsed_sectors_t* 
   return launch_pass(*st, d, 2, stream);
 }
 
-extern "C" int rsed_lanczos_iterate(const rsed_model_t* md, const rsed_sectors_t* sc, rsed_lanczos_t* st,
-                                    int32_t n_iter, int32_t check_every, int32_t apply_variant,
-                                    void* stream_) {
+// n_iter iterations: H X, Gram passes 1 and 2, then the Ritz check and the
+// restart after every iteration (ritz_mode 0), after the last one only (1)
+// or never (2).
+static int lz_iterate(const rsed_model_t* md, const rsed_sectors_t* sc, rsed_lanczos_t* st, int32_t n_iter,
+                      int ritz_mode, int32_t check_every, int32_t apply_variant, void* stream_) {
   int rc = check_lz(md, sc, st);
   if (rc) return rc;
   rc = set_ritz_smem();
   if (rc) return rc;
   RSED_REQUIRE(check_every >= 1, RSED_EINVAL, "check_every must be >= 1");
+  RSED_REQUIRE(n_iter >= 0, RSED_EINVAL, "n_iter must be >= 0");
   cudaStream_t stream = as_stream(stream_);
   const LzDims d = make_dims(md, sc, st);
   const double2* X = reinterpret_cast<const double2*>(st->V) + (int64_t)(st->n_slots + 1) * d.n_orb * d.ld;
@@ -1867,12 +1870,26 @@ extern "C" int rsed_lanczos_iterate(const rsed_model_t* md, const rsed_sectors_t
     if (rc) return rc;
     rc = launch_pass(*st, d, 2, stream);
     if (rc) return rc;
-    k_lz_ritz<<<d.n_inst, kRitzThreads, kRitzSmem, stream>>>(*st, d, check_every, 0, 0);
-    RSED_CHECK_LAUNCH();
-    k_lz_restart<<<dim3((unsigned)((d.n_orb + 255) / 256), d.n_inst), 256, 0, stream>>>(*st, d);
-    RSED_CHECK_LAUNCH();
+    if (ritz_mode == 0 || (ritz_mode == 1 && it == n_iter - 1)) {
+      k_lz_ritz<<<d.n_inst, kRitzThreads, kRitzSmem, stream>>>(*st, d, check_every, 0, 0);
+      RSED_CHECK_LAUNCH();
+      k_lz_restart<<<dim3((unsigned)((d.n_orb + 255) / 256), d.n_inst), 256, 0, stream>>>(*st, d);
+      RSED_CHECK_LAUNCH();
+    }
   }
   return RSED_OK;
+}
+
+extern "C" int rsed_lanczos_iterate(const rsed_model_t* md, const rsed_sectors_t* sc, rsed_lanczos_t* st,
+                                    int32_t n_iter, int32_t check_every, int32_t apply_variant,
+                                    void* stream_) {
+  return lz_iterate(md, sc, st, n_iter, 0, check_every, apply_variant, stream_);
+}
+
+extern "C" int rsed_lanczos_iterate_span(const rsed_model_t* md, const rsed_sectors_t* sc, rsed_lanczos_t* st,
+                                         int32_t n_iter, int32_t ritz_last, int32_t check_every,
+                                         int32_t apply_variant, void* stream_) {
+  return lz_iterate(md, sc, st, n_iter, ritz_last ? 1 : 2, check_every, apply_variant, stream_);
 }
 
 extern "C" int rsed_lanczos_rayleigh_ritz(const rsed_model_t* md, const rsed_sectors_t* sc,

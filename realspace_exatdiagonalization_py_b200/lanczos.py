@@ -148,9 +148,11 @@ class LanczosBatch:
         )
         self.sc = sset.sectors_struct(self.col_sector, self.n_cols, self.ld)
         self.replays = 0
+        self.replayed_launches = 0  # kernels launched by graph replays
         self.launches_per_graph = None
         self._graph = None
         self._graph_iters = None
+        self._spans = None  # restart-aligned graphs: ((head, launches), (cycle, launches))
 
     @property
     def n_inst(self) -> int:
@@ -199,6 +201,20 @@ class LanczosBatch:
             ctypes.byref(self.model.c), ctypes.byref(self.sc), ctypes.byref(self.c), n_iter,
             self.p.check_every, self.p.apply_variant, _lib.stream_ptr(stream)))
 
+    def iterate_span(self, n_iter: int, ritz_last: bool, stream=None) -> None:
+        """``n_iter`` steps with the Ritz check and restart after the last step
+        only (``ritz_last``) or not at all; see ``restart_period``."""
+        _lib.check(_lib.lib().rsed_lanczos_iterate_span(
+            ctypes.byref(self.model.c), ctypes.byref(self.sc), ctypes.byref(self.c), n_iter,
+            int(bool(ritz_last)), self.p.check_every, self.p.apply_variant, _lib.stream_ptr(stream)))
+
+    @property
+    def restart_period(self) -> int:
+        """Steps between two thick restarts.  Every active instance adds one
+        block per step, so the first restart falls due ``n_slots`` steps after
+        ``start()`` and the next ones every ``n_slots - keep`` steps."""
+        return self.p.n_slots - self.keep
+
     def status(self) -> np.ndarray:
         return self.state.cpu().numpy()
 
@@ -226,11 +242,70 @@ class LanczosBatch:
             if g is not None:
                 g.replay()
                 self.replays += 1
+                self.replayed_launches += self.launches_per_graph or 0
             else:
                 self.iterate(poll, stream)
             it += poll
             if self.done():
                 break
+        return self._final_status()
+
+    def run_aligned(self, max_iter: int = 4000, poll: int = 8) -> np.ndarray:
+        """``run(graph=True)`` from a fresh ``start()``, with the graphs cut at
+        the restarts: a head graph of ``keep`` steps that launches no Ritz
+        check, then a cycle graph of ``restart_period`` steps that checks (and
+        restarts) after its last step only, replayed until every instance
+        converged.  Convergence is only decided at restarts (unless
+        ``check_every`` falls due first), so the host polls once per cycle and
+        no step runs past the restart that finished the batch.  The kernels
+        and their order are those of ``run`` minus the launches that find no
+        check due, so the results are the same.  A periodic check that would
+        fall inside a graph hands the rest of the solve to ``run``'s per-step
+        path."""
+        h, period, ce = self.keep, self.restart_period, self.p.check_every
+
+        def check_inside(first: int, last: int) -> bool:
+            # the state's iteration count is 1 after start() and i + 1 after
+            # step i; a periodic check runs at step i when (i + 1) % ce == 0
+            return any((i + 1) % ce == 0 for i in range(first, last + 1))
+
+        if h < 1 or period < 1 or check_inside(1, h):
+            return self.run(max_iter, poll, graph=True)
+        if self._spans is None:
+            self.iterate(h)  # first solve: every kernel runs once before the captures
+            self._spans = (self._capture_span(h, False), self._capture_span(period, True))
+        else:
+            g, n = self._spans[0]
+            g.replay()
+            self.replays += 1
+            self.replayed_launches += n
+        it = h
+        g, n = self._spans[1]
+        converged = False
+        while it < max_iter and not check_inside(it + 1, it + period - 1):
+            g.replay()
+            self.replays += 1
+            self.replayed_launches += n
+            it += period
+            if self.done():
+                converged = True
+                break
+        while not converged and it < max_iter:
+            self.iterate(poll)
+            it += poll
+            converged = self.done()
+        return self._final_status()
+
+    def _capture_span(self, n_iter: int, ritz_last: bool):
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        g = torch.cuda.CUDAGraph()
+        n0 = _lib.load().rsed_launch_count()
+        with torch.cuda.graph(g, stream=s):
+            self.iterate_span(n_iter, ritz_last, s)
+        return g, int(_lib.load().rsed_launch_count() - n0)
+
+    def _final_status(self) -> np.ndarray:
         st = self.status()
         bad = [i for i in range(self.n_inst) if st[i, S_STATUS] != 1]
         if bad:
