@@ -405,6 +405,15 @@ int rsed_gather_rows(int64_t n_rows, const int32_t* orbit_of_row, const double* 
                      int32_t src_col, double* dst, int64_t dst_stride, void* stream);
 int rsed_scatter_rows(int64_t n_rows, const int32_t* orbit_of_row, const double* src,
                       int64_t src_stride, double* dst, int64_t dst_ld, int32_t dst_col, void* stream);
+/* n_cols orbit-layout columns (column j at src + j*src_col_stride) into a
+ * row-major [n_rows, dst_ld] complex128 block in one launch:
+ * dst[r*dst_ld + j] = src[j*src_col_stride + orbit_of_row[r]]. */
+int rsed_gather_block(int64_t n_rows, const int32_t* orbit_of_row, const double* src, int32_t n_cols,
+                      int64_t src_col_stride, double* dst, int64_t dst_ld, void* stream);
+/* The first n_cols columns of a row-major [n_rows, src_ld] complex128 block in
+ * one launch: dst[orbit_of_row[r]*dst_ld + dst_col0 + j] = src[r*src_ld + j]. */
+int rsed_scatter_block(int64_t n_rows, const int32_t* orbit_of_row, const double* src, int32_t n_cols,
+                       int64_t src_ld, double* dst, int64_t dst_ld, int32_t dst_col0, void* stream);
 int rsed_device_sync(void* stream);
 /* Kernel launches issued by the library so far (process-wide counter; a
  * CUDA graph replay re-runs the launches counted while it was captured). */

@@ -242,6 +242,14 @@ SIGNATURES = {
         c_int,
         [c_int64, c_void_p, c_void_p, c_int64, c_void_p, c_int64, c_int32, c_void_p],
     ),
+    "rsed_gather_block": (
+        c_int,
+        [c_int64, c_void_p, c_void_p, c_int32, c_int64, c_void_p, c_int64, c_void_p],
+    ),
+    "rsed_scatter_block": (
+        c_int,
+        [c_int64, c_void_p, c_void_p, c_int32, c_int64, c_void_p, c_int64, c_int32, c_void_p],
+    ),
     "rsed_device_sync": (c_int, [c_void_p]),
     "rsed_launch_count": (ctypes.c_longlong, []),
 }

@@ -21,7 +21,7 @@ import numpy as np
 import torch
 
 from .hamiltonian import DeviceModel
-from .lanczos import LanczosBatch, LanczosParams
+from .lanczos import LanczosBatch, LanczosParams, vectors_to_host
 from .sector import SectorSet
 
 # rsed_apply_h variants: 0 = automatic (projection table when present),
@@ -118,7 +118,7 @@ class BatchedSectorSolver:
         if host:
             vals = vals.cpu().numpy()
             if vecs is not None:
-                vecs = [v.cpu().numpy() for v in vecs]
+                vecs = vectors_to_host(vecs)
         return vals, vecs
 
     def fp32_error(self) -> np.ndarray | None:

@@ -1802,6 +1802,26 @@ __global__ void k_scatter_rows(int64_t n_rows, const int32_t* orbit_of_row, cons
   if (r < n_rows) dst[(int64_t)orbit_of_row[r] * dst_ld + dst_col] = src[r * src_stride];
 }
 
+// One thread per (row, column) of a row-major [n_rows, dst_ld] block.
+__global__ void k_gather_block(int64_t n_rows, const int32_t* orbit_of_row, const double2* src, int n_cols,
+                               int64_t src_col_stride, double2* dst, int64_t dst_ld) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n_rows * n_cols) return;
+  const int64_t r = e / n_cols;
+  const int j = (int)(e - r * n_cols);
+  dst[r * dst_ld + j] = src[(int64_t)j * src_col_stride + orbit_of_row[r]];
+}
+
+// One thread per (row, column) of a row-major [n_rows, src_ld] block.
+__global__ void k_scatter_block(int64_t n_rows, const int32_t* orbit_of_row, const double2* src, int n_cols,
+                                int64_t src_ld, double2* dst, int64_t dst_ld, int dst_col0) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n_rows * n_cols) return;
+  const int64_t r = e / n_cols;
+  const int j = (int)(e - r * n_cols);
+  dst[(int64_t)orbit_of_row[r] * dst_ld + dst_col0 + j] = src[r * src_ld + j];
+}
+
 }  // namespace
 
 extern "C" int64_t rsed_lanczos_partial_len(int64_t n_orbits, int32_t chunk_rows, int32_t n_inst,
@@ -1994,6 +2014,33 @@ extern "C" int rsed_scatter_rows(int64_t n_rows, const int32_t* orbit_of_row, co
   k_scatter_rows<<<(unsigned)((n_rows + 255) / 256), 256, 0, as_stream(stream_)>>>(
       n_rows, orbit_of_row, reinterpret_cast<const double2*>(src), src_stride,
       reinterpret_cast<double2*>(dst), dst_ld, dst_col);
+  RSED_CHECK_LAUNCH();
+  return RSED_OK;
+}
+
+extern "C" int rsed_gather_block(int64_t n_rows, const int32_t* orbit_of_row, const double* src, int32_t n_cols,
+                                 int64_t src_col_stride, double* dst, int64_t dst_ld, void* stream_) {
+  RSED_REQUIRE(n_rows >= 0 && n_cols >= 1 && dst_ld >= n_cols && orbit_of_row && src && dst, RSED_EINVAL,
+               "bad gather arguments");
+  if (n_rows == 0) return RSED_OK;
+  const int64_t n = n_rows * n_cols;
+  k_gather_block<<<(unsigned)((n + 255) / 256), 256, 0, as_stream(stream_)>>>(
+      n_rows, orbit_of_row, reinterpret_cast<const double2*>(src), n_cols, src_col_stride,
+      reinterpret_cast<double2*>(dst), dst_ld);
+  RSED_CHECK_LAUNCH();
+  return RSED_OK;
+}
+
+extern "C" int rsed_scatter_block(int64_t n_rows, const int32_t* orbit_of_row, const double* src,
+                                  int32_t n_cols, int64_t src_ld, double* dst, int64_t dst_ld,
+                                  int32_t dst_col0, void* stream_) {
+  RSED_REQUIRE(n_rows >= 0 && n_cols >= 1 && src_ld >= n_cols && orbit_of_row && src && dst, RSED_EINVAL,
+               "bad scatter arguments");
+  if (n_rows == 0) return RSED_OK;
+  const int64_t n = n_rows * n_cols;
+  k_scatter_block<<<(unsigned)((n + 255) / 256), 256, 0, as_stream(stream_)>>>(
+      n_rows, orbit_of_row, reinterpret_cast<const double2*>(src), n_cols, src_ld,
+      reinterpret_cast<double2*>(dst), dst_ld, dst_col0);
   RSED_CHECK_LAUNCH();
   return RSED_OK;
 }

@@ -217,19 +217,29 @@ def solve_sectors_batched(ed_data, sector_ids: list[int], *, nev: int = 5, preci
             free, _ = torch.cuda.mem_get_info()
             if dm.projection_bytes((precision,)) <= 0.5 * free:
                 dm.build_projection(sset.sqrt_stab, precisions=projection_precisions(dm, precision))
-        free, _ = torch.cuda.mem_get_info()
-        n_orb = ed_data.orbit_catalog.n_orbits
-        bs = list(config.block_sizes) if config is not None else [p.block] * len(big)
-        budget = int(0.7 * free)
-        if lanczos_footprint_bytes(n_orb, sum(bs), p.n_slots, precision) <= budget:
+        cache = ed_data.__dict__.setdefault("_solvers", {})
+        resident = None
+        if not (config is None and autotune):
+            resident = cache.get((tuple(big), nev, precision,
+                                  None if params is None else tuple(params.__dict__.items()), graph, config))
+        if resident is not None and resident.model is dm:
+            # the solver of an earlier call with the same sectors holds all its
+            # buffers: no wave plan, and no free-memory query (cudaMemGetInfo
+            # takes about 0.4 ms per call and at times stalls for ~100 ms)
             waves = [list(range(len(big)))]
         else:
-            waves = plan_waves(n_orb, bs, budget, p.n_slots, precision)
-        if config is None and autotune and len(waves) == 1:
-            from .autotune import default_tuner
+            free, _ = torch.cuda.mem_get_info()
+            n_orb = ed_data.orbit_catalog.n_orbits
+            bs = list(config.block_sizes) if config is not None else [p.block] * len(big)
+            budget = int(0.7 * free)
+            if lanczos_footprint_bytes(n_orb, sum(bs), p.n_slots, precision) <= budget:
+                waves = [list(range(len(big)))]
+            else:
+                waves = plan_waves(n_orb, bs, budget, p.n_slots, precision)
+            if config is None and autotune and len(waves) == 1:
+                from .autotune import default_tuner
 
-            config = default_tuner().best(dm, sset, big, nev, precision, params)
-        cache = ed_data.__dict__.setdefault("_solvers", {})
+                config = default_tuner().best(dm, sset, big, nev, precision, params)
         for wave in waves:
             secs = [big[i] for i in wave]
             cfg = config if len(waves) == 1 else (None if config is None else type(config)(

@@ -182,15 +182,12 @@ class LanczosBatch:
                 blk = cache[key]
             if isinstance(blk, np.ndarray):
                 blk = torch.from_numpy(np.ascontiguousarray(blk, dtype=np.complex128))
-            blk = blk.to(self.dev, non_blocking=True).reshape(d, -1)
+            blk = blk.to(self.dev, torch.complex128, non_blocking=True).reshape(d, -1).contiguous()
             if blk.shape[1] < b:
                 raise ValueError(f"start block of sector {s} has {blk.shape[1]} columns, the instance needs {b}")
-            blk = blk[:, :b].to(torch.complex128)
-            blk = blk.t().contiguous()  # [b, d]
             oor, _ = self.sset.rows(s)
-            for j in range(b):
-                _lib.check(lib.rsed_scatter_rows(d, _lib.ptr(oor), _lib.ptr(blk[j]), 1, _lib.ptr(self.W),
-                                                 self.ld, int(self.col0[i]) + j, sp))
+            _lib.check(lib.rsed_scatter_block(d, _lib.ptr(oor), _lib.ptr(blk), b, blk.shape[1], _lib.ptr(self.W),
+                                              self.ld, int(self.col0[i]), sp))
 
     def start(self, stream=None) -> None:
         _lib.check(_lib.lib().rsed_lanczos_start(ctypes.byref(self.model.c), ctypes.byref(self.sc),
@@ -372,20 +369,50 @@ class LanczosBatch:
         return U
 
     def eigenvectors(self, U: torch.Tensor | None = None, stream=None) -> list[torch.Tensor]:
-        """Per instance ``[D_s, nev]`` eigenvectors in the sector's basis order."""
+        """Per instance ``[D_s, nev]`` eigenvectors in the sector's basis order:
+        row-major views, one after the other, of one device buffer (one
+        gather launch per instance)."""
         U = self.ritz_vectors_orbit(stream) if U is None else U
-        out = []
         lib = _lib.lib()
         sp = _lib.stream_ptr(stream)
+        dims = [self.sset.dims[s] for s in self.inst_sectors]
+        flat = torch.empty((sum(dims) * self.nev,), dtype=torch.complex128, device=self.dev)
+        out = []
+        off = 0
         for i, s in enumerate(self.inst_sectors):
-            d = self.sset.dims[s]
+            d = dims[i]
             oor, _ = self.sset.rows(s)
-            vec = torch.empty((self.nev, d), dtype=torch.complex128, device=self.dev)
-            for j in range(self.nev):
-                _lib.check(lib.rsed_gather_rows(d, _lib.ptr(oor), _lib.ptr(U[i, j]), 1, 0,
-                                                _lib.ptr(vec[j]), 1, sp))
-            out.append(vec.t())
+            vec = flat[off: off + d * self.nev].view(d, self.nev)
+            _lib.check(lib.rsed_gather_block(d, _lib.ptr(oor), _lib.ptr(U[i]), self.nev, U.stride(1),
+                                             _lib.ptr(vec), self.nev, sp))
+            out.append(vec)
+            off += d * self.nev
         return out
+
+
+def vectors_to_host(vecs: list[torch.Tensor]) -> list[np.ndarray]:
+    """Host copies of ``eigenvectors()``'s blocks in ONE device-to-host copy
+    when they are consecutive views of one buffer (as returned), else one
+    copy per block."""
+    if not vecs:
+        return []
+    base = vecs[0]
+    start = base.storage_offset()
+    n = sum(v.numel() for v in vecs)
+    consecutive = all(v.is_contiguous() for v in vecs) and all(
+        v.untyped_storage().data_ptr() == base.untyped_storage().data_ptr() for v in vecs)
+    off = start
+    for v in vecs:
+        consecutive = consecutive and v.storage_offset() == off
+        off += v.numel()
+    if not consecutive:
+        return [v.cpu().numpy() for v in vecs]
+    h = base.as_strided((n,), (1,), start).cpu().numpy()
+    out, off = [], 0
+    for v in vecs:
+        out.append(h[off: off + v.numel()].reshape(v.shape))
+        off += v.numel()
+    return out
 
 
 def refine(batch: LanczosBatch) -> LanczosBatch:

@@ -205,3 +205,24 @@ def test_library_rejects_bad_arguments_without_gpu():
     assert b"n_site" in lib.rsed_last_error()
     with pytest.raises(ValueError):
         _lib.check(rc)
+    # block gather and scatter validate their shapes before any CUDA call
+    assert lib.rsed_gather_block(4, None, None, 2, 8, None, 2, None) == _lib.RSED_EINVAL
+    assert lib.rsed_scatter_block(4, None, None, 3, 2, None, 8, 0, None) == _lib.RSED_EINVAL
+
+
+def test_vectors_to_host_single_copy_layout():
+    """Consecutive row-major views of one buffer come back as one host copy,
+    split in order; any other list is copied block by block."""
+    import torch
+
+    from realspace_exatdiagonalization_py_b200.lanczos import vectors_to_host
+
+    flat = torch.arange(30, dtype=torch.float64).to(torch.complex128)
+    for vs in ([flat[0:12].view(4, 3), flat[12:30].view(6, 3)],
+               [flat[12:30].view(6, 3), flat[0:12].view(4, 3)],
+               [torch.ones(3, 2, dtype=torch.complex128).t(), torch.zeros(2, 2, dtype=torch.complex128)]):
+        hs = vectors_to_host(vs)
+        assert [h.shape for h in hs] == [tuple(v.shape) for v in vs]
+        for h, v in zip(hs, vs):
+            np.testing.assert_array_equal(h, v.numpy())
+    assert vectors_to_host([]) == []
