@@ -205,6 +205,15 @@ class LanczosBatch:
             ctypes.byref(self.model.c), ctypes.byref(self.sc), ctypes.byref(self.c), n_iter,
             int(bool(ritz_last)), self.p.check_every, self.p.apply_variant, _lib.stream_ptr(stream)))
 
+    def periodic_check_in(self, first: int, last: int) -> bool:
+        """Whether a periodic Ritz check (every ``check_every`` iterations)
+        can fall due at a step in ``first..last`` (steps counted from 1 after
+        ``start()``).  The state's iteration count is 1 after ``start()`` and
+        i + 1 after step i; the check of step i runs when (i + 1) is a
+        multiple of ``check_every``."""
+        ce = self.p.check_every
+        return last >= first and (last + 1) // ce > first // ce
+
     @property
     def restart_period(self) -> int:
         """Steps between two thick restarts.  Every active instance adds one
@@ -259,18 +268,13 @@ class LanczosBatch:
         check due, so the results are the same.  A periodic check that would
         fall inside a graph hands the rest of the solve to ``run``'s per-step
         path."""
-        h, period, ce = self.keep, self.restart_period, self.p.check_every
-
-        def check_inside(first: int, last: int) -> bool:
-            # the state's iteration count is 1 after start() and i + 1 after
-            # step i; a periodic check runs at step i when (i + 1) % ce == 0
-            return any((i + 1) % ce == 0 for i in range(first, last + 1))
-
+        h, period = self.keep, self.restart_period
+        check_inside = self.periodic_check_in
         if h < 1 or period < 1 or check_inside(1, h):
             return self.run(max_iter, poll, graph=True)
         if self._spans is None:
             self.iterate(h)  # first solve: every kernel runs once before the captures
-            self._spans = (self._capture_span(h, False), self._capture_span(period, True))
+            self._spans = (self.capture_span(h, False), self.capture_span(period, True))
         else:
             g, n = self._spans[0]
             g.replay()
@@ -292,15 +296,6 @@ class LanczosBatch:
             it += poll
             converged = self.done()
         return self._final_status()
-
-    def _capture_span(self, n_iter: int, ritz_last: bool):
-        s = torch.cuda.Stream()
-        s.wait_stream(torch.cuda.current_stream())
-        g = torch.cuda.CUDAGraph()
-        n0 = _lib.load().rsed_launch_count()
-        with torch.cuda.graph(g, stream=s):
-            self.iterate_span(n_iter, ritz_last, s)
-        return g, int(_lib.load().rsed_launch_count() - n0)
 
     def _final_status(self) -> np.ndarray:
         st = self.status()
@@ -338,20 +333,31 @@ class LanczosBatch:
         with torch.cuda.stream(s):
             self.iterate(1, s)  # warm-up outside the graph (kernel attributes, lazy loading)
         torch.cuda.current_stream().wait_stream(s)
+        g, self.launches_per_graph = self._capture(lambda st: self.iterate(n_iter, st), sync)
+        return g
+
+    def capture_span(self, n_iter: int, ritz_last: bool, sync: bool = True):
+        """``(graph, launches)`` of ``iterate_span(n_iter, ritz_last)``.  No
+        warm-up: every kernel must have run once before (e.g. an eager first
+        span of the same batch)."""
+        return self._capture(lambda st: self.iterate_span(n_iter, ritz_last, st), sync)
+
+    def _capture(self, launch, sync: bool):
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
         g = torch.cuda.CUDAGraph()
         n0 = _lib.load().rsed_launch_count()
         if sync:
             with torch.cuda.graph(g, stream=s):
-                self.iterate(n_iter, s)
+                launch(s)
         else:
             with torch.cuda.stream(s):
                 g.capture_begin(capture_error_mode="thread_local")
                 try:
-                    self.iterate(n_iter, s)
+                    launch(s)
                 finally:
                     g.capture_end()
-        self.launches_per_graph = int(_lib.load().rsed_launch_count() - n0)
-        return g
+        return g, int(_lib.load().rsed_launch_count() - n0)
 
     # -- results ----------------------------------------------------------
     def eigenvalues(self) -> np.ndarray:

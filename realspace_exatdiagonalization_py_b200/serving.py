@@ -15,9 +15,9 @@ projected matrices, state) of 1..``max_width`` instances on its own CUDA
 stream, plus the lane's own copy of one flux point's weights and sector
 membership.  A lane serves any flux point of its model: taking a request, it
 copies that flux point's weights and membership into its buffers (a device
-copy of a few hundred MB at most) and replays the Lanczos iterations from a
-CUDA graph captured once, when the lane was created -- its kernels only ever
-see the lane's own buffers.
+copy of a few hundred MB at most) and replays the Lanczos iterations from
+CUDA graphs captured once, with the lane's first solve -- its kernels only
+ever see the lane's own buffers.
 
 Scheduling (``step``), one host thread, no blocking waits on the device:
   * admission: pending requests are grouped by (model, flux); a group takes an
@@ -26,8 +26,9 @@ Scheduling (``step``), one host thread, no blocking waits on the device:
     bytes they need (measured for contexts, computed for lanes) fit the
     budget; idle lanes and flux contexts no running lane uses are evicted
     (least recently used) to make room.  Requests that do not fit wait.
-  * progress: every running lane gets ``poll`` more Lanczos iterations (one
-    graph replay) on its stream, followed by an asynchronous copy of its state
+  * progress: every running lane gets the Lanczos steps up to its next thick
+    restart (one graph replay; convergence is decided at restarts) on its
+    stream, followed by an asynchronous copy of its state
     into pinned host memory and an event; lanes whose event completed and
     whose instances all stopped move on to the FP64 Rayleigh-Ritz refinement
     (FP32 matvec; run against the flux context's own model) and the
@@ -239,7 +240,11 @@ class _Lane:
         self.model = _LaneModel(base, self.w, params.precision)
         self.sectors = _LaneSectors(base, self.member)
         self.batch: LanczosBatch | None = None
+        # restart-aligned graphs ((head, launches), (cycle, launches)),
+        # captured with the lane's first solve
         self.graph = None
+        self.it = 0          # Lanczos steps of the current solve
+        self.aligned = True  # False once a periodic check moved the solve to per-step launches
         self.state = "idle"
         self.ctx: FluxContext | None = None
         self.reqs: list[SolveRequest] = []
@@ -289,16 +294,38 @@ class _Lane:
                 b.inst_sectors = sectors
                 cs = np.concatenate([[s] * self.params.block for s in sectors]).astype(np.int32)
                 b.col_sector.copy_(torch.from_numpy(cs), non_blocking=False)
-            self.batch.load_start(self._start_blocks())
-            self.batch.start()
-            if self.graph is None:
-                self.graph = self.batch.capture(self.poll, sync=False)
+            b = self.batch
+            b.load_start(self._start_blocks())
+            b.start()
+            # head: keep steps, no restart can fall due (see LanczosBatch.run_aligned)
+            self.aligned = b.keep >= 1 and b.restart_period >= 1 and not b.periodic_check_in(1, b.keep)
+            if not self.aligned:
+                b.iterate(self.poll, self.stream)
+                self.it = self.poll
+            elif self.graph is None:
+                b.iterate(b.keep, self.stream)  # the first solve runs every kernel once before the captures
+                self.graph = (b.capture_span(b.keep, False, sync=False),
+                              b.capture_span(b.restart_period, True, sync=False))
+                self.it = b.keep
+            else:
+                self.graph[0][0].replay()
+                self.it = b.keep
             self._advance()
         self.state = "running"
 
     def _advance(self) -> None:
+        """The next cycle of restart_period steps, ending at a restart (or,
+        once a periodic check would fall inside a cycle, poll single steps
+        for the rest of the solve), then an asynchronous copy of the state."""
         b = self.batch
-        self.graph.replay()
+        if self.aligned and b.periodic_check_in(self.it + 1, self.it + b.restart_period - 1):
+            self.aligned = False
+        if self.aligned:
+            self.graph[1][0].replay()
+            self.it += b.restart_period
+        else:
+            b.iterate(self.poll, self.stream)
+            self.it += self.poll
         self.h_state.copy_(b.state, non_blocking=True)
         self.event.record(self.stream)
 

@@ -226,3 +226,18 @@ def test_vectors_to_host_single_copy_layout():
         for h, v in zip(hs, vs):
             np.testing.assert_array_equal(h, v.numpy())
     assert vectors_to_host([]) == []
+
+
+def test_periodic_check_schedule():
+    """The O(1) test for a periodic Ritz check inside a span of steps agrees
+    with stepping through the span (the state's count is i + 1 after step i)."""
+    from types import SimpleNamespace
+
+    from realspace_exatdiagonalization_py_b200.lanczos import LanczosBatch
+
+    for ce in range(1, 25):
+        stub = SimpleNamespace(p=SimpleNamespace(check_every=ce))
+        for first in range(0, 50):
+            for last in range(first - 2, first + 30):
+                want = any((i + 1) % ce == 0 for i in range(first, last + 1))
+                assert LanczosBatch.periodic_check_in(stub, first, last) == want
