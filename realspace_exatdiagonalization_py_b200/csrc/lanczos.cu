@@ -487,15 +487,36 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-__device__ int sturm_count(const double* dd, const double* ee, int M, double x, double pivmin) {
-  int c = 0;
-  double q = dd[0] - x;
-  if (fabs(q) < pivmin) q = -pivmin;
-  if (q < 0.0) ++c;
+// Number of eigenvalues of the symmetric tridiagonal (d, e) below x, by
+// Sturm's theorem on the leading principal minors p_{-1} = 1,
+// p_i = (d_i - x) p_{i-1} - e_{i-1}^2 p_{i-2} (the recurrence of Wilkinson's
+// bisection, 1962): a sign change between consecutive minors is a negative
+// pivot q_i = p_i / p_{i-1}, and the recurrence needs no division.
+// de[i] = (d_i, e_i^2) and x come scaled by one power of two so that
+// |d_i| + |e_i| <= 1 (exact: every sign and rounding is the unscaled one);
+// the two live minors are rescaled by a power of two whenever the newer one
+// leaves [2^-400, 2^400].  A minor that vanishes against its predecessor,
+// |p_i| < piv |p_{i-1}|, becomes -piv p_{i-1} (the pivmin rule of the ratio
+// form).  piv >= 2^-500 keeps piv |p_{i-1}| a normal number.
+__device__ int sturm_count(const double2* de, int M, double x, double piv) {
+  double pm = de[0].x - x;  // p_0
+  if (fabs(pm) < piv) pm = -piv;
+  int c = pm < 0.0;
+  double pmm = 1.0;  // p_{-1}
   for (int i = 1; i < M; ++i) {
-    q = dd[i] - x - ee[i - 1] * ee[i - 1] / q;
-    if (fabs(q) < pivmin) q = -pivmin;
-    if (q < 0.0) ++c;
+    const double2 v = de[i];
+    const double t = de[i - 1].y * pmm;
+    double p = fma(v.x - x, pm, -t);
+    if (fabs(p) < piv * fabs(pm)) p = -piv * pm;
+    c += (p < 0.0) != (pm < 0.0);
+    pmm = pm;
+    pm = p;
+    if (!(fabs(pm) <= 0x1p400 && fabs(pm) >= 0x1p-400)) {
+      int ex;
+      frexp(pm, &ex);
+      pm = ldexp(pm, -ex);
+      pmm = ldexp(pmm, -ex);
+    }
   }
   return c;
 }
@@ -637,6 +658,16 @@ __device__ void herm_lowest(double2* A, int M, int Kp, double* theta, double2* S
   }
   const double tnorm = fmax(fabs(lo), fabs(hi));
   const double pivmin = 1e-300 * fmax(1.0, emax2);
+  // (d_i, e_i^2) scaled by 2^-ks (|d_i| + |e_i| <= tnorm < 2^ks) into pw, free
+  // since the tridiagonalisation, for the division-free Sturm counts
+  int ks;
+  frexp(tnorm, &ks);
+  for (int i = tid; i < M; i += nt) {
+    const double es = ldexp(ee[i], -ks);
+    pw[i] = make_double2(ldexp(dd[i], -ks), es * es);
+  }
+  const double piv = fmax(ldexp(pivmin, -ks), 0x1p-500);
+  __syncthreads();
   {
     const int j = tid >> 4, sub = tid & 15;  // eigenvalue j, sample point sub
     double a = lo - 1e-12 * tnorm - 1e-300, bnd = hi + 1e-12 * tnorm + 1e-300;
@@ -647,7 +678,7 @@ __device__ void herm_lowest(double2* A, int M, int Kp, double* theta, double2* S
       if (__all_sync(0xffffffffu, bnd - a <= 4e-16 * fmax(fabs(a), fabs(bnd)) + pivmin)) break;
       const double w = (bnd - a) * (1.0 / 16.0);
       const double x = a + w * (sub + 1);
-      const int c = (j < Kp && sub < 15) ? sturm_count(dd, ee, M, x, pivmin) : 1 << 30;
+      const int c = (j < Kp && sub < 15) ? sturm_count(pw, M, ldexp(x, -ks), piv) : 1 << 30;
       // first sample whose count exceeds j bounds the eigenvalue from above
       const unsigned ballot = __ballot_sync(0xffffffffu, c > j);
       const unsigned mine = (ballot >> ((lane >> 4) << 4)) & 0xFFFFu;
