@@ -181,3 +181,34 @@ def test_large_site_count_rank():
     assert rr.min() == 0 and rr.max() == cat.n_orbits - 1
     counts = np.bincount(rr, minlength=cat.n_orbits)
     np.testing.assert_array_equal(counts, 24 // np.array(cat.stabilizer_order_list))
+
+
+def test_maximum_site_count():
+    """63 sites, the most a 64-bit mask holds (the reference's limit is the
+    same, n_site <= 63): fillings 2 and 61 under the cyclic group of order 7
+    generated by a shift of 9 sites, with random phases, for both statistics.
+    Every table entry equals the oracle's."""
+    import realspace_exatdiagonalization_py_b200 as ed
+    from oracle import port
+
+    n = 63
+    gen = (np.arange(n) + 9) % n
+    perms0 = [np.arange(n)]
+    while not np.array_equal(gen[perms0[-1]], perms0[0]):
+        perms0.append(gen[perms0[-1]])
+    assert len(perms0) == 7
+    rng = np.random.default_rng(3)
+    phases = [np.ones(n)] + [np.exp(2j * np.pi * rng.random(n)) for _ in range(len(perms0) - 1)]
+    ops = [ed.Symmetry_Operation(i, list(p + 1), perm_phases=e) for i, (p, e) in enumerate(zip(perms0, phases))]
+    G = ed.Finite_Symmetry_Group("shift9", ops)
+    perm0 = np.array(perms0, dtype=np.uint8)
+    for k, fermion in [(2, True), (61, False), (61, True)]:
+        stats = ed.Particle_Statistics.FERMIONIC if fermion else ed.Particle_Statistics.BOSONIC
+        cat = ed.build_symmetry_orbit_catalog(second_quantized_model=_Model(n), n_filled=k,
+                                              symmetry_group=G, particle_statistics=stats)
+        ref = port.catalog(n, k, perm0, np.array(phases, dtype=np.complex128), fermion)
+        assert cat.n_orbits == len(ref["reprs"]) == 279
+        np.testing.assert_array_equal(np.array(cat.representative_mask_list, dtype=np.uint64), ref["reprs"])
+        np.testing.assert_array_equal(cat.rep_rank_table, ref["rep_rank"])
+        np.testing.assert_array_equal(cat.rep_sym_table, ref["rep_sym"])
+        assert_amplitudes(cat.rep_amp_table, ref["rep_amp"])
