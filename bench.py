@@ -1,18 +1,22 @@
 #!/usr/bin/env python
 """Sector-solve throughput of the symmetry-resolved ED path on B200.
 
-Workload (default ``checkerboard24``): spinless fermions on the 3x4x2
-checkerboard (24 sites, 4 particles, 10,626 states, 892 orbits), translation
-group of order 12; one step = all 12 momentum sectors, lowest 6 eigenvalues
-each, solved in one batched block-Lanczos (FP32 matvec, FP64 recurrence and
-reorthogonalisation, FP64 refinement) to |dE| < 1e-10 against the CPU oracle.
+Workload (default ``haldane32``): hard-core bosons on the 4x4x2 Haldane
+honeycomb (32 sites, 8 bosons, 10,518,300 states, 657,756 orbits, t = 1,
+t' = 0.6 exp(+-0.4 pi i), V1 = 1, zero flux), translation group of order 16;
+one step = all 16 momentum sectors, lowest 4 eigenvalues each, solved in one
+batched block Lanczos (FP32 matvec, FP64 recurrence and reorthogonalisation,
+FP64 Rayleigh-Ritz refinement) to |dE| < 1e-10 against the reference's own
+ARPACK eigenvalues (tests/golden/haldane32.npz).  ``--workload
+checkerboard24`` selects the 24-site checkerboard fermions (12 sectors, nev 6).
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
 One JSON line on rank 0.  N > 1 runs independent replicas (one per GPU, no
 collective in the data path); ``value`` is the total over all ranks divided
-by the slowest rank's time.  ``--impl reference`` times the CPU restatement
-of the reference's numpy/ARPACK path on the host cores instead.
+by the slowest rank's time.  ``--impl reference`` times the reference's own
+numpy/scipy path (``ed_scan_at_irrep_matrixfree``: projection table, CSR,
+ARPACK) on the host cores instead.
 """
 
 from __future__ import annotations
@@ -24,6 +28,8 @@ for _v in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
     os.environ.setdefault(_v, str(_NCPU))
 
 import argparse  # noqa: E402
+import contextlib  # noqa: E402
+import io  # noqa: E402
 import json  # noqa: E402
 import statistics  # noqa: E402
 import subprocess  # noqa: E402
@@ -37,10 +43,21 @@ import numpy as np  # noqa: E402
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+HALDANE_PARAMS = {"t": 1.0, "t'": 0.6, "t''": 0.0, "phi_over_2pi": 0.2, "V1": 1.0, "V2": 0.0}
 WORKLOADS = {
-    "checkerboard24": dict(nev=6, desc="checkerboard 3x4x2, 24 sites, 4 fermions, |G|=12, 12 sectors"),
-    "heisenberg16": dict(nev=4, desc="Heisenberg ring N=16, 8 up spins, |G|=16, 16 sectors"),
+    "haldane32": dict(nev=4, golden="haldane32", golden_key="zf_eig",
+                      desc="Haldane bosons 4x4x2 = 32 sites, 8 bosons (nu = 1/2), t=1, t'=0.6 e^{+-0.4 pi i}, "
+                           "t''=0, V1=1, zero flux; C(32,8) = 10,518,300 states, 657,756 orbits, |G|=16, "
+                           "all 16 momentum sectors"),
+    "checkerboard24": dict(nev=6, golden="checkerboard24", golden_key="eig_vals",
+                           desc="checkerboard 3x4x2 = 24 sites, 4 fermions, |G|=12, all 12 sectors"),
+    "heisenberg16": dict(nev=4, golden="heisenberg16", golden_key="eig_vals",
+                         desc="Heisenberg ring N=16, 8 up spins, |G|=16, all 16 sectors"),
 }
+# DRAM bytes per launch of the dominant kernels from one ncu capture each
+# (dram__bytes_read.sum + dram__bytes_write.sum); the capture commands and the
+# workloads are in the named profiles/ summaries.
+NCU_TRAFFIC: dict = {}
 
 
 def _dist():
@@ -69,98 +86,170 @@ def replica_throughput(ws: int, units_per_rank: int, t_max: float) -> float:
     return ws * units_per_rank / t_max
 
 
+def golden_eigs(name: str):
+    """``{sector: lowest eigenvalues}`` of a workload from the reference's own
+    ARPACK results committed under tests/golden (None if absent)."""
+    wl = WORKLOADS[name]
+    path = os.path.join(ROOT, "tests", "golden", wl["golden"] + ".npz")
+    if not os.path.isfile(path):
+        return None
+    f = np.load(path)
+    vals = f[wl["golden_key"]]
+    secs = f["eig_sectors"] if "eig_sectors" in f else np.arange(len(vals))
+    return {int(s): np.asarray(v, dtype=np.float64) for s, v in zip(secs, vals)}
+
+
 # ---------------------------------------------------------------------------
-# CPU side: the oracle (restatement of the reference's numpy/scipy path)
+# CPU side: the reference's own numpy/scipy path (or the oracle port)
 # ---------------------------------------------------------------------------
 
 
-def cpu_sector_solves(model, n_filled, G, irreps, nev, budget_s=20.0, min_sectors=3, cat=None):
-    """Time the reference algorithm (projection table + CSR + ARPACK per
-    sector, catalog built outside the timing as in the reference benchmark)
-    on a bounded sample of sectors; returns (solves/s, n_timed, eigvals)."""
-    from oracle import port
+def _reference_model(R, name):
+    """The workload's model built by the reference's own model builders."""
+    if name == "haldane32":
+        return R.bosonic.build_zero_flux_bosonic_fci_second_quantized_model(
+            sample_size=[4, 4], params=dict(HALDANE_PARAMS)), 8
+    if name == "checkerboard24":
+        p = dict(R.fermionic.params_Sun_Gu_Katsura_Sarma)
+        p.update({"V1": 1.0, "V2": 0.0, "V3": 0.0})
+        with contextlib.redirect_stdout(io.StringIO()):
+            return R.fermionic.build_zero_flux_fermionic_fci_second_quantized_model(
+                sample_size=[3, 4], params=p), 4
+    if name == "heisenberg16":
+        with contextlib.redirect_stdout(io.StringIO()):
+            return R.heisenberg.build_heisenberg_second_quantized_model(16, 1.0), 8
+    raise ValueError(name)
 
-    n = G.n_site
-    fermion = model.particle_statistics.name == "FERMIONIC"
-    if cat is None:
-        perm0, eta = port.group_arrays(G)
-        cat = port.catalog(n, n_filled, perm0, eta, fermion)
-    # sectors in order, cycling through the workload again until the budget
-    # is spent (a bounded sample of about budget_s seconds of host work)
-    t_all, done, vals = 0.0, 0, {}
-    s = 0
-    while t_all < budget_s or done < min_sectors:
-        chi = np.asarray(irreps[s].values, dtype=np.complex128)
+
+class CpuSectorSolver:
+    """Times whole sector solves of a workload on the host cores.
+
+    ``kind == "reference"``: the reference package itself (installed under
+    baseline/_ref by oracle/install_reference.py, loaded through
+    oracle/ref_shim.py), one ``ed_scan_at_irrep_matrixfree(label, ed_data,
+    nev)`` per sector -- its projection table, CSR and ARPACK ``eigs``, the
+    unit its own benchmark times.  ``kind == "port"``: the oracle's
+    restatement of the same steps, used only where the reference package is
+    absent.  The orbit catalog is built once in the constructor (untimed, as
+    in the reference's benchmark)."""
+
+    # below this sector size the reference's ARPACK/BLAS calls are tiny and
+    # multi-threaded BLAS only adds synchronisation (measured: 0.055 s per
+    # 892-row sector with one thread, 0.2-7 s with eight); above it all cores
+    # help (657,756 rows: 45 s with eight threads, 50 s with one)
+    SMALL_SECTOR = 20000
+
+    def __init__(self, name: str, nev: int):
+        from oracle import ref_shim
+
+        self.name, self.nev = name, nev
         t0 = time.perf_counter()
-        orbits = port.sector_orbits(cat, chi)
-        H = port.csr_block(cat, n, orbits, model.bilinear_terms, model.density_density_terms, chi, fermion)
-        w, _ = port.solve(H, nev)
-        t_all += time.perf_counter() - t0
-        vals[s] = w
-        done += 1
-        s = (s + 1) % len(irreps)
-    return done / t_all, done, vals, t_all
+        if ref_shim.available():
+            self.kind = "reference"
+            R = ref_shim.load()
+            self.sre = R.sre
+            model, nf = _reference_model(R, name)
+            G = R.sre.build_translation_group(model.lattice, None)
+            with contextlib.redirect_stdout(io.StringIO()):
+                self.data = R.sre.build_ed_data(model, filling_fraction=Fraction(nf, model.lattice.n_site),
+                                                symmetry_group=G)
+            self.labels = [ir.label for ir in self.data.irrep_list]
+        else:
+            from oracle import port
+            from realspace_exatdiagonalization_py_b200 import models
+            import realspace_exatdiagonalization_py_b200.symmetry as sym
 
+            self.kind = "port"
+            model, nf = models.config_model(name)
+            G = sym.build_translation_group(model.lattice)
+            self.irreps = sym.build_irrep_list(G, model.lattice)
+            self.model, self.n = model, G.n_site
+            self.fermion = model.particle_statistics.name == "FERMIONIC"
+            perm0, eta = port.group_arrays(G)
+            self.cat = port.catalog(G.n_site, nf, perm0, eta, self.fermion)
+            self.labels = [ir.label for ir in self.irreps]
+        self.catalog_s = time.perf_counter() - t0
+        n_orb = (len(self.data.orbit_catalog.representative_mask_list) if self.kind == "reference"
+                 else len(self.cat["reprs"]))
+        self.threads = 1 if n_orb < self.SMALL_SECTOR else _NCPU
 
-def oracle_eigs(model, n_filled, G, irreps, nev):
-    from oracle import port
+    def solve(self, s: int) -> tuple[np.ndarray, float]:
+        """Eigenvalues of sector ``s`` and the seconds the solve took."""
+        from threadpoolctl import threadpool_limits
 
-    fermion = model.particle_statistics.name == "FERMIONIC"
-    perm0, eta = port.group_arrays(G)
-    cat = port.catalog(G.n_site, n_filled, perm0, eta, fermion)
-    out = {}
-    for s, ir in enumerate(irreps):
-        chi = np.asarray(ir.values, dtype=np.complex128)
-        orbits = port.sector_orbits(cat, chi)
-        H = port.csr_block(cat, G.n_site, orbits, model.bilinear_terms, model.density_density_terms, chi,
-                           fermion)
-        out[s] = port.solve(H, nev)[0]
-    return out
+        with threadpool_limits(limits=self.threads):
+            return self._solve(s)
+
+    def _solve(self, s: int) -> tuple[np.ndarray, float]:
+        t0 = time.perf_counter()
+        if self.kind == "reference":
+            with contextlib.redirect_stdout(io.StringIO()):
+                w, _ = self.sre.ed_scan_at_irrep_matrixfree(self.labels[s], self.data, nev=self.nev)
+        else:
+            from oracle import port
+
+            chi = np.asarray(self.irreps[s].values, dtype=np.complex128)
+            orbits = port.sector_orbits(self.cat, chi)
+            H = port.csr_block(self.cat, self.n, orbits, self.model.bilinear_terms,
+                               self.model.density_density_terms, chi, self.fermion)
+            w, _ = port.solve(H, self.nev)
+        return np.asarray(w, dtype=np.float64), time.perf_counter() - t0
+
+    def sample(self, budget_s: float, min_solves: int = 1, start: int = 0):
+        """Sector solves in order (from ``start``, cycling) until ``budget_s``
+        seconds of solving are spent; returns (solves/s, solves, seconds,
+        {sector: eigenvalues})."""
+        t_all, done, vals = 0.0, 0, {}
+        s = start % len(self.labels)
+        while t_all < budget_s or done < min_solves:
+            w, t = self.solve(s)
+            t_all += t
+            vals[s] = w
+            done += 1
+            s = (s + 1) % len(self.labels)
+        return done / t_all, done, t_all, vals
 
 
 def run_reference(args):
+    """``--impl reference``: the reference's own path on the host cores, on
+    rank 0 only (the other ranks exit without work).  One reference sector
+    solve of the 32-site workload takes tens of seconds, so the arm times
+    whole sector solves until ``--ref-budget`` seconds are spent (at least
+    one) instead of ``--steps`` full steps of 16 sectors each; ``ms_per_step``
+    is the measured time per sector times the sectors of one step."""
     ws, rank, _ = _dist()
     if rank != 0:
         return
-    from realspace_exatdiagonalization_py_b200 import models
-    import realspace_exatdiagonalization_py_b200.symmetry as sym
-
     wl = WORKLOADS[args.workload]
-    model, nf = models.config_model(args.workload)
-    G = sym.build_translation_group(model.lattice)
-    irreps = sym.build_irrep_list(G, model.lattice)
-    from oracle import port
-
-    perm0, eta = port.group_arrays(G)
-    cat = port.catalog(G.n_site, nf, perm0, eta, model.particle_statistics.name == "FERMIONIC")
-    per_step = []
-    for it in range(args.warmup + args.steps):
-        rate, n_done, _, t = cpu_sector_solves(model, nf, G, irreps, wl["nev"], budget_s=4.0, min_sectors=2,
-                                               cat=cat)
-        if it >= args.warmup:
-            per_step.append((n_done, t))
-    tot_n = sum(n for n, _ in per_step)
-    tot_t = sum(t for _, t in per_step)
-    val = tot_n / tot_t
+    cpu = CpuSectorSolver(args.workload, wl["nev"])
+    n_sec = len(cpu.labels)
+    budget = getattr(args, "ref_budget", 150.0)
+    if args.workload != "haldane32":
+        budget = min(budget, 4.0 * max(1, args.steps))
+    rate, n_done, t, _ = cpu.sample(budget, min_solves=1)
     line = {
         "impl": "reference",
         "metric": "sector-solves/s",
-        "value": val,
+        "value": rate,
         "unit": "sector-solves/s",
         "n_gpus": args.gpus,
         "steps": args.steps,
         "warmup": args.warmup,
-        "ms_per_step": 1e3 * tot_t / len(per_step),
+        "ms_per_step": 1e3 * n_sec / rate,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": args.workload, "desc": wl["desc"], "nev": wl["nev"],
-                   "step": "bounded sample of sectors: projection table + CSR + ARPACK eigs(which=SR)"},
-        "cpu_baseline": {"value": val, "unit": "sector-solves/s", "cores": _NCPU, "kind": "port",
-                         "sample": f"{tot_n} sector solves over {args.steps} steps (catalog built once, untimed)"},
-        "e2e": {"value": val, "unit": "sector-solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "config": {"workload": args.workload, "desc": wl["desc"], "nev": wl["nev"], "sectors_per_step": n_sec,
+                   "step": "one sector solve = ed_scan_at_irrep_matrixfree (projection table + CSR + "
+                           "ARPACK eigs(which='SR', tol=1e-10)); ms_per_step = seconds per sector x sectors"},
+        "cpu_baseline": {"value": rate, "unit": "sector-solves/s", "cores": cpu.threads, "kind": cpu.kind,
+                         "sample": f"{n_done} whole sector solve(s) in {t:.1f} s, sectors in order from 0 "
+                                   f"(the reference's catalog built once in {cpu.catalog_s:.1f} s, untimed); "
+                                   f"the arm times solves up to a {budget:.0f} s budget rather than "
+                                   f"{args.steps} steps of {n_sec} sectors"},
+        "e2e": {"value": rate, "unit": "sector-solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
@@ -225,7 +314,7 @@ class ClockSampler:
 
 
 def sector_matvec_bytes(dm, sset, col_sector, x_bytes):
-    """Algorithmic bytes of one apply over the given columns: per column
+    """Survey per-unit bytes of one apply over the given columns: per column
     (one sector matvec) D_s * (8 + 2 s) + H_s * 16 -- the representative
     mask, x read and y write per row and one 16-B table entry per hop of the
     sector's rows.  H_s comes from the projection table's row lengths."""
@@ -241,6 +330,80 @@ def sector_matvec_bytes(dm, sset, col_sector, x_bytes):
         h = float(hops_row[on].sum().item())
         total += d * (8 + 2 * x_bytes) + h * 16
     return total
+
+
+def proj_apply_unique_bytes(n_hops: int, n_orb: int, n_cols: int, prec: int) -> int:
+    """Bytes one projection-table apply must move at least once: the table
+    (per hop the 4-B target/group word and the 8-B or 16-B weight, 8-B row
+    offsets), per row the 8-B sector membership and the 16-B diagonal, x read
+    once (8 or 16 B per element) and y written once (16 B per element)."""
+    wb = 8 if prec == 32 else 16
+    return n_hops * (4 + wb) + (n_orb + 1) * 8 + n_orb * (8 + 16) + n_orb * n_cols * (wb + 16)
+
+
+def lanczos_step_bytes(n_orb: int, batch, iters: list[int]) -> dict:
+    """Algorithmic bytes of the Gram reductions and the block updates of one
+    batched solve, from each instance's iteration count.  After
+    ``rsed_lanczos_start`` the basis holds 1 block; iteration k (1-based)
+    reduces against the current nb blocks and appends one; at nb = n_slots + 1
+    a thick restart leaves keep + 1.  Per instance (b columns, 16-B complex128
+    entries, all n_orb rows of the orbit layout) and iteration with basis
+    length nb, each of the two passes: the reduction reads the nb blocks and W
+    once ((nb + 1) n b 16 B); the update reads them once and writes W (pass 1)
+    or the new basis block (pass 2) once ((nb + 2) n b 16 B), plus the FP32
+    copy of the new block (n b 8 B) in an FP32-matvec solve."""
+    S, keep = batch.p.n_slots, batch.keep
+    red = upd = 0
+    for b, it in zip(batch.block_sizes, iters):
+        nb = 1
+        for _ in range(it):
+            blk = n_orb * b * 16
+            red += 2 * (nb + 1) * blk
+            upd += 2 * (nb + 2) * blk + (n_orb * b * 8 if batch.p.precision == 32 else 0)
+            nb += 1
+            if nb == S + 1:
+                nb = keep + 1
+    return {"reduce": red, "update": upd}
+
+
+def cupti_kernels(step):
+    """Device time per kernel over one (untimed) call of ``step``, from CUPTI
+    through torch.profiler: {kernel name: [launches, total_us]}."""
+    from torch.profiler import ProfilerActivity, profile
+
+    import torch
+
+    torch.cuda.synchronize()
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        step()
+        torch.cuda.synchronize()
+    agg = {}
+    for ev in prof.events():
+        if ev.device_type.name != "CUDA":
+            continue
+        name = ev.name.replace("(anonymous namespace)::", "").replace("<unnamed>::", "").replace("void ", "")
+        if "(" in name:
+            name = name.split("(")[0]
+        a = agg.setdefault(name, [0, 0.0])
+        a[0] += 1
+        a[1] += ev.device_time_total
+    return agg
+
+
+def kernel_shares(agg, top=10):
+    tot = sum(v[1] for v in agg.values()) or 1.0
+    rows = sorted(agg.items(), key=lambda kv: -kv[1][1])[:top]
+    return [{"kernel": k, "launches": v[0], "total_us": round(v[1], 1), "share": round(v[1] / tot, 4)}
+            for k, v in rows]
+
+
+def _family(agg, prefix, contains=""):
+    n = us = 0.0
+    for k, (c, t) in agg.items():
+        if k.startswith(prefix) and contains in k:
+            n += c
+            us += t
+    return int(n), us
 
 
 def _zero_outside(X, sset, col_sector):
@@ -266,25 +429,6 @@ def time_apply(dm, sset, cs, X, Y, prec, variant, n_launch, warm=3):
     e1.record()
     torch.cuda.synchronize()
     return e0.elapsed_time(e1) / n_launch * 1e-3
-
-
-def apply_roofline(ed, data, sset, solver, peak_gbs, n_launch=200):
-    """The batch's FP32 matvec (all columns of the bench workload) timed with
-    CUDA events, against the per-sector-matvec algorithmic bytes."""
-    import torch
-
-    dm, _ = data._device()
-    b = solver.batch
-    n_orb = data.orbit_catalog.n_orbits
-    X = _zero_outside(torch.randn((n_orb, b.ld), dtype=torch.complex64, device="cuda"), sset, b.col_sector)
-    Y = torch.empty((n_orb, b.ld), dtype=torch.complex128, device="cuda")
-    t = time_apply(dm, sset, b.col_sector, X, Y, 32, 0, n_launch, warm=5)
-    alg = sector_matvec_bytes(dm, sset, b.col_sector, 8)
-    ach = alg / t / 1e9
-    return {"kernel": "k_proj_spmv<32,*> (rsed_apply_h, projection table)", "bound": "hbm",
-            "achieved": ach, "peak": peak_gbs, "unit": "GB/s", "frac": ach / peak_gbs, "traffic": None,
-            "alg_bytes_per_launch": alg, "avg_launch_us": t * 1e6, "hops_per_launch": dm.proj["n_hops"],
-            "columns": b.n_cols, "note": "latency-bound size (892 orbits): see matvec_at_scale"}
 
 
 def matvec_at_scale(ed, models, peak_gbs, n_launch=20, precisions=(32, 64), per_sector=4, otf=True):
@@ -345,7 +489,7 @@ def serving_at_scale(ed, models, n_req=32, rate=20.0, block=2, plain_samples=2):
     of (sector, flux) requests over a 16 x 16 flux grid and 16 sectors,
     served with continuous batching (FP32 matvec + FP64 refinement, nev 4),
     against the plain FP64 path (one request at a time, block 1, no graph,
-    host polling every iteration) on the first requests of the stream."""
+    the solver's default check schedule) on the first requests of the stream."""
     import torch
     from realspace_exatdiagonalization_py_b200.serving import poisson_requests
 
@@ -380,13 +524,13 @@ def serving_at_scale(ed, models, n_req=32, rate=20.0, block=2, plain_samples=2):
     plain_t, dE = [], []
     for r in reqs[:plain_samples]:
         ctx = ed.FluxContext(sm, sm.normalize_flux(r.flux), 64)
-        p = ed.LanczosParams(block=1, n_slots=48, precision=64, check_every=1)
+        p = ed.LanczosParams(block=1, precision=64)
         b = ed.LanczosBatch(ctx.dm, ctx.sset, [r.sector], 4, p)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         b.load_start(None)
         b.start()
-        b.run(poll=1, graph=False)
+        b.run(graph=False)
         torch.cuda.synchronize()
         plain_t.append(time.perf_counter() - t0)
         dE.append(float(np.max(np.abs(b.eigenvalues()[0] - by_id[r.rid].eigenvalues))))
@@ -647,31 +791,54 @@ def model_basis_size(model, nf):
     return math.comb(model.lattice.n_site, nf)
 
 
-def step_kernel_shares(step, top=10):
-    """Device time per kernel over one (untimed) step, from CUPTI through
-    torch.profiler: [{kernel, launches, total_us, share}] sorted by time."""
-    from torch.profiler import ProfilerActivity, profile
+def _load_peaks():
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        peaks = {}
+    if "hbm_gbs" in peaks:
+        return float(peaks["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    return 6650.0, "fallback (6.65 TB/s, no MEASURED_PEAKS.json)"
 
+
+def small_config_line(ed, models, name, precision=32, steps=10):
+    """A short batched run of a small workload (all sectors, autotuned) with
+    parity against the reference's goldens: the latency-bound end of the
+    range, beside the HBM-bound headline."""
     import torch
+    from realspace_exatdiagonalization_py_b200.batched import BatchedSectorSolver
 
-    torch.cuda.synchronize()
-    with profile(activities=[ProfilerActivity.CUDA]) as prof:
-        step()
+    wl = WORKLOADS[name]
+    nev = wl["nev"]
+    model, nf = models.config_model(name)
+    G = ed.build_translation_group(model.lattice)
+    data = ed.build_ed_data(model, filling_fraction=Fraction(nf, model.lattice.n_site), symmetry_group=G)
+    dm, sset = data._device()
+    dm.build_projection(sset.sqrt_stab)
+    sectors = list(range(len(data.irrep_list)))
+    params = ed.LanczosParams(precision=precision)
+    config, _ = ed.Autotuner(trials=2).tune(dm, sset, sectors, nev, precision=precision, params=params)
+    solver = BatchedSectorSolver(dm, sset, sectors, nev, precision=precision, params=params, config=config)
+    blocks = [torch.from_numpy(ed.lanczos.start_block(sset.dims[s], solver.batch.block_sizes[i], 12345 + s)).cuda()
+              for i, s in enumerate(sectors)]
+    for _ in range(3):
+        solver.solve(blocks, vectors=False, host=False)
+    ref = golden_eigs(name)
+    times, de = [], 0.0
+    for _ in range(steps):
         torch.cuda.synchronize()
-    agg = {}
-    for ev in prof.events():
-        if ev.device_type.name != "CUDA":
-            continue
-        name = ev.name.replace("(anonymous namespace)::", "").replace("<unnamed>::", "").replace("void ", "")
-        if "(" in name:
-            name = name.split("(")[0]
-        a = agg.setdefault(name, [0, 0.0])
-        a[0] += 1
-        a[1] += ev.device_time_total
-    tot = sum(v[1] for v in agg.values()) or 1.0
-    rows = sorted(agg.items(), key=lambda kv: -kv[1][1])[:top]
-    return [{"kernel": k, "launches": v[0], "total_us": round(v[1], 1), "share": round(v[1] / tot, 4)}
-            for k, v in rows]
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        vals, _ = solver.solve(blocks, vectors=False, host=False)
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1) * 1e-3)
+        v = vals.cpu().numpy()
+        if ref is not None:
+            de = max(de, max(float(np.max(np.abs(v[i] - ref[s][:nev]))) for i, s in enumerate(sectors)))
+    return {"workload": name, "desc": wl["desc"], "nev": nev, "precision": precision,
+            "solver": config.describe(), "sector_solves_per_s": len(sectors) * steps / sum(times),
+            "ms_per_step": 1e3 * sum(times) / steps, "max_abs_dE_vs_reference": de if ref is not None else None}
 
 
 def run_b200(args):
@@ -687,29 +854,30 @@ def run_b200(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     import realspace_exatdiagonalization_py_b200 as ed
     from realspace_exatdiagonalization_py_b200 import _lib, models
-    from realspace_exatdiagonalization_py_b200.batched import BatchedSectorSolver
+    from realspace_exatdiagonalization_py_b200.batched import BatchedSectorSolver, projection_precisions
 
-    peaks = {}
-    try:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-    except OSError:
-        pass
-    peak_gbs = float(peaks.get("hbm_gbs", 6650.0))
-    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
-
+    peak_gbs, peak_src = _load_peaks()
     wl = WORKLOADS[args.workload]
     nev = wl["nev"]
     model, nf = models.config_model(args.workload)
     G = ed.build_translation_group(model.lattice)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
     data = ed.build_ed_data(model, filling_fraction=Fraction(nf, model.lattice.n_site), symmetry_group=G)
     dm, sset = data._device()
-    dm.build_projection(sset.sqrt_stab)
+    torch.cuda.synchronize()
+    t_cat = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    dm.build_projection(sset.sqrt_stab, precisions=projection_precisions(dm, args.precision))
+    torch.cuda.synchronize()
+    t_proj = time.perf_counter() - t0
     sectors = list(range(len(data.irrep_list)))
     n_sec = len(sectors)
+    n_orb = data.orbit_catalog.n_orbits
     assert all(d > 500 for d in sset.dims), "bench workload expects every sector on the Lanczos path"
 
     # how the batch runs (block sizes, persistent cluster or graph path,
-    # projection table) is picked by the autotuner, untimed, before warm-up
+    # projection table, basis length) is picked by the autotuner, untimed
     params = ed.LanczosParams(precision=args.precision)
     tuner = ed.Autotuner(trials=2)
     t0 = time.perf_counter()
@@ -722,14 +890,11 @@ def run_b200(args):
     tune_s = time.perf_counter() - t0
     solver = BatchedSectorSolver(dm, sset, sectors, nev, precision=args.precision, params=params, config=config)
     b = solver.batch
-    host_blocks = [ed.lanczos.start_block(sset.dims[s], b.block_sizes[i], 12345 + s)
-                   for i, s in enumerate(sectors)]
+    host_blocks = [ed.lanczos.start_block(sset.dims[s], b.block_sizes[i], 12345 + s) for i, s in enumerate(sectors)]
     dev_blocks = [torch.from_numpy(x).cuda() for x in host_blocks]
     pinned_blocks = [torch.from_numpy(x).pin_memory() for x in host_blocks]
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-
-    # oracle eigenvalues (|dE| check of every step's result)
-    ref = oracle_eigs(model, nf, G, data.irrep_list, nev) if rank == 0 else None
+    ref = golden_eigs(args.workload) if rank == 0 else None
 
     def step():
         return solver.solve(dev_blocks, vectors=False, host=False)
@@ -760,16 +925,22 @@ def run_b200(args):
             if ref is not None:
                 v = vals.cpu().numpy()
                 max_de = max(max_de, max(float(np.max(np.abs(v[i] - ref[s][:nev]))) for i, s in enumerate(sectors)))
-    shares = step_kernel_shares(step) if rank == 0 else None
+    if ws > 1:
+        torch.distributed.barrier()
     t_step = max_over_ranks(float(np.sum(times)), ws)
     value = replica_throughput(ws, n_sec * args.steps, t_step)
     lat = sorted(times)
+    st = b.status()
+    iters = [int(x) - 1 for x in st[:, 3]]
+    fe = solver.fp32_error()
+    resid_max = float(solver.residuals().max())
 
     # e2e through the public API: pinned host start blocks in, numpy eigenpairs out
     e2e_times = []
     h2d = sum(x.numel() * 16 for x in pinned_blocks)
     d2h = 0
-    for it in range(args.warmup + args.steps):
+    e2e_de = 0.0
+    for it in range(min(args.warmup, 2) + args.steps):
         flush.zero_()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -778,99 +949,144 @@ def run_b200(args):
                                        start_blocks=pinned_blocks, config=config)
         e1.record()
         torch.cuda.synchronize()
-        if it >= args.warmup:
+        if it >= min(args.warmup, 2):
             e2e_times.append(e0.elapsed_time(e1) * 1e-3)
         d2h = sum(res[s][0].nbytes + res[s][1].nbytes for s in sectors)
+        if ref is not None:
+            e2e_de = max(e2e_de, max(float(np.max(np.abs(res[s][0] - ref[s][:nev]))) for s in sectors))
+    data.__dict__.pop("_solvers", None)
+    torch.cuda.empty_cache()
+    if ws > 1:
+        torch.distributed.barrier()
     e2e_val = replica_throughput(ws, n_sec * len(e2e_times), max_over_ranks(sum(e2e_times), ws))
 
-    extra = {}
+    extra = {"setup_s": {"catalog": t_cat, "projection_table": t_proj, "autotune": tune_s,
+                         "note": "untimed: the catalog and the projection table are built once per catalog and "
+                                 "shared by all sectors and steps"}}
+    roof = None
     if rank == 0:
-        # plain FP64 GPU path: one sector at a time, block 1, no graph, host
-        # polling every iteration
-        p_plain = ed.LanczosParams(block=1, n_slots=48, precision=64, check_every=1)
-        plain_t = []
-        for s in sectors[: max(3, min(n_sec, args.plain_sectors))]:
+        # per-kernel device time of one step (CUPTI) and algorithmic bytes
+        agg = cupti_kernels(step)
+        extra["step_kernel_shares"] = kernel_shares(agg)
+        fams = {}
+        nh = dm.proj["n_hops"]
+        n_mv, us_mv = _family(agg, "k_proj_spmv<" + str(args.precision))
+        if n_mv:
+            fams["k_proj_spmv<%d>" % args.precision] = {
+                "kernel": f"k_proj_spmv<{args.precision},...> (FP{args.precision} projection-table matvec, all "
+                          f"{b.n_cols} columns of the batch)",
+                "launches": n_mv, "avg_launch_us": us_mv / n_mv,
+                "alg_bytes_per_launch": proj_apply_unique_bytes(nh, n_orb, b.n_cols, args.precision),
+                "unit_bytes": "per hop 4 + 8 B table, per row 8 + 8 + 16 B, per element x 8 B + y 16 B, once each"}
+        lb = lanczos_step_bytes(n_orb, b, iters)
+        for key, fam in (("reduce", "k_lz_reduce"), ("update", "k_lz_update")):
+            n_k, us_k = _family(agg, fam)
+            if n_k:
+                fams[fam] = {"kernel": f"{fam}* (FP64 block Gram-Schmidt, two passes per iteration)",
+                             "launches": n_k, "avg_launch_us": us_k / n_k,
+                             "alg_bytes_per_launch": lb[key] / n_k,
+                             "unit_bytes": "per pass (nb + 1) resp. (nb + 2) basis blocks of n_orb x b x 16 B"}
+        for k, f in fams.items():
+            f["achieved_GBs"] = f["alg_bytes_per_launch"] / (f["avg_launch_us"] * 1e-6) / 1e9
+            f["frac"] = f["achieved_GBs"] / peak_gbs
+            f["share_of_step"] = f["avg_launch_us"] * f["launches"] / max(1e-9, sum(v[1] for v in agg.values()))
+        extra["kernel_rooflines"] = fams
+        if fams:
+            top = max(fams, key=lambda k: fams[k]["share_of_step"])
+            f = fams[top]
+            tr = NCU_TRAFFIC.get((args.workload, top))
+            roof = {"bound": "hbm", "achieved": f["achieved_GBs"], "peak": peak_gbs, "unit": "GB/s",
+                    "frac": f["frac"], "traffic": None if tr is None else tr["bytes_per_launch"],
+                    "kernel": f["kernel"], "avg_launch_us": f["avg_launch_us"],
+                    "alg_bytes_per_launch": f["alg_bytes_per_launch"], "timing": "CUPTI kernel durations, one step",
+                    "peak_source": peak_src, "share_of_step": f["share_of_step"]}
+            if tr is not None:
+                roof["traffic_source"] = tr["profile"]
+        extra["lanczos_iterations"] = {"min": min(iters), "max": max(iters)}
+        extra["residual_norm_max"] = resid_max
+        if fe is not None:
+            extra["fp32_matvec_error_before_refinement"] = {"max": float(fe.max()), "median": float(np.median(fe))}
+        extra["autotune"] = {"chosen": config.describe(), "tune_s": tune_s,
+                             "candidates": [{"config": r["config"], "solve_ms": None if r["time_s"] is None
+                                             else 1e3 * r["time_s"], "ok": r["ok"]} for r in tune_table]}
+        # plain FP64 GPU path: one sector at a time, block 1, FP64 matvec, no
+        # graph, the solver's default check schedule (Ritz checks at restarts)
+        p_plain = ed.LanczosParams(block=1, precision=64)
+        plain_t, plain_de = [], 0.0
+        for s in sectors[: max(1, min(n_sec, args.plain_sectors))]:
             pb = ed.LanczosBatch(dm, sset, [s], nev, p_plain)
             torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
             pb.load_start([dev_blocks[s][:, :1]])
             pb.start()
-            pb.run(poll=1, graph=False)
+            pb.run(graph=False)
             e1.record()
             torch.cuda.synchronize()
             plain_t.append(e0.elapsed_time(e1) * 1e-3)
             if ref is not None:
-                max_de_plain = float(np.max(np.abs(pb.eigenvalues()[0] - ref[s][:nev])))
-                extra.setdefault("plain_fp64_max_abs_dE", 0.0)
-                extra["plain_fp64_max_abs_dE"] = max(extra["plain_fp64_max_abs_dE"], max_de_plain)
+                plain_de = max(plain_de, float(np.max(np.abs(pb.eigenvalues()[0] - ref[s][:nev]))))
+            del pb
         plain_rate = len(plain_t) / sum(plain_t)
         ps = sorted(plain_t)
         extra.update({
-            "plain_fp64_sector_solves_per_s": plain_rate,
-            "plain_fp64_latency_ms": {"p50": 1e3 * ps[len(ps) // 2], "p99": 1e3 * ps[-1]},
+            "plain_fp64": {"sector_solves_per_s": plain_rate, "sectors_timed": len(plain_t),
+                           "latency_ms": {"p50": 1e3 * ps[len(ps) // 2], "p99": 1e3 * ps[-1]},
+                           "max_abs_dE_vs_reference": plain_de if ref is not None else None,
+                           "path": "one sector per solve, block 1, FP64 projection-table matvec, no graph, "
+                                   "default check schedule"},
             "batched_over_plain": value / ws / plain_rate,
+            "e2e_over_plain": e2e_val / ws / plain_rate,
         })
-    # with several ranks the others wait in the closing barrier: only the
-    # N = 1 run carries the longer diagnostics and the CPU baseline
+        torch.cuda.empty_cache()
+    # only the N = 1 run carries the longer diagnostics and the CPU baseline,
+    # so no rank waits in the closing barrier for rank 0's extra work
+    cpu_base = None
     if rank == 0 and ws == 1:
-        # FP64-matvec batched variant (its own tuned configuration)
-        cfg64 = config if args.solver != "auto" else tuner.tune(
-            dm, sset, sectors, nev, precision=64, params=ed.LanczosParams(precision=64))[0]
-        extra["fp64_batched_config"] = cfg64.describe()
-        s64 = BatchedSectorSolver(dm, sset, sectors, nev, precision=64,
-                                  params=ed.LanczosParams(precision=64), config=cfg64)
-        for _ in range(2):
-            s64.solve(None, vectors=False, host=False)
-        t64 = []
-        for _ in range(max(3, args.steps // 2)):
-            torch.cuda.synchronize()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            v64, _ = s64.solve(None, vectors=False, host=False)
-            e1.record()
-            torch.cuda.synchronize()
-            t64.append(e0.elapsed_time(e1) * 1e-3)
-        extra["fp64_batched_sector_solves_per_s"] = n_sec * len(t64) / sum(t64)
-        extra["fp64_batched_max_abs_dE"] = max(float(np.max(np.abs(v64.cpu().numpy()[i] - ref[s][:nev])))
-                                               for i, s in enumerate(sectors))
-        fe = solver.fp32_error()
-        if fe is not None:
-            extra["fp32_matvec_error_before_refinement"] = {"max": float(fe.max()), "median": float(np.median(fe))}
+        if not args.skip_fp64:
+            s64 = BatchedSectorSolver(dm, sset, sectors, nev, precision=64,
+                                      params=ed.LanczosParams(precision=64), config=config)
+            s64.solve(dev_blocks, vectors=False, host=False)
+            t64 = []
+            for _ in range(3):
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                v64, _ = s64.solve(dev_blocks, vectors=False, host=False)
+                e1.record()
+                torch.cuda.synchronize()
+                t64.append(e0.elapsed_time(e1) * 1e-3)
+            extra["fp64_batched"] = {"sector_solves_per_s": n_sec * len(t64) / sum(t64), "config": config.describe(),
+                                     "max_abs_dE_vs_reference": None if ref is None else max(
+                                         float(np.max(np.abs(v64.cpu().numpy()[i] - ref[s][:nev])))
+                                         for i, s in enumerate(sectors))}
+            del s64
+        del solver
+        torch.cuda.empty_cache()
+        if not args.skip_scale:
+            for key, fn in (("serving_at_scale", lambda: serving_at_scale(ed, models)),
+                            ("config2_checkerboard24", lambda: small_config_line(ed, models, "checkerboard24")),
+                            ("reference_benchmark", lambda: reference_benchmark(ed, models))):
+                if key == "config2_checkerboard24" and args.workload == "checkerboard24":
+                    continue
+                try:
+                    extra[key] = fn()
+                except Exception as exc:  # noqa: BLE001 - reported, not fatal
+                    extra[key] = {"error": repr(exc)}
+                torch.cuda.empty_cache()
+        # CPU baseline: the reference's own path on the host cores, N = 1 only
+        cpu = CpuSectorSolver(args.workload, nev)
+        rate, n_done, t_cpu, cvals = cpu.sample(args.cpu_budget, min_solves=1)
+        cpu_de = None
+        if ref is not None:
+            cpu_de = max(float(np.max(np.abs(cvals[s][:nev] - ref[s][:nev]))) for s in cvals)
+        cpu_base = {"value": rate, "unit": "sector-solves/s", "cores": cpu.threads, "kind": cpu.kind,
+                    "sample": f"{n_done} whole sector solve(s) of this workload in {t_cpu:.1f} s: "
+                              + ("the reference's ed_scan_at_irrep_matrixfree (projection table + CSR + ARPACK)"
+                                 if cpu.kind == "reference" else "the oracle port of the reference's steps")
+                              + f", catalog built once ({cpu.catalog_s:.1f} s, untimed)",
+                    "max_abs_dE_vs_golden": cpu_de}
     if rank == 0:
-        extra["residual_norm_max"] = float(solver.residuals().max())
-        extra["step_kernel_shares"] = shares
-        extra["autotune"] = {"chosen": config.describe(), "tune_s": tune_s,
-                             "candidates": [{"config": r["config"], "solve_ms": None if r["time_s"] is None
-                                             else 1e3 * r["time_s"], "ok": r["ok"]} for r in tune_table]}
-        st = b.status()
-        extra["lanczos_iterations"] = {"min": int(st[:, 3].min()), "max": int(st[:, 3].max())}
-        roof = apply_roofline(ed, data, sset, solver, peak_gbs)
-        roof["peak_source"] = peak_src
-        if not args.skip_scale and ws == 1:
-            try:
-                extra["matvec_at_scale"] = matvec_at_scale(ed, models, peak_gbs)
-            except Exception as exc:  # noqa: BLE001 - reported, not fatal
-                extra["matvec_at_scale"] = {"error": repr(exc)}
-            torch.cuda.empty_cache()
-            try:
-                extra["serving_at_scale"] = serving_at_scale(ed, models)
-            except Exception as exc:  # noqa: BLE001 - reported, not fatal
-                extra["serving_at_scale"] = {"error": repr(exc)}
-            torch.cuda.empty_cache()
-            try:
-                extra["reference_benchmark"] = reference_benchmark(ed, models)
-            except Exception as exc:  # noqa: BLE001 - reported, not fatal
-                extra["reference_benchmark"] = {"error": repr(exc)}
-        # CPU baseline: the oracle (reference algorithm) on the host cores, N = 1 only
-        cpu_base = None
-        if ws == 1:
-            cpu_rate, cpu_n, _, cpu_t = cpu_sector_solves(model, nf, G, data.irrep_list, nev,
-                                                          budget_s=args.cpu_budget)
-            cpu_base = {"value": cpu_rate, "unit": "sector-solves/s", "cores": _NCPU, "kind": "port",
-                        "sample": f"{cpu_n} sector solves of the same workload (its 12 sectors, "
-                                  f"cycled) in {cpu_t:.1f} s: projection table + CSR + ARPACK per "
-                                  "sector, catalog untimed"}
         line = {
             "metric": "sector-solves/s",
             "value": value,
@@ -886,13 +1102,17 @@ def run_b200(args):
             "data": "synthetic",
             "config": {"workload": args.workload, "desc": wl["desc"], "nev": nev,
                        "sectors_per_step": n_sec, "solver": config.describe(), "precision": args.precision,
-                       "l2": "256 MB buffer written between timed steps",
+                       "l2": "inputs larger than L2 (Lanczos blocks of 0.17-0.67 GB); 256 MB buffer also "
+                             "written between timed steps",
                        "parallelism": f"replicas x{ws}"},
-            "latency_ms": {"p50": 1e3 * lat[len(lat) // 2], "p99": 1e3 * lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
-            "parity": {"max_abs_dE_vs_oracle": max_de, "tolerance": 1e-10},
+            "latency_ms": {"p50": 1e3 * lat[len(lat) // 2], "p99": 1e3 * lat[min(len(lat) - 1, int(0.99 * len(lat)))],
+                           "unit": "one step (all sectors)"},
+            "parity": {"max_abs_dE_vs_reference": max_de if ref is not None else None, "tolerance": 1e-10,
+                       "e2e_max_abs_dE": e2e_de if ref is not None else None,
+                       "reference": f"tests/golden/{wl['golden']}.npz (the reference's ARPACK eigenvalues)"},
             "e2e": {"value": e2e_val, "unit": "sector-solves/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h),
-                    "api": "solve_sectors_batched(start_blocks=pinned host) -> numpy eigenpairs"},
+                    "api": "solve_sectors_batched(start_blocks=pinned host) -> numpy eigenvalues + eigenvectors"},
             "roofline": roof,
             "cpu_baseline": cpu_base,
             "clocks": clk.summary(),
@@ -913,11 +1133,15 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="checkerboard24", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="haldane32", choices=sorted(WORKLOADS))
     ap.add_argument("--precision", type=int, default=32, choices=[32, 64])
-    ap.add_argument("--plain-sectors", type=int, default=12)
-    ap.add_argument("--cpu-budget", type=float, default=12.0)
-    ap.add_argument("--skip-scale", action="store_true")
+    ap.add_argument("--plain-sectors", type=int, default=3)
+    ap.add_argument("--cpu-budget", type=float, default=30.0,
+                    help="seconds of reference sector solves for cpu_baseline (at least one solve)")
+    ap.add_argument("--ref-budget", type=float, default=150.0,
+                    help="seconds of reference sector solves for --impl reference (at least one solve)")
+    ap.add_argument("--skip-scale", action="store_true", help="skip the serving / config-2 / benchmark extras")
+    ap.add_argument("--skip-fp64", action="store_true", help="skip the FP64-matvec batched variant")
     ap.add_argument("--solver", default="auto",
                     help='"auto" (measured by the autotuner) or "graph:<block>:<proj|otf>:<n_slots>"')
     ap.add_argument("--matvec-only", action="store_true",
@@ -936,6 +1160,7 @@ def main():
     ap.add_argument("--chern", type=int, default=0,
                     help="only the many-body Chern number of the 32-site Haldane pair on this flux grid")
     args = ap.parse_args()
+    peak_gbs = None
     if args.solve_scale:
         import realspace_exatdiagonalization_py_b200 as ed
         import torch
@@ -954,56 +1179,32 @@ def main():
         print(json.dumps({"workload": f"haldane32: {len(secs)} sectors, FP32 + FP64 refinement, b=2, nev 4",
                           "solve_s": time.perf_counter() - t0, "E0": [float(res[s][0][0]) for s in secs]}))
         return
-    if args.reference_benchmark:
-        import realspace_exatdiagonalization_py_b200 as ed
-        from realspace_exatdiagonalization_py_b200 import models
-
-        print(json.dumps(reference_benchmark(ed, models)), flush=True)
-        return
-    if args.corr:
-        import realspace_exatdiagonalization_py_b200 as ed
-        from realspace_exatdiagonalization_py_b200 import models
-
-        print(json.dumps(correlators_at_scale(ed, models)), flush=True)
-        return
-    if args.serving_only:
-        import realspace_exatdiagonalization_py_b200 as ed
-        from realspace_exatdiagonalization_py_b200 import models
-
-        print(json.dumps(serving_at_scale(ed, models)), flush=True)
-        return
-    if args.overlap_only:
-        import realspace_exatdiagonalization_py_b200 as ed
-
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
-            os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
-        print(json.dumps({"workload": f"one row of Chern links: {args.overlap_only}x{args.overlap_only} grid, "
-                                      "2 states per flux point, 10,518,300 amplitudes per state (32-site Haldane)",
-                          **overlap_row(ed, 10_518_300, 2, args.overlap_only,
-                                        float(peaks.get("hbm_gbs", 6650.0)))}), flush=True)
-        return
-    if args.chern:
-        import realspace_exatdiagonalization_py_b200 as ed
-        from realspace_exatdiagonalization_py_b200 import models
-
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
-            os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
-        print(json.dumps(chern_at_scale(ed, models, grid=args.chern, peak_gbs=float(peaks.get("hbm_gbs", 6650.0)))),
-              flush=True)
-        return
-    if args.matvec_only:
-        import realspace_exatdiagonalization_py_b200 as ed
-        from realspace_exatdiagonalization_py_b200 import models
-
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
-            os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
-        precs = (args.matvec_precision,) if args.matvec_precision else (32, 64)
-        print(json.dumps(matvec_at_scale(ed, models, float(peaks.get("hbm_gbs", 6650.0)),
-                                         n_launch=args.matvec_launches, precisions=precs,
-                                         otf=not args.matvec_no_otf)), flush=True)
-        return
     if args.impl == "reference":
         run_reference(args)
+        return
+    special = args.reference_benchmark or args.corr or args.serving_only or args.overlap_only or args.chern \
+        or args.matvec_only
+    if special:
+        import realspace_exatdiagonalization_py_b200 as ed
+        from realspace_exatdiagonalization_py_b200 import models
+
+        peak_gbs, _ = _load_peaks()
+    if args.reference_benchmark:
+        print(json.dumps(reference_benchmark(ed, models)), flush=True)
+    elif args.corr:
+        print(json.dumps(correlators_at_scale(ed, models)), flush=True)
+    elif args.serving_only:
+        print(json.dumps(serving_at_scale(ed, models)), flush=True)
+    elif args.overlap_only:
+        print(json.dumps({"workload": f"one row of Chern links: {args.overlap_only}x{args.overlap_only} grid, "
+                                      "2 states per flux point, 10,518,300 amplitudes per state (32-site Haldane)",
+                          **overlap_row(ed, 10_518_300, 2, args.overlap_only, peak_gbs)}), flush=True)
+    elif args.chern:
+        print(json.dumps(chern_at_scale(ed, models, grid=args.chern, peak_gbs=peak_gbs)), flush=True)
+    elif args.matvec_only:
+        precs = (args.matvec_precision,) if args.matvec_precision else (32, 64)
+        print(json.dumps(matvec_at_scale(ed, models, peak_gbs, n_launch=args.matvec_launches, precisions=precs,
+                                         otf=not args.matvec_no_otf)), flush=True)
     else:
         run_b200(args)
 

@@ -242,7 +242,10 @@ int rsed_triplets_fill(const rsed_model_t* model, int64_t n_rows, const int32_t*
                        const int64_t* col_off, int64_t* rows, int64_t* cols, double* vals,
                        void* stream);
 /* y_v = A x_v (v < n_vec, vectors contiguous) for a complex128 CSR matrix
- * (scipy.sparse csr_matrix @ x, symmetry_resolved_ed.py:1976). */
+ * (scipy.sparse csr_matrix @ x, symmetry_resolved_ed.py:1976).  With the
+ * sector block assembled from the triplets above, this is the reference's
+ * operator y = H x (MatrixFreeHamiltonian.__call__, apply_hamiltonian,
+ * symmetry_resolved_ed.py:1965-1976, 1979-2069). */
 int rsed_csr_spmv(int64_t n_rows, const int64_t* row_ptr, const int32_t* col_idx,
                   const double* vals, int32_t n_vec, const double* x, double* y, void* stream);
 

@@ -1,10 +1,10 @@
 """Loader for the reference's own Python engine (golden-vector generation only).
 
-TEST INFRASTRUCTURE.  Nothing in the product imports this module; it is run
-in the build container (where the read-only reference checkout lives) by
-``tests/golden/make_golden.py`` to produce the committed fixtures, and by the
-CPU-only tests that pin the oracle against the reference when the checkout is
-present.  It never runs on the GPU box.
+TEST INFRASTRUCTURE.  Nothing in the product imports this module.  It is used
+by ``tests/golden/make_*.py`` to produce the committed fixtures, by the
+CPU-only tests that pin the oracle against the reference when the reference
+is present, and by ``bench.py``'s reference arm (the reference's own
+numpy/scipy path timed on the host cores).
 
 The reference package ``realspace_exactdiagonalization_py`` cannot be imported
 normally here: its ``__init__`` pulls in ``models/`` which imports the absent
@@ -25,20 +25,35 @@ import os
 import sys
 import types
 
-REFERENCE_ROOT = os.environ.get("RSED_REFERENCE_ROOT", "/root/reference")
 PKG = "realspace_exactdiagonalization_py"
+_REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+# the reference as installed by oracle/install_reference.py (travels with the
+# working tree), else a checkout named by RSED_REFERENCE_ROOT
+INSTALLED = os.path.join(_REPO, "baseline", "_ref", PKG)
+
+
+def package_dir() -> str | None:
+    """Directory of the reference package's sources, or None."""
+    cands = []
+    root = os.environ.get("RSED_REFERENCE_ROOT")
+    if root:
+        cands.append(os.path.join(root, "src", PKG))
+    cands.append(INSTALLED)
+    for d in cands:
+        if os.path.isfile(os.path.join(d, "symmetry_resolved_ed.py")):
+            return d
+    return None
 
 
 def available() -> bool:
-    return os.path.isfile(
-        os.path.join(REFERENCE_ROOT, "src", PKG, "symmetry_resolved_ed.py")
-    )
+    return package_dir() is not None
 
 
 def load():
     """Return a namespace with the reference engine and model modules."""
-    if not available():
-        raise RuntimeError("reference checkout not present")
+    src = package_dir()
+    if src is None:
+        raise RuntimeError("reference package not present (run oracle/install_reference.py)")
     if PKG in sys.modules and hasattr(sys.modules[PKG], "_rsed_shim"):
         return sys.modules[PKG]._rsed_shim
 
@@ -65,12 +80,12 @@ def load():
     )
 
     pkg = types.ModuleType(PKG)
-    pkg.__path__ = [os.path.join(REFERENCE_ROOT, "src", PKG)]
+    pkg.__path__ = [src]
     sys.modules[PKG] = pkg
     sre = importlib.import_module(PKG + ".symmetry_resolved_ed")
     sqm = importlib.import_module(PKG + ".second_quantized_model")
     models_pkg = types.ModuleType(PKG + ".models")
-    models_pkg.__path__ = [os.path.join(REFERENCE_ROOT, "src", PKG, "models")]
+    models_pkg.__path__ = [os.path.join(src, "models")]
     sys.modules[PKG + ".models"] = models_pkg
     heis = importlib.import_module(PKG + ".models.heisenberg")
     hub = importlib.import_module(PKG + ".models.hubbard")

@@ -10,6 +10,20 @@ beside the plain API.
 """
 
 from .autotune import Autotuner, candidate_configs, default_tuner
+from .bits import (
+    as_uint64_array,
+    bitmask_of_site,
+    decode_bit_mask_to_configuration,
+    decode_bit_mask_to_configuration_inplace,
+    empty_site_for_mask,
+    empty_site_iter_for_mask,
+    encode_configuration_to_bit_mask,
+    filled_site_iter_for_mask,
+    is_site_empty,
+    is_site_occupied,
+    n_occupied_for_mask,
+    occupy_site_for_mask,
+)
 from .batched import BatchedSectorSolver, SolverConfig
 from .correlators import (compute_odlro_map, compute_structure_factor_manifold_average_map,
                           compute_structure_factor_map, off_diagonal_long_range_order, static_structure_factor,
@@ -17,6 +31,24 @@ from .correlators import (compute_odlro_map, compute_structure_factor_manifold_a
                           structure_factor_manifold_allowed_momenta)
 from .catalog import Symmetry_Orbit_Catalog, build_symmetry_orbit_catalog, update_orbit_stabilizer_phases
 from .fock import expand_sector_state_to_fock_amplitudes, expand_sector_state_to_fock_dense, fock_overlaps
+from .models import (
+    CHECKERBOARD_TPP_DENOMINATOR,
+    build_bosonic_fci_ed_data,
+    build_fermionic_checkerboard_tb_model,
+    build_fermionic_fci_ed_data,
+    build_heisenberg_ed_data,
+    build_heisenberg_second_quantized_model,
+    build_phase_explore_fermionic_checkerboard_model,
+    build_spinful_hubbard_ed_data,
+    build_spinful_hubbard_second_quantized_model,
+    build_zero_flux_bosonic_fci_second_quantized_model,
+    build_zero_flux_fermionic_fci_second_quantized_model,
+    default_fci_sectors,
+    default_fci_sectors_fermionic,
+    my_optimal_param,
+    params_DNSheng,
+    params_Sun_Gu_Katsura_Sarma,
+)
 from .observables import flux_charge_pump, flux_spectrum_flow, many_body_chern_number, many_body_position_phases
 from .ed import (
     Symmetry_Resolved_ED_Data,

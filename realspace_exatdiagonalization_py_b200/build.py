@@ -58,16 +58,22 @@ def build(verbose: bool = False, ptxas_info: bool = False, force: bool = False) 
     nvcc = _nvcc()
     objdir = os.path.join(PKG_DIR, "_build")
     os.makedirs(objdir, exist_ok=True)
-    objs = []
+    cmds, objs = [], []
     for src in sources():
         obj = os.path.join(objdir, os.path.basename(src)[:-3] + ".o")
-        cmd = [nvcc, *ARCH_FLAGS, *BASE_FLAGS, "-dc" if False else "-c", src, "-o", obj]
+        cmd = [nvcc, *ARCH_FLAGS, *BASE_FLAGS, "-c", src, "-o", obj]
         if ptxas_info:
             cmd.insert(1, "-Xptxas=-v")
         if verbose:
             print(" ".join(cmd), flush=True)
-        subprocess.run(cmd, check=True)
+        cmds.append(cmd)
         objs.append(obj)
+    # one nvcc per translation unit, in parallel
+    from concurrent.futures import ThreadPoolExecutor
+
+    with ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as ex:
+        for r in list(ex.map(lambda c: subprocess.run(c, check=True), cmds)):
+            pass
     tmp = LIB_PATH + ".tmp"
     cmd = [nvcc, *ARCH_FLAGS, "-shared", "-o", tmp, *objs, "-lcudart"]
     if verbose:

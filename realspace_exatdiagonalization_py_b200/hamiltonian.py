@@ -4,7 +4,8 @@
   of the apply kernel visits only occupied sites), density diagonal per orbit.
 * ``MatrixFreeHamiltonian`` / ``hamiltonian_linear_operator`` /
   ``apply_hamiltonian``: the reference's operator API
-  (``symmetry_resolved_ed.py:1884-2094``) on top of the K6 kernel.
+  (``symmetry_resolved_ed.py:1884-2094``), ``y = H x`` from the sector's
+  exact CSR block; the eigen-solvers stream the K6b projection table instead.
 * ``build_ed_Hamiltonian_symmetry_block``: matrix mode (``:2102-2174``), with
   the triplets produced by the K7 kernel.
 
@@ -190,12 +191,23 @@ class DeviceModel:
 
 
 class MatrixFreeHamiltonian:
-    """``H_op(x) -> y`` for one sector, evaluated on the fly by the K6 kernel.
+    """``H_op(x) -> y = H x`` for one sector (``symmetry_resolved_ed.py:1884-1976``).
 
-    Same constructor and call contract as the reference
-    (``symmetry_resolved_ed.py:1884-1976``): ``x`` and the result are complex128
-    of length ``sector_dim``; numpy arrays stay numpy, CUDA tensors stay on
-    the device.
+    Same constructor and call contract as the reference: ``x`` and the result
+    are complex128 of length ``sector_dim`` (or ``[sector_dim, k]`` blocks);
+    numpy arrays stay numpy, CUDA tensors stay on the device.  Like the
+    reference, the operator is the sector block in CSR form, assembled from
+    the exact projected hops and the density diagonal (K7 triplets, the
+    reference's element formula and product order) and applied by
+    ``rsed_csr_spmv``; the CSR is built on the first call.
+
+    The eigen-solvers do not go through ``__call__``: they stream the
+    sector-independent orbit-space projection table (``DeviceModel``,
+    ``rsed_apply_h``), whose pull form yields ``H^dagger x`` -- equal to
+    ``H x`` for the reference's zero-flux blocks and, for flux blocks
+    (Hermitian only to the complex64 rounding of the amplitude table), with
+    the same real spectrum.  ``precision=32`` makes ``__call__`` that FP32
+    streaming apply (``H^dagger x`` in FP32 arithmetic).
     """
 
     def __init__(self, basis: Symmetry_Sector_Basis, bilinear_terms, density_terms, cmap,
@@ -210,17 +222,33 @@ class MatrixFreeHamiltonian:
         dev = basis.catalog.table.device
         self._col_sector = torch.tensor([basis.sector_index], dtype=torch.int32, device=dev)
         self._orbit_of_row = basis.orbit_of_row if self.n else None
+        self._csr: DeviceCSR | None = None
+
+    def csr(self) -> "DeviceCSR":
+        """The sector block as a device CSR matrix (built once)."""
+        if self._csr is None:
+            rows, cols, vals = _sector_triplets(self.basis, self.model)
+            self._csr = DeviceCSR(rows, cols, vals, self.n)
+        return self._csr
 
     def matvec_device(self, x: torch.Tensor, ncols: int = 1) -> torch.Tensor:
-        """Apply to ``ncols`` compact column vectors ``x [n, ncols]`` on the device."""
+        """``H x`` for ``ncols`` compact column vectors ``x [n, ncols]`` on the device."""
+        if self.precision == 32:
+            return self.adjoint_device(x, ncols, precision=32)
+        xt = x.reshape(self.n, ncols).to(torch.complex128).T.contiguous()
+        return self.csr().matvec(xt).T.reshape(self.n, ncols)
+
+    def adjoint_device(self, x: torch.Tensor, ncols: int = 1, precision: int = 64) -> torch.Tensor:
+        """``H^dagger x`` through the streaming orbit-layout apply of the
+        eigensolver (``rsed_apply_h``) for ``x [n, ncols]`` on the device."""
         dev = x.device
         n_orb = self.basis.catalog.n_orbits
         ld = ncols + (ncols & 1)
         X = torch.zeros((n_orb, ld), dtype=torch.complex128, device=dev)
-        X[self._orbit_of_row.long(), :ncols] = x.reshape(self.n, ncols)
+        X[self._orbit_of_row.long(), :ncols] = x.reshape(self.n, ncols).to(torch.complex128)
         col_sector = self._col_sector.repeat(ncols)
         Y = torch.empty_like(X)
-        if self.precision == 32:
+        if precision == 32:
             self.model.apply_block(self.basis.sector_set, col_sector, X.to(torch.complex64), Y, 32)
         else:
             self.model.apply_block(self.basis.sector_set, col_sector, X, Y, 64)
@@ -228,26 +256,47 @@ class MatrixFreeHamiltonian:
 
     def __call__(self, x):
         if self.n == 0:
-            return np.zeros(0, dtype=np.complex128)
+            if isinstance(x, torch.Tensor):
+                return torch.zeros_like(x, dtype=torch.complex128)
+            return np.zeros(np.shape(x), dtype=np.complex128)
         if isinstance(x, torch.Tensor) and x.is_cuda:
-            return self.matvec_device(x.to(torch.complex128)).reshape(x.shape)
+            k = x.numel() // self.n
+            return self.matvec_device(x, k).reshape(x.shape)
         xa = np.ascontiguousarray(x, dtype=np.complex128)
-        xt = torch.from_numpy(xa.reshape(self.n, -1)).to(self.basis.catalog.table.device)
-        y = self.matvec_device(xt, xt.shape[1])
+        k = xa.size // self.n
+        xt = torch.from_numpy(xa.reshape(self.n, k)).to(self.basis.catalog.table.device)
+        y = self.matvec_device(xt, k)
         return y.cpu().numpy().reshape(xa.shape)
 
 
 def hamiltonian_linear_operator(basis, bilinear_terms, density_terms, cmap):
-    """``(H_op, n)`` (``symmetry_resolved_ed.py:2072-2094``)."""
+    """``(H_op, n)`` with ``H_op(x) = H x`` (``symmetry_resolved_ed.py:2072-2094``)."""
     return MatrixFreeHamiltonian(basis, bilinear_terms, density_terms, cmap), basis.dim
 
 
+def _cached_operator(basis, bilinear_terms, density_terms, cmap) -> MatrixFreeHamiltonian:
+    """The sector's operator for these terms, kept on the basis object so
+    that repeated ``apply_hamiltonian`` calls build the device model and the
+    CSR once (the reference re-derives its lookup arrays on every call)."""
+    key = (tuple((int(i), int(j), complex(t)) for (i, j, t) in bilinear_terms),
+           tuple((int(i), int(j), complex(v)) for (i, j, v) in density_terms),
+           basis.catalog.version)
+    cache = basis.__dict__.setdefault("_operators", {})
+    op = cache.get(key)
+    if op is None:
+        cache.clear()
+        op = MatrixFreeHamiltonian(basis, bilinear_terms, density_terms, cmap)
+        cache[key] = op
+    return op
+
+
 def apply_hamiltonian_with_threads(y, x, basis, bilinear_terms, density_terms, cmap, y_threads=None):
-    """``y[:] = H x`` on the fly (``symmetry_resolved_ed.py:2011-2069``);
-    ``y_threads`` is accepted for API parity and unused."""
+    """``y[:] = H x``, written into the caller's ``y`` and returned
+    (``symmetry_resolved_ed.py:2011-2069``); ``y_threads`` (the reference's
+    per-thread buffers) is accepted for API parity and unused."""
     n = len(x)
-    assert len(y) == n
-    op = MatrixFreeHamiltonian(basis, bilinear_terms, density_terms, cmap)
+    assert len(y) == n, "apply_hamiltonian: y and x must have the same length"
+    op = _cached_operator(basis, bilinear_terms, density_terms, cmap)
     y[:] = op(x)
     return y
 
@@ -288,7 +337,7 @@ class DeviceCSR:
     """Sector block in CSR form on the device, applied by ``rsed_csr_spmv``."""
 
     def __init__(self, rows, cols, vals, n):
-        order = torch.argsort(rows * n + cols)
+        order = torch.argsort(rows * n + cols, stable=True)
         r = rows[order]
         self.n = n
         self.col = cols[order].to(torch.int32)
@@ -297,7 +346,16 @@ class DeviceCSR:
         self.row_ptr = torch.zeros(n + 1, dtype=torch.int64, device=rows.device)
         self.row_ptr[1:] = torch.cumsum(counts, 0)
 
+    def to_dense(self) -> torch.Tensor:
+        """The matrix as a dense device tensor (duplicates summed)."""
+        A = torch.zeros((self.n, self.n), dtype=torch.complex128, device=self.val.device)
+        rows = torch.repeat_interleave(torch.arange(self.n, device=self.val.device),
+                                       self.row_ptr[1:] - self.row_ptr[:-1])
+        A.index_put_((rows, self.col.long()), self.val, accumulate=True)
+        return A
+
     def matvec(self, x: torch.Tensor) -> torch.Tensor:
+        """``A x_v`` for ``x [n]`` or ``x [n_vec, n]`` (vectors contiguous)."""
         x = x.to(torch.complex128).contiguous()
         nvec = 1 if x.dim() == 1 else x.shape[0]
         y = torch.empty_like(x)

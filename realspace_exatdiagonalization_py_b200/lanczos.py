@@ -459,41 +459,107 @@ def _solve_sector(model: DeviceModel, sset: SectorSet, s: int, nev: int, params:
     return vals, vecs
 
 
+def _csr_lanczos(csr, nev: int, *, tol: float = 1e-10, m: int | None = None, max_restarts: int = 500,
+                 seed: int = 12345):
+    """Lowest ``nev`` eigenpairs of a device CSR block (``DeviceCSR``) by
+    thick-restart Lanczos with full FP64 reorthogonalisation (classical
+    Gram-Schmidt applied twice), all on the GPU; the start vector is the
+    reference's ``v0`` (``default_rng(12345)`` complex normal).  The Ritz
+    problem is the Hermitian part of the projected matrix, as in the batched
+    solver; convergence is ``||r_j|| <= tol * max(1, |theta_j|)``."""
+    n = csr.n
+    dev = csr.val.device
+    m = min(n - 1, m or max(2 * nev + 16, 40))
+    keep = max(nev, min(m - 2, nev + (m - nev) // 2))
+    V = torch.zeros((m + 1, n), dtype=torch.complex128, device=dev)
+    T = torch.zeros((m + 1, m), dtype=torch.complex128, device=dev)
+    V[0] = torch.from_numpy(start_block(n, 1, seed)[:, 0]).to(dev)
+    j0 = 0
+    for _ in range(max_restarts):
+        for j in range(j0, m):
+            w = csr.matvec(V[j])
+            Vj = V[: j + 1]
+            c = Vj.conj() @ w
+            w = w - Vj.T @ c
+            c2 = Vj.conj() @ w
+            w = w - Vj.T @ c2
+            T[: j + 1, j] = c + c2
+            beta = torch.linalg.vector_norm(w)
+            T[j + 1, j] = beta
+            if float(beta) <= 1e-14 * max(1.0, float(torch.linalg.vector_norm(c + c2))):
+                # invariant subspace: continue from a random vector orthogonal to V
+                g = torch.Generator(device=dev).manual_seed(seed + j)
+                w = torch.randn(n, dtype=torch.complex128, device=dev, generator=g)
+                for _ in range(2):
+                    w = w - Vj.T @ (Vj.conj() @ w)
+                T[j + 1, j] = 0
+                beta = torch.linalg.vector_norm(w)
+            V[j + 1] = w / beta
+        A = T[:m, :m]
+        A = 0.5 * (A + A.conj().T)
+        theta, Y = torch.linalg.eigh(A)
+        bm = T[m, m - 1]
+        resid = (bm.abs() * Y[m - 1, :].abs()).cpu().numpy()
+        th = theta.cpu().numpy()
+        if np.all(resid[:nev] <= tol * np.maximum(1.0, np.abs(th[:nev]))):
+            U = Y[:, :nev].T @ V[:m]
+            return th[:nev].copy(), U.T.contiguous().cpu().numpy()
+        # thick restart: the lowest `keep` Ritz vectors plus the residual vector
+        Vk = Y[:, :keep].T @ V[:m]
+        V[:keep] = Vk
+        V[keep] = V[m]
+        coupling = bm * Y[m - 1, :keep]
+        T.zero_()
+        T[torch.arange(keep), torch.arange(keep)] = theta[:keep].to(torch.complex128)
+        T[keep, :keep] = coupling
+        T[:keep, keep] = coupling.conj()
+        j0 = keep
+    raise _lib.RsedError(_lib.RSED_ENOTCONV, f"CSR Lanczos did not converge in {max_restarts} restarts")
+
+
 def diagonalize_block_arpack(H, *, nev: int = 5, params: LanczosParams | None = None,
                              basis=None, model: DeviceModel | None = None):
-    """Lowest ``nev`` eigenpairs of a sector block: dense for ``n <= 500``,
-    else the device block Lanczos (``symmetry_resolved_ed.py:2214-2245``)."""
-    n = H.shape[0]
+    """Lowest ``nev`` eigenpairs of a sector block, ascending: dense for
+    ``n <= 500`` (``diagonalize_block_dense``), else a device Lanczos
+    (``symmetry_resolved_ed.py:2214-2245``).  With the block's ``basis`` and
+    device ``model`` the batched block Lanczos streams the projection table;
+    a bare CSR block (scipy or ``DeviceCSR``) is solved by a thick-restart
+    Lanczos on the device CSR."""
+    n = H.shape[0] if hasattr(H, "shape") else H.n
     if n == 0:
         return np.zeros(0, dtype=np.float64), np.zeros((0, 0), dtype=np.complex128)
-    if n <= 500 or basis is None or model is None:
-        if n > 500:
-            raise ValueError("diagonalize_block_arpack needs the sector basis for n > 500")
-        return diagonalize_block_dense(H, nev=nev)
-    vals, vecs = _solve_sector(model, basis.sector_set, basis.sector_index, nev,
-                               params or LanczosParams())
-    return vals, vecs.cpu().numpy()
+    if n <= 500:
+        return diagonalize_block_dense(H.to_dense().cpu().numpy() if hasattr(H, "to_dense") else H, nev=nev)
+    if basis is not None and model is not None:
+        vals, vecs = _solve_sector(model, basis.sector_set, basis.sector_index, nev, params or LanczosParams())
+        return vals, vecs.cpu().numpy()
+    from .hamiltonian import DeviceCSR
+
+    csr = H if isinstance(H, DeviceCSR) else _scipy_to_device_csr(H)
+    return _csr_lanczos(csr, min(nev, n - 1), tol=(params or LanczosParams()).tol)
+
+
+def _scipy_to_device_csr(H):
+    from .hamiltonian import DeviceCSR
+
+    c = H.tocoo()
+    dev = torch.device("cuda", torch.cuda.current_device())
+    return DeviceCSR(torch.from_numpy(c.row.astype(np.int64)).to(dev), torch.from_numpy(c.col.astype(np.int64)).to(dev),
+                     torch.from_numpy(np.ascontiguousarray(c.data, dtype=np.complex128)).to(dev), H.shape[0])
 
 
 def diagonalize_block_matrixfree(H_op, n: int, *, nev: int = 5, params: LanczosParams | None = None):
     """Lowest ``nev`` eigenpairs of a matrix-free sector operator
-    (``symmetry_resolved_ed.py:2248-2299``).  ``n <= 500``: the dense block is
-    assembled on the GPU from ``H_op`` applied to the unit vectors and solved
-    on the triangle matching the reference's ``eigh(UPLO="U")``; larger
-    sectors use the device block Lanczos."""
+    (``symmetry_resolved_ed.py:2248-2299``).  ``n <= 500``: the dense block
+    (the operator's exact CSR, which is what the reference obtains by applying
+    ``H_op`` to the unit vectors) solved on its upper triangle like the
+    reference's ``eigh(UPLO="U")``; larger sectors use the device block
+    Lanczos over the projection table."""
     if n == 0:
         return np.zeros(0, dtype=np.float64), np.zeros((0, 0), dtype=np.complex128)
     if n <= 500:
-        dev = torch.device("cuda", torch.cuda.current_device())
-        cols = []
-        for c0 in range(0, n, 64):
-            c1 = min(n, c0 + 64)
-            E = torch.zeros((n, c1 - c0), dtype=torch.complex128, device=dev)
-            E[torch.arange(c0, c1, device=dev), torch.arange(c1 - c0, device=dev)] = 1.0
-            cols.append(H_op.matvec_device(E, c1 - c0))
-        A = torch.cat(cols, dim=1)
-        # the kernel returns H^dagger; its lower triangle is the reference's upper one
-        vals, vecs = torch.linalg.eigh(A, UPLO="L")
+        A = H_op.csr().to_dense()
+        vals, vecs = torch.linalg.eigh(A, UPLO="U")
         k = min(nev, n)
         return vals[:k].cpu().numpy().real, vecs[:, :k].cpu().numpy()
     params = params or LanczosParams()

@@ -33,8 +33,20 @@ __all__ = [
     "build_zero_flux_bosonic_fci_second_quantized_model",
     "build_zero_flux_fermionic_fci_second_quantized_model",
     "build_phase_explore_fermionic_checkerboard_model",
+    "build_fermionic_checkerboard_tb_model",
+    "CHECKERBOARD_TPP_DENOMINATOR",
+    "default_fci_sectors",
+    "default_fci_sectors_fermionic",
+    "build_heisenberg_ed_data",
+    "build_spinful_hubbard_ed_data",
+    "build_bosonic_fci_ed_data",
+    "build_fermionic_fci_ed_data",
     "config_model",
 ]
+
+# t'' = 1 / CHECKERBOARD_TPP_DENOMINATOR in the Sun-Gu-Katsura-Das Sarma
+# couplings (models/fermionic_fci.py:55)
+CHECKERBOARD_TPP_DENOMINATOR = 2 + 2 * math.sqrt(2)
 
 # Parameter sets of the reference's model modules (models/bosonic_fci.py:33-40,
 # models/fermionic_fci.py:42-51, :759-772).
@@ -228,16 +240,24 @@ def _checkerboard_density(lat, V1, V2, V3):
     return out
 
 
+def build_fermionic_checkerboard_tb_model(*, sample_size=None, params=None, flip_bands: bool = True):
+    """Checkerboard tight-binding model with staggered flux
+    (``models/fermionic_fci.py:58-131``): NN ``-t e^{-+i phi}``, NNN
+    ``-t'_1 / -t'_2``, NNNN ``-t''``; ``flip_bands`` negates t, t'_1, t'_2 and
+    t'' first (the flat band becomes the lower one)."""
+    sample_size = [3, 4] if sample_size is None else sample_size
+    q = dict(params_Sun_Gu_Katsura_Sarma if params is None else params)
+    if flip_bands:
+        for k in ("t", "t'_1", "t'_2", "t''"):
+            q[k] = -q[k]
+    return _checkerboard_tb(sample_size, q["t"], q["t'_1"], q["t'_2"], q["t''"], 2 * math.pi * q["phi_over_2pi"])
+
+
 def build_zero_flux_fermionic_fci_second_quantized_model(*, sample_size=None, params=None,
                                                          flip_bands: bool = True):
     sample_size = [3, 4] if sample_size is None else sample_size
     p = dict(params_Sun_Gu_Katsura_Sarma if params is None else params)
-    q = dict(p)
-    if flip_bands:
-        for k in ("t", "t'_1", "t'_2", "t''"):
-            q[k] = -q[k]
-    tb = _checkerboard_tb(sample_size, q["t"], q["t'_1"], q["t'_2"], q["t''"],
-                          2 * math.pi * q["phi_over_2pi"])
+    tb = build_fermionic_checkerboard_tb_model(sample_size=sample_size, params=p, flip_bands=flip_bands)
     lat = tb.lattice
     return Real_Space_Second_Quantized_Model(
         params=p, lattice=lat, tb_model=tb, particle_statistics=Particle_Statistics.FERMIONIC,
@@ -247,8 +267,10 @@ def build_zero_flux_fermionic_fci_second_quantized_model(*, sample_size=None, pa
 
 
 def build_phase_explore_fermionic_checkerboard_model(params, sample_size, filling_fraction_per_band):
-    """Pre-flipped hoppings, interactions scaled by ``params["λ"]``; returns
-    ``(model, n_filled, filling_fraction)`` (the ED data is built by the caller)."""
+    """Pre-flipped hoppings, interactions scaled by ``params["λ"]``
+    (``models/fermionic_fci.py:599-757``); returns ``(model, ed_data,
+    n_filled, filling_fraction)`` with the translation-group ED data built on
+    the device."""
     p = dict(params)
     tb = _checkerboard_tb(sample_size, p["t"], p["t'_1"], p["t'_2"], p["t''"],
                           2 * math.pi * p["phi_over_2pi"])
@@ -260,7 +282,76 @@ def build_phase_explore_fermionic_checkerboard_model(params, sample_size, fillin
         density_density_terms=_checkerboard_density(lat, p["V1"] * lam, p["V2"] * lam, p["V3"] * lam),
     )
     ff = Fraction(filling_fraction_per_band) / lat.n_sub
-    return model, int(lat.n_site * ff), ff
+    return model, _translation_ed_data(model, ff), int(lat.n_site * ff), ff
+
+
+# ---------------------------------------------------------------------------
+# ED data of the model families (the reference's convenience builders)
+# ---------------------------------------------------------------------------
+
+
+def _translation_ed_data(model, filling_fraction):
+    from .ed import build_ed_data
+    from .symmetry import build_translation_group
+
+    return build_ed_data(model, filling_fraction=Fraction(filling_fraction),
+                         symmetry_group=build_translation_group(model.lattice))
+
+
+def default_fci_sectors(sample_size: list[int]) -> list[tuple[int, int]]:
+    """Momentum labels of the two bosonic semion FCI ground states
+    (``models/bosonic_fci.py:171-196``); unknown sizes warn and give [(0, 0)]."""
+    known = {(2, 3): [(0, 0), (1, 0)], (3, 2): [(0, 0), (0, 1)],
+             (3, 4): [(0, 0), (0, 2)], (4, 3): [(0, 0), (2, 0)]}
+    key = tuple(sample_size)
+    if key in known:
+        return list(known[key])
+    print(f"WARNING: Unknown `sample_size={sample_size}` — defaulting sector labels to [(0,0)]. "
+          "The user should manually specify the FCI ground-state sectors.")
+    return [(0, 0)]
+
+
+def default_fci_sectors_fermionic(sample_size: list[int]) -> list[tuple[int, int]]:
+    """Momentum labels of the three fermionic checkerboard FCI ground states
+    (``models/fermionic_fci.py:222-255``); unknown sizes raise ValueError."""
+    known = {(2, 3): [(0, 0), (0, 1), (0, 2)], (3, 2): [(0, 0), (1, 0), (2, 0)],
+             (3, 4): [(0, 0), (1, 0), (2, 0)], (4, 3): [(0, 0), (0, 1), (0, 2)]}
+    key = tuple(sample_size)
+    if key in known:
+        return list(known[key])
+    raise ValueError(f"Unknown sample_size={sample_size} — run a full ED scan to identify the FCI sectors.")
+
+
+def build_heisenberg_ed_data(N: int, J: float = 1.0):
+    """Heisenberg ring at S^z = 0 (N/2 up spins) with the translation group
+    (``models/heisenberg.py:97-118``)."""
+    model = build_heisenberg_second_quantized_model(N, J)
+    return _translation_ed_data(model, Fraction(N // 2, model.lattice.n_site))
+
+
+def build_spinful_hubbard_ed_data(sample_size: list[int], t: float = 1.0, U: float = 8.0):
+    """Spinful Hubbard at half filling (Lx * Ly particles on 2 Lx Ly
+    spin-orbitals, total particle number) with the translation group
+    (``models/hubbard.py:102-127``)."""
+    model = build_spinful_hubbard_second_quantized_model(sample_size, t, U)
+    return _translation_ed_data(model, Fraction(sample_size[0] * sample_size[1], model.lattice.n_site))
+
+
+def build_bosonic_fci_ed_data(*, sample_size=None, params=None, filling_fraction_per_band=Fraction(1, 2)):
+    """Haldane-boson FCI ED data (``models/bosonic_fci.py:394-424``): filling
+    per flat band over the number of sublattices."""
+    model = build_zero_flux_bosonic_fci_second_quantized_model(
+        sample_size=[3, 4] if sample_size is None else sample_size,
+        params=dict(params_DNSheng) if params is None else params)
+    return _translation_ed_data(model, Fraction(filling_fraction_per_band) / model.lattice.n_sub)
+
+
+def build_fermionic_fci_ed_data(*, sample_size=None, params=None, filling_fraction_per_band=Fraction(1, 3)):
+    """Checkerboard-fermion FCI ED data (``models/fermionic_fci.py:548-581``)."""
+    model = build_zero_flux_fermionic_fci_second_quantized_model(
+        sample_size=[3, 4] if sample_size is None else sample_size,
+        params=dict(params_Sun_Gu_Katsura_Sarma) if params is None else params)
+    return _translation_ed_data(model, Fraction(filling_fraction_per_band) / model.lattice.n_sub)
 
 
 # ---------------------------------------------------------------------------

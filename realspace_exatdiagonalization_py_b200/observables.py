@@ -55,6 +55,17 @@ import numpy as np
 __all__ = ["flux_spectrum_flow", "many_body_chern_number", "flux_charge_pump", "many_body_position_phases"]
 
 
+def _no_figure(fig_path) -> None:
+    """The drivers accept the reference's ``fig_path`` and return it in their
+    results, but draw no figure: plotting is presentation, outside this
+    package (the reference draws with matplotlib)."""
+    if fig_path is not None:
+        import warnings
+
+        warnings.warn(f"fig_path={fig_path!r}: figures are not drawn by this package; the results carry the data",
+                      stacklevel=3)
+
+
 def _labels(sector_labels):
     if isinstance(sector_labels, str):
         ident = sector_labels == "identity"
@@ -131,20 +142,7 @@ def flux_spectrum_flow(model, sector_labels, *, filling_fraction, flux_direction
             checkpoint_paths.append(ck.path_of(sm, tuple(flux)))
     else:
         raise ValueError(f"unknown engine {engine!r}")
-    if fig_path is not None:
-        import matplotlib.pyplot as plt  # optional, as in the reference
-
-        os.makedirs(os.path.dirname(os.path.abspath(fig_path)), exist_ok=True)
-        fig, ax = plt.subplots(figsize=(8.0, 6.0))
-        ax.set_xlabel(f"Inserted Flux [2π] along Direction-{flux_direction}")
-        ax.set_ylabel("E")
-        for isec in range(len(labels)):
-            for level in range(nev):
-                ax.plot(thetas, energies[:, isec, level], alpha=1 - level / nev, linewidth=2,
-                        label=f"sector {labels[isec]!r}" if level == 0 else None)
-        ax.legend(loc="best")
-        fig.tight_layout()
-        fig.savefig(fig_path)
+    _no_figure(fig_path)
     return SimpleNamespace(twisted_phases_over_2π_list=thetas, energies=energies, sector_labels=labels,
                            flux_direction=flux_direction, nev=nev, is_identity=is_identity, fig_path=fig_path,
                            checkpoint_paths=checkpoint_paths)
@@ -258,21 +256,6 @@ def _chern_point(model, labels, base, filling_fraction, flux, nev_per_sector, mo
             level_labels.append((label, level + 1))
             row += 1
     return energies, level_labels, path
-
-
-def _plot_many_body_chern_curvature(result, *, fig_path: str | None = None):
-    import matplotlib.pyplot as plt  # optional, as in the reference
-
-    fig, ax = plt.subplots(figsize=(6.5, 5.4))
-    ax.set_xlabel("θ_x / 2π")
-    ax.set_ylabel("θ_y / 2π")
-    ax.set_title(f"Flux-torus Berry curvature, C={result.chern_number:.6f}")
-    mesh = ax.pcolormesh(result.flux_x, result.flux_y, result.berry_curvature.T, shading="auto", cmap="RdBu")
-    fig.colorbar(mesh, ax=ax, label="plaquette phase")
-    if fig_path is not None:
-        os.makedirs(os.path.dirname(os.path.abspath(fig_path)), exist_ok=True)
-        fig.savefig(fig_path)
-    return fig, ax
 
 
 def _chern_served(model, labels, n_filled, flux_x, flux_y, nev_per_sector, checkpoint_dir, overwrite):
@@ -427,8 +410,7 @@ def many_body_chern_number(model, sector_labels, *, filling_fraction, flux_grid_
                           min_link_det=min(float(det_abs_x.min()), float(det_abs_y.min())),
                           link_det_abs_x=det_abs_x, link_det_abs_y=det_abs_y, checkpoint_paths=checkpoint_paths,
                           fig_path=fig_path)
-    if fig_path is not None:
-        _plot_many_body_chern_curvature(res, fig_path=fig_path)
+    _no_figure(fig_path)
     return res
 
 
@@ -666,21 +648,7 @@ def flux_charge_pump(model, sector_labels, *, filling_fraction, flux_direction: 
     polarizations = _tracked_phase_branches(raw)
     trajectories = polarizations - polarizations[0:1, :]
     pumped = trajectories[-1, :]
-    if fig_path is not None:
-        import matplotlib.pyplot as plt  # optional, as in the reference
-
-        os.makedirs(os.path.dirname(os.path.abspath(fig_path)), exist_ok=True)
-        fig, ax = plt.subplots(figsize=(8.0, 6.0))
-        ax.set_xlabel(f"Inserted Flux [2π] along Direction-{flux_direction}")
-        ax.set_ylabel("Pumped Charge ΔQ")
-        ax.set_title(f"{model.lattice.sample_size}-sample Charge Pump — sectors: "
-                     + ", ".join(repr(lab) for lab in labels))
-        for b, st in enumerate(specs):
-            ax.plot(thetas, trajectories[:, b], linewidth=2, label=f"sector {st.sector!r}, level {st.level}")
-            ax.scatter(thetas, trajectories[:, b], s=12)
-        ax.legend(loc="best")
-        fig.tight_layout()
-        fig.savefig(fig_path)
+    _no_figure(fig_path)
     return SimpleNamespace(twisted_phases_over_2π_list=thetas, energies=energies, sector_labels=labels,
                            flux_direction=flux_direction, polarization_direction=polarization_direction,
                            nev_per_sector=max_level, manifold_states=specs, polarization_eigenvalues=pol_ev,

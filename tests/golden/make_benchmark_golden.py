@@ -6,10 +6,10 @@ single-sector times of both modes (seconds on the reference's 12-core CPU).  The
 benchmark builds the models with build_heisenberg_ed_data(N) (J = 1, half
 filling), build_bosonic_fci_ed_data(sample_size=...) (params_DNSheng, a
 quarter of the vertices filled) and build_spinful_hubbard_ed_data(sample_size)
-(t = 1, U = 8, half filling, total particle number).  Runs where the
-reference checkout is present:
+(t = 1, U = 8, half filling, total particle number).  Runs where a
+reference checkout is present (its root in RSED_REFERENCE_ROOT):
 
-    python tests/golden/make_benchmark_golden.py
+    RSED_REFERENCE_ROOT=<checkout> python tests/golden/make_benchmark_golden.py
 """
 
 import csv
@@ -18,10 +18,14 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-CSV = "/root/reference/benchmark/benchmark_data/benchmark_raw_latest_py.csv"
+CSV_REL = os.path.join("benchmark", "benchmark_data", "benchmark_raw_latest_py.csv")
 
 
 def main():
+    root = os.environ.get("RSED_REFERENCE_ROOT")
+    if not root:
+        raise SystemExit("set RSED_REFERENCE_ROOT to the reference checkout")
+    CSV = os.path.join(root, CSV_REL)
     allrows = list(csv.DictReader(open(CSV)))
     rows = [r for r in allrows if r["mode"] == "matrixfree"]
     t_matrix = {(r["model"], r["label"]): float(r["elapsed_s"]) for r in allrows if r["mode"] == "matrix"}

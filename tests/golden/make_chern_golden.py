@@ -60,7 +60,7 @@ def main():
     pkg = ref_shim.PKG
     if pkg + ".observables" not in sys.modules:
         obs = types.ModuleType(pkg + ".observables")
-        obs.__path__ = [os.path.join(ref_shim.REFERENCE_ROOT, "src", pkg, "observables")]
+        obs.__path__ = [os.path.join(ref_shim.package_dir(), "observables")]
         sys.modules[pkg + ".observables"] = obs
     mbc = importlib.import_module(pkg + ".observables.many_body_chern_number")
     for name, (kind, sample, n_part, labels, nev, grid) in CASES.items():

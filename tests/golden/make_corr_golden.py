@@ -70,7 +70,7 @@ def main():
     pkg = ref_shim.PKG
     if pkg + ".observables" not in sys.modules:
         obs = types.ModuleType(pkg + ".observables")
-        obs.__path__ = [os.path.join(ref_shim.REFERENCE_ROOT, "src", pkg, "observables")]
+        obs.__path__ = [os.path.join(ref_shim.package_dir(), "observables")]
         sys.modules[pkg + ".observables"] = obs
     ssf = importlib.import_module(pkg + ".observables.static_structure_factor")
     odl = importlib.import_module(pkg + ".observables.off_diagonal_long_range_order")

@@ -31,7 +31,7 @@ def main():
     pkg = ref_shim.PKG
     if pkg + ".observables" not in sys.modules:
         obs = types.ModuleType(pkg + ".observables")
-        obs.__path__ = [os.path.join(ref_shim.REFERENCE_ROOT, "src", pkg, "observables")]
+        obs.__path__ = [os.path.join(ref_shim.package_dir(), "observables")]
         sys.modules[pkg + ".observables"] = obs
     sf = importlib.import_module(pkg + ".observables.spectrum_flow")
     model = R.bosonic.build_zero_flux_bosonic_fci_second_quantized_model(sample_size=[2, 3],

@@ -43,7 +43,7 @@ def load_expand():
     pkg = ref_shim.PKG
     if pkg + ".observables" not in sys.modules:
         obs = types.ModuleType(pkg + ".observables")
-        obs.__path__ = [os.path.join(ref_shim.REFERENCE_ROOT, "src", pkg, "observables")]
+        obs.__path__ = [os.path.join(ref_shim.package_dir(), "observables")]
         sys.modules[pkg + ".observables"] = obs
     es = importlib.import_module(pkg + ".observables.entanglement_spectrum")
     return R, es._expand_sector_state_to_fock_amplitudes

@@ -61,7 +61,7 @@ def main():
     pkg = ref_shim.PKG
     if pkg + ".observables" not in sys.modules:
         obs = types.ModuleType(pkg + ".observables")
-        obs.__path__ = [os.path.join(ref_shim.REFERENCE_ROOT, "src", pkg, "observables")]
+        obs.__path__ = [os.path.join(ref_shim.package_dir(), "observables")]
         sys.modules[pkg + ".observables"] = obs
     cp = importlib.import_module(pkg + ".observables.charge_pump")
     for name, c in CASES.items():

@@ -167,7 +167,7 @@ def test_served_request_vectors_are_eigenvectors():
         basis = ed.Symmetry_Sector_Basis(ctx.irreps[s], ctx.catalog, ctx.sset, s)
         H = ed.MatrixFreeHamiltonian(basis, ctx.dm.bilinear_terms, ctx.dm.density_terms, None, model=ctx.dm)
         Hv = H.matvec_device(v.contiguous(), 2)
-        # the operator applies H^dagger = H
+        # the operator applies H
         for j in range(2):
             r = torch.linalg.vector_norm(Hv[:, j] - res[rid].eigenvalues[j] * v[:, j]).item()
             assert r < 1e-8, r

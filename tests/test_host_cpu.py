@@ -19,7 +19,10 @@ from realspace_exatdiagonalization_py_b200.symmetry import (
     unrank_combination,
 )
 
+from oracle import ref_shim
+
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLDEN = os.path.join(ROOT, "tests", "golden")
 
 
 def _multiset(terms, digits=14):
@@ -241,3 +244,84 @@ def test_periodic_check_schedule():
             for last in range(first - 2, first + 30):
                 want = any((i + 1) % ce == 0 for i in range(first, last + 1))
                 assert LanczosBatch.periodic_check_in(stub, first, last) == want
+
+
+# Names of the reference's top-level API that this package does not provide,
+# each outside the hot path: plotting (matplotlib figures), entanglement
+# spectra and the full-ED density distribution (post-processing observables),
+# and the model modules' figure-writing example drivers.
+OUT_OF_SCOPE_EXPORTS = {
+    "plot_ed_scan_res", "plot_spectrum", "plot_entanglement_spectrum", "plot_odlro_map", "plot_odlro_map_panels",
+    "plot_particle_entanglement_spectrum", "plot_structure_factor_allowed_momenta",
+    "plot_structure_factor_allowed_momenta_panels", "plot_structure_factor_map", "plot_structure_factor_map_panels",
+    "entanglement_spectrum", "particle_entanglement_spectrum", "vertices_occupation_distribution_full_ed",
+    "test_bosonic_fci_charge_pump", "test_bosonic_fci_spectrum_flow", "test_fermionic_fci_charge_pump",
+    "test_fermionic_fci_full_ed", "test_fermionic_fci_spectrum_flow",
+}
+
+
+def test_package_exports_the_reference_api():
+    """Every name the reference re-exports at top level is importable from
+    this package, except the explicit out-of-scope list above."""
+    import json
+
+    import realspace_exatdiagonalization_py_b200 as pkg
+
+    names = json.load(open(os.path.join(GOLDEN, "reference_exports.json")))["names"]
+    missing = sorted(n for n in names if n not in OUT_OF_SCOPE_EXPORTS and not hasattr(pkg, n))
+    assert not missing, missing
+    assert OUT_OF_SCOPE_EXPORTS <= set(names)
+
+
+def test_bit_utilities_known_answers():
+    from realspace_exatdiagonalization_py_b200 import bits
+
+    m = 0b10110
+    assert list(bits.filled_site_iter_for_mask(m, 5)) == [2, 3, 5]
+    assert list(bits.empty_site_iter_for_mask(m, 5)) == [1, 4]
+    assert bits.decode_bit_mask_to_configuration(m, 5) == [2, 3, 5]
+    assert bits.encode_configuration_to_bit_mask([2, 3, 5]) == m
+    occ = [0, 0, 0]
+    assert bits.decode_bit_mask_to_configuration_inplace(occ, m, 5) is occ and occ == [2, 3, 5]
+    with pytest.raises(AssertionError):
+        bits.decode_bit_mask_to_configuration_inplace([0, 0], m, 5)
+    assert bits.bitmask_of_site(1) == 1 and bits.bitmask_of_site(63) == 1 << 62
+    assert bits.occupy_site_for_mask(m, 1) == 0b10111 and bits.empty_site_for_mask(m, 2) == 0b10100
+    assert bits.is_site_occupied(m, 2) and bits.is_site_empty(m, 1) and bits.n_occupied_for_mask(m) == 3
+    assert bits.as_uint64_array([m, 1 << 62]).dtype == np.uint64
+
+
+@pytest.mark.skipif(not ref_shim.available(), reason="reference package not present")
+def test_bit_utilities_match_reference():
+    import importlib
+
+    from realspace_exatdiagonalization_py_b200 import bits
+
+    ref_shim.load()
+    rb = importlib.import_module(ref_shim.PKG + ".utils.bitwise_operations")
+    rng = np.random.default_rng(5)
+    for _ in range(200):
+        n = int(rng.integers(1, 64))
+        m = int(rng.integers(0, 1 << n, dtype=np.uint64))
+        i = int(rng.integers(1, n + 1))
+        for f in ("occupy_site_for_mask", "empty_site_for_mask", "is_site_occupied", "is_site_empty"):
+            assert getattr(bits, f)(m, i) == getattr(rb, f)(m, i), f
+        assert bits.n_occupied_for_mask(m) == rb.n_occupied_for_mask(m)
+        assert list(bits.filled_site_iter_for_mask(m, n)) == list(rb.filled_site_iter_for_mask(m, n))
+        assert list(bits.empty_site_iter_for_mask(m, n)) == list(rb.empty_site_iter_for_mask(m, n))
+        occ = rb.decode_bit_mask_to_configuration(m, n)
+        assert bits.decode_bit_mask_to_configuration(m, n) == occ
+        assert bits.encode_configuration_to_bit_mask(occ) == rb.encode_configuration_to_bit_mask(occ)
+
+
+def test_default_fci_sectors():
+    from realspace_exatdiagonalization_py_b200 import models
+
+    assert models.default_fci_sectors([3, 4]) == [(0, 0), (0, 2)]
+    assert models.default_fci_sectors([9, 9]) == [(0, 0)]
+    assert models.default_fci_sectors_fermionic([2, 3]) == [(0, 0), (0, 1), (0, 2)]
+    with pytest.raises(ValueError):
+        models.default_fci_sectors_fermionic([9, 9])
+    tb = models.build_fermionic_checkerboard_tb_model(sample_size=[2, 3])
+    assert tb.lattice.n_site == 12
+    assert models.CHECKERBOARD_TPP_DENOMINATOR == pytest.approx(2 + 2 * np.sqrt(2))
