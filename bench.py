@@ -341,28 +341,20 @@ def proj_apply_unique_bytes(n_hops: int, n_orb: int, n_cols: int, prec: int) -> 
     return n_hops * (4 + wb) + (n_orb + 1) * 8 + n_orb * (8 + 16) + n_orb * n_cols * (wb + 16)
 
 
-def lanczos_step_bytes(n_orb: int, batch, iters: list[int]) -> dict:
-    """Algorithmic bytes of the Gram reductions and the block updates of one
-    batched solve, from each instance's iteration count.  After
-    ``rsed_lanczos_start`` the basis holds 1 block; iteration k (1-based)
-    reduces against the current nb blocks and appends one; at nb = n_slots + 1
-    a thick restart leaves keep + 1.  Per instance (b columns, 16-B complex128
-    entries, all n_orb rows of the orbit layout) and iteration with basis
-    length nb, each of the two passes: the reduction reads the nb blocks and W
-    once ((nb + 1) n b 16 B); the update reads them once and writes W (pass 1)
-    or the new basis block (pass 2) once ((nb + 2) n b 16 B), plus the FP32
-    copy of the new block (n b 8 B) in an FP32-matvec solve."""
-    S, keep = batch.p.n_slots, batch.keep
+def lanczos_step_bytes(n_orb: int, batch, state) -> dict:
+    """Algorithmic bytes of the Gram reductions and block updates of one
+    batched solve, from the counters the kernels keep per instance
+    (state[:, 12] = basis blocks + W read by every executed Gram-Schmidt
+    pass, state[:, 13] = executed passes).  A reduction reads its nb blocks
+    and W once ((nb + 1) n b 16 B); the update after it reads them once more
+    and writes W or the new basis block once ((nb + 2) n b 16 B), plus the
+    FP32 copy of every new block (n b 8 B) in an FP32-matvec solve."""
     red = upd = 0
-    for b, it in zip(batch.block_sizes, iters):
-        nb = 1
-        for _ in range(it):
-            blk = n_orb * b * 16
-            red += 2 * (nb + 1) * blk
-            upd += 2 * (nb + 2) * blk + (n_orb * b * 8 if batch.p.precision == 32 else 0)
-            nb += 1
-            if nb == S + 1:
-                nb = keep + 1
+    for i, b in enumerate(batch.block_sizes):
+        blk = n_orb * b * 16
+        blocks, passes, steps = int(state[i, 12]), int(state[i, 13]), int(state[i, 3])
+        red += blocks * blk
+        upd += (blocks + passes) * blk + (steps * n_orb * b * 8 if batch.p.precision == 32 else 0)
     return {"reduce": red, "update": upd}
 
 
@@ -841,6 +833,82 @@ def small_config_line(ed, models, name, precision=32, steps=10):
             "ms_per_step": 1e3 * sum(times) / steps, "max_abs_dE_vs_reference": de if ref is not None else None}
 
 
+def config5_line(ed, models, n_sectors=4, nev=6, cpp_threads=0):
+    """The 48-site checkerboard (4x6x2, 8 fermions, C(48,8) = 377,348,994
+    states, |G| = 24): device catalog, then a batched solve (FP32 matvec + FP64
+    refinement, nev 6) of ``n_sectors`` sectors, timed; the C++ restatement
+    (oracle/cpu_ref.cpp, OpenMP on the host cores -- the reference cannot rank
+    beyond 42 sites) builds the same catalog, compared by SHA-256 digests of
+    the tables, and applies the first sector's operator once to a seeded
+    vector, compared with the device's apply; its catalog and apply times are
+    the CPU figures, a sector solve extrapolated from one apply times the
+    device solve's matvec count (labelled: not the reference, extrapolated)."""
+    import hashlib
+
+    import torch
+
+    from oracle import cpu, port
+
+    model, nf = models.config_model("checkerboard48")
+    G = ed.build_translation_group(model.lattice)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    data = ed.build_ed_data(model, filling_fraction=Fraction(nf, 48), symmetry_group=G)
+    dm, sset = data._device()
+    torch.cuda.synchronize()
+    t_cat = time.perf_counter() - t0
+    secs = list(range(n_sectors))
+    cfg = ed.SolverConfig((2,) * n_sectors, 0, True, 16)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = ed.solve_sectors_batched(data, secs, nev=nev, precision=32, config=cfg, return_vectors=False)
+    torch.cuda.synchronize()
+    t_solve = time.perf_counter() - t0
+    solver = next(iter(data.__dict__.get("_solvers", {}).values()), None)
+    st = solver.batch.status() if solver is not None else None
+    iters = [int(x) - 1 for x in st[:, 3]] if st is not None else []
+    cat = data.orbit_catalog
+    tab = cat.table.cpu().numpy()
+    dev_digest = {k: hashlib.sha256(np.ascontiguousarray(tab[:, i]).tobytes()).hexdigest()
+                  for k, i in (("rep_rank", 0), ("rep_sym", 1), ("rep_amp_re", 2), ("rep_amp_im", 3))}
+    dev_digest["reprs"] = hashlib.sha256(cat.repr_masks.cpu().numpy().view(np.uint64).tobytes()).hexdigest()
+    del tab
+    perm0, eta = port.group_arrays(G)
+    t0 = time.perf_counter()
+    ref = cpu.catalog(48, nf, perm0, eta, True, nthreads=cpp_threads)
+    t_cpp_cat = time.perf_counter() - t0
+    amp = ref["rep_amp"].view(np.int32).reshape(-1, 2)
+    cpp_digest = {"rep_rank": hashlib.sha256(ref["rep_rank"].tobytes()).hexdigest(),
+                  "rep_sym": hashlib.sha256(ref["rep_sym"].tobytes()).hexdigest(),
+                  "rep_amp_re": hashlib.sha256(np.ascontiguousarray(amp[:, 0]).tobytes()).hexdigest(),
+                  "rep_amp_im": hashlib.sha256(np.ascontiguousarray(amp[:, 1]).tobytes()).hexdigest(),
+                  "reprs": hashlib.sha256(ref["reprs"].tobytes()).hexdigest()}
+    del amp
+    chi = np.asarray(data.irrep_list[0].values, dtype=np.complex128)
+    op = cpu.SectorOperator(ref, chi, model.bilinear_terms, model.density_density_terms, nthreads=cpp_threads)
+    x = np.random.default_rng(48).standard_normal(op.n) + 1j * np.random.default_rng(49).standard_normal(op.n)
+    t0 = time.perf_counter()
+    y_cpp = op(x)
+    t_cpp_apply = time.perf_counter() - t0
+    basis = ed.Symmetry_Sector_Basis(data.irrep_list[0], cat, sset, 0)
+    H = ed.MatrixFreeHamiltonian(basis, model.bilinear_terms, model.density_density_terms, None, model=dm)
+    y_dev = H.adjoint_device(torch.from_numpy(x).cuda()).cpu().numpy()[:, 0]
+    mv_err = float(np.abs(y_dev - y_cpp).max() / np.abs(y_cpp).max())
+    applies = (max(iters) + 1) if iters else None
+    return {"workload": "checkerboard48: 4x6x2 = 48 sites, 8 fermions, C(48,8) = 377,348,994 states, |G| = 24, "
+                        f"{cat.n_orbits:,} orbits; {n_sectors} sectors, nev {nev}, FP32 matvec + FP64 refinement",
+            "sector_dims": [int(sset.dims[s]) for s in secs],
+            "device": {"catalog_s": t_cat, "solve_s": t_solve, "sector_solves_per_s": n_sectors / t_solve,
+                       "lanczos_steps": iters, "single_pass_steps": None if st is None else int(st[:, 11].sum()),
+                       "E0": [float(res[s][0][0]) for s in secs]},
+            "cpp_restatement": {"kind": "port", "label": "C++ restatement of the reference's algorithm, not the "
+                                "reference (which cannot rank beyond 42 sites)", "threads": cpp_threads or _NCPU,
+                                "catalog_s": t_cpp_cat, "apply_s": t_cpp_apply,
+                                "sector_solve_s_extrapolated": None if applies is None else t_cpp_apply * applies,
+                                "extrapolation": "one apply x (device Lanczos steps + 1) of the slowest sector"},
+            "parity": {"catalog_digests_equal": dev_digest == cpp_digest, "apply_max_rel_diff": mv_err}}
+
+
 def run_b200(args):
     import torch
 
@@ -878,7 +946,7 @@ def run_b200(args):
 
     # how the batch runs (block sizes, persistent cluster or graph path,
     # projection table, basis length) is picked by the autotuner, untimed
-    params = ed.LanczosParams(precision=args.precision)
+    params = ed.LanczosParams(precision=args.precision, single_pass=not args.two_pass)
     tuner = ed.Autotuner(trials=2)
     t0 = time.perf_counter()
     if args.solver == "auto":
@@ -967,6 +1035,7 @@ def run_b200(args):
     if rank == 0:
         # per-kernel device time of one step (CUPTI) and algorithmic bytes
         agg = cupti_kernels(step)
+        st_prof = b.status()  # the kernels' counters for the profiled step
         extra["step_kernel_shares"] = kernel_shares(agg)
         fams = {}
         nh = dm.proj["n_hops"]
@@ -978,14 +1047,15 @@ def run_b200(args):
                 "launches": n_mv, "avg_launch_us": us_mv / n_mv,
                 "alg_bytes_per_launch": proj_apply_unique_bytes(nh, n_orb, b.n_cols, args.precision),
                 "unit_bytes": "per hop 4 + 8 B table, per row 8 + 8 + 16 B, per element x 8 B + y 16 B, once each"}
-        lb = lanczos_step_bytes(n_orb, b, iters)
+        lb = lanczos_step_bytes(n_orb, b, st_prof)
         for key, fam in (("reduce", "k_lz_reduce"), ("update", "k_lz_update")):
             n_k, us_k = _family(agg, fam)
             if n_k:
                 fams[fam] = {"kernel": f"{fam}* (FP64 block Gram-Schmidt, two passes per iteration)",
                              "launches": n_k, "avg_launch_us": us_k / n_k,
                              "alg_bytes_per_launch": lb[key] / n_k,
-                             "unit_bytes": "per pass (nb + 1) resp. (nb + 2) basis blocks of n_orb x b x 16 B"}
+                             "unit_bytes": "per executed pass (nb + 1) resp. (nb + 2) blocks of n_orb x b x 16 B "
+                                           "(kernel-side counters)"}
         for k, f in fams.items():
             f["achieved_GBs"] = f["alg_bytes_per_launch"] / (f["avg_launch_us"] * 1e-6) / 1e9
             f["frac"] = f["achieved_GBs"] / peak_gbs
@@ -1002,7 +1072,9 @@ def run_b200(args):
                     "peak_source": peak_src, "share_of_step": f["share_of_step"]}
             if tr is not None:
                 roof["traffic_source"] = tr["profile"]
-        extra["lanczos_iterations"] = {"min": min(iters), "max": max(iters)}
+        extra["lanczos_iterations"] = {"min": min(iters), "max": max(iters), "steps": int(sum(iters)),
+                                       "single_pass_steps": int(st[:, 11].sum()),
+                                       "gram_schmidt": "two passes" if args.two_pass else "adaptive single pass"}
         extra["residual_norm_max"] = resid_max
         if fe is not None:
             extra["fp32_matvec_error_before_refinement"] = {"max": float(fe.max()), "median": float(np.median(fe))}
@@ -1142,6 +1214,10 @@ def main():
                     help="seconds of reference sector solves for --impl reference (at least one solve)")
     ap.add_argument("--skip-scale", action="store_true", help="skip the serving / config-2 / benchmark extras")
     ap.add_argument("--skip-fp64", action="store_true", help="skip the FP64-matvec batched variant")
+    ap.add_argument("--two-pass", action="store_true",
+                    help="always two Gram-Schmidt passes per step (no adaptive single pass)")
+    ap.add_argument("--config5", type=int, default=0,
+                    help="only the 48-site checkerboard line for this many sectors (device vs C++ restatement)")
     ap.add_argument("--solver", default="auto",
                     help='"auto" (measured by the autotuner) or "graph:<block>:<proj|otf>:<n_slots>"')
     ap.add_argument("--matvec-only", action="store_true",
@@ -1183,7 +1259,7 @@ def main():
         run_reference(args)
         return
     special = args.reference_benchmark or args.corr or args.serving_only or args.overlap_only or args.chern \
-        or args.matvec_only
+        or args.matvec_only or args.config5
     if special:
         import realspace_exatdiagonalization_py_b200 as ed
         from realspace_exatdiagonalization_py_b200 import models
@@ -1201,6 +1277,8 @@ def main():
                           **overlap_row(ed, 10_518_300, 2, args.overlap_only, peak_gbs)}), flush=True)
     elif args.chern:
         print(json.dumps(chern_at_scale(ed, models, grid=args.chern, peak_gbs=peak_gbs)), flush=True)
+    elif args.config5:
+        print(json.dumps(config5_line(ed, models, n_sectors=args.config5)), flush=True)
     elif args.matvec_only:
         precs = (args.matvec_precision,) if args.matvec_precision else (32, 64)
         print(json.dumps(matvec_at_scale(ed, models, peak_gbs, n_launch=args.matvec_launches, precisions=precs,

@@ -328,7 +328,11 @@ int rsed_density_pairs(int32_t n_site, int64_t n_orbits, const uint64_t* repr_ma
  * buffers described by rsed_lanczos_t.  rsed_lanczos_iterate advances every
  * active instance by n_iter block steps without host synchronisation or
  * allocation (capturable in a CUDA graph); per-instance status is read from
- * state[16*i + 1] (0 running, 1 converged, RSED_E* on failure). */
+ * state[16*i + 1] (0 running, 1 converged, RSED_E* on failure); state[16*i + 3]
+ * counts block steps + 1, state[16*i + 11] the steps that took a single
+ * Gram-Schmidt pass, state[16*i + 12] the basis blocks (plus W) read by all
+ * executed Gram-Schmidt passes and state[16*i + 13] those passes (each
+ * pass's update reads one block more and writes one). */
 typedef struct {
   int32_t n_inst;        /* instances (sector solves) in the batch */
   int32_t n_slots;       /* basis blocks before a thick restart (n_slots*bmax <= 64) */
@@ -339,7 +343,10 @@ typedef struct {
   int32_t bmax;          /* largest instance block size (<= 8) */
   int32_t chunk_rows;    /* rows per reduction chunk */
   int32_t pm;            /* leading dimension of the projected matrices >= (n_slots+1)*bmax */
-  int32_t reserved;
+  int32_t reserved;      /* bit 0: adaptive single Gram-Schmidt pass (pass 1 removes the part of
+                          * the recurrence known from the projected matrix; pass 2 is skipped per
+                          * instance when no Cholesky pivot of pass 1 lost more than 7/8 of its
+                          * column's norm^2) */
   double tol;            /* converged when ||r_j|| <= tol * max(1, |theta_j|) for j < nev */
   const int32_t* inst_col0;  /* n_inst: first column of each instance */
   const int32_t* inst_b;     /* n_inst: block size of each instance */

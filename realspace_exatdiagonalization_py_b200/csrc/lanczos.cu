@@ -18,7 +18,17 @@
 //   restart  V_0..keep-1 = V S_keep, residual block moved behind them
 //
 // The reorthogonalisation is block classical Gram-Schmidt with the Pythagorean
-// Cholesky update, applied twice (one reduction per pass).
+// Cholesky update, one reduction per pass.  With the adaptive single pass
+// (st.reserved bit 0), pass 1 orthogonalises W_loc = W - sigma X - sum_{l<j}
+// V_l P[j, l]^H, i.e. W with the part of the Lanczos recurrence already known
+// from the projected matrix removed (the coupling to the previous block, or
+// to the Ritz vectors after a thick restart, and a shift sigma = diag of the
+// previous diagonal block), formed row by row while W is staged; when the
+// smallest Cholesky pivot of W_loc - V C still carries at least 1/8 of its
+// column's squared norm (little cancellation: orthogonality and
+// normalisation after one pass are within a few ulps of two passes), pass 1
+// writes the new basis block directly and pass 2 is skipped for that
+// instance; otherwise pass 2 runs as before.
 #include <cooperative_groups.h>
 #include <type_traits>
 #include "rsed_internal.cuh"
@@ -45,7 +55,11 @@ constexpr size_t kRitzSmem = sizeof(double2) * (kJacobiMax * (kJacobiMax + 1) + 
                              sizeof(double) * kJacobiMax * kKeepMax + kHermWork;
 // state fields
 constexpr int S_NB = 0, S_STATUS = 1, S_RESTARTS = 2, S_ITERS = 3, S_ACTIVE = 4, S_RESTART_NB = 5,
-              S_NEWSLOT = 6, S_NCONV = 7, S_TICKET = 8, S_RR = 9;
+              S_NEWSLOT = 6, S_NCONV = 7, S_TICKET = 8, S_RR = 9, S_ONEPASS = 10, S_ONEPASS_N = 11,
+              S_RED_BLOCKS = 12, S_PASSES = 13;  // basis blocks + W read by the executed passes, passes
+// single pass allowed when every Cholesky pivot^2 >= G_qq / kOnePassKappa2
+constexpr double kOnePassKappa2 = 8.0;
+constexpr int kFlagSinglePass = 1;
 
 struct LzDims {
   int64_t n_orb;
@@ -84,7 +98,7 @@ constexpr int kTileRows = 256;  // rows of W staged in shared memory per tile
 template <int BB>
 __device__ void lz_gram_chunk(const double2* __restrict__ V, const double2* __restrict__ W, int64_t slot_stride,
                               int64_t ld, int c0, int nb, int64_t r0, int64_t r1, double2* __restrict__ out,
-                              double2* buf) {
+                              double2* buf, const double2* Lc, const int* lnz, const double* sig, int jloc) {
   constexpr int SW = (kJacobiMax / BB + 1 + 7) / 8;  // most slots one warp owns
   constexpr int RPW = 32 / BB;                       // rows per warp pass
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -101,7 +115,21 @@ __device__ void lz_gram_chunk(const double2* __restrict__ V, const double2* __re
     __syncthreads();
     for (int i = threadIdx.x; i < nr * BB; i += kRT) {
       const int rr = i / BB, q = i % BB;
-      Wt[rr * BB + q] = W[(t0 + rr) * ld + c0 + q];
+      const int64_t row = t0 + rr;
+      double2 w = W[row * ld + c0 + q];
+      if (jloc > 0) {
+        // W_loc = W - sigma_q X_q - sum over the known couplings P[j, l]^H
+        const double2 x = V[(int64_t)jloc * slot_stride + row * ld + c0 + q];
+        w.x -= sig[q] * x.x;
+        w.y -= sig[q] * x.y;
+        for (int l = 0; l < jloc; ++l) {
+          if (!lnz[l]) continue;
+          const double2* Vl = V + (int64_t)l * slot_stride + row * ld + c0;
+#pragma unroll
+          for (int pp = 0; pp < BB; ++pp) w = csub(w, cmul(Vl[pp], Lc[(l * BB + pp) * kBMax + q]));
+        }
+      }
+      Wt[rr * BB + q] = w;
     }
     __syncthreads();
     if (act) {
@@ -155,7 +183,8 @@ __device__ void lz_gram_chunk(const double2* __restrict__ V, const double2* __re
 // then in order: deterministic for a given chunk count), form
 // G' = G - C^H C, its Cholesky factor R and the projected-matrix entries.
 __device__ void lz_finalize(const rsed_lanczos_t& st, const LzDims& d, int inst, int pass, int b, int nb, int* stt,
-                            double2* sc, double2* sR, double2* sG, int* s_ok, double2* fin) {
+                            double2* sc, double2* sR, double2* sG, int* s_ok, double2* fin, bool loc,
+                            int* s_one) {
   const double2* part = reinterpret_cast<const double2*>(st.partial);
   // ---- finalisation (one block per instance) ----
   // G threads per entry sum interleaved chunk subsets, then the G partial
@@ -216,9 +245,38 @@ __device__ void lz_finalize(const rsed_lanczos_t& st, const LzDims& d, int inst,
       stt[S_STATUS] = RSED_EBREAKDOWN;
       stt[S_ACTIVE] = 0;
     }
+    // single pass when no pivot lost more than 7/8 of its column's norm^2
+    bool one = ok && pass == 1 && nb >= 1 && (st.reserved & kFlagSinglePass);
+    for (int q = 0; q < b && one; ++q) {
+      const double gq = sc[(nb * b + q) * kBMax + q].x;
+      one = sR[q * kBMax + q].x * sR[q * kBMax + q].x * kOnePassKappa2 >= gq;
+    }
+    *s_one = one;
+    if (pass == 1) stt[S_ONEPASS] = one;
+    if (ok) {
+      stt[S_RED_BLOCKS] += nb + 1;
+      stt[S_PASSES] += 1;
+    }
   }
   __syncthreads();
   if (!*s_ok) return;
+  if (loc) {
+    // coefficients of W itself: C + the local part taken off before the Gram
+    const double2* Pi = reinterpret_cast<const double2*>(st.P) + (int64_t)inst * d.pm * d.pm;
+    const int j = nb - 1;
+    for (int e = threadIdx.x; e < nb * b * b; e += blockDim.x) {
+      const int r = e / b, q = e % b;
+      double2 add;
+      if (r < j * b) {
+        add = cconj(Pi[(int64_t)(j * b + q) * d.pm + r]);
+      } else {
+        const int p = r - j * b;
+        add = make_double2(p == q ? Pi[(int64_t)((j - 1) * b + q) * d.pm + (j - 1) * b + q].x : 0.0, 0.0);
+      }
+      sc[r * kBMax + q] = cadd(sc[r * kBMax + q], add);
+    }
+    __syncthreads();
+  }
   double2* coefp = reinterpret_cast<double2*>(st.coef) + (int64_t)inst * 2 * d.pslots * kBMax * kBMax;
   double2* cp = coefp + (pass - 1) * d.pslots * kBMax * kBMax;
   for (int e = threadIdx.x; e < nb * b * b; e += blockDim.x) {
@@ -227,6 +285,27 @@ __device__ void lz_finalize(const rsed_lanczos_t& st, const LzDims& d, int inst,
   }
   double2* Rout = cp + (d.pslots - 1) * kBMax * kBMax;
   for (int e = threadIdx.x; e < kBMax * kBMax; e += blockDim.x) Rout[e] = sR[e];
+  if (pass == 1 && *s_one) {
+    // one pass: P[:, cur] = C1, P[new, cur] = R1
+    double2* P = reinterpret_cast<double2*>(st.P) + (int64_t)inst * d.pm * d.pm;
+    const int cb = nb - 1;
+    for (int e = threadIdx.x; e < nb * b * b; e += blockDim.x) {
+      const int r = e / b, q = e % b;
+      P[(int64_t)r * d.pm + cb * b + q] = sc[r * kBMax + q];
+    }
+    for (int e = threadIdx.x; e < b * b; e += blockDim.x) {
+      const int p = e / b, q = e % b;
+      P[(int64_t)(nb * b + p) * d.pm + cb * b + q] = sR[p * kBMax + q];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      stt[S_NEWSLOT] = nb;
+      stt[S_NB] = nb + 1;
+      stt[S_ITERS] += 1;
+      stt[S_ONEPASS_N] += 1;
+    }
+    return;
+  }
   if (pass == 2) {
     const int nb_old = nb;
     if (nb_old >= 1) {
@@ -258,15 +337,21 @@ __device__ void lz_finalize(const rsed_lanczos_t& st, const LzDims& d, int inst,
 }
 
 __global__ void __launch_bounds__(kRT) k_lz_reduce(rsed_lanczos_t st, LzDims d, int pass) {
-  const int chunk = blockIdx.x;
-  const int inst = blockIdx.y;
+  // blocks of all instances over one row chunk are adjacent in launch order:
+  // they read the same rows (each its own columns), so L2 serves the rest of
+  // every DRAM line one of them fetched
+  const int chunk = blockIdx.x / d.n_inst;
+  const int inst = blockIdx.x % d.n_inst;
   int* stt = st.state + inst * kStateInts;
   if (pass == 1 && chunk == 0 && threadIdx.x == 0) stt[S_RESTART_NB] = 0;
   if (!stt[S_ACTIVE]) return;
+  if (pass == 2 && stt[S_ONEPASS]) return;  // pass 1 already wrote the new block
   const int b = st.inst_b[inst];
   const int c0 = st.inst_col0[inst];
   const int nb = stt[S_NB];
-  __shared__ int s_last;
+  __shared__ int s_last, s_one;
+  __shared__ double s_sig[kBMax];
+  __shared__ int s_lnz[kJacobiMax];
   __shared__ double2 sc[(kJacobiMax / 1 + kBMax + kBMax) * kBMax];  // C (nb*b rows) + G rows
   __shared__ double2 sR[kBMax * kBMax];
   __shared__ double2 sG[kBMax * kBMax];
@@ -288,18 +373,43 @@ __global__ void __launch_bounds__(kRT) k_lz_reduce(rsed_lanczos_t st, LzDims d, 
   const int64_t slot_stride = d.n_orb * d.ld;
   const int64_t pbase = ((int64_t)chunk * d.n_inst + inst) * (int64_t)d.pslots * kBMax * kBMax;
   __shared__ double2 red_l[kRT / 32][32][kBMax];  // W tile, lane sums, then the finalisation's partials
+  // the known part of the recurrence (pass 1 of a single-pass-enabled batch,
+  // basis of two or more blocks): L[l*b + p][q] = conj(P[j*b + q][l*b + p])
+  // for l < j = nb - 1 (staged in sc, which the finalisation rebuilds), and
+  // sigma_q = Re P[(j-1)*b + q][(j-1)*b + q]
+  const bool loc = pass == 1 && nb >= 2 && (st.reserved & kFlagSinglePass);
+  const int jloc = loc ? nb - 1 : 0;
+  if (loc) {
+    const double2* Pi = reinterpret_cast<const double2*>(st.P) + (int64_t)inst * d.pm * d.pm;
+    for (int e = threadIdx.x; e < jloc * b * b; e += kRT) {
+      const int r = e / b, q = e % b;
+      sc[r * kBMax + q] = cconj(Pi[(int64_t)(jloc * b + q) * d.pm + r]);
+    }
+    if (threadIdx.x < b)
+      s_sig[threadIdx.x] = Pi[(int64_t)((jloc - 1) * b + threadIdx.x) * d.pm + (jloc - 1) * b + threadIdx.x].x;
+    __syncthreads();
+    for (int l = threadIdx.x; l < jloc; l += kRT) {
+      int nz = 0;
+      for (int e = 0; e < b * b; ++e) {
+        const double2 v = sc[(l * b + e / b) * kBMax + e % b];
+        nz |= (v.x != 0.0) || (v.y != 0.0);
+      }
+      s_lnz[l] = nz;
+    }
+    __syncthreads();
+  }
   {
     double2* buf = &red_l[0][0][0];
     double2* out = part + pbase;
     switch (b) {
-      case 1: lz_gram_chunk<1>(V, W, slot_stride, d.ld, c0, nb, r0, r1, out, buf); break;
-      case 2: lz_gram_chunk<2>(V, W, slot_stride, d.ld, c0, nb, r0, r1, out, buf); break;
-      case 3: lz_gram_chunk<3>(V, W, slot_stride, d.ld, c0, nb, r0, r1, out, buf); break;
-      case 4: lz_gram_chunk<4>(V, W, slot_stride, d.ld, c0, nb, r0, r1, out, buf); break;
-      case 5: lz_gram_chunk<5>(V, W, slot_stride, d.ld, c0, nb, r0, r1, out, buf); break;
-      case 6: lz_gram_chunk<6>(V, W, slot_stride, d.ld, c0, nb, r0, r1, out, buf); break;
-      case 7: lz_gram_chunk<7>(V, W, slot_stride, d.ld, c0, nb, r0, r1, out, buf); break;
-      default: lz_gram_chunk<8>(V, W, slot_stride, d.ld, c0, nb, r0, r1, out, buf); break;
+      case 1: lz_gram_chunk<1>(V, W, slot_stride, d.ld, c0, nb, r0, r1, out, buf, sc, s_lnz, s_sig, jloc); break;
+      case 2: lz_gram_chunk<2>(V, W, slot_stride, d.ld, c0, nb, r0, r1, out, buf, sc, s_lnz, s_sig, jloc); break;
+      case 3: lz_gram_chunk<3>(V, W, slot_stride, d.ld, c0, nb, r0, r1, out, buf, sc, s_lnz, s_sig, jloc); break;
+      case 4: lz_gram_chunk<4>(V, W, slot_stride, d.ld, c0, nb, r0, r1, out, buf, sc, s_lnz, s_sig, jloc); break;
+      case 5: lz_gram_chunk<5>(V, W, slot_stride, d.ld, c0, nb, r0, r1, out, buf, sc, s_lnz, s_sig, jloc); break;
+      case 6: lz_gram_chunk<6>(V, W, slot_stride, d.ld, c0, nb, r0, r1, out, buf, sc, s_lnz, s_sig, jloc); break;
+      case 7: lz_gram_chunk<7>(V, W, slot_stride, d.ld, c0, nb, r0, r1, out, buf, sc, s_lnz, s_sig, jloc); break;
+      default: lz_gram_chunk<8>(V, W, slot_stride, d.ld, c0, nb, r0, r1, out, buf, sc, s_lnz, s_sig, jloc); break;
     }
   }
   __threadfence();
@@ -312,7 +422,8 @@ __global__ void __launch_bounds__(kRT) k_lz_reduce(rsed_lanczos_t st, LzDims d, 
   if (!s_last) return;
   __threadfence();
   if (threadIdx.x == 0) stt[S_TICKET] = 0;
-  lz_finalize(st, d, inst, pass, b, nb, stt, sc, sR, sG, &s_ok, &red_l[0][0][0]);
+  __syncthreads();  // sc (local coefficients) is rebuilt by the finalisation
+  lz_finalize(st, d, inst, pass, b, nb, stt, sc, sR, sG, &s_ok, &red_l[0][0][0], loc, &s_one);
 }
 
 // W <- (W - V C) R^-1 ; pass 2 writes the new basis block and the matvec input.
@@ -320,12 +431,15 @@ __global__ void __launch_bounds__(kRT) k_lz_reduce(rsed_lanczos_t st, LzDims d, 
 // memory; one thread per (row, column q) -- the b lanes of a row read the
 // row's segment together and solve with R across lanes by shuffles.
 __global__ void __launch_bounds__(256) k_lz_update(rsed_lanczos_t st, LzDims d, int pass) {
-  const int inst = blockIdx.y;
+  const int inst = blockIdx.x % d.n_inst;  // instances of one row group adjacent in launch order
+  const int64_t rgroup = blockIdx.x / d.n_inst;
   const int* stt = st.state + inst * kStateInts;
   if (!stt[S_ACTIVE]) return;
+  const bool one = stt[S_ONEPASS] != 0;  // pass 1 writes the new block, pass 2 is skipped
+  if (pass == 2 && one) return;
   const int b = st.inst_b[inst];
   const int c0 = st.inst_col0[inst];
-  const int nb = (pass == 2) ? stt[S_NEWSLOT] : stt[S_NB];
+  const int nb = (pass == 2 || one) ? stt[S_NEWSLOT] : stt[S_NB];
   if (nb * b > kJacobiMax || b > kBMax) return;  // guarded by k_lz_reduce (status set there)
   const double2* coef = reinterpret_cast<const double2*>(st.coef) +
                         (int64_t)inst * 2 * d.pslots * kBMax * kBMax + (pass - 1) * d.pslots * kBMax * kBMax;
@@ -340,7 +454,7 @@ __global__ void __launch_bounds__(256) k_lz_update(rsed_lanczos_t st, LzDims d, 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int rpw = 32 / b;
   const int rl = lane / b, q = lane % b;
-  const int64_t row = ((int64_t)blockIdx.x * (blockDim.x >> 5) + warp) * rpw + rl;
+  const int64_t row = (rgroup * (blockDim.x >> 5) + warp) * rpw + rl;
   const bool act = rl < rpw && row < d.n_orb;
   double2* V = reinterpret_cast<double2*>(st.V);
   double2* W = reinterpret_cast<double2*>(st.W);
@@ -368,7 +482,7 @@ __global__ void __launch_bounds__(256) k_lz_update(rsed_lanczos_t st, LzDims d, 
     if (q > pp) acc = cadd(acc, cmul(make_double2(xpx, xpy), Rs[pp * kBMax + q]));
   }
   if (!act) return;
-  if (pass == 1) {
+  if (pass == 1 && !one) {
     W[row * d.ld + c0 + q] = xq;
   } else {
     V[(int64_t)nb * slot_stride + row * d.ld + c0 + q] = xq;
@@ -398,10 +512,11 @@ __global__ void __launch_bounds__(256) k_lz_update_rows(rsed_lanczos_t st, LzDim
   for (int inst = 0; inst < d.n_inst; ++inst) {
     const int* stt = st.state + inst * kStateInts;
     const int b = st.inst_b[inst];
-    const int nb = (pass == 2) ? stt[S_NEWSLOT] : stt[S_NB];
+    const bool one = stt[S_ONEPASS] != 0;
+    const int nb = (pass == 2 || one) ? stt[S_NEWSLOT] : stt[S_NB];
     const double2* coef = reinterpret_cast<const double2*>(st.coef) +
                           (int64_t)inst * 2 * d.pslots * kBMax * kBMax + (pass - 1) * d.pslots * kBMax * kBMax;
-    if (!stt[S_ACTIVE] || nb * b > kJacobiMax) continue;
+    if (!stt[S_ACTIVE] || nb * b > kJacobiMax || (pass == 2 && one)) continue;
     for (int e = threadIdx.x; e < nb * b * b; e += blockDim.x) {
       const int r = e / b, q = e % b;  // r = s * b + p
       cs[(size_t)inst * cs_stride + r * b + q] = coef[(r / b) * kBMax * kBMax + (r % b) * kBMax + q];
@@ -415,14 +530,15 @@ __global__ void __launch_bounds__(256) k_lz_update_rows(rsed_lanczos_t st, LzDim
   const bool lane_ok = rloc < rows_pg;
   const int inst = lane_ok ? meta[col] : -1;
   int b = 1, c0 = 0, nb = 0, q = 0;
-  bool act = false;
+  bool act = false, one = false;
   if (inst >= 0) {
     const int* stt = st.state + inst * kStateInts;
     b = st.inst_b[inst];
     c0 = st.inst_col0[inst];
-    nb = (pass == 2) ? stt[S_NEWSLOT] : stt[S_NB];
+    one = stt[S_ONEPASS] != 0;
+    nb = (pass == 2 || one) ? stt[S_NEWSLOT] : stt[S_NB];
     q = col - c0;
-    act = stt[S_ACTIVE] && nb * b <= kJacobiMax;
+    act = stt[S_ACTIVE] && nb * b <= kJacobiMax && !(pass == 2 && one);
   }
   const double2* csi = cs + (size_t)(inst < 0 ? 0 : inst) * cs_stride;
   const double2* Ri = Rs + (inst < 0 ? 0 : inst) * kBMax * kBMax;
@@ -458,7 +574,7 @@ __global__ void __launch_bounds__(256) k_lz_update_rows(rsed_lanczos_t st, LzDim
         xs[pp] = make_double2(v.x / rr, v.y / rr);
         xq = xs[pp];
       }
-      if (pass == 1) {
+      if (pass == 1 && !one) {
         W[row * d.ld + col] = xq;
       } else {
         V[(int64_t)nb * slot_stride + row * d.ld + col] = xq;
@@ -1014,7 +1130,8 @@ __global__ void __launch_bounds__(kRitzThreads) k_lz_ritz(rsed_lanczos_t st, LzD
 // Block (row range, instance) with the instance's Ritz coefficients staged in
 // shared memory; one row per thread.
 __global__ void __launch_bounds__(256) k_lz_restart(rsed_lanczos_t st, LzDims d) {
-  const int inst = blockIdx.y;
+  const int inst = blockIdx.x % d.n_inst;  // instances of one row range adjacent in launch order
+  const int64_t rblock = blockIdx.x / d.n_inst;
   const int* stt = st.state + inst * kStateInts;
   const int nb_old = stt[S_RESTART_NB];
   if (nb_old == 0) return;
@@ -1027,7 +1144,7 @@ __global__ void __launch_bounds__(256) k_lz_restart(rsed_lanczos_t st, LzDims d)
   const double2* S = reinterpret_cast<const double2*>(st.ritz_vec) + (int64_t)inst * d.pm * d.pm;
   for (int e = threadIdx.x; e < Mold * K; e += blockDim.x) Ss[(e / K) * kKeepMax + e % K] = S[(int64_t)(e / K) * d.pm + e % K];
   __syncthreads();
-  const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t row = rblock * blockDim.x + threadIdx.x;
   if (row >= d.n_orb) return;
   double2* V = reinterpret_cast<double2*>(st.V);
   const int64_t slot_stride = d.n_orb * d.ld;
@@ -1055,7 +1172,8 @@ __global__ void __launch_bounds__(256) k_lz_restart(rsed_lanczos_t st, LzDims d)
 
 // U[inst][j][row] = sum_l V_l[row] S[l][j], j < nev (Ritz vectors of the last check).
 __global__ void __launch_bounds__(256) k_lz_extract(rsed_lanczos_t st, LzDims d, double2* U, int64_t u_stride) {
-  const int inst = blockIdx.y;
+  const int inst = blockIdx.x % d.n_inst;
+  const int64_t rblock = blockIdx.x / d.n_inst;
   const int* stt = st.state + inst * kStateInts;
   const int b = st.inst_b[inst];
   const int c0 = st.inst_col0[inst];
@@ -1068,7 +1186,7 @@ __global__ void __launch_bounds__(256) k_lz_extract(rsed_lanczos_t st, LzDims d,
   for (int e = threadIdx.x; e < M * nev; e += blockDim.x)
     Ss[(e / nev) * kKeepMax + e % nev] = S[(int64_t)(e / nev) * d.pm + e % nev];
   __syncthreads();
-  const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t row = rblock * blockDim.x + threadIdx.x;
   if (row >= d.n_orb) return;
   const double2* V = reinterpret_cast<const double2*>(st.V);
   const int64_t slot_stride = d.n_orb * d.ld;
@@ -1106,8 +1224,8 @@ __global__ void k_rr_prepare(rsed_lanczos_t st) {
 }
 
 __global__ void __launch_bounds__(128) k_rr_gram(rsed_lanczos_t st, LzDims d) {
-  const int chunk = blockIdx.x;
-  const int inst = blockIdx.y;
+  const int chunk = blockIdx.x / d.n_inst;
+  const int inst = blockIdx.x % d.n_inst;
   int* stt = st.state + inst * kStateInts;
   if (stt[S_RR] != 1) return;
   const int b = st.inst_b[inst];
@@ -1176,8 +1294,8 @@ __global__ void __launch_bounds__(128) k_rr_gram(rsed_lanczos_t st, LzDims d) {
 
 // True FP64 residual norms of the nev refined pairs.
 __global__ void __launch_bounds__(128) k_rr_resid(rsed_lanczos_t st, LzDims d) {
-  const int chunk = blockIdx.x;
-  const int inst = blockIdx.y;
+  const int chunk = blockIdx.x / d.n_inst;
+  const int inst = blockIdx.x % d.n_inst;
   int* stt = st.state + inst * kStateInts;
   if (stt[S_RR] != 2) return;
   const int b = st.inst_b[inst];
@@ -1775,8 +1893,7 @@ int check_lz(const rsed_model_t* md, const rsed_sectors_t* sc, const rsed_lanczo
 }
 
 int launch_pass(const rsed_lanczos_t& st, const LzDims& d, int pass, cudaStream_t stream) {
-  dim3 g1(d.n_chunks, d.n_inst);
-  k_lz_reduce<<<g1, kRT, 0, stream>>>(st, d, pass);
+  k_lz_reduce<<<(unsigned)(d.n_chunks * d.n_inst), kRT, 0, stream>>>(st, d, pass);
   RSED_CHECK_LAUNCH();
   // all instances per block when their coefficients fit in shared memory
   const int cs_stride = st.n_slots * st.bmax * st.bmax;
@@ -1799,7 +1916,7 @@ int launch_pass(const rsed_lanczos_t& st, const LzDims& d, int pass, cudaStream_
   } else {
     // rows per block: 8 warps x (32 / b) rows; sized for the largest block of the batch
     const int64_t rows_per_block = 8 * (32 / st.bmax);
-    k_lz_update<<<dim3((unsigned)((d.n_orb + rows_per_block - 1) / rows_per_block), d.n_inst), 256, 0, stream>>>(
+    k_lz_update<<<(unsigned)(((d.n_orb + rows_per_block - 1) / rows_per_block) * d.n_inst), 256, 0, stream>>>(
         st, d, pass);
   }
   RSED_CHECK_LAUNCH();
@@ -1924,7 +2041,7 @@ static int lz_iterate(const rsed_model_t* md, const rsed_sectors_t* sc, rsed_lan
     if (ritz_mode == 0 || (ritz_mode == 1 && it == n_iter - 1)) {
       k_lz_ritz<<<d.n_inst, kRitzThreads, kRitzSmem, stream>>>(*st, d, check_every, 0, 0);
       RSED_CHECK_LAUNCH();
-      k_lz_restart<<<dim3((unsigned)((d.n_orb + 255) / 256), d.n_inst), 256, 0, stream>>>(*st, d);
+      k_lz_restart<<<(unsigned)(((d.n_orb + 255) / 256) * d.n_inst), 256, 0, stream>>>(*st, d);
       RSED_CHECK_LAUNCH();
     }
   }
@@ -1955,7 +2072,7 @@ extern "C" int rsed_lanczos_rayleigh_ritz(const rsed_model_t* md, const rsed_sec
   const LzDims d = make_dims(md, sc, st);
   k_rr_prepare<<<(st->n_inst + 63) / 64, 64, 0, stream>>>(*st);
   RSED_CHECK_LAUNCH();
-  k_lz_restart<<<dim3((unsigned)((d.n_orb + 255) / 256), d.n_inst), 256, 0, stream>>>(*st, d);
+  k_lz_restart<<<(unsigned)(((d.n_orb + 255) / 256) * d.n_inst), 256, 0, stream>>>(*st, d);
   RSED_CHECK_LAUNCH();
   const int64_t slot = d.n_orb * d.ld;
   double2* V = reinterpret_cast<double2*>(st->V);
@@ -1963,7 +2080,7 @@ extern "C" int rsed_lanczos_rayleigh_ritz(const rsed_model_t* md, const rsed_sec
     rc = rsed_apply_h(md, sc, V + l * slot, V + (st->keep_blocks + 1 + l) * slot, 64, apply_variant, stream_);
     if (rc) return rc;
   }
-  dim3 g(d.n_chunks, d.n_inst);
+  const unsigned g = (unsigned)(d.n_chunks * d.n_inst);
   k_rr_gram<<<g, 128, 0, stream>>>(*st, d);
   RSED_CHECK_LAUNCH();
   k_lz_ritz<<<d.n_inst, kRitzThreads, kRitzSmem, stream>>>(*st, d, 1, 1, 1);
@@ -2019,7 +2136,7 @@ extern "C" int rsed_lanczos_extract(const rsed_model_t* md, const rsed_sectors_t
   RSED_REQUIRE(U != nullptr && u_stride >= md->n_orbits, RSED_EINVAL, "bad U buffer");
   cudaStream_t stream = as_stream(stream_);
   const LzDims d = make_dims(md, sc, st);
-  k_lz_extract<<<dim3((unsigned)((d.n_orb + 255) / 256), d.n_inst), 256, 0, stream>>>(
+  k_lz_extract<<<(unsigned)(((d.n_orb + 255) / 256) * d.n_inst), 256, 0, stream>>>(
       *st, d, reinterpret_cast<double2*>(U), u_stride);
   RSED_CHECK_LAUNCH();
   return RSED_OK;

@@ -23,7 +23,7 @@ from .hamiltonian import DeviceModel
 from .sector import SectorSet
 
 S_NB, S_STATUS, S_RESTARTS, S_ITERS, S_ACTIVE = 0, 1, 2, 3, 4
-S_NCONV, S_RR = 7, 9
+S_NCONV, S_RR, S_ONEPASS_N, S_RED_BLOCKS, S_PASSES = 7, 9, 11, 12, 13
 STATE_INTS = 16
 
 __all__ = [
@@ -56,6 +56,7 @@ class LanczosParams:
     check_every: int = 1000
     precision: int = 64
     apply_variant: int = 0
+    single_pass: bool = True  # skip the second Gram-Schmidt pass when pass 1 lost little norm
 
 
 def start_block(n: int, b: int, seed: int = 12345) -> np.ndarray:
@@ -140,7 +141,8 @@ class LanczosBatch:
         self.resid = torch.zeros((n_inst, self.pm), dtype=torch.float64, device=dev)
         self.state = torch.zeros((n_inst, STATE_INTS), dtype=torch.int32, device=dev)
         self.c = _lib.RsedLanczos(
-            n_inst, S, nev, self.keep, p.max_restarts, p.precision, bmax, self.chunk_rows, self.pm, 0,
+            n_inst, S, nev, self.keep, p.max_restarts, p.precision, bmax, self.chunk_rows, self.pm,
+            1 if p.single_pass else 0,
             float(p.tol if p.precision == 64 else max(p.tol, p.tol32)), _lib.ptr(self.inst_col0), _lib.ptr(self.inst_b), _lib.ptr(self.V),
             _lib.ptr(self.W), _lib.ptr(self.Xf), _lib.ptr(self.P), _lib.ptr(self.coef),
             _lib.ptr(self.partial), plen, _lib.ptr(self.ritz_val), _lib.ptr(self.ritz_vec),

@@ -113,3 +113,30 @@ def test_two_species_lanczos_and_projection(golden):
         H = port.csr_block(ref, n, orb, bil, den, chi, True)
         ev = np.linalg.eigvalsh(H.toarray())
         np.testing.assert_allclose(res[s][0], ev[:4], atol=1e-10, rtol=0)
+
+
+def test_config3_per_spin_union_is_total_n_at_gamma():
+    """Hubbard 4x4 (32 spin-orbitals), U = 4, 10 electrons, momentum Gamma:
+    the lowest levels of the reference's total-N sector (about 4.03M orbits)
+    equal the lowest levels of the union over N_down of the per-spin sectors
+    (N_up = N_down = 5: 19,079,424 states; the multiplets' other S_z
+    components in N_down = 4, 6), each solved on the device, 1e-9."""
+    import realspace_exatdiagonalization_py_b200 as ed
+    from realspace_exatdiagonalization_py_b200 import models
+
+    m, nf = models.config_model("hubbard32")
+    G = ed.build_translation_group(m.lattice)
+    total = ed.build_ed_data(m, filling_fraction=Fraction(nf, 32), symmetry_group=G)
+    cfg = ed.SolverConfig((4,), 0, True, 12)
+    e_total = ed.solve_sectors_batched(total, [0], nev=4, precision=64, config=cfg, return_vectors=False)[0][0]
+    del total
+    union = []
+    for kb in (4, 5, 6):
+        d = ed.build_ed_data(m, filling_fraction=Fraction(nf, 32), symmetry_group=G,
+                             species=models.hubbard_spin_species(m, kb))
+        if kb == 5:
+            assert d.orbit_catalog.n_states == 19_079_424
+        union.extend(ed.solve_sectors_batched(d, [0], nev=4, precision=64, config=cfg,
+                                              return_vectors=False)[0][0].tolist())
+        del d
+    np.testing.assert_allclose(np.sort(union)[:4], e_total, atol=1e-9, rtol=0)
