@@ -1146,6 +1146,7 @@ def run_b200(args):
                 except Exception as exc:  # noqa: BLE001 - reported, not fatal
                     extra[key] = {"error": repr(exc)}
                 torch.cuda.empty_cache()
+    if rank == 0 and ws == 1 and not args.no_cpu:
         # CPU baseline: the reference's own path on the host cores, N = 1 only
         cpu = CpuSectorSolver(args.workload, nev)
         rate, n_done, t_cpu, cvals = cpu.sample(args.cpu_budget, min_solves=1)
@@ -1214,6 +1215,7 @@ def main():
                     help="seconds of reference sector solves for --impl reference (at least one solve)")
     ap.add_argument("--skip-scale", action="store_true", help="skip the serving / config-2 / benchmark extras")
     ap.add_argument("--skip-fp64", action="store_true", help="skip the FP64-matvec batched variant")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (e.g. for kernel profiling)")
     ap.add_argument("--two-pass", action="store_true",
                     help="always two Gram-Schmidt passes per step (no adaptive single pass)")
     ap.add_argument("--config5", type=int, default=0,
