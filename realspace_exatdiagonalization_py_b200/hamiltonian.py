@@ -38,11 +38,14 @@ __all__ = [
 ]
 
 
-def _merge_terms(bilinear_terms, n_site):
-    """Group directed terms by source site; duplicate (i, j) amplitudes add."""
-    acc: dict[tuple[int, int], complex] = {}
-    order: list[tuple[int, int]] = []
-    for (i, j, t) in bilinear_terms:
+def _merge_terms(bilinear_terms, n_site, merge: bool = True):
+    """Group directed terms by source site.  ``merge``: duplicate (i, j)
+    amplitudes add (one hop per site pair, what the solvers stream);
+    otherwise every term stays its own entry, in input order within a site
+    pair (one triplet per term, as the reference's per-term builder emits)."""
+    acc: dict[tuple[int, ...], complex] = {}
+    order: list[tuple[int, ...]] = []
+    for n_in, (i, j, t) in enumerate(bilinear_terms):
         i, j = int(i), int(j)
         if not (1 <= i <= n_site and 1 <= j <= n_site):
             raise ValueError(f"bilinear term ({i}, {j}) outside sites 1..{n_site}")
@@ -50,20 +53,20 @@ def _merge_terms(bilinear_terms, n_site):
             raise ValueError(
                 f"bilinear term ({i}, {i}) is on-site; put on-site energies in the density terms"
             )
-        key = (i - 1, j - 1)
+        key = (i - 1, j - 1) if merge else (i - 1, j - 1, n_in)
         if key not in acc:
             acc[key] = 0j
             order.append(key)
         acc[key] += complex(t)
-    keys = sorted(order)  # by source site, then target
+    keys = sorted(order)  # by source site, then target (then input order)
     begin = np.zeros(n_site + 1, dtype=np.int32)
-    for (i, _) in keys:
-        begin[i + 1] += 1
+    for k in keys:
+        begin[k[0] + 1] += 1
     begin = np.cumsum(begin).astype(np.int32)
-    to = np.array([j for (_, j) in keys], dtype=np.uint8)
+    to = np.array([k[1] for k in keys], dtype=np.uint8)
     amp = np.array([acc[k] for k in keys], dtype=np.complex128)
     jw = np.zeros(len(keys), dtype=np.uint64)
-    for n, (i, j) in enumerate(keys):
+    for n, (i, j, *_) in enumerate(keys):
         lo, hi = min(i, j), max(i, j)
         jw[n] = np.uint64(((1 << (hi - lo - 1)) - 1) << (lo + 1)) if hi - lo > 1 else np.uint64(0)
     return begin, to, amp, jw
@@ -72,14 +75,15 @@ def _merge_terms(bilinear_terms, n_site):
 class DeviceModel:
     """Hamiltonian terms of one model on one catalog (``rsed_model_t``)."""
 
-    def __init__(self, catalog: Symmetry_Orbit_Catalog, bilinear_terms, density_terms, stream=None):
+    def __init__(self, catalog: Symmetry_Orbit_Catalog, bilinear_terms, density_terms, stream=None,
+                 merge_terms: bool = True):
         lib = _lib.lib()
         dev = catalog.table.device
         n_site = catalog.n_site
         self.catalog = catalog
         self.bilinear_terms = [(int(i), int(j), complex(t)) for (i, j, t) in bilinear_terms]
         self.density_terms = [(int(i), int(j), complex(v)) for (i, j, v) in density_terms]
-        begin, to, amp, jw = _merge_terms(self.bilinear_terms, n_site)
+        begin, to, amp, jw = _merge_terms(self.bilinear_terms, n_site, merge_terms)
         self.n_terms = int(len(to))
         self.term_begin = torch.from_numpy(begin).to(dev)
         self.term_to = torch.from_numpy(to if len(to) else np.zeros(1, np.uint8)).to(dev)
@@ -382,21 +386,20 @@ def build_ed_Hamiltonian_symmetry_block(basis, bilinear_terms, density_terms, cm
 
 def build_matrixfree_projection_table(basis, bilinear_terms, density_terms, cmap):
     """``(row_ind, col_ind, vals, h_diag)`` of the off-diagonal projected
-    hops and the diagonal (``symmetry_resolved_ed.py:1719-1769``)."""
-    model = DeviceModel(basis.catalog, bilinear_terms, density_terms)
+    hops and the diagonal (``symmetry_resolved_ed.py:1719-1769``): one
+    triplet per term and valid hop, as the reference's per-term builder
+    (duplicate site pairs, e.g. bonds that meet across both periodic
+    boundaries of a small lattice, stay separate triplets)."""
+    model = DeviceModel(basis.catalog, bilinear_terms, density_terms, merge_terms=False)
     rows, cols, vals = _sector_triplets(basis, model)
-    diag = rows == cols
-    # the first entry of every column is its density diagonal
-    first = torch.zeros_like(diag)
     n = basis.dim
-    col_first = torch.zeros(n, dtype=torch.bool, device=rows.device)
     h_diag = model.hdiag[basis.orbit_of_row.long()]
-    keep = torch.ones_like(diag)
-    # drop exactly one diagonal entry per column: the leading one
+    # the K7 triplets come column by column, each column led by its density
+    # diagonal entry (rsed_triplets_fill): drop exactly that leading entry
     counts = torch.bincount(cols, minlength=n)
     starts = torch.zeros(n, dtype=torch.int64, device=rows.device)
     starts[1:] = torch.cumsum(counts, 0)[:-1]
+    keep = torch.ones(rows.numel(), dtype=torch.bool, device=rows.device)
     keep[starts] = False
-    del first, col_first
     return (rows[keep].cpu().numpy(), cols[keep].cpu().numpy(), vals[keep].cpu().numpy(),
             h_diag.cpu().numpy())
