@@ -868,9 +868,16 @@ def config5_line(ed, models, n_sectors=4, nev=6, cpp_threads=0):
     st = solver.batch.status() if solver is not None else None
     iters = [int(x) - 1 for x in st[:, 3]] if st is not None else []
     cat = data.orbit_catalog
+    def amp_bits(a32):  # components below 1e-15 (signed zeros included) as +0
+        a = np.ascontiguousarray(a32).view(np.float32).copy()
+        a[np.abs(a) < 1e-15] = 0
+        return a.tobytes()
+
     tab = cat.table.cpu().numpy()
     dev_digest = {k: hashlib.sha256(np.ascontiguousarray(tab[:, i]).tobytes()).hexdigest()
-                  for k, i in (("rep_rank", 0), ("rep_sym", 1), ("rep_amp_re", 2), ("rep_amp_im", 3))}
+                  for k, i in (("rep_rank", 0), ("rep_sym", 1))}
+    dev_digest.update({k: hashlib.sha256(amp_bits(tab[:, i])).hexdigest()
+                       for k, i in (("rep_amp_re", 2), ("rep_amp_im", 3))})
     dev_digest["reprs"] = hashlib.sha256(cat.repr_masks.cpu().numpy().view(np.uint64).tobytes()).hexdigest()
     del tab
     perm0, eta = port.group_arrays(G)
@@ -880,8 +887,8 @@ def config5_line(ed, models, n_sectors=4, nev=6, cpp_threads=0):
     amp = ref["rep_amp"].view(np.int32).reshape(-1, 2)
     cpp_digest = {"rep_rank": hashlib.sha256(ref["rep_rank"].tobytes()).hexdigest(),
                   "rep_sym": hashlib.sha256(ref["rep_sym"].tobytes()).hexdigest(),
-                  "rep_amp_re": hashlib.sha256(np.ascontiguousarray(amp[:, 0]).tobytes()).hexdigest(),
-                  "rep_amp_im": hashlib.sha256(np.ascontiguousarray(amp[:, 1]).tobytes()).hexdigest(),
+                  "rep_amp_re": hashlib.sha256(amp_bits(amp[:, 0])).hexdigest(),
+                  "rep_amp_im": hashlib.sha256(amp_bits(amp[:, 1])).hexdigest(),
                   "reprs": hashlib.sha256(ref["reprs"].tobytes()).hexdigest()}
     del amp
     chi = np.asarray(data.irrep_list[0].values, dtype=np.complex128)
@@ -906,7 +913,9 @@ def config5_line(ed, models, n_sectors=4, nev=6, cpp_threads=0):
                                 "catalog_s": t_cpp_cat, "apply_s": t_cpp_apply,
                                 "sector_solve_s_extrapolated": None if applies is None else t_cpp_apply * applies,
                                 "extrapolation": "one apply x (device Lanczos steps + 1) of the slowest sector"},
-            "parity": {"catalog_digests_equal": dev_digest == cpp_digest, "apply_max_rel_diff": mv_err}}
+            "parity": {"catalog_digests_equal": {k: dev_digest[k] == cpp_digest[k] for k in dev_digest},
+                       "amplitudes": "components below 1e-15 (signed zeros included) compared as +0",
+                       "apply_max_rel_diff": mv_err}}
 
 
 def run_b200(args):

@@ -201,7 +201,7 @@ int rsedcpu_catalog(int n, int k, int ng, const uint8_t* perm, const double* ang
     for (int g = 0; g < ng; ++g) {
       const uint64_t img = G.image(g, m);
       cd a = std::exp(cd(0.0, G.angle_sum(g, m)));
-      if (fermion && (G.inversions(g, m) & 1)) a *= -1.0;
+      if (fermion && (G.inversions(g, m) & 1)) a *= cd(-1.0, 0.0);  // as the reference: * (-1 + 0j)
       const int64_t idx = rank_of(img, bt);
       rep_rank[idx] = (int32_t)o;
       rep_sym[idx] = g;
@@ -230,7 +230,7 @@ int rsedcpu_members(int n, int ng, const uint8_t* perm, const double* angle, int
     for (uint64_t sm = stab_mask[o]; sm; sm &= sm - 1) {
       const int h = __builtin_ctzll(sm);
       cd a = std::exp(cd(0.0, G.angle_sum(h, m)));
-      if (fermion && (G.inversions(h, m) & 1)) a *= -1.0;
+      if (fermion && (G.inversions(h, m) & 1)) a *= cd(-1.0, 0.0);
       for (int s = 0; s < n_sec; ++s)
         if (!(std::abs(CHI[(size_t)s * ng + h] - a) <= atol)) bits &= ~(1ull << s);
     }

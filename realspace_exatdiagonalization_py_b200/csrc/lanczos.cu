@@ -505,9 +505,13 @@ __global__ void __launch_bounds__(256) k_lz_update_rows(rsed_lanczos_t st, LzDim
   int* meta = reinterpret_cast<int*>(wsh + 256);                        // [ld]: inst of each column
   for (int c = threadIdx.x; c < d.ld; c += blockDim.x) meta[c] = -1;
   __syncthreads();
+  __shared__ int s_split;  // 1 if an instance's columns straddle two warps
+  if (threadIdx.x == 0) s_split = !(32 % d.ld == 0 || d.ld % 32 == 0);
+  __syncthreads();
   for (int inst = threadIdx.x; inst < d.n_inst; inst += blockDim.x) {
     const int b = st.inst_b[inst], c0 = st.inst_col0[inst];
     for (int q = 0; q < b; ++q) meta[c0 + q] = inst;
+    if (d.ld % 32 == 0 && c0 / 32 != (c0 + b - 1) / 32) s_split = 1;
   }
   for (int inst = 0; inst < d.n_inst; ++inst) {
     const int* stt = st.state + inst * kStateInts;
@@ -546,6 +550,47 @@ __global__ void __launch_bounds__(256) k_lz_update_rows(rsed_lanczos_t st, LzDim
   double2* W = reinterpret_cast<double2*>(st.W);
   const int64_t slot_stride = d.n_orb * d.ld;
   const int64_t n_groups = (d.n_orb + rows_pg - 1) / rows_pg;
+  if (!s_split) {
+    // every instance's columns lie in one warp: the b lanes of an instance
+    // solve x R = w by shuffles, so warps stream their rows without block
+    // barriers (more loads in flight than the shared-memory exchange below)
+    const int lane = threadIdx.x & 31;
+    const int base = lane - q;
+    for (int64_t grp = blockIdx.x; grp < n_groups; grp += gridDim.x) {
+      const int64_t row = grp * rows_pg + rloc;
+      const bool live = act && lane_ok && row < d.n_orb;
+      double2 w = make_double2(0.0, 0.0);
+      if (live) {
+        w = W[row * d.ld + col];
+#pragma unroll 4
+        for (int s = 0; s < nb; ++s) {
+          const double2* Vs = V + s * slot_stride + row * d.ld + c0;
+          for (int p = 0; p < b; ++p) w = csub(w, cmul(Vs[p], csi[(s * b + p) * b + q]));
+        }
+      }
+      double2 acc = make_double2(0.0, 0.0), xq = make_double2(0.0, 0.0);
+      for (int pp = 0; pp < st.bmax; ++pp) {
+        if (q == pp) {
+          const double rr = Ri[pp * kBMax + pp].x;
+          xq = make_double2((w.x - acc.x) / rr, (w.y - acc.y) / rr);
+        }
+        const int src = min(base + pp, 31);
+        const double xpx = __shfl_sync(0xffffffffu, xq.x, src);
+        const double xpy = __shfl_sync(0xffffffffu, xq.y, src);
+        if (q > pp && pp < b) acc = cadd(acc, cmul(make_double2(xpx, xpy), Ri[pp * kBMax + q]));
+      }
+      if (live) {
+        if (pass == 1 && !one) {
+          W[row * d.ld + col] = xq;
+        } else {
+          V[(int64_t)nb * slot_stride + row * d.ld + col] = xq;
+          V[(int64_t)(d.n_slots + 1) * slot_stride + row * d.ld + col] = xq;
+          if (st.Xf) reinterpret_cast<float2*>(st.Xf)[row * d.ld + col] = make_float2((float)xq.x, (float)xq.y);
+        }
+      }
+    }
+    return;
+  }
   for (int64_t grp = blockIdx.x; grp < n_groups; grp += gridDim.x) {
     const int64_t row = grp * rows_pg + rloc;
     const bool live = act && lane_ok && row < d.n_orb;
@@ -1151,7 +1196,7 @@ __global__ void __launch_bounds__(256) k_lz_restart(rsed_lanczos_t st, LzDims d)
   double2 acc[kKeepMax];
 #pragma unroll
   for (int j = 0; j < kKeepMax; ++j) acc[j] = make_double2(0.0, 0.0);
-#pragma unroll 2
+#pragma unroll 8
   for (int l = 0; l < Mold; ++l) {
     const double2 v = V[(int64_t)(l / b) * slot_stride + row * d.ld + c0 + (l % b)];
 #pragma unroll

@@ -151,7 +151,6 @@ class FluxContext:
         # FP32 serving also keeps FP64 weights: the refinement's FP64 products
         # then stream the table instead of re-deriving every hop
         want = (32, 64) if precision == 32 else (64,)
-        before = torch.cuda.memory_allocated()
         zero = not any(flux)
         if zero:
             terms, group, cat = sm.model.bilinear_terms, sm.group0, sm.catalog
@@ -171,8 +170,16 @@ class FluxContext:
             if not torch.equal(self.sset.chi, base.sset.chi):
                 raise ValueError("the flux point changes the sector characters; lanes cannot share it")
             self.dm.build_projection(self.sset.sqrt_stab, precisions=want, share=base.dm.proj)
-        # allocation accounting is host-side: no device synchronisation needed
-        self.bytes = max(0, torch.cuda.memory_allocated() - before)
+        # the device bytes this flux point owns, summed over its own tensors
+        # (host-side: no device synchronisation; a flux point shares the
+        # zero-flux catalog's masks and stabilizers and the table structure)
+        own = [self.dm.hdiag, self.dm.term_begin, self.dm.term_to, self.dm.term_amp, self.dm.term_jw,
+               self.sset.member, self.sset.sqrt_stab, self.sset.chi]
+        if not zero:
+            own += [cat.table, cat.stab_phase]
+        skip = ("rowptr", "cg") if self.dm.proj.get("shared") else ()
+        own += [t for k, t in self.dm.proj.items() if torch.is_tensor(t) and k not in skip]
+        self.bytes = int(sum(t.numel() * t.element_size() for t in own))
         if not zero:
             sm.ctx_bytes = max(sm.ctx_bytes or 0, self.bytes)
         self.users = 0
