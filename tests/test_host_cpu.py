@@ -325,3 +325,25 @@ def test_default_fci_sectors():
     tb = models.build_fermionic_checkerboard_tb_model(sample_size=[2, 3])
     assert tb.lattice.n_site == 12
     assert models.CHECKERBOARD_TPP_DENOMINATOR == pytest.approx(2 + 2 * np.sqrt(2))
+
+
+@pytest.mark.skipif(not ref_shim.available(), reason="reference package not present")
+def test_scalar_api_matches_reference():
+    """Jordan-Wigner sign, colex rank and single-mask group actions against
+    the reference's own scalar functions on random masks."""
+    R = ref_shim.load()
+    sre = R.sre
+    rng = np.random.default_rng(11)
+    for stats in (ed.Particle_Statistics.BOSONIC, ed.Particle_Statistics.FERMIONIC):
+        rstats = getattr(sre.Particle_Statistics, stats.name)
+        for _ in range(300):
+            n = int(rng.integers(2, 40))
+            m = int(rng.integers(0, 1 << n, dtype=np.uint64))
+            i, j = (int(x) for x in rng.integers(1, n + 1, size=2))
+            assert ed.hopping_phase_for_stats(stats, m, i, j) == sre.hopping_phase_for_stats(rstats, m, i, j)
+    for _ in range(200):
+        n = int(rng.integers(2, 42))
+        k = int(rng.integers(1, n))
+        m = sum(1 << int(s) for s in rng.choice(n, size=k, replace=False))
+        bt = sre._binom_table(n, k)
+        assert ed.rank_combination(m, bt) == sre.rank_combination(m, bt)
