@@ -486,32 +486,31 @@ __global__ void __launch_bounds__(256) k_lz_update(rsed_lanczos_t st, LzDims d, 
     W[row * d.ld + c0 + q] = xq;
   } else {
     V[(int64_t)nb * slot_stride + row * d.ld + c0 + q] = xq;
-    V[(int64_t)(d.n_slots + 1) * slot_stride + row * d.ld + c0 + q] = xq;
+    if (st.Xf == nullptr) V[(int64_t)(d.n_slots + 1) * slot_stride + row * d.ld + c0 + q] = xq;
     if (st.Xf) reinterpret_cast<float2*>(st.Xf)[row * d.ld + c0 + q] = make_float2((float)xq.x, (float)xq.y);
   }
 }
 
 // The same update for all instances at once (batches of 2+ instances whose
 // coefficients fit in shared memory): a block holds every instance's
-// coefficients and walks groups of whole rows (thread = one column of one
-// row), so each slot is read as contiguous rows.  x R = w is solved per
-// thread by forward substitution over its instance's columns, from the row's
-// w values exchanged through shared memory.  Grid-stride over row groups.
+// coefficients and walks pairs of row groups (thread = one column of one row
+// in each group), so each slot is read as contiguous rows and every thread
+// keeps the loads of two rows in flight.  x R = w is solved per thread by
+// forward substitution over its instance's columns, from the rows' w values
+// exchanged through shared memory.  Grid-stride over pairs of row groups.
+// The copy of a new block into the current-block slot is written only when
+// the matvec reads it (FP64 matvec); an FP32-matvec batch reads Xf.
 __global__ void __launch_bounds__(256) k_lz_update_rows(rsed_lanczos_t st, LzDims d, int pass, int cs_stride) {
   extern __shared__ __align__(16) unsigned char smem_u[];
   double2* cs = reinterpret_cast<double2*>(smem_u);                    // [inst][cs_stride]
   double2* Rs = cs + (size_t)d.n_inst * cs_stride;                      // [inst][kBMax*kBMax]
-  double2* wsh = Rs + (size_t)d.n_inst * kBMax * kBMax;                 // [256] row-group w values
-  int* meta = reinterpret_cast<int*>(wsh + 256);                        // [ld]: inst of each column
+  double2* wsh = Rs + (size_t)d.n_inst * kBMax * kBMax;                 // [2][256] row-group w values
+  int* meta = reinterpret_cast<int*>(wsh + 512);                        // [ld]: inst of each column
   for (int c = threadIdx.x; c < d.ld; c += blockDim.x) meta[c] = -1;
-  __syncthreads();
-  __shared__ int s_split;  // 1 if an instance's columns straddle two warps
-  if (threadIdx.x == 0) s_split = !(32 % d.ld == 0 || d.ld % 32 == 0);
   __syncthreads();
   for (int inst = threadIdx.x; inst < d.n_inst; inst += blockDim.x) {
     const int b = st.inst_b[inst], c0 = st.inst_col0[inst];
     for (int q = 0; q < b; ++q) meta[c0 + q] = inst;
-    if (d.ld % 32 == 0 && c0 / 32 != (c0 + b - 1) / 32) s_split = 1;
   }
   for (int inst = 0; inst < d.n_inst; ++inst) {
     const int* stt = st.state + inst * kStateInts;
@@ -550,64 +549,35 @@ __global__ void __launch_bounds__(256) k_lz_update_rows(rsed_lanczos_t st, LzDim
   double2* W = reinterpret_cast<double2*>(st.W);
   const int64_t slot_stride = d.n_orb * d.ld;
   const int64_t n_groups = (d.n_orb + rows_pg - 1) / rows_pg;
-  if (!s_split) {
-    // every instance's columns lie in one warp: the b lanes of an instance
-    // solve x R = w by shuffles, so warps stream their rows without block
-    // barriers (more loads in flight than the shared-memory exchange below)
-    const int lane = threadIdx.x & 31;
-    const int base = lane - q;
-    for (int64_t grp = blockIdx.x; grp < n_groups; grp += gridDim.x) {
-      const int64_t row = grp * rows_pg + rloc;
-      const bool live = act && lane_ok && row < d.n_orb;
-      double2 w = make_double2(0.0, 0.0);
-      if (live) {
-        w = W[row * d.ld + col];
-#pragma unroll 4
-        for (int s = 0; s < nb; ++s) {
-          const double2* Vs = V + s * slot_stride + row * d.ld + c0;
-          for (int p = 0; p < b; ++p) w = csub(w, cmul(Vs[p], csi[(s * b + p) * b + q]));
-        }
-      }
-      double2 acc = make_double2(0.0, 0.0), xq = make_double2(0.0, 0.0);
-      for (int pp = 0; pp < st.bmax; ++pp) {
-        if (q == pp) {
-          const double rr = Ri[pp * kBMax + pp].x;
-          xq = make_double2((w.x - acc.x) / rr, (w.y - acc.y) / rr);
-        }
-        const int src = min(base + pp, 31);
-        const double xpx = __shfl_sync(0xffffffffu, xq.x, src);
-        const double xpy = __shfl_sync(0xffffffffu, xq.y, src);
-        if (q > pp && pp < b) acc = cadd(acc, cmul(make_double2(xpx, xpy), Ri[pp * kBMax + q]));
-      }
-      if (live) {
-        if (pass == 1 && !one) {
-          W[row * d.ld + col] = xq;
-        } else {
-          V[(int64_t)nb * slot_stride + row * d.ld + col] = xq;
-          V[(int64_t)(d.n_slots + 1) * slot_stride + row * d.ld + col] = xq;
-          if (st.Xf) reinterpret_cast<float2*>(st.Xf)[row * d.ld + col] = make_float2((float)xq.x, (float)xq.y);
-        }
-      }
-    }
-    return;
-  }
-  for (int64_t grp = blockIdx.x; grp < n_groups; grp += gridDim.x) {
-    const int64_t row = grp * rows_pg + rloc;
-    const bool live = act && lane_ok && row < d.n_orb;
-    double2 w = make_double2(0.0, 0.0);
-    if (live) {
-      w = W[row * d.ld + col];
+  const bool copy_cur = st.Xf == nullptr;  // the FP64 matvec reads the current-block slot
+  for (int64_t grp = 2 * (int64_t)blockIdx.x; grp < n_groups; grp += 2 * (int64_t)gridDim.x) {
+    const int64_t row0 = grp * rows_pg + rloc, row1 = row0 + rows_pg;
+    const bool live0 = act && lane_ok && row0 < d.n_orb;
+    const bool live1 = act && lane_ok && row1 < d.n_orb;
+    double2 w0 = make_double2(0.0, 0.0), w1 = make_double2(0.0, 0.0);
+    if (live0) {
+      w0 = W[row0 * d.ld + col];
+      if (live1) w1 = W[row1 * d.ld + col];
 #pragma unroll 4
       for (int s = 0; s < nb; ++s) {
-        const double2* Vs = V + s * slot_stride + row * d.ld + c0;
-        for (int p = 0; p < b; ++p) w = csub(w, cmul(Vs[p], csi[(s * b + p) * b + q]));
+        const double2* Vs = V + s * slot_stride + row0 * d.ld + c0;
+        for (int p = 0; p < b; ++p) {
+          const double2 c = csi[(s * b + p) * b + q];
+          w0 = csub(w0, cmul(Vs[p], c));
+          if (live1) w1 = csub(w1, cmul(Vs[(int64_t)rows_pg * d.ld + p], c));
+        }
       }
     }
-    wsh[threadIdx.x] = w;
+    wsh[threadIdx.x] = w0;
+    wsh[256 + threadIdx.x] = w1;
     __syncthreads();
-    if (live) {
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const bool live = h == 0 ? live0 : live1;
+      if (!live) continue;
+      const int64_t row = h == 0 ? row0 : row1;
       // forward substitution over this instance's columns 0..q
-      const double2* wr = wsh + rloc * d.ld + c0;
+      const double2* wr = wsh + h * 256 + rloc * d.ld + c0;
       double2 xs[kBMax];
       double2 xq = make_double2(0.0, 0.0);
 #pragma unroll
@@ -623,7 +593,7 @@ __global__ void __launch_bounds__(256) k_lz_update_rows(rsed_lanczos_t st, LzDim
         W[row * d.ld + col] = xq;
       } else {
         V[(int64_t)nb * slot_stride + row * d.ld + col] = xq;
-        V[(int64_t)(d.n_slots + 1) * slot_stride + row * d.ld + col] = xq;
+        if (copy_cur) V[(int64_t)(d.n_slots + 1) * slot_stride + row * d.ld + col] = xq;
         if (st.Xf) reinterpret_cast<float2*>(st.Xf)[row * d.ld + col] = make_float2((float)xq.x, (float)xq.y);
       }
     }
@@ -1942,7 +1912,7 @@ int launch_pass(const rsed_lanczos_t& st, const LzDims& d, int pass, cudaStream_
   RSED_CHECK_LAUNCH();
   // all instances per block when their coefficients fit in shared memory
   const int cs_stride = st.n_slots * st.bmax * st.bmax;
-  const size_t smem = sizeof(double2) * ((size_t)d.n_inst * (cs_stride + kBMax * kBMax) + 256) +
+  const size_t smem = sizeof(double2) * ((size_t)d.n_inst * (cs_stride + kBMax * kBMax) + 512) +
                       sizeof(int) * (size_t)d.ld;
   // (measured: above ~48 KB the lower occupancy costs more than whole-row reads save)
   if (d.n_inst >= 2 && d.ld <= 256 && smem <= 48 * 1024) {
@@ -1956,7 +1926,8 @@ int launch_pass(const rsed_lanczos_t& st, const LzDims& d, int pass, cudaStream_
     int dev = 0, n_sm = 148;
     RSED_TRY_CUDA(cudaGetDevice(&dev));
     RSED_TRY_CUDA(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
-    const int64_t grid = groups < (int64_t)n_sm * 8 ? groups : (int64_t)n_sm * 8;
+    const int64_t pairs = (groups + 1) / 2;  // each block iteration takes two row groups
+    const int64_t grid = pairs < (int64_t)n_sm * 8 ? pairs : (int64_t)n_sm * 8;
     k_lz_update_rows<<<(unsigned)grid, 256, smem, stream>>>(st, d, pass, cs_stride);
   } else {
     // rows per block: 8 warps x (32 / b) rows; sized for the largest block of the batch
