@@ -139,7 +139,7 @@ __device__ void lz_gram_chunk(const double2* __restrict__ V, const double2* __re
         if (sl > nb) break;
         if (sl < nb) {
           const double2* Y = V + sl * slot_stride + c0 + p;
-#pragma unroll 8
+#pragma unroll 4
           for (int rr = rl; rr < nr; rr += RPW) {
             const double2 y = Y[(t0 + rr) * ld];
 #pragma unroll

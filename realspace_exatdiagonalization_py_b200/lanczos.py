@@ -53,7 +53,7 @@ class LanczosParams:
     keep_blocks: int = 0  # 0 = automatic
     tol: float = 1e-10
     tol32: float = 5e-7  # measured: 1e-6 -> 5e-7 cuts the refined error ~3x at the same speed
-    max_restarts: int = 200
+    max_restarts: int = 1000  # a cap, not a budget: a 48-site sector with a 3e-4 gap at nev needed 218 (b = 2)
     check_every: int = 1000
     precision: int = 64
     apply_variant: int = 0
@@ -237,7 +237,7 @@ class LanczosBatch:
     def done(self) -> bool:
         return not bool(self.state[:, S_ACTIVE].any().item())
 
-    def run(self, max_iter: int = 4000, poll: int = 8, graph: bool = False, stream=None) -> np.ndarray:
+    def run(self, max_iter: int = 12000, poll: int = 8, graph: bool = False, stream=None) -> np.ndarray:
         """Iterate until every instance converged or failed; returns the state."""
         it = 0
         g = None
@@ -259,7 +259,7 @@ class LanczosBatch:
                 break
         return self._final_status()
 
-    def run_aligned(self, max_iter: int = 4000, poll: int = 8) -> np.ndarray:
+    def run_aligned(self, max_iter: int = 12000, poll: int = 8) -> np.ndarray:
         """``run(graph=True)`` from a fresh ``start()``, with the graphs cut at
         the restarts: a head graph of ``keep`` steps that launches no Ritz
         check, then a cycle graph of ``restart_period`` steps that checks (and
