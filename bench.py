@@ -1060,11 +1060,12 @@ def run_b200(args):
         for key, fam in (("reduce", "k_lz_reduce"), ("update", "k_lz_update")):
             n_k, us_k = _family(agg, fam)
             if n_k:
-                fams[fam] = {"kernel": f"{fam}* (FP64 block Gram-Schmidt, two passes per iteration)",
+                fams[fam] = {"kernel": f"{fam}* (FP64 block Gram-Schmidt, "
+                                       + ("two passes" if args.two_pass else "adaptive single pass") + ")",
                              "launches": n_k, "avg_launch_us": us_k / n_k,
                              "alg_bytes_per_launch": lb[key] / n_k,
-                             "unit_bytes": "per executed pass (nb + 1) resp. (nb + 2) blocks of n_orb x b x 16 B "
-                                           "(kernel-side counters)"}
+                             "unit_bytes": "per executed pass (nb + 1) resp. (nb + 2) blocks of n_orb x b x 16 B, "
+                                           "+ n_orb x b x 8 B FP32 copy per new block (kernel-side counters)"}
         for k, f in fams.items():
             f["achieved_GBs"] = f["alg_bytes_per_launch"] / (f["avg_launch_us"] * 1e-6) / 1e9
             f["frac"] = f["achieved_GBs"] / peak_gbs

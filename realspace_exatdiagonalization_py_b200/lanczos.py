@@ -402,7 +402,11 @@ class LanczosBatch:
 def vectors_to_host(vecs: list[torch.Tensor]) -> list[np.ndarray]:
     """Host copies of ``eigenvectors()``'s blocks in ONE device-to-host copy
     when they are consecutive views of one buffer (as returned), else one
-    copy per block."""
+    copy per block.  Device blocks land in page-locked host memory from
+    torch's caching host allocator (a full-bandwidth copy with no page faults
+    on fresh memory); the returned arrays are views that keep their block
+    alive, and a block is reused by a later call only after every array of
+    the earlier one is gone."""
     if not vecs:
         return []
     base = vecs[0]
@@ -416,7 +420,13 @@ def vectors_to_host(vecs: list[torch.Tensor]) -> list[np.ndarray]:
         off += v.numel()
     if not consecutive:
         return [v.cpu().numpy() for v in vecs]
-    h = base.as_strided((n,), (1,), start).cpu().numpy()
+    src = base.as_strided((n,), (1,), start)
+    if src.is_cuda:
+        pinned = torch.empty(n, dtype=src.dtype, pin_memory=True)
+        pinned.copy_(src)
+        h = pinned.numpy()
+    else:
+        h = src.numpy()
     out, off = [], 0
     for v in vecs:
         out.append(h[off: off + v.numel()].reshape(v.shape))
