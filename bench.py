@@ -955,7 +955,7 @@ def run_b200(args):
 
     # how the batch runs (block sizes, persistent cluster or graph path,
     # projection table, basis length) is picked by the autotuner, untimed
-    params = ed.LanczosParams(precision=args.precision, single_pass=not args.two_pass)
+    params = ed.LanczosParams(precision=args.precision, single_pass=not args.two_pass, stream=not args.no_stream)
     tuner = ed.Autotuner(trials=2)
     t0 = time.perf_counter()
     if args.solver == "auto":
@@ -1057,10 +1057,22 @@ def run_b200(args):
                 "alg_bytes_per_launch": proj_apply_unique_bytes(nh, n_orb, b.n_cols, args.precision),
                 "unit_bytes": "per hop 4 + 8 B table, per row 8 + 8 + 16 B, per element x 8 B + y 16 B, once each"}
         lb = lanczos_step_bytes(n_orb, b, st_prof)
-        for key, fam in (("reduce", "k_lz_reduce"), ("update", "k_lz_update")):
+        # the streamed forms: k_lz_gram_stream + k_lz_finalize (reduction),
+        # k_lz_update_stream (update); the per-instance forms k_lz_reduce,
+        # k_lz_update / k_lz_update_rows
+        for key, fam, extra_fam in (("reduce", "k_lz_reduce", ("k_lz_gram_stream", "k_lz_finalize")),
+                                    ("update", "k_lz_update", ())):
             n_k, us_k = _family(agg, fam)
+            names = [fam + "*"] if n_k else []
+            for ef in extra_fam:
+                n_e, us_e = _family(agg, ef)
+                us_k += us_e
+                if n_e:
+                    names.append(ef)
+                if ef != "k_lz_finalize":
+                    n_k += n_e
             if n_k:
-                fams[fam] = {"kernel": f"{fam}* (FP64 block Gram-Schmidt, "
+                fams[fam] = {"kernel": " + ".join(names) + " (FP64 block Gram-Schmidt, "
                                        + ("two passes" if args.two_pass else "adaptive single pass") + ")",
                              "launches": n_k, "avg_launch_us": us_k / n_k,
                              "alg_bytes_per_launch": lb[key] / n_k,
@@ -1228,6 +1240,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (e.g. for kernel profiling)")
     ap.add_argument("--two-pass", action="store_true",
                     help="always two Gram-Schmidt passes per step (no adaptive single pass)")
+    ap.add_argument("--no-stream", action="store_true",
+                    help="per-instance Gram-Schmidt kernels instead of the streamed whole-row panels")
     ap.add_argument("--config5", type=int, default=0,
                     help="only the 48-site checkerboard line for this many sectors (device vs C++ restatement)")
     ap.add_argument("--solver", default="auto",

@@ -34,6 +34,7 @@ extern "C" {
 #define RSED_ERANGE -4      /* size beyond a compiled or documented limit */
 #define RSED_EBREAKDOWN -5  /* Krylov block lost rank (Cholesky pivot <= 0) */
 #define RSED_ESCRATCH -6    /* scratch buffer smaller than the query returned */
+#define RSED_ETIMEOUT -7    /* a device-side wait ran past its time limit (no result written) */
 
 /* One representative-table entry (16 bytes), indexed by combinadic rank:
  * the reference's rep_rank_table / rep_sym_table / rep_amp_table

@@ -20,6 +20,7 @@ RSED_ENOTCONV = -3
 RSED_ERANGE = -4
 RSED_EBREAKDOWN = -5
 RSED_ESCRATCH = -6
+RSED_ETIMEOUT = -7
 
 _ERR_NAMES = {
     RSED_EINVAL: "RSED_EINVAL",
@@ -28,6 +29,7 @@ _ERR_NAMES = {
     RSED_ERANGE: "RSED_ERANGE",
     RSED_EBREAKDOWN: "RSED_EBREAKDOWN",
     RSED_ESCRATCH: "RSED_ESCRATCH",
+    RSED_ETIMEOUT: "RSED_ETIMEOUT",
 }
 
 

@@ -602,6 +602,601 @@ __global__ void __launch_bounds__(256) k_lz_update_rows(rsed_lanczos_t st, LzDim
 }
 
 // ---------------------------------------------------------------------------
+// Row-panel streaming forms of the Gram reduction and of the block update.
+//
+// A panel is pr consecutive rows of one [n_orb][ld] block buffer (W or a basis
+// slot): pr * ld * 16 contiguous bytes, at most kPanelElems entries.  A
+// streaming block owns the row chunks blockIdx.x, blockIdx.x + gridDim.x, ...
+// and walks, per chunk, a fixed sequence of panels (W first, then the slots
+// it needs).  Warp kSW (the producer) issues one cp.async.bulk per panel into
+// a ring of ns shared-memory stages; the copy completes the stage's "full"
+// mbarrier by its byte count.  The kSW consumer warps wait on "full", use the
+// panel from shared memory and arrive on the stage's "empty" mbarrier, which
+// the producer waits on before it refills the stage.  Every consumer warp
+// waits on every panel in order (also on panels it does not use), so a stage
+// cannot be refilled before all of them are past it.  With up to ns panels in
+// flight per block and two blocks per SM the HBM streams at full rate, and
+// the warps do their arithmetic on shared memory with no loads outstanding.
+//
+// Every mbarrier wait is bounded (kWaitNs of %globaltimer).  A wait that runs
+// out raises the block's abort flag; the other warps then stop waiting (they
+// still pass every named barrier, so none is left behind), the producer stops
+// issuing and waits, bounded again, for the copies it has issued, nothing is
+// written, and every instance the block served ends with RSED_ETIMEOUT.
+constexpr int kSW = 8;                        // consumer warps
+constexpr int kSThreads = (kSW + 1) * 32;     // + the producer warp
+constexpr int kPanelElems = 512;              // entries of one panel at most (8 KB)
+constexpr int kStreamGridMax = 320;           // streaming blocks at most (Gram partials per instance)
+constexpr int kStreamInstMax = 64;            // instances of a streamed batch at most (ld <= 64)
+constexpr int kListMax = 2 * kJacobiMax + 8;  // panels of one chunk at most
+constexpr unsigned long long kWaitNs = 2000000000ull;
+constexpr int kFlagNoStream = 2;              // st.reserved bit 1: use the per-instance kernels
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(done)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+// Waits for the completion of the phase with the given parity.  False when the
+// block's abort flag is up or the wait ran out of kWaitNs (which raises it).
+__device__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort) {
+  if (*abort) return false;
+  if (mbar_test(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  for (uint32_t it = 1;; ++it) {
+    if (mbar_test(bar, parity)) return true;
+    if ((it & 63u) == 0) {
+      if (*abort) return false;
+      if (global_ns() - t0 > kWaitNs) {
+        *abort = 1;
+        return false;
+      }
+    }
+  }
+}
+// global -> shared bulk copy of one panel (16-B aligned, multiple of 16 B),
+// completing on bar's transaction count
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+// barrier of the kSW consumer warps only (the producer warp never joins it)
+__device__ __forceinline__ void consumer_sync() { asm volatile("bar.sync 1, %0;" ::"n"(kSW * 32) : "memory"); }
+
+// After an abort: waits, bounded, for the last copy issued into each stage.
+__device__ void stream_drain(uint64_t* full, int ns, int64_t issued) {
+  for (int64_t k = issued > ns ? issued - ns : 0; k < issued; ++k) {
+    const int stg = (int)(k % ns);
+    const uint32_t par = (uint32_t)((k / ns) & 1);
+    const uint64_t t0 = global_ns();
+    while (!mbar_test(&full[stg], par) && global_ns() - t0 < kWaitNs) {
+    }
+  }
+}
+
+struct StreamLayout {
+  size_t bars, ring, wl, coef, rs, total;
+};
+// dynamic shared memory of a streaming block: ns full + ns empty barriers,
+// the ring, one panel-sized work buffer, the instances' coefficients
+// (n_inst x cs_stride) and, for the update, their R factors
+__host__ __device__ inline StreamLayout stream_layout(int ns, int n_inst, int cs_stride, bool with_r) {
+  StreamLayout l;
+  size_t off = 0;
+  l.bars = off;
+  off += 16 * (size_t)ns;
+  off = (off + 127) & ~(size_t)127;
+  l.ring = off;
+  off += sizeof(double2) * kPanelElems * (size_t)ns;
+  l.wl = off;
+  off += sizeof(double2) * kPanelElems;
+  l.coef = off;
+  off += sizeof(double2) * (size_t)n_inst * cs_stride;
+  l.rs = off;
+  off += with_r ? sizeof(double2) * (size_t)n_inst * kBMax * kBMax : 0;
+  l.total = off;
+  return l;
+}
+
+// The producer: lane 0 of warp kSW issues the block's panels in order.
+// list[t] names panel t of a chunk: -1 = W, s >= 0 = basis slot s.
+__device__ void stream_produce(const rsed_lanczos_t& st, const LzDims& d, int ns, int pr, const int* list, int npc,
+                               int64_t my_chunks, uint64_t* full, uint64_t* empty, double2* ring,
+                               volatile int* abort) {
+  const double2* V = reinterpret_cast<const double2*>(st.V);
+  const double2* W = reinterpret_cast<const double2*>(st.W);
+  const int64_t slot_stride = d.n_orb * d.ld;
+  const int64_t total = my_chunks * npc;
+  int64_t issued = 0;
+  for (int64_t k = 0; k < total; ++k) {
+    const int stg = (int)(k % ns);
+    if (k >= ns && !mbar_wait(&empty[stg], (uint32_t)((k / ns - 1) & 1), abort)) break;
+    const int64_t r0 = (blockIdx.x + (k / npc) * gridDim.x) * (int64_t)pr;
+    const int64_t rows = min((int64_t)pr, d.n_orb - r0);
+    const int sl = list[k % npc];
+    const double2* src = (sl < 0 ? W : V + (int64_t)sl * slot_stride) + r0 * d.ld;
+    const uint32_t bytes = (uint32_t)(rows * d.ld * (int64_t)sizeof(double2));
+    mbar_expect_tx(&full[stg], bytes);
+    bulk_load(ring + (size_t)stg * kPanelElems, src, bytes, &full[stg]);
+    issued = k + 1;
+  }
+  if (*abort) stream_drain(full, ns, issued);
+}
+
+// Gram partials of all instances over the block's row chunks:
+//   partial[blk][inst][s][p][q] = sum_rows conj(Y_s[row][c0+p]) W_loc[row][c0+q]
+// with Y_s = V[s] for s < nb and Y_nb = W_loc (the finalisation, k_lz_finalize,
+// sums the gridDim.x partials).  Per chunk: W and the slots the local
+// transform needs are streamed first and W_loc is formed element-wise into
+// shared memory (thread = entry of the panel); then every basis slot s < max
+// nb is streamed, and warp s % kSW adds it into its registers (lane = column
+// c0 + p, all q of the instance), reading W_loc from shared memory.  BB is
+// the largest block of the batch rounded up to a power of two, CPL the
+// columns per lane (ld <= 32 * CPL).
+template <int BB, int CPL>
+__global__ void __launch_bounds__(kSThreads, 2)
+    k_lz_gram_stream(rsed_lanczos_t st, LzDims d, int pass, int ns, int pr, int cs_stride) {
+  constexpr int SW = kJacobiMax / BB / kSW + 1;  // slots one warp owns at most
+  extern __shared__ __align__(128) unsigned char smem_s[];
+  const StreamLayout L = stream_layout(ns, d.n_inst, cs_stride, false);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem_s + L.bars);
+  uint64_t* empty = full + ns;
+  double2* ring = reinterpret_cast<double2*>(smem_s + L.ring);
+  double2* wl = reinterpret_cast<double2*>(smem_s + L.wl);
+  double2* lc = reinterpret_cast<double2*>(smem_s + L.coef);
+  __shared__ int s_b[kStreamInstMax], s_c0[kStreamInstMax], s_nb[kStreamInstMax], s_jloc[kStreamInstMax];
+  __shared__ unsigned long long s_lnz[kStreamInstMax];
+  __shared__ double s_sig[kStreamInstMax][kBMax];
+  __shared__ int s_col_inst[32 * CPL];
+  __shared__ int s_list[kListMax];
+  __shared__ int s_npc, s_nloc, s_nbmax;
+  __shared__ int s_abort_store;
+  volatile int* s_abort = &s_abort_store;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int ld = d.ld;
+  if (tid == 0) s_abort_store = 0;
+  for (int c = tid; c < 32 * CPL; c += kSThreads) s_col_inst[c] = -1;
+  __syncthreads();
+  for (int i = tid; i < d.n_inst; i += kSThreads) {
+    const int* stt = st.state + i * kStateInts;
+    const int b = st.inst_b[i], c0 = st.inst_col0[i], nb = stt[S_NB];
+    const bool valid = nb <= d.n_slots && b >= 1 && b <= kBMax && nb * b <= kJacobiMax + kBMax;
+    const bool act = stt[S_ACTIVE] && !(pass == 2 && stt[S_ONEPASS]) && valid;
+    s_b[i] = b;
+    s_c0[i] = c0;
+    s_nb[i] = act ? nb : -1;
+    s_jloc[i] = (act && pass == 1 && nb >= 2 && (st.reserved & kFlagSinglePass)) ? nb - 1 : 0;
+    if (act)
+      for (int q = 0; q < b; ++q) s_col_inst[c0 + q] = i;
+  }
+  __syncthreads();
+  // the known part of the recurrence per instance (pass 1, single pass on):
+  // lc[i][(l*b + p)*b + q] = conj(P[j*b + q][l*b + p]) for l < j = nb - 1,
+  // sigma_q = Re P[(j-1)*b + q][(j-1)*b + q]
+  for (int i = 0; i < d.n_inst; ++i) {
+    const int jl = s_jloc[i];
+    if (jl == 0) continue;
+    const int b = s_b[i];
+    const double2* Pi = reinterpret_cast<const double2*>(st.P) + (int64_t)i * d.pm * d.pm;
+    for (int e = tid; e < jl * b * b; e += kSThreads) {
+      const int r = e / b, q = e % b;
+      lc[(size_t)i * cs_stride + r * b + q] = cconj(Pi[(int64_t)(jl * b + q) * d.pm + r]);
+    }
+    if (tid < b) s_sig[i][tid] = Pi[(int64_t)((jl - 1) * b + tid) * d.pm + (jl - 1) * b + tid].x;
+  }
+  __syncthreads();
+  for (int i = tid; i < d.n_inst; i += kSThreads) {
+    unsigned long long m = 0;
+    const int jl = s_jloc[i], b = s_b[i];
+    for (int l = 0; l < jl; ++l) {
+      bool nz = false;
+      for (int e = 0; e < b * b; ++e) {
+        const double2 v = lc[(size_t)i * cs_stride + l * b * b + e];
+        nz |= (v.x != 0.0) || (v.y != 0.0);
+      }
+      if (nz) m |= 1ull << l;
+    }
+    s_lnz[i] = m;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    int nbmax = -1;
+    unsigned long long need = 0;
+    for (int i = 0; i < d.n_inst; ++i) {
+      nbmax = max(nbmax, s_nb[i]);
+      if (s_jloc[i]) need |= s_lnz[i] | (1ull << s_jloc[i]);
+    }
+    int n = 0;
+    s_list[n++] = -1;
+    for (int l = 0; l < 64; ++l)
+      if ((need >> l) & 1ull) s_list[n++] = l;
+    s_nloc = n - 1;
+    for (int s = 0; s < nbmax; ++s) s_list[n++] = s;
+    s_npc = n;
+    s_nbmax = nbmax;
+    for (int k = 0; k < ns; ++k) {
+      mbar_init(&full[k], 1);
+      mbar_init(&empty[k], kSW);
+    }
+    mbar_init_fence();
+  }
+  __syncthreads();
+  const int nbmax = s_nbmax;
+  if (nbmax < 0) return;  // no instance has work in this pass
+  const int npc = s_npc, nloc = s_nloc;
+  const int64_t n_rchunks = (d.n_orb + pr - 1) / pr;
+  const int64_t my_chunks = blockIdx.x < n_rchunks ? (n_rchunks - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  if (warp == kSW) {
+    if (lane == 0) stream_produce(st, d, ns, pr, s_list, npc, my_chunks, full, empty, ring, s_abort);
+  } else {
+    double2 acc[SW][CPL][BB];
+#pragma unroll
+    for (int j = 0; j < SW; ++j)
+#pragma unroll
+      for (int c = 0; c < CPL; ++c)
+#pragma unroll
+        for (int q = 0; q < BB; ++q) acc[j][c][q] = make_double2(0.0, 0.0);
+    // this lane's columns (Gram) and this thread's two entries (W_loc)
+    int cinst[CPL], cnb[CPL], cb[CPL], cc0[CPL];
+#pragma unroll
+    for (int c = 0; c < CPL; ++c) {
+      const int col = lane + 32 * c;
+      const int i = col < ld ? s_col_inst[col] : -1;
+      cinst[c] = i;
+      cnb[c] = i >= 0 ? s_nb[i] : -1;
+      cb[c] = i >= 0 ? s_b[i] : 0;
+      cc0[c] = i >= 0 ? s_c0[i] : 0;
+    }
+    int einst[2], erow[2], ecol[2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const int e = tid + u * kSW * 32;
+      erow[u] = e / ld;
+      ecol[u] = e % ld;
+      einst[u] = (erow[u] < pr) ? s_col_inst[ecol[u]] : -1;
+    }
+    for (int64_t ci = 0; ci < my_chunks; ++ci) {
+      const int64_t r0 = (blockIdx.x + ci * gridDim.x) * (int64_t)pr;
+      const int rows = (int)min((int64_t)pr, d.n_orb - r0);
+      int64_t k = ci * npc;
+      double2 w[2];
+      {
+        const int stg = (int)(k % ns);
+        mbar_wait(&full[stg], (uint32_t)((k / ns) & 1), s_abort);
+        const double2* pnl = ring + (size_t)stg * kPanelElems;
+#pragma unroll
+        for (int u = 0; u < 2; ++u) w[u] = erow[u] < rows ? pnl[erow[u] * ld + ecol[u]] : make_double2(0.0, 0.0);
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[stg]);
+        ++k;
+      }
+      for (int t = 1; t <= nloc; ++t, ++k) {
+        const int sl = s_list[t];
+        const int stg = (int)(k % ns);
+        mbar_wait(&full[stg], (uint32_t)((k / ns) & 1), s_abort);
+        const double2* pnl = ring + (size_t)stg * kPanelElems;
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const int i = einst[u];
+          if (i < 0 || erow[u] >= rows) continue;
+          const int jl = s_jloc[i];
+          if (jl == 0) continue;
+          const int b = s_b[i], c0 = s_c0[i], q = ecol[u] - c0;
+          const double2* prow = pnl + erow[u] * ld + c0;
+          if (sl == jl) {
+            const double2 x = prow[q];
+            w[u].x -= s_sig[i][q] * x.x;
+            w[u].y -= s_sig[i][q] * x.y;
+          } else if (sl < jl && ((s_lnz[i] >> sl) & 1ull)) {
+            const double2* Li = lc + (size_t)i * cs_stride + sl * b * b;
+            for (int p = 0; p < b; ++p) w[u] = csub(w[u], cmul(prow[p], Li[p * b + q]));
+          }
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[stg]);
+      }
+      consumer_sync();  // every warp is done with the previous chunk's W_loc
+#pragma unroll
+      for (int u = 0; u < 2; ++u)
+        if (erow[u] < pr) wl[erow[u] * ld + ecol[u]] = w[u];
+      consumer_sync();
+      // Gram of W_loc itself: slot nb of the lane's instance
+#pragma unroll
+      for (int c = 0; c < CPL; ++c) {
+        if (cinst[c] < 0) continue;
+        const int col = lane + 32 * c;
+#pragma unroll
+        for (int jj = 0; jj < SW; ++jj) {
+          if (cnb[c] != jj * kSW + warp) continue;
+          for (int r = 0; r < rows; ++r) {
+            const double2 y = wl[r * ld + col];
+            const double2* wr = wl + r * ld + cc0[c];
+#pragma unroll
+            for (int q = 0; q < BB; ++q)
+              if (q < cb[c]) acc[jj][c][q] = cadd(acc[jj][c][q], cdotc(y, wr[q]));
+          }
+        }
+      }
+      // basis slots 0 .. nbmax-1, slot s added by warp s % kSW
+#pragma unroll
+      for (int jj = 0; jj < SW; ++jj) {
+        for (int ww = 0; ww < kSW; ++ww) {
+          const int s = jj * kSW + ww;
+          if (s >= nbmax) break;
+          const int64_t kk = k + s;
+          const int stg = (int)(kk % ns);
+          mbar_wait(&full[stg], (uint32_t)((kk / ns) & 1), s_abort);
+          if (ww == warp) {
+            const double2* pnl = ring + (size_t)stg * kPanelElems;
+#pragma unroll
+            for (int c = 0; c < CPL; ++c) {
+              if (s >= cnb[c]) continue;
+              const int col = lane + 32 * c;
+#pragma unroll 4
+              for (int r = 0; r < rows; ++r) {
+                const double2 y = pnl[r * ld + col];
+                const double2* wr = wl + r * ld + cc0[c];
+#pragma unroll
+                for (int q = 0; q < BB; ++q)
+                  if (q < cb[c]) acc[jj][c][q] = cadd(acc[jj][c][q], cdotc(y, wr[q]));
+              }
+            }
+          }
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&empty[stg]);
+        }
+      }
+    }
+    if (!*s_abort) {
+      double2* part = reinterpret_cast<double2*>(st.partial);
+#pragma unroll
+      for (int c = 0; c < CPL; ++c) {
+        const int i = cinst[c];
+        if (i < 0) continue;
+        const int p = lane + 32 * c - cc0[c];
+#pragma unroll
+        for (int jj = 0; jj < SW; ++jj) {
+          const int s = jj * kSW + warp;
+          if (s > cnb[c]) continue;
+          double2* out = part + (((int64_t)blockIdx.x * d.n_inst + i) * d.pslots + s) * kBMax * kBMax + p * kBMax;
+#pragma unroll
+          for (int q = 0; q < BB; ++q)
+            if (q < cb[c]) out[q] = acc[jj][c][q];
+        }
+      }
+    }
+  }
+  __syncthreads();
+  if (*s_abort && tid == 0) {
+    for (int i = 0; i < d.n_inst; ++i) {
+      if (s_nb[i] < 0) continue;
+      int* stt = st.state + i * kStateInts;
+      stt[S_STATUS] = RSED_ETIMEOUT;
+      stt[S_ACTIVE] = 0;
+    }
+  }
+}
+
+// Finalisation of the streamed Gram partials, one block per instance (the
+// same arithmetic as the last block of k_lz_reduce).
+__global__ void __launch_bounds__(kRT) k_lz_finalize(rsed_lanczos_t st, LzDims d, int pass) {
+  const int inst = blockIdx.x;
+  int* stt = st.state + inst * kStateInts;
+  if (pass == 1 && threadIdx.x == 0) stt[S_RESTART_NB] = 0;
+  if (!stt[S_ACTIVE]) return;
+  if (pass == 2 && stt[S_ONEPASS]) return;
+  const int b = st.inst_b[inst];
+  const int nb = stt[S_NB];
+  __shared__ int s_ok, s_one;
+  __shared__ double2 sc[(kJacobiMax / 1 + kBMax + kBMax) * kBMax];
+  __shared__ double2 sR[kBMax * kBMax];
+  __shared__ double2 sG[kBMax * kBMax];
+  __shared__ double2 fin[kRT * kBMax];
+  if (nb > d.n_slots || b < 1 || b > kBMax || nb * b > kJacobiMax + kBMax) {
+    if (threadIdx.x == 0) {
+      stt[S_STATUS] = RSED_EINVAL;
+      stt[S_ACTIVE] = 0;
+    }
+    return;
+  }
+  const bool loc = pass == 1 && nb >= 2 && (st.reserved & kFlagSinglePass);
+  lz_finalize(st, d, inst, pass, b, nb, stt, sc, sR, sG, &s_ok, fin, loc, &s_one);
+}
+
+// W <- (W_loc - V C) R^-1 for all instances, streamed: per chunk W and the
+// basis slots s < max nb; thread = entry (row, column c0 + q) of the panel,
+// subtracting sum_p V_s[row][c0+p] C[s p][q] from shared memory; the rows are
+// then solved with R by forward substitution over the instance's columns
+// (exchanged through shared memory) and stored as in k_lz_update_rows.
+__global__ void __launch_bounds__(kSThreads, 2)
+    k_lz_update_stream(rsed_lanczos_t st, LzDims d, int pass, int ns, int pr, int cs_stride) {
+  extern __shared__ __align__(128) unsigned char smem_s[];
+  const StreamLayout L = stream_layout(ns, d.n_inst, cs_stride, true);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem_s + L.bars);
+  uint64_t* empty = full + ns;
+  double2* ring = reinterpret_cast<double2*>(smem_s + L.ring);
+  double2* wsh = reinterpret_cast<double2*>(smem_s + L.wl);
+  double2* cs = reinterpret_cast<double2*>(smem_s + L.coef);
+  double2* Rs = reinterpret_cast<double2*>(smem_s + L.rs);
+  __shared__ int s_b[kStreamInstMax], s_c0[kStreamInstMax], s_nb[kStreamInstMax], s_one[kStreamInstMax];
+  __shared__ int s_col_inst[64];
+  __shared__ int s_list[kJacobiMax + 2];
+  __shared__ int s_nbmax;
+  __shared__ int s_abort_store;
+  volatile int* s_abort = &s_abort_store;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int ld = d.ld;
+  if (tid == 0) s_abort_store = 0;
+  for (int c = tid; c < 64; c += kSThreads) s_col_inst[c] = -1;
+  __syncthreads();
+  for (int i = tid; i < d.n_inst; i += kSThreads) {
+    const int* stt = st.state + i * kStateInts;
+    const int b = st.inst_b[i], c0 = st.inst_col0[i];
+    const bool one = stt[S_ONEPASS] != 0;
+    const int nb = (pass == 2 || one) ? stt[S_NEWSLOT] : stt[S_NB];
+    const bool act = stt[S_ACTIVE] && b >= 1 && b <= kBMax && nb * b <= kJacobiMax && !(pass == 2 && one);
+    s_b[i] = b;
+    s_c0[i] = c0;
+    s_one[i] = one;
+    s_nb[i] = act ? nb : -1;
+    if (act)
+      for (int q = 0; q < b; ++q) s_col_inst[c0 + q] = i;
+  }
+  __syncthreads();
+  for (int i = 0; i < d.n_inst; ++i) {
+    const int nb = s_nb[i], b = s_b[i];
+    if (nb < 0) continue;
+    const double2* coef = reinterpret_cast<const double2*>(st.coef) +
+                          (int64_t)i * 2 * d.pslots * kBMax * kBMax + (pass - 1) * d.pslots * kBMax * kBMax;
+    for (int e = tid; e < nb * b * b; e += kSThreads) {
+      const int r = e / b, q = e % b;  // r = s * b + p
+      cs[(size_t)i * cs_stride + r * b + q] = coef[(r / b) * kBMax * kBMax + (r % b) * kBMax + q];
+    }
+    for (int e = tid; e < kBMax * kBMax; e += kSThreads)
+      Rs[i * kBMax * kBMax + e] = coef[(d.pslots - 1) * kBMax * kBMax + e];
+  }
+  if (tid == 0) {
+    int nbmax = -1;
+    for (int i = 0; i < d.n_inst; ++i) nbmax = max(nbmax, s_nb[i]);
+    s_list[0] = -1;
+    for (int s = 0; s < nbmax; ++s) s_list[1 + s] = s;
+    s_nbmax = nbmax;
+    for (int k = 0; k < ns; ++k) {
+      mbar_init(&full[k], 1);
+      mbar_init(&empty[k], kSW);
+    }
+    mbar_init_fence();
+  }
+  __syncthreads();
+  const int nbmax = s_nbmax;
+  if (nbmax < 0) return;
+  const int npc = 1 + nbmax;
+  const int64_t n_rchunks = (d.n_orb + pr - 1) / pr;
+  const int64_t my_chunks = blockIdx.x < n_rchunks ? (n_rchunks - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  if (warp == kSW) {
+    if (lane == 0) stream_produce(st, d, ns, pr, s_list, npc, my_chunks, full, empty, ring, s_abort);
+  } else {
+    double2* V = reinterpret_cast<double2*>(st.V);
+    double2* W = reinterpret_cast<double2*>(st.W);
+    const int64_t slot_stride = d.n_orb * d.ld;
+    const bool copy_cur = st.Xf == nullptr;  // the FP64 matvec reads the current-block slot
+    int einst[2], erow[2], ecol[2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const int e = tid + u * kSW * 32;
+      erow[u] = e / ld;
+      ecol[u] = e % ld;
+      einst[u] = (erow[u] < pr) ? s_col_inst[ecol[u]] : -1;
+    }
+    for (int64_t ci = 0; ci < my_chunks; ++ci) {
+      const int64_t r0 = (blockIdx.x + ci * gridDim.x) * (int64_t)pr;
+      const int rows = (int)min((int64_t)pr, d.n_orb - r0);
+      int64_t k = ci * npc;
+      double2 w[2];
+      {
+        const int stg = (int)(k % ns);
+        mbar_wait(&full[stg], (uint32_t)((k / ns) & 1), s_abort);
+        const double2* pnl = ring + (size_t)stg * kPanelElems;
+#pragma unroll
+        for (int u = 0; u < 2; ++u) w[u] = erow[u] < rows ? pnl[erow[u] * ld + ecol[u]] : make_double2(0.0, 0.0);
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[stg]);
+        ++k;
+      }
+#pragma unroll 2
+      for (int s = 0; s < nbmax; ++s, ++k) {
+        const int stg = (int)(k % ns);
+        mbar_wait(&full[stg], (uint32_t)((k / ns) & 1), s_abort);
+        const double2* pnl = ring + (size_t)stg * kPanelElems;
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const int i = einst[u];
+          if (i < 0 || erow[u] >= rows || s >= s_nb[i]) continue;
+          const int b = s_b[i], c0 = s_c0[i], q = ecol[u] - c0;
+          const double2* prow = pnl + erow[u] * ld + c0;
+          const double2* ci_ = cs + (size_t)i * cs_stride + s * b * b + q;
+          for (int p = 0; p < b; ++p) w[u] = csub(w[u], cmul(prow[p], ci_[p * b]));
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[stg]);
+      }
+      consumer_sync();  // every warp is done with the previous chunk's rows
+#pragma unroll
+      for (int u = 0; u < 2; ++u)
+        if (erow[u] < pr) wsh[erow[u] * ld + ecol[u]] = w[u];
+      consumer_sync();
+      if (*s_abort) continue;
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const int i = einst[u];
+        if (i < 0 || erow[u] >= rows) continue;
+        const int b = s_b[i], c0 = s_c0[i], q = ecol[u] - c0, nb = s_nb[i];
+        const double2* wr = wsh + erow[u] * ld + c0;
+        const double2* Ri = Rs + i * kBMax * kBMax;
+        double2 xs[kBMax];
+        double2 xq = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int pp = 0; pp < kBMax; ++pp) {
+          if (pp > q) break;
+          double2 v = wr[pp];
+          for (int kq = 0; kq < pp; ++kq) v = csub(v, cmul(xs[kq], Ri[kq * kBMax + pp]));
+          const double rr = Ri[pp * kBMax + pp].x;
+          xs[pp] = make_double2(v.x / rr, v.y / rr);
+          xq = xs[pp];
+        }
+        (void)b;
+        const int64_t at = (r0 + erow[u]) * ld + ecol[u];
+        if (pass == 1 && !s_one[i]) {
+          W[at] = xq;
+        } else {
+          V[(int64_t)nb * slot_stride + at] = xq;
+          if (copy_cur) V[(int64_t)(d.n_slots + 1) * slot_stride + at] = xq;
+          if (st.Xf) reinterpret_cast<float2*>(st.Xf)[at] = make_float2((float)xq.x, (float)xq.y);
+        }
+      }
+    }
+  }
+  __syncthreads();
+  if (*s_abort && tid == 0) {
+    for (int i = 0; i < d.n_inst; ++i) {
+      if (s_nb[i] < 0) continue;
+      int* stt = st.state + i * kStateInts;
+      stt[S_STATUS] = RSED_ETIMEOUT;
+      stt[S_ACTIVE] = 0;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Lowest Kp eigenpairs of a Hermitian M x M matrix held in shared memory
 // (full row-major storage, destroyed), one thread block:
 //   1. Householder reduction to a real symmetric tridiagonal T = Q^H A Q
@@ -1907,7 +2502,89 @@ int check_lz(const rsed_model_t* md, const rsed_sectors_t* sc, const rsed_lanczo
   return RSED_OK;
 }
 
+// Streaming configuration of a batch: panel rows pr (kPanelElems / ld), ring
+// depth ns (the deepest ring, 4..12 stages, that leaves two blocks per SM),
+// grid.  False when the batch does not fit the streaming kernels.
+struct StreamConfig {
+  int pr, ns_gram, ns_upd, grid;
+  size_t smem_gram, smem_upd;
+};
+
+bool stream_config(const rsed_lanczos_t& st, const LzDims& d, StreamConfig* c) {
+  if (st.reserved & kFlagNoStream) return false;
+  if (d.ld > 64 || d.n_inst > kStreamInstMax || d.n_orb < 1) return false;
+  const int cs_stride = st.n_slots * st.bmax * st.bmax;
+  constexpr size_t kBudget = 104 * 1024;  // dynamic shared memory per block (two blocks per SM)
+  c->pr = kPanelElems / d.ld;
+  c->ns_gram = c->ns_upd = 0;
+  for (int ns = 12; ns >= 4 && !c->ns_gram; --ns)
+    if (stream_layout(ns, d.n_inst, cs_stride, false).total <= kBudget) c->ns_gram = ns;
+  for (int ns = 12; ns >= 4 && !c->ns_upd; --ns)
+    if (stream_layout(ns, d.n_inst, cs_stride, true).total <= kBudget) c->ns_upd = ns;
+  if (!c->ns_gram || !c->ns_upd) return false;
+  c->smem_gram = stream_layout(c->ns_gram, d.n_inst, cs_stride, false).total;
+  c->smem_upd = stream_layout(c->ns_upd, d.n_inst, cs_stride, true).total;
+  int dev = 0, n_sm = 148;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    return false;
+  const int64_t n_rchunks = (d.n_orb + c->pr - 1) / c->pr;
+  int64_t grid = 2 * (int64_t)n_sm;
+  if (grid > kStreamGridMax) grid = kStreamGridMax;
+  if (grid > n_rchunks) grid = n_rchunks;
+  c->grid = (int)grid;
+  return true;
+}
+
+template <int BB, int CPL>
+int launch_gram_stream(const rsed_lanczos_t& st, const LzDims& d, int pass, const StreamConfig& c,
+                       cudaStream_t stream) {
+  static bool attr_set = false;
+  if (!attr_set) {
+    RSED_TRY_CUDA(cudaFuncSetAttribute(k_lz_gram_stream<BB, CPL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       110 * 1024));
+    attr_set = true;
+  }
+  k_lz_gram_stream<BB, CPL><<<(unsigned)c.grid, kSThreads, c.smem_gram, stream>>>(
+      st, d, pass, c.ns_gram, c.pr, st.n_slots * st.bmax * st.bmax);
+  RSED_CHECK_LAUNCH();
+  return RSED_OK;
+}
+
+int launch_pass_stream(const rsed_lanczos_t& st, const LzDims& d, int pass, const StreamConfig& c,
+                       cudaStream_t stream) {
+  LzDims ds = d;
+  ds.n_chunks = c.grid;  // one Gram partial per streaming block
+  const int bb = st.bmax <= 1 ? 1 : st.bmax <= 2 ? 2 : st.bmax <= 4 ? 4 : 8;
+  int rc;
+  if (d.ld <= 32) {
+    rc = bb == 1   ? launch_gram_stream<1, 1>(st, ds, pass, c, stream)
+         : bb == 2 ? launch_gram_stream<2, 1>(st, ds, pass, c, stream)
+         : bb == 4 ? launch_gram_stream<4, 1>(st, ds, pass, c, stream)
+                   : launch_gram_stream<8, 1>(st, ds, pass, c, stream);
+  } else {
+    rc = bb == 1   ? launch_gram_stream<1, 2>(st, ds, pass, c, stream)
+         : bb == 2 ? launch_gram_stream<2, 2>(st, ds, pass, c, stream)
+         : bb == 4 ? launch_gram_stream<4, 2>(st, ds, pass, c, stream)
+                   : launch_gram_stream<8, 2>(st, ds, pass, c, stream);
+  }
+  if (rc != RSED_OK) return rc;
+  k_lz_finalize<<<(unsigned)d.n_inst, kRT, 0, stream>>>(st, ds, pass);
+  RSED_CHECK_LAUNCH();
+  static bool attr_set = false;
+  if (!attr_set) {
+    RSED_TRY_CUDA(cudaFuncSetAttribute(k_lz_update_stream, cudaFuncAttributeMaxDynamicSharedMemorySize, 110 * 1024));
+    attr_set = true;
+  }
+  k_lz_update_stream<<<(unsigned)c.grid, kSThreads, c.smem_upd, stream>>>(st, ds, pass, c.ns_upd, c.pr,
+                                                                            st.n_slots * st.bmax * st.bmax);
+  RSED_CHECK_LAUNCH();
+  return RSED_OK;
+}
+
 int launch_pass(const rsed_lanczos_t& st, const LzDims& d, int pass, cudaStream_t stream) {
+  StreamConfig sc;
+  if (stream_config(st, d, &sc)) return launch_pass_stream(st, d, pass, sc, stream);
   k_lz_reduce<<<(unsigned)(d.n_chunks * d.n_inst), kRT, 0, stream>>>(st, d, pass);
   RSED_CHECK_LAUNCH();
   // all instances per block when their coefficients fit in shared memory
@@ -1990,7 +2667,8 @@ __global__ void k_scatter_block(int64_t n_rows, const int32_t* orbit_of_row, con
 
 extern "C" int64_t rsed_lanczos_partial_len(int64_t n_orbits, int32_t chunk_rows, int32_t n_inst,
                                             int32_t n_slots) {
-  const int64_t n_chunks = (n_orbits + chunk_rows - 1) / chunk_rows;
+  int64_t n_chunks = (n_orbits + chunk_rows - 1) / chunk_rows;
+  if (n_chunks < kStreamGridMax) n_chunks = kStreamGridMax;  // the streaming reduction's partials
   const int64_t lz = (int64_t)(n_slots + 3) * kBMax * kBMax * 2;
   const int64_t rr = (int64_t)kRRMax * kRRMax * 2;
   return n_chunks * n_inst * (lz > rr ? lz : rr);
