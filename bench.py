@@ -955,7 +955,8 @@ def run_b200(args):
 
     # how the batch runs (block sizes, persistent cluster or graph path,
     # projection table, basis length) is picked by the autotuner, untimed
-    params = ed.LanczosParams(precision=args.precision, single_pass=not args.two_pass, stream=not args.no_stream)
+    params = ed.LanczosParams(precision=args.precision, single_pass=not args.two_pass, stream=not args.no_stream,
+                              stream_update=args.stream_update)
     tuner = ed.Autotuner(trials=2)
     t0 = time.perf_counter()
     if args.solver == "auto":
@@ -1242,6 +1243,8 @@ def main():
                     help="always two Gram-Schmidt passes per step (no adaptive single pass)")
     ap.add_argument("--no-stream", action="store_true",
                     help="per-instance Gram-Schmidt kernels instead of the streamed whole-row panels")
+    ap.add_argument("--stream-update", action="store_true",
+                    help="the streamed update after the streamed Gram reduction (default: the row-group update)")
     ap.add_argument("--config5", type=int, default=0,
                     help="only the 48-site checkerboard line for this many sectors (device vs C++ restatement)")
     ap.add_argument("--solver", default="auto",
@@ -1273,10 +1276,14 @@ def main():
         data = ed.build_ed_data(model, filling_fraction=Fraction(nf, model.lattice.n_site), symmetry_group=G)
         secs = list(range(args.solve_scale))
         cfg = ed.SolverConfig((2,) * len(secs), 0, True, 16)
-        res = ed.solve_sectors_batched(data, secs, nev=4, precision=32, config=cfg, return_vectors=False)
+        prm = ed.LanczosParams(block=2, precision=32, single_pass=not args.two_pass, stream=not args.no_stream,
+                               stream_update=args.stream_update)
+        res = ed.solve_sectors_batched(data, secs, nev=4, precision=32, params=prm, config=cfg,
+                                       return_vectors=False)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        res = ed.solve_sectors_batched(data, secs, nev=4, precision=32, config=cfg, return_vectors=False)
+        res = ed.solve_sectors_batched(data, secs, nev=4, precision=32, params=prm, config=cfg,
+                                       return_vectors=False)
         torch.cuda.synchronize()
         print(json.dumps({"workload": f"haldane32: {len(secs)} sectors, FP32 + FP64 refinement, b=2, nev 4",
                           "solve_s": time.perf_counter() - t0, "E0": [float(res[s][0][0]) for s in secs]}))

@@ -500,10 +500,10 @@ __global__ void __launch_bounds__(256) k_lz_update(rsed_lanczos_t st, LzDims d, 
 // exchanged through shared memory.  Grid-stride over pairs of row groups.
 // The copy of a new block into the current-block slot is written only when
 // the matvec reads it (FP64 matvec); an FP32-matvec batch reads Xf.
-__global__ void __launch_bounds__(256) k_lz_update_rows(rsed_lanczos_t st, LzDims d, int pass, int cs_stride) {
+__global__ void __launch_bounds__(256, 3) k_lz_update_rows(rsed_lanczos_t st, LzDims d, int pass, int crows) {
   extern __shared__ __align__(16) unsigned char smem_u[];
-  double2* cs = reinterpret_cast<double2*>(smem_u);                    // [inst][cs_stride]
-  double2* Rs = cs + (size_t)d.n_inst * cs_stride;                      // [inst][kBMax*kBMax]
+  double2* cs = reinterpret_cast<double2*>(smem_u);                    // [(s*bmax + p)][ld]: C[s p][q] of column c0+q
+  double2* Rs = cs + (size_t)crows * d.ld;                               // [k*kBMax + p][inst]
   double2* wsh = Rs + (size_t)d.n_inst * kBMax * kBMax;                 // [2][256] row-group w values
   int* meta = reinterpret_cast<int*>(wsh + 512);                        // [ld]: inst of each column
   for (int c = threadIdx.x; c < d.ld; c += blockDim.x) meta[c] = -1;
@@ -512,9 +512,10 @@ __global__ void __launch_bounds__(256) k_lz_update_rows(rsed_lanczos_t st, LzDim
     const int b = st.inst_b[inst], c0 = st.inst_col0[inst];
     for (int q = 0; q < b; ++q) meta[c0 + q] = inst;
   }
+  const int bmax = st.bmax;
   for (int inst = 0; inst < d.n_inst; ++inst) {
     const int* stt = st.state + inst * kStateInts;
-    const int b = st.inst_b[inst];
+    const int b = st.inst_b[inst], c0i = st.inst_col0[inst];
     const bool one = stt[S_ONEPASS] != 0;
     const int nb = (pass == 2 || one) ? stt[S_NEWSLOT] : stt[S_NB];
     const double2* coef = reinterpret_cast<const double2*>(st.coef) +
@@ -522,10 +523,10 @@ __global__ void __launch_bounds__(256) k_lz_update_rows(rsed_lanczos_t st, LzDim
     if (!stt[S_ACTIVE] || nb * b > kJacobiMax || (pass == 2 && one)) continue;
     for (int e = threadIdx.x; e < nb * b * b; e += blockDim.x) {
       const int r = e / b, q = e % b;  // r = s * b + p
-      cs[(size_t)inst * cs_stride + r * b + q] = coef[(r / b) * kBMax * kBMax + (r % b) * kBMax + q];
+      cs[(size_t)((r / b) * bmax + r % b) * d.ld + c0i + q] = coef[(r / b) * kBMax * kBMax + (r % b) * kBMax + q];
     }
     for (int e = threadIdx.x; e < kBMax * kBMax; e += blockDim.x)
-      Rs[inst * kBMax * kBMax + e] = coef[(d.pslots - 1) * kBMax * kBMax + e];
+      Rs[e * d.n_inst + inst] = coef[(d.pslots - 1) * kBMax * kBMax + e];
   }
   __syncthreads();
   const int rows_pg = blockDim.x / d.ld;  // rows per group
@@ -543,8 +544,9 @@ __global__ void __launch_bounds__(256) k_lz_update_rows(rsed_lanczos_t st, LzDim
     q = col - c0;
     act = stt[S_ACTIVE] && nb * b <= kJacobiMax && !(pass == 2 && one);
   }
-  const double2* csi = cs + (size_t)(inst < 0 ? 0 : inst) * cs_stride;
-  const double2* Ri = Rs + (inst < 0 ? 0 : inst) * kBMax * kBMax;
+  const double2* ccol = cs + col;                    // C[s p][q] at ccol[(s*bmax + p)*ld]
+  const double2* Ri = Rs + (inst < 0 ? 0 : inst);  // R[k][p] at Ri[(k*kBMax + p)*n_inst]
+  const int ni = d.n_inst;
   double2* V = reinterpret_cast<double2*>(st.V);
   double2* W = reinterpret_cast<double2*>(st.W);
   const int64_t slot_stride = d.n_orb * d.ld;
@@ -562,7 +564,7 @@ __global__ void __launch_bounds__(256) k_lz_update_rows(rsed_lanczos_t st, LzDim
       for (int s = 0; s < nb; ++s) {
         const double2* Vs = V + s * slot_stride + row0 * d.ld + c0;
         for (int p = 0; p < b; ++p) {
-          const double2 c = csi[(s * b + p) * b + q];
+          const double2 c = ccol[(size_t)(s * bmax + p) * d.ld];
           w0 = csub(w0, cmul(Vs[p], c));
           if (live1) w1 = csub(w1, cmul(Vs[(int64_t)rows_pg * d.ld + p], c));
         }
@@ -584,8 +586,8 @@ __global__ void __launch_bounds__(256) k_lz_update_rows(rsed_lanczos_t st, LzDim
       for (int pp = 0; pp < kBMax; ++pp) {
         if (pp > q) break;
         double2 v = wr[pp];
-        for (int k = 0; k < pp; ++k) v = csub(v, cmul(xs[k], Ri[k * kBMax + pp]));
-        const double rr = Ri[pp * kBMax + pp].x;
+        for (int k = 0; k < pp; ++k) v = csub(v, cmul(xs[k], Ri[(k * kBMax + pp) * ni]));
+        const double rr = Ri[(pp * kBMax + pp) * ni].x;
         xs[pp] = make_double2(v.x / rr, v.y / rr);
         xq = xs[pp];
       }
@@ -631,6 +633,7 @@ constexpr int kStreamInstMax = 64;            // instances of a streamed batch a
 constexpr int kListMax = 2 * kJacobiMax + 8;  // panels of one chunk at most
 constexpr unsigned long long kWaitNs = 2000000000ull;
 constexpr int kFlagNoStream = 2;              // st.reserved bit 1: use the per-instance kernels
+constexpr int kFlagNoStreamUpdate = 4;        // st.reserved bit 2: streamed reduction, row-group update
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -666,7 +669,7 @@ __device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
 }
 // Waits for the completion of the phase with the given parity.  False when the
 // block's abort flag is up or the wait ran out of kWaitNs (which raises it).
-__device__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort) {
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort) {
   if (*abort) return false;
   if (mbar_test(bar, parity)) return true;
   const uint64_t t0 = global_ns();
@@ -692,6 +695,14 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t b
 // barrier of the kSW consumer warps only (the producer warp never joins it)
 __device__ __forceinline__ void consumer_sync() { asm volatile("bar.sync 1, %0;" ::"n"(kSW * 32) : "memory"); }
 
+// The ring position after a panel: next stage, parity flipped on wrap-around.
+__device__ __forceinline__ void ring_next(int& stg, uint32_t& ph, int ns) {
+  if (++stg == ns) {
+    stg = 0;
+    ph ^= 1u;
+  }
+}
+
 // After an abort: waits, bounded, for the last copy issued into each stage.
 __device__ void stream_drain(uint64_t* full, int ns, int64_t issued) {
   for (int64_t k = issued > ns ? issued - ns : 0; k < issued; ++k) {
@@ -707,9 +718,10 @@ struct StreamLayout {
   size_t bars, ring, wl, coef, rs, total;
 };
 // dynamic shared memory of a streaming block: ns full + ns empty barriers,
-// the ring, one panel-sized work buffer, the instances' coefficients
-// (n_inst x cs_stride) and, for the update, their R factors
-__host__ __device__ inline StreamLayout stream_layout(int ns, int n_inst, int cs_stride, bool with_r) {
+// the ring, one panel-sized work buffer, the coefficients (column-major:
+// crows rows of ld columns, so the lanes of a warp read consecutive words)
+// and, for the update, the instances' R factors ([k][p][instance])
+__host__ __device__ inline StreamLayout stream_layout(int ns, int n_inst, int crows, int ld, bool with_r) {
   StreamLayout l;
   size_t off = 0;
   l.bars = off;
@@ -720,7 +732,7 @@ __host__ __device__ inline StreamLayout stream_layout(int ns, int n_inst, int cs
   l.wl = off;
   off += sizeof(double2) * kPanelElems;
   l.coef = off;
-  off += sizeof(double2) * (size_t)n_inst * cs_stride;
+  off += sizeof(double2) * (size_t)crows * ld;
   l.rs = off;
   off += with_r ? sizeof(double2) * (size_t)n_inst * kBMax * kBMax : 0;
   l.total = off;
@@ -737,17 +749,24 @@ __device__ void stream_produce(const rsed_lanczos_t& st, const LzDims& d, int ns
   const int64_t slot_stride = d.n_orb * d.ld;
   const int64_t total = my_chunks * npc;
   int64_t issued = 0;
+  int stg = 0, t = 0;
+  uint32_t ph = 0;  // parity of this stage's current use
+  int64_t r0 = (int64_t)blockIdx.x * pr;
   for (int64_t k = 0; k < total; ++k) {
-    const int stg = (int)(k % ns);
-    if (k >= ns && !mbar_wait(&empty[stg], (uint32_t)((k / ns - 1) & 1), abort)) break;
-    const int64_t r0 = (blockIdx.x + (k / npc) * gridDim.x) * (int64_t)pr;
+    // the stage's previous use (panel k - ns) must be released by every consumer
+    if (k >= ns && !mbar_wait(&empty[stg], ph ^ 1u, abort)) break;
     const int64_t rows = min((int64_t)pr, d.n_orb - r0);
-    const int sl = list[k % npc];
+    const int sl = list[t];
     const double2* src = (sl < 0 ? W : V + (int64_t)sl * slot_stride) + r0 * d.ld;
     const uint32_t bytes = (uint32_t)(rows * d.ld * (int64_t)sizeof(double2));
     mbar_expect_tx(&full[stg], bytes);
     bulk_load(ring + (size_t)stg * kPanelElems, src, bytes, &full[stg]);
     issued = k + 1;
+    ring_next(stg, ph, ns);
+    if (++t == npc) {
+      t = 0;
+      r0 += (int64_t)gridDim.x * pr;
+    }
   }
   if (*abort) stream_drain(full, ns, issued);
 }
@@ -764,10 +783,10 @@ __device__ void stream_produce(const rsed_lanczos_t& st, const LzDims& d, int ns
 // columns per lane (ld <= 32 * CPL).
 template <int BB, int CPL>
 __global__ void __launch_bounds__(kSThreads, 2)
-    k_lz_gram_stream(rsed_lanczos_t st, LzDims d, int pass, int ns, int pr, int cs_stride) {
+    k_lz_gram_stream(rsed_lanczos_t st, LzDims d, int pass, int ns, int pr, int crows) {
   constexpr int SW = kJacobiMax / BB / kSW + 1;  // slots one warp owns at most
   extern __shared__ __align__(128) unsigned char smem_s[];
-  const StreamLayout L = stream_layout(ns, d.n_inst, cs_stride, false);
+  const StreamLayout L = stream_layout(ns, d.n_inst, crows, d.ld, false);
   uint64_t* full = reinterpret_cast<uint64_t*>(smem_s + L.bars);
   uint64_t* empty = full + ns;
   double2* ring = reinterpret_cast<double2*>(smem_s + L.ring);
@@ -775,7 +794,7 @@ __global__ void __launch_bounds__(kSThreads, 2)
   double2* lc = reinterpret_cast<double2*>(smem_s + L.coef);
   __shared__ int s_b[kStreamInstMax], s_c0[kStreamInstMax], s_nb[kStreamInstMax], s_jloc[kStreamInstMax];
   __shared__ unsigned long long s_lnz[kStreamInstMax];
-  __shared__ double s_sig[kStreamInstMax][kBMax];
+  __shared__ double s_sig[32 * CPL];  // sigma of each column
   __shared__ int s_col_inst[32 * CPL];
   __shared__ int s_list[kListMax];
   __shared__ int s_npc, s_nloc, s_nbmax;
@@ -800,27 +819,28 @@ __global__ void __launch_bounds__(kSThreads, 2)
   }
   __syncthreads();
   // the known part of the recurrence per instance (pass 1, single pass on):
-  // lc[i][(l*b + p)*b + q] = conj(P[j*b + q][l*b + p]) for l < j = nb - 1,
-  // sigma_q = Re P[(j-1)*b + q][(j-1)*b + q]
+  // lc[(l*bmax + p)*ld + c0 + q] = conj(P[j*b + q][l*b + p]) for l < j = nb - 1,
+  // sigma of column c0 + q = Re P[(j-1)*b + q][(j-1)*b + q]
+  const int bmax = st.bmax;
   for (int i = 0; i < d.n_inst; ++i) {
     const int jl = s_jloc[i];
     if (jl == 0) continue;
-    const int b = s_b[i];
+    const int b = s_b[i], c0 = s_c0[i];
     const double2* Pi = reinterpret_cast<const double2*>(st.P) + (int64_t)i * d.pm * d.pm;
     for (int e = tid; e < jl * b * b; e += kSThreads) {
-      const int r = e / b, q = e % b;
-      lc[(size_t)i * cs_stride + r * b + q] = cconj(Pi[(int64_t)(jl * b + q) * d.pm + r]);
+      const int r = e / b, q = e % b;  // r = l*b + p
+      lc[(size_t)((r / b) * bmax + r % b) * ld + c0 + q] = cconj(Pi[(int64_t)(jl * b + q) * d.pm + r]);
     }
-    if (tid < b) s_sig[i][tid] = Pi[(int64_t)((jl - 1) * b + tid) * d.pm + (jl - 1) * b + tid].x;
+    if (tid < b) s_sig[c0 + tid] = Pi[(int64_t)((jl - 1) * b + tid) * d.pm + (jl - 1) * b + tid].x;
   }
   __syncthreads();
   for (int i = tid; i < d.n_inst; i += kSThreads) {
     unsigned long long m = 0;
-    const int jl = s_jloc[i], b = s_b[i];
+    const int jl = s_jloc[i], b = s_b[i], c0 = s_c0[i];
     for (int l = 0; l < jl; ++l) {
       bool nz = false;
       for (int e = 0; e < b * b; ++e) {
-        const double2 v = lc[(size_t)i * cs_stride + l * b * b + e];
+        const double2 v = lc[(size_t)(l * bmax + e / b) * ld + c0 + e % b];
         nz |= (v.x != 0.0) || (v.y != 0.0);
       }
       if (nz) m |= 1ull << l;
@@ -884,25 +904,24 @@ __global__ void __launch_bounds__(kSThreads, 2)
       ecol[u] = e % ld;
       einst[u] = (erow[u] < pr) ? s_col_inst[ecol[u]] : -1;
     }
+    int stg = 0;      // ring stage of the next panel
+    uint32_t ph = 0;  // parity of that stage's current use
     for (int64_t ci = 0; ci < my_chunks; ++ci) {
       const int64_t r0 = (blockIdx.x + ci * gridDim.x) * (int64_t)pr;
       const int rows = (int)min((int64_t)pr, d.n_orb - r0);
-      int64_t k = ci * npc;
       double2 w[2];
       {
-        const int stg = (int)(k % ns);
-        mbar_wait(&full[stg], (uint32_t)((k / ns) & 1), s_abort);
+        mbar_wait(&full[stg], ph, s_abort);
         const double2* pnl = ring + (size_t)stg * kPanelElems;
 #pragma unroll
         for (int u = 0; u < 2; ++u) w[u] = erow[u] < rows ? pnl[erow[u] * ld + ecol[u]] : make_double2(0.0, 0.0);
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty[stg]);
-        ++k;
+        ring_next(stg, ph, ns);
       }
-      for (int t = 1; t <= nloc; ++t, ++k) {
+      for (int t = 1; t <= nloc; ++t) {
         const int sl = s_list[t];
-        const int stg = (int)(k % ns);
-        mbar_wait(&full[stg], (uint32_t)((k / ns) & 1), s_abort);
+        mbar_wait(&full[stg], ph, s_abort);
         const double2* pnl = ring + (size_t)stg * kPanelElems;
 #pragma unroll
         for (int u = 0; u < 2; ++u) {
@@ -910,19 +929,20 @@ __global__ void __launch_bounds__(kSThreads, 2)
           if (i < 0 || erow[u] >= rows) continue;
           const int jl = s_jloc[i];
           if (jl == 0) continue;
-          const int b = s_b[i], c0 = s_c0[i], q = ecol[u] - c0;
+          const int b = s_b[i], c0 = s_c0[i];
           const double2* prow = pnl + erow[u] * ld + c0;
           if (sl == jl) {
-            const double2 x = prow[q];
-            w[u].x -= s_sig[i][q] * x.x;
-            w[u].y -= s_sig[i][q] * x.y;
+            const double2 x = pnl[erow[u] * ld + ecol[u]];
+            w[u].x -= s_sig[ecol[u]] * x.x;
+            w[u].y -= s_sig[ecol[u]] * x.y;
           } else if (sl < jl && ((s_lnz[i] >> sl) & 1ull)) {
-            const double2* Li = lc + (size_t)i * cs_stride + sl * b * b;
-            for (int p = 0; p < b; ++p) w[u] = csub(w[u], cmul(prow[p], Li[p * b + q]));
+            const double2* Lc = lc + (size_t)sl * bmax * ld + ecol[u];
+            for (int p = 0; p < b; ++p) w[u] = csub(w[u], cmul(prow[p], Lc[p * ld]));
           }
         }
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty[stg]);
+        ring_next(stg, ph, ns);
       }
       consumer_sync();  // every warp is done with the previous chunk's W_loc
 #pragma unroll
@@ -952,9 +972,7 @@ __global__ void __launch_bounds__(kSThreads, 2)
         for (int ww = 0; ww < kSW; ++ww) {
           const int s = jj * kSW + ww;
           if (s >= nbmax) break;
-          const int64_t kk = k + s;
-          const int stg = (int)(kk % ns);
-          mbar_wait(&full[stg], (uint32_t)((kk / ns) & 1), s_abort);
+          mbar_wait(&full[stg], ph, s_abort);
           if (ww == warp) {
             const double2* pnl = ring + (size_t)stg * kPanelElems;
 #pragma unroll
@@ -973,6 +991,7 @@ __global__ void __launch_bounds__(kSThreads, 2)
           }
           __syncwarp();
           if (lane == 0) mbar_arrive(&empty[stg]);
+          ring_next(stg, ph, ns);
         }
       }
     }
@@ -1038,9 +1057,9 @@ __global__ void __launch_bounds__(kRT) k_lz_finalize(rsed_lanczos_t st, LzDims d
 // then solved with R by forward substitution over the instance's columns
 // (exchanged through shared memory) and stored as in k_lz_update_rows.
 __global__ void __launch_bounds__(kSThreads, 2)
-    k_lz_update_stream(rsed_lanczos_t st, LzDims d, int pass, int ns, int pr, int cs_stride) {
+    k_lz_update_stream(rsed_lanczos_t st, LzDims d, int pass, int ns, int pr, int crows) {
   extern __shared__ __align__(128) unsigned char smem_s[];
-  const StreamLayout L = stream_layout(ns, d.n_inst, cs_stride, true);
+  const StreamLayout L = stream_layout(ns, d.n_inst, crows, d.ld, true);
   uint64_t* full = reinterpret_cast<uint64_t*>(smem_s + L.bars);
   uint64_t* empty = full + ns;
   double2* ring = reinterpret_cast<double2*>(smem_s + L.ring);
@@ -1072,17 +1091,19 @@ __global__ void __launch_bounds__(kSThreads, 2)
       for (int q = 0; q < b; ++q) s_col_inst[c0 + q] = i;
   }
   __syncthreads();
+  // cs[(s*bmax + p)*ld + c0 + q] = C[s p][q], Rs[(k*kBMax + p)*n_inst + i] = R_i[k][p]
+  const int bmax = st.bmax;
   for (int i = 0; i < d.n_inst; ++i) {
-    const int nb = s_nb[i], b = s_b[i];
+    const int nb = s_nb[i], b = s_b[i], c0 = s_c0[i];
     if (nb < 0) continue;
     const double2* coef = reinterpret_cast<const double2*>(st.coef) +
                           (int64_t)i * 2 * d.pslots * kBMax * kBMax + (pass - 1) * d.pslots * kBMax * kBMax;
     for (int e = tid; e < nb * b * b; e += kSThreads) {
       const int r = e / b, q = e % b;  // r = s * b + p
-      cs[(size_t)i * cs_stride + r * b + q] = coef[(r / b) * kBMax * kBMax + (r % b) * kBMax + q];
+      cs[(size_t)((r / b) * bmax + r % b) * ld + c0 + q] = coef[(r / b) * kBMax * kBMax + (r % b) * kBMax + q];
     }
     for (int e = tid; e < kBMax * kBMax; e += kSThreads)
-      Rs[i * kBMax * kBMax + e] = coef[(d.pslots - 1) * kBMax * kBMax + e];
+      Rs[e * d.n_inst + i] = coef[(d.pslots - 1) * kBMax * kBMax + e];
   }
   if (tid == 0) {
     int nbmax = -1;
@@ -1117,37 +1138,37 @@ __global__ void __launch_bounds__(kSThreads, 2)
       ecol[u] = e % ld;
       einst[u] = (erow[u] < pr) ? s_col_inst[ecol[u]] : -1;
     }
+    int stg = 0;      // ring stage of the next panel
+    uint32_t ph = 0;  // parity of that stage's current use
     for (int64_t ci = 0; ci < my_chunks; ++ci) {
       const int64_t r0 = (blockIdx.x + ci * gridDim.x) * (int64_t)pr;
       const int rows = (int)min((int64_t)pr, d.n_orb - r0);
-      int64_t k = ci * npc;
       double2 w[2];
       {
-        const int stg = (int)(k % ns);
-        mbar_wait(&full[stg], (uint32_t)((k / ns) & 1), s_abort);
+        mbar_wait(&full[stg], ph, s_abort);
         const double2* pnl = ring + (size_t)stg * kPanelElems;
 #pragma unroll
         for (int u = 0; u < 2; ++u) w[u] = erow[u] < rows ? pnl[erow[u] * ld + ecol[u]] : make_double2(0.0, 0.0);
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty[stg]);
-        ++k;
+        ring_next(stg, ph, ns);
       }
 #pragma unroll 2
-      for (int s = 0; s < nbmax; ++s, ++k) {
-        const int stg = (int)(k % ns);
-        mbar_wait(&full[stg], (uint32_t)((k / ns) & 1), s_abort);
+      for (int s = 0; s < nbmax; ++s) {
+        mbar_wait(&full[stg], ph, s_abort);
         const double2* pnl = ring + (size_t)stg * kPanelElems;
 #pragma unroll
         for (int u = 0; u < 2; ++u) {
           const int i = einst[u];
           if (i < 0 || erow[u] >= rows || s >= s_nb[i]) continue;
-          const int b = s_b[i], c0 = s_c0[i], q = ecol[u] - c0;
+          const int b = s_b[i], c0 = s_c0[i];
           const double2* prow = pnl + erow[u] * ld + c0;
-          const double2* ci_ = cs + (size_t)i * cs_stride + s * b * b + q;
-          for (int p = 0; p < b; ++p) w[u] = csub(w[u], cmul(prow[p], ci_[p * b]));
+          const double2* ccol = cs + (size_t)s * bmax * ld + ecol[u];
+          for (int p = 0; p < b; ++p) w[u] = csub(w[u], cmul(prow[p], ccol[p * ld]));
         }
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty[stg]);
+        ring_next(stg, ph, ns);
       }
       consumer_sync();  // every warp is done with the previous chunk's rows
 #pragma unroll
@@ -1161,15 +1182,16 @@ __global__ void __launch_bounds__(kSThreads, 2)
         if (i < 0 || erow[u] >= rows) continue;
         const int b = s_b[i], c0 = s_c0[i], q = ecol[u] - c0, nb = s_nb[i];
         const double2* wr = wsh + erow[u] * ld + c0;
-        const double2* Ri = Rs + i * kBMax * kBMax;
+        const double2* Ri = Rs + i;  // R_i[k][p] at Ri[(k*kBMax + p)*n_inst]
+        const int ni = d.n_inst;
         double2 xs[kBMax];
         double2 xq = make_double2(0.0, 0.0);
 #pragma unroll
         for (int pp = 0; pp < kBMax; ++pp) {
           if (pp > q) break;
           double2 v = wr[pp];
-          for (int kq = 0; kq < pp; ++kq) v = csub(v, cmul(xs[kq], Ri[kq * kBMax + pp]));
-          const double rr = Ri[pp * kBMax + pp].x;
+          for (int kq = 0; kq < pp; ++kq) v = csub(v, cmul(xs[kq], Ri[(kq * kBMax + pp) * ni]));
+          const double rr = Ri[(pp * kBMax + pp) * ni].x;
           xs[pp] = make_double2(v.x / rr, v.y / rr);
           xq = xs[pp];
         }
@@ -2502,6 +2524,36 @@ int check_lz(const rsed_model_t* md, const rsed_sectors_t* sc, const rsed_lanczo
   return RSED_OK;
 }
 
+int launch_update(const rsed_lanczos_t& st, const LzDims& d, int pass, cudaStream_t stream) {
+  // all instances per block when their coefficients fit in shared memory
+  const int crows = st.n_slots * st.bmax;
+  const size_t smem = sizeof(double2) * ((size_t)crows * d.ld + (size_t)d.n_inst * kBMax * kBMax + 512) +
+                      sizeof(int) * (size_t)d.ld;
+  // (measured: above ~48 KB the lower occupancy costs more than whole-row reads save)
+  if (d.n_inst >= 2 && d.ld <= 256 && smem <= 48 * 1024) {
+    static bool attr_set = false;
+    if (!attr_set) {
+      RSED_TRY_CUDA(cudaFuncSetAttribute(k_lz_update_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+      attr_set = true;
+    }
+    const int rows_pg = 256 / d.ld;
+    const int64_t groups = (d.n_orb + rows_pg - 1) / rows_pg;
+    int dev = 0, n_sm = 148;
+    RSED_TRY_CUDA(cudaGetDevice(&dev));
+    RSED_TRY_CUDA(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
+    const int64_t pairs = (groups + 1) / 2;  // each block iteration takes two row groups
+    const int64_t grid = pairs < (int64_t)n_sm * 8 ? pairs : (int64_t)n_sm * 8;
+    k_lz_update_rows<<<(unsigned)grid, 256, smem, stream>>>(st, d, pass, crows);
+  } else {
+    // rows per block: 8 warps x (32 / b) rows; sized for the largest block of the batch
+    const int64_t rows_per_block = 8 * (32 / st.bmax);
+    k_lz_update<<<(unsigned)(((d.n_orb + rows_per_block - 1) / rows_per_block) * d.n_inst), 256, 0, stream>>>(
+        st, d, pass);
+  }
+  RSED_CHECK_LAUNCH();
+  return RSED_OK;
+}
+
 // Streaming configuration of a batch: panel rows pr (kPanelElems / ld), ring
 // depth ns (the deepest ring, 4..12 stages, that leaves two blocks per SM),
 // grid.  False when the batch does not fit the streaming kernels.
@@ -2513,17 +2565,17 @@ struct StreamConfig {
 bool stream_config(const rsed_lanczos_t& st, const LzDims& d, StreamConfig* c) {
   if (st.reserved & kFlagNoStream) return false;
   if (d.ld > 64 || d.n_inst > kStreamInstMax || d.n_orb < 1) return false;
-  const int cs_stride = st.n_slots * st.bmax * st.bmax;
+  const int crows = st.n_slots * st.bmax;
   constexpr size_t kBudget = 104 * 1024;  // dynamic shared memory per block (two blocks per SM)
   c->pr = kPanelElems / d.ld;
   c->ns_gram = c->ns_upd = 0;
   for (int ns = 12; ns >= 4 && !c->ns_gram; --ns)
-    if (stream_layout(ns, d.n_inst, cs_stride, false).total <= kBudget) c->ns_gram = ns;
+    if (stream_layout(ns, d.n_inst, crows, d.ld, false).total <= kBudget) c->ns_gram = ns;
   for (int ns = 12; ns >= 4 && !c->ns_upd; --ns)
-    if (stream_layout(ns, d.n_inst, cs_stride, true).total <= kBudget) c->ns_upd = ns;
+    if (stream_layout(ns, d.n_inst, crows, d.ld, true).total <= kBudget) c->ns_upd = ns;
   if (!c->ns_gram || !c->ns_upd) return false;
-  c->smem_gram = stream_layout(c->ns_gram, d.n_inst, cs_stride, false).total;
-  c->smem_upd = stream_layout(c->ns_upd, d.n_inst, cs_stride, true).total;
+  c->smem_gram = stream_layout(c->ns_gram, d.n_inst, crows, d.ld, false).total;
+  c->smem_upd = stream_layout(c->ns_upd, d.n_inst, crows, d.ld, true).total;
   int dev = 0, n_sm = 148;
   if (cudaGetDevice(&dev) != cudaSuccess ||
       cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
@@ -2546,7 +2598,7 @@ int launch_gram_stream(const rsed_lanczos_t& st, const LzDims& d, int pass, cons
     attr_set = true;
   }
   k_lz_gram_stream<BB, CPL><<<(unsigned)c.grid, kSThreads, c.smem_gram, stream>>>(
-      st, d, pass, c.ns_gram, c.pr, st.n_slots * st.bmax * st.bmax);
+      st, d, pass, c.ns_gram, c.pr, st.n_slots * st.bmax);
   RSED_CHECK_LAUNCH();
   return RSED_OK;
 }
@@ -2571,13 +2623,14 @@ int launch_pass_stream(const rsed_lanczos_t& st, const LzDims& d, int pass, cons
   if (rc != RSED_OK) return rc;
   k_lz_finalize<<<(unsigned)d.n_inst, kRT, 0, stream>>>(st, ds, pass);
   RSED_CHECK_LAUNCH();
+  if (st.reserved & kFlagNoStreamUpdate) return launch_update(st, d, pass, stream);
   static bool attr_set = false;
   if (!attr_set) {
     RSED_TRY_CUDA(cudaFuncSetAttribute(k_lz_update_stream, cudaFuncAttributeMaxDynamicSharedMemorySize, 110 * 1024));
     attr_set = true;
   }
   k_lz_update_stream<<<(unsigned)c.grid, kSThreads, c.smem_upd, stream>>>(st, ds, pass, c.ns_upd, c.pr,
-                                                                            st.n_slots * st.bmax * st.bmax);
+                                                                            st.n_slots * st.bmax);
   RSED_CHECK_LAUNCH();
   return RSED_OK;
 }
@@ -2587,33 +2640,7 @@ int launch_pass(const rsed_lanczos_t& st, const LzDims& d, int pass, cudaStream_
   if (stream_config(st, d, &sc)) return launch_pass_stream(st, d, pass, sc, stream);
   k_lz_reduce<<<(unsigned)(d.n_chunks * d.n_inst), kRT, 0, stream>>>(st, d, pass);
   RSED_CHECK_LAUNCH();
-  // all instances per block when their coefficients fit in shared memory
-  const int cs_stride = st.n_slots * st.bmax * st.bmax;
-  const size_t smem = sizeof(double2) * ((size_t)d.n_inst * (cs_stride + kBMax * kBMax) + 512) +
-                      sizeof(int) * (size_t)d.ld;
-  // (measured: above ~48 KB the lower occupancy costs more than whole-row reads save)
-  if (d.n_inst >= 2 && d.ld <= 256 && smem <= 48 * 1024) {
-    static bool attr_set = false;
-    if (!attr_set) {
-      RSED_TRY_CUDA(cudaFuncSetAttribute(k_lz_update_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
-      attr_set = true;
-    }
-    const int rows_pg = 256 / d.ld;
-    const int64_t groups = (d.n_orb + rows_pg - 1) / rows_pg;
-    int dev = 0, n_sm = 148;
-    RSED_TRY_CUDA(cudaGetDevice(&dev));
-    RSED_TRY_CUDA(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
-    const int64_t pairs = (groups + 1) / 2;  // each block iteration takes two row groups
-    const int64_t grid = pairs < (int64_t)n_sm * 8 ? pairs : (int64_t)n_sm * 8;
-    k_lz_update_rows<<<(unsigned)grid, 256, smem, stream>>>(st, d, pass, cs_stride);
-  } else {
-    // rows per block: 8 warps x (32 / b) rows; sized for the largest block of the batch
-    const int64_t rows_per_block = 8 * (32 / st.bmax);
-    k_lz_update<<<(unsigned)(((d.n_orb + rows_per_block - 1) / rows_per_block) * d.n_inst), 256, 0, stream>>>(
-        st, d, pass);
-  }
-  RSED_CHECK_LAUNCH();
-  return RSED_OK;
+  return launch_update(st, d, pass, stream);
 }
 
 __global__ void k_lz_init_state(rsed_lanczos_t st) {

@@ -124,27 +124,23 @@ struct ProjTypes<32> {
   using Real = float;
 };
 
-// CPL columns of one x row, loaded as 16-B vectors (two FP32 or one FP64
-// complex value each).  The L lanes of an entry slot interleave their
-// vectors: vector k of slot lane li holds columns (k * L + li) * kPer + h, so
-// each load instruction of the slot reads one contiguous 16 * L-byte piece of
-// the row (whole 32-B sectors) instead of L pieces strided by the lane's
-// segment.  Vectors whose bit in ok is clear (at or beyond the row's leading
-// dimension) read as zero, so a lane never leaves its row.
+// CPL contiguous columns of one x row, loaded as 16-B vectors (two FP32 or one
+// FP64 complex value each); vectors at or beyond the row's leading dimension
+// read as zero, so a lane's segment never leaves its row.
 template <int PREC, int CPL>
 struct XVec {
   using W = typename ProjTypes<PREC>::W;
   static constexpr int kPer = (PREC == 64) ? 1 : 2;  // columns per 16-B vector
   static constexpr int kVec = CPL / kPer;
   W v[CPL];
-  __device__ __forceinline__ void load(const char* base, int stride, unsigned ok) {
+  __device__ __forceinline__ void load(const char* base, int avail) {
 #pragma unroll
     for (int k = 0; k < kVec; ++k) {
-      if ((ok >> k) & 1u) {
+      if (k * kPer < avail) {
         if constexpr (PREC == 64) {
-          v[k] = __ldg(reinterpret_cast<const double2*>(base + (size_t)k * stride));
+          v[k] = __ldg(reinterpret_cast<const double2*>(base) + k);
         } else {
-          const float4 q = __ldg(reinterpret_cast<const float4*>(base + (size_t)k * stride));
+          const float4 q = __ldg(reinterpret_cast<const float4*>(base) + k);
           v[2 * k] = make_float2(q.x, q.y);
           v[2 * k + 1] = make_float2(q.z, q.w);
         }
@@ -190,28 +186,22 @@ __global__ void __launch_bounds__(256) k_proj_spmv(rsed_model_t md, rsed_sectors
                                                                     : (const void*)md.proj_w32);
   const uint32_t* __restrict__ cgt = md.proj_cg;
   const int64_t* __restrict__ rp = md.proj_rowptr;
-  using XV = XVec<PREC, CPL>;
   const int lane = threadIdx.x & 31;
   const int eslot = lane / L;
-  const int li = lane % L;
-  const int cbase = (chunk0 + (int)blockIdx.y) * NC;  // first column of this chunk
+  const int c0 = (chunk0 + (int)blockIdx.y) * NC + (lane % L) * CPL;
   const int64_t ld = sc.ld;
-  int col[CPL], sec[CPL];
+  const int avail = (int)ld - c0;
+  int sec[CPL];
   bool colv[CPL], fresh[CPL];
-  unsigned vok = 0;
-#pragma unroll
-  for (int k = 0; k < XV::kVec; ++k)
-    if (cbase + (k * L + li) * XV::kPer < ld) vok |= 1u << k;
 #pragma unroll
   for (int j = 0; j < CPL; ++j) {
-    col[j] = cbase + ((j / XV::kPer) * L + li) * XV::kPer + j % XV::kPer;
-    colv[j] = col[j] < sc.n_cols;
-    sec[j] = colv[j] ? sc.col_sector[col[j]] : -1;
-    // the block vectors of one sector sit in adjacent columns, so the two
-    // columns of a vector usually share the hop weight
+    colv[j] = c0 + j < sc.n_cols;
+    sec[j] = colv[j] ? sc.col_sector[c0 + j] : -1;
+    // the block vectors of one sector sit in adjacent columns, so a lane's
+    // columns usually share the hop weight
     fresh[j] = (j == 0) || sec[j] != sec[j - 1];
   }
-  const char* xb = reinterpret_cast<const char*>(xin) + (size_t)(cbase + li * XV::kPer) * sizeof(W);
+  const char* xb = reinterpret_cast<const char*>(xin) + (size_t)c0 * sizeof(W);
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
   for (int64_t r = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < md.n_orbits; r += warps) {
     const uint64_t memr = sc.member[r];
@@ -230,7 +220,7 @@ __global__ void __launch_bounds__(256) k_proj_spmv(rsed_model_t md, rsed_sectors
       for (int64_t base = e0; base < e1; base += EPW * U) {
         uint32_t cgv[U];
         W wv[U];
-        XV xv[U];
+        XVec<PREC, CPL> xv[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
           const int64_t idx = base + u * EPW + eslot;
@@ -245,7 +235,7 @@ __global__ void __launch_bounds__(256) k_proj_spmv(rsed_model_t md, rsed_sectors
 #pragma unroll
         for (int u = 0; u < U; ++u) {
           if (cgv[u] != 0xffffffffu && any)
-            xv[u].load(xb + (size_t)(cgv[u] & kOrbitMask) * ld * sizeof(W), L * 16, vok);
+            xv[u].load(xb + (size_t)(cgv[u] & kOrbitMask) * ld * sizeof(W), avail);
           else
             xv[u].zero();
         }
@@ -284,12 +274,12 @@ __global__ void __launch_bounds__(256) k_proj_spmv(rsed_model_t md, rsed_sectors
         if (!colv[j]) continue;
         double2 o = make_double2(0.0, 0.0);
         if (on[j]) {
-          const W xr = reinterpret_cast<const W*>(xin)[r * ld + col[j]];
+          const W xr = reinterpret_cast<const W*>(xin)[r * ld + c0 + j];
           const double xx = (double)xr.x, xy = (double)xr.y;
           o.x = (double)acc[j].x + (hd.x * xx + hd.y * xy);
           o.y = (double)acc[j].y + (hd.x * xy - hd.y * xx);
         }
-        y[r * ld + col[j]] = o;
+        y[r * ld + c0 + j] = o;
       }
     }
   }

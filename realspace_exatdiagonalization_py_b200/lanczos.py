@@ -59,6 +59,9 @@ class LanczosParams:
     apply_variant: int = 0
     single_pass: bool = True  # skip the second Gram-Schmidt pass when pass 1 lost little norm
     stream: bool = True  # Gram-Schmidt kernels stream whole-row panels by bulk copies (batches with ld <= 64)
+    # the update streams too; off by default: on the 32-site workload the
+    # row-group update takes 615 us per launch, the streamed one 727 us
+    stream_update: bool = False
 
 
 def start_block(n: int, b: int, seed: int = 12345) -> np.ndarray:
@@ -144,7 +147,7 @@ class LanczosBatch:
         self.state = torch.zeros((n_inst, STATE_INTS), dtype=torch.int32, device=dev)
         self.c = _lib.RsedLanczos(
             n_inst, S, nev, self.keep, p.max_restarts, p.precision, bmax, self.chunk_rows, self.pm,
-            (1 if p.single_pass else 0) | (0 if p.stream else 2),
+            (1 if p.single_pass else 0) | (0 if p.stream else 2) | (0 if p.stream_update else 4),
             float(p.tol if p.precision == 64 else max(p.tol, p.tol32)), _lib.ptr(self.inst_col0), _lib.ptr(self.inst_b), _lib.ptr(self.V),
             _lib.ptr(self.W), _lib.ptr(self.Xf), _lib.ptr(self.P), _lib.ptr(self.coef),
             _lib.ptr(self.partial), plen, _lib.ptr(self.ritz_val), _lib.ptr(self.ritz_vec),

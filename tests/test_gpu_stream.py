@@ -20,7 +20,7 @@ from _cases import ed_data_for
 pytestmark = pytest.mark.gpu
 
 
-def _solve(data, sectors, nev, block_sizes, *, stream, precision=64, single=True, n_slots=16):
+def _solve(data, sectors, nev, block_sizes, *, stream, precision=64, single=True, n_slots=16, stream_update=True):
     import realspace_exatdiagonalization_py_b200 as ed
 
     dm, sset = data._device()
@@ -29,7 +29,7 @@ def _solve(data, sectors, nev, block_sizes, *, stream, precision=64, single=True
 
         dm.build_projection(sset.sqrt_stab, precisions=projection_precisions(dm, 32))
     p = ed.LanczosParams(block=max(block_sizes), n_slots=n_slots, precision=precision, single_pass=single,
-                         stream=stream)
+                         stream=stream, stream_update=stream_update)
     sol = ed.BatchedSectorSolver(dm, sset, sectors, nev, precision=precision, params=p,
                                  config=ed.SolverConfig(tuple(block_sizes), 0, True, n_slots))
     vals, _ = sol.solve(None, vectors=False)
@@ -76,6 +76,23 @@ def test_streamed_gram_schmidt_matches_reference_and_per_instance_kernels(golden
     assert np.abs(st_str[:, 3] - st_per[:, 3]).max() <= 16
     if not single:
         assert st_str[:, 11].sum() == 0
+
+
+@pytest.mark.parametrize("single", [True, False])
+def test_streamed_reduction_with_row_group_update(golden, single):
+    """The streamed reduction followed by the row-group update
+    (``stream_update=False``) gives the same eigenvalues."""
+    g = golden("heisenberg16")
+    data = ed_data_for("heisenberg16", g)
+    nev = int(g["nev"])
+    sectors = [int(s) for s in g["eig_sectors"]]
+    v1, st1 = _solve(data, sectors, nev, [2] * len(sectors), stream=True, single=single, stream_update=False)
+    v2, _ = _solve(data, sectors, nev, [2] * len(sectors), stream=False, single=single)
+    np.testing.assert_allclose(v1, v2, atol=1e-10, rtol=0)
+    for i, ref in enumerate(g["eig_vals"]):
+        k = min(nev, len(ref))
+        np.testing.assert_allclose(v1[i, :k], ref[:k], atol=1e-10, rtol=0)
+    assert (st1[:, 1] == 1).all()
 
 
 def test_batch_wider_than_the_stream_limit(golden):
