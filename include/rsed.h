@@ -395,6 +395,15 @@ int rsed_lanczos_iterate_span(const rsed_model_t* model, const rsed_sectors_t* s
  * written to resid[inst*pm + j].  Needs n_slots >= 2*keep_blocks + 1. */
 int rsed_lanczos_rayleigh_ritz(const rsed_model_t* model, const rsed_sectors_t* sec,
                                rsed_lanczos_t* st, int32_t apply_variant, void* stream);
+/* The thick restart alone, as rsed_lanczos_iterate runs it after a Ritz
+ * check: every instance with state[S_RESTART_NB] = nb_old > 0 gets
+ * V_j = sum_{l < (nb_old-1)*b} V_l S[l][j] for j < keep_blocks*b (S =
+ * ritz_vec, columns of block j/b, column j%b) and its residual block (slot
+ * nb_old-1) moved to slot keep_blocks.  Instances with nb_old = 0 are left
+ * alone.  No reference counterpart (the reference's ARPACK restarts inside
+ * scipy); exposed so the restart can be checked on its own. */
+int rsed_lanczos_restart(const rsed_model_t* model, const rsed_sectors_t* sec, rsed_lanczos_t* st,
+                         void* stream);
 /* The whole thick-restart loop for every active instance in ONE launch: one
  * thread-block cluster of cluster_size (1..8) CTAs per instance, each CTA
  * owning a slice of the orbit rows; Gram reductions go through distributed

@@ -228,6 +228,10 @@ SIGNATURES = {
         c_int,
         [POINTER(RsedModel), POINTER(RsedSectors), POINTER(RsedLanczos), c_int32, c_void_p],
     ),
+    "rsed_lanczos_restart": (
+        c_int,
+        [POINTER(RsedModel), POINTER(RsedSectors), POINTER(RsedLanczos), c_void_p],
+    ),
     "rsed_lanczos_persistent": (
         c_int,
         [POINTER(RsedModel), POINTER(RsedSectors), POINTER(RsedLanczos), c_int32, c_int32, c_void_p],

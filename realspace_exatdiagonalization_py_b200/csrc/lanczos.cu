@@ -634,6 +634,7 @@ constexpr int kListMax = 2 * kJacobiMax + 8;  // panels of one chunk at most
 constexpr unsigned long long kWaitNs = 2000000000ull;
 constexpr int kFlagNoStream = 2;              // st.reserved bit 1: use the per-instance kernels
 constexpr int kFlagNoStreamUpdate = 4;        // st.reserved bit 2: streamed reduction, row-group update
+constexpr int kFlagNoRowRestart = 8;          // st.reserved bit 3: per-instance restart kernel
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -1802,6 +1803,100 @@ __global__ void __launch_bounds__(256) k_lz_restart(rsed_lanczos_t st, LzDims d)
     if (q < b) V[(int64_t)st.keep_blocks * slot_stride + row * d.ld + c0 + q] = resid[q];
 }
 
+// The same restart for all instances at once: thread = (row, column c0 + q)
+// of two row groups per grid-stride iteration, so every basis slot is read
+// as whole contiguous rows.  The Ritz coefficients of all restarting
+// instances sit in shared memory column-major,
+//   St[((l*bmax + p)*keep + jb)*ld + c0 + q] = S_i[l*b + p][jb*b + q],
+// so the lanes of a warp read consecutive words.  Every thread of the block
+// finishes reading its two rows (block barrier) before the rows are
+// overwritten in place.  KM bounds keep_blocks (register accumulators).
+template <int KM>
+__global__ void __launch_bounds__(256, 2) k_lz_restart_rows(rsed_lanczos_t st, LzDims d) {
+  extern __shared__ __align__(16) unsigned char smem_r[];
+  const int keep = st.keep_blocks, bmax = st.bmax, ld = d.ld;
+  double2* St = reinterpret_cast<double2*>(smem_r);
+  int* meta = reinterpret_cast<int*>(St + (size_t)d.n_slots * bmax * keep * ld);  // [ld]
+  for (int c = threadIdx.x; c < ld; c += blockDim.x) meta[c] = -1;
+  __syncthreads();
+  for (int inst = threadIdx.x; inst < d.n_inst; inst += blockDim.x) {
+    const int nb_old = st.state[inst * kStateInts + S_RESTART_NB];
+    const int b = st.inst_b[inst], c0 = st.inst_col0[inst];
+    // a restart comes when the basis holds n_slots + 1 blocks (the last in the spare slot)
+    if (nb_old < 1 || nb_old > d.n_slots + 1 || (nb_old - 1) * b > kJacobiMax || keep * b > kKeepMax) continue;
+    for (int q = 0; q < b; ++q) meta[c0 + q] = inst;
+  }
+  __syncthreads();
+  for (int inst = 0; inst < d.n_inst; ++inst) {
+    const int b = st.inst_b[inst], c0 = st.inst_col0[inst];
+    if (meta[c0] != inst) continue;
+    const int nb_old = st.state[inst * kStateInts + S_RESTART_NB];
+    const int Mold = (nb_old - 1) * b, K = keep * b;
+    const double2* S = reinterpret_cast<const double2*>(st.ritz_vec) + (int64_t)inst * d.pm * d.pm;
+    for (int e = threadIdx.x; e < Mold * K; e += blockDim.x) {
+      const int l = e / K, j = e % K;
+      St[((size_t)((l / b) * bmax + l % b) * keep + j / b) * ld + c0 + j % b] = S[(int64_t)l * d.pm + j];
+    }
+  }
+  __syncthreads();
+  const int rows_pg = blockDim.x / ld;
+  const int rloc = threadIdx.x / ld, col = threadIdx.x % ld;
+  const int inst = rloc < rows_pg ? meta[col] : -1;
+  int b = 1, c0 = 0, nslot = 0;
+  if (inst >= 0) {
+    b = st.inst_b[inst];
+    c0 = st.inst_col0[inst];
+    nslot = st.state[inst * kStateInts + S_RESTART_NB] - 1;  // basis blocks combined
+  }
+  double2* V = reinterpret_cast<double2*>(st.V);
+  const int64_t slot_stride = d.n_orb * d.ld;
+  const int64_t n_groups = (d.n_orb + rows_pg - 1) / rows_pg;
+  const double2* scol = St + col;
+  for (int64_t grp = 2 * (int64_t)blockIdx.x; grp < n_groups; grp += 2 * (int64_t)gridDim.x) {
+    const int64_t row0 = grp * rows_pg + rloc, row1 = row0 + rows_pg;
+    const bool live0 = inst >= 0 && row0 < d.n_orb;
+    const bool live1 = inst >= 0 && row1 < d.n_orb;
+    double2 a0[KM], a1[KM];
+#pragma unroll
+    for (int j = 0; j < KM; ++j) a0[j] = a1[j] = make_double2(0.0, 0.0);
+    double2 r0 = make_double2(0.0, 0.0), r1 = make_double2(0.0, 0.0);
+    if (live0) {
+#pragma unroll 2
+      for (int l = 0; l < nslot; ++l) {
+        const double2* Vs = V + (int64_t)l * slot_stride + row0 * ld + c0;
+        for (int p = 0; p < b; ++p) {
+          const double2 v0 = Vs[p];
+          const double2 v1 = live1 ? Vs[(int64_t)rows_pg * ld + p] : make_double2(0.0, 0.0);
+          const double2* sp = scol + (size_t)((l * bmax + p) * keep) * ld;
+#pragma unroll
+          for (int j = 0; j < KM; ++j) {
+            if (j < keep) {
+              const double2 c = sp[(size_t)j * ld];
+              a0[j] = cadd(a0[j], cmul(v0, c));
+              a1[j] = cadd(a1[j], cmul(v1, c));
+            }
+          }
+        }
+      }
+      r0 = V[(int64_t)nslot * slot_stride + row0 * ld + col];
+      if (live1) r1 = V[(int64_t)nslot * slot_stride + row1 * ld + col];
+    }
+    __syncthreads();  // the rows of this pair are read by every thread before any is overwritten
+    if (live0) {
+#pragma unroll
+      for (int j = 0; j < KM; ++j)
+        if (j < keep) V[(int64_t)j * slot_stride + row0 * ld + col] = a0[j];
+      V[(int64_t)keep * slot_stride + row0 * ld + col] = r0;
+      if (live1) {
+#pragma unroll
+        for (int j = 0; j < KM; ++j)
+          if (j < keep) V[(int64_t)j * slot_stride + row1 * ld + col] = a1[j];
+        V[(int64_t)keep * slot_stride + row1 * ld + col] = r1;
+      }
+    }
+  }
+}
+
 // U[inst][j][row] = sum_l V_l[row] S[l][j], j < nev (Ritz vectors of the last check).
 __global__ void __launch_bounds__(256) k_lz_extract(rsed_lanczos_t st, LzDims d, double2* U, int64_t u_stride) {
   const int inst = blockIdx.x % d.n_inst;
@@ -2524,6 +2619,39 @@ int check_lz(const rsed_model_t* md, const rsed_sectors_t* sc, const rsed_lanczo
   return RSED_OK;
 }
 
+// Thick restart of every instance whose Ritz step asked for one: the
+// whole-row form when its coefficients fit shared memory (two blocks per SM
+// up to 115 KB, one up to 220 KB), else the per-instance form.
+int launch_restart(const rsed_lanczos_t& st, const LzDims& d, cudaStream_t stream) {
+  const size_t smem = sizeof(double2) * (size_t)st.n_slots * st.bmax * st.keep_blocks * d.ld +
+                      sizeof(int) * (size_t)d.ld;
+  if (!(st.reserved & kFlagNoRowRestart) && d.ld <= 256 && smem <= 220 * 1024 && st.keep_blocks <= 16) {
+    static bool attr_set = false;
+    if (!attr_set) {
+      RSED_TRY_CUDA(cudaFuncSetAttribute(k_lz_restart_rows<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         220 * 1024));
+      RSED_TRY_CUDA(cudaFuncSetAttribute(k_lz_restart_rows<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         220 * 1024));
+      attr_set = true;
+    }
+    int dev = 0, n_sm = 148;
+    RSED_TRY_CUDA(cudaGetDevice(&dev));
+    RSED_TRY_CUDA(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
+    const int rows_pg = 256 / d.ld;
+    const int64_t pairs = ((d.n_orb + rows_pg - 1) / rows_pg + 1) / 2;
+    const int64_t per_sm = smem <= 115 * 1024 ? 2 : 1;  // 228 KB per SM, 1 KB reserved per block
+    const int64_t grid = pairs < n_sm * per_sm ? pairs : n_sm * per_sm;
+    if (st.keep_blocks <= 8)
+      k_lz_restart_rows<8><<<(unsigned)grid, 256, smem, stream>>>(st, d);
+    else
+      k_lz_restart_rows<16><<<(unsigned)grid, 256, smem, stream>>>(st, d);
+  } else {
+    k_lz_restart<<<(unsigned)(((d.n_orb + 255) / 256) * d.n_inst), 256, 0, stream>>>(st, d);
+  }
+  RSED_CHECK_LAUNCH();
+  return RSED_OK;
+}
+
 int launch_update(const rsed_lanczos_t& st, const LzDims& d, int pass, cudaStream_t stream) {
   // all instances per block when their coefficients fit in shared memory
   const int crows = st.n_slots * st.bmax;
@@ -2762,8 +2890,8 @@ static int lz_iterate(const rsed_model_t* md, const rsed_sectors_t* sc, rsed_lan
     if (ritz_mode == 0 || (ritz_mode == 1 && it == n_iter - 1)) {
       k_lz_ritz<<<d.n_inst, kRitzThreads, kRitzSmem, stream>>>(*st, d, check_every, 0, 0);
       RSED_CHECK_LAUNCH();
-      k_lz_restart<<<(unsigned)(((d.n_orb + 255) / 256) * d.n_inst), 256, 0, stream>>>(*st, d);
-      RSED_CHECK_LAUNCH();
+      rc = launch_restart(*st, d, stream);
+      if (rc) return rc;
     }
   }
   return RSED_OK;
@@ -2793,8 +2921,8 @@ extern "C" int rsed_lanczos_rayleigh_ritz(const rsed_model_t* md, const rsed_sec
   const LzDims d = make_dims(md, sc, st);
   k_rr_prepare<<<(st->n_inst + 63) / 64, 64, 0, stream>>>(*st);
   RSED_CHECK_LAUNCH();
-  k_lz_restart<<<(unsigned)(((d.n_orb + 255) / 256) * d.n_inst), 256, 0, stream>>>(*st, d);
-  RSED_CHECK_LAUNCH();
+  rc = launch_restart(*st, d, stream);
+  if (rc) return rc;
   const int64_t slot = d.n_orb * d.ld;
   double2* V = reinterpret_cast<double2*>(st->V);
   for (int l = 0; l <= st->keep_blocks; ++l) {
@@ -2848,6 +2976,13 @@ extern "C" int rsed_lanczos_persistent(const rsed_model_t* md, const rsed_sector
   }
   rsed_count_launch();
   return RSED_OK;
+}
+
+extern "C" int rsed_lanczos_restart(const rsed_model_t* md, const rsed_sectors_t* sc, rsed_lanczos_t* st,
+                                    void* stream_) {
+  int rc = check_lz(md, sc, st);
+  if (rc) return rc;
+  return launch_restart(*st, make_dims(md, sc, st), as_stream(stream_));
 }
 
 extern "C" int rsed_lanczos_extract(const rsed_model_t* md, const rsed_sectors_t* sc, rsed_lanczos_t* st,

@@ -22,7 +22,7 @@ from . import _lib
 from .hamiltonian import DeviceModel
 from .sector import SectorSet
 
-S_NB, S_STATUS, S_RESTARTS, S_ITERS, S_ACTIVE = 0, 1, 2, 3, 4
+S_NB, S_STATUS, S_RESTARTS, S_ITERS, S_ACTIVE, S_RESTART_NB = 0, 1, 2, 3, 4, 5
 S_NCONV, S_RR, S_ONEPASS_N, S_RED_BLOCKS, S_PASSES = 7, 9, 11, 12, 13
 STATE_INTS = 16
 
@@ -62,6 +62,7 @@ class LanczosParams:
     # the update streams too; off by default: on the 32-site workload the
     # row-group update takes 615 us per launch, the streamed one 727 us
     stream_update: bool = False
+    row_restart: bool = True  # thick restart over whole rows (all instances per block)
 
 
 def start_block(n: int, b: int, seed: int = 12345) -> np.ndarray:
@@ -147,7 +148,8 @@ class LanczosBatch:
         self.state = torch.zeros((n_inst, STATE_INTS), dtype=torch.int32, device=dev)
         self.c = _lib.RsedLanczos(
             n_inst, S, nev, self.keep, p.max_restarts, p.precision, bmax, self.chunk_rows, self.pm,
-            (1 if p.single_pass else 0) | (0 if p.stream else 2) | (0 if p.stream_update else 4),
+            (1 if p.single_pass else 0) | (0 if p.stream else 2) | (0 if p.stream_update else 4)
+            | (0 if p.row_restart else 8),
             float(p.tol if p.precision == 64 else max(p.tol, p.tol32)), _lib.ptr(self.inst_col0), _lib.ptr(self.inst_b), _lib.ptr(self.V),
             _lib.ptr(self.W), _lib.ptr(self.Xf), _lib.ptr(self.P), _lib.ptr(self.coef),
             _lib.ptr(self.partial), plen, _lib.ptr(self.ritz_val), _lib.ptr(self.ritz_vec),
@@ -237,6 +239,14 @@ class LanczosBatch:
         _lib.check(_lib.lib().rsed_lanczos_rayleigh_ritz(
             ctypes.byref(self.model.c), ctypes.byref(self.sc), ctypes.byref(self.c),
             self.p.apply_variant, _lib.stream_ptr(stream)))
+
+    def restart(self, stream=None) -> None:
+        """The thick restart alone for every instance whose ``state[:, 5]``
+        (S_RESTART_NB) is nonzero: ``V_j = sum_l V_l S[l, j]`` over the old
+        basis with ``S = ritz_vec``, the residual block moved behind the
+        ``keep`` new blocks."""
+        _lib.check(_lib.lib().rsed_lanczos_restart(ctypes.byref(self.model.c), ctypes.byref(self.sc),
+                                                   ctypes.byref(self.c), _lib.stream_ptr(stream)))
 
     def done(self) -> bool:
         return not bool(self.state[:, S_ACTIVE].any().item())
