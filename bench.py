@@ -1254,6 +1254,8 @@ def main():
     ap.add_argument("--matvec-launches", type=int, default=20)
     ap.add_argument("--solve-scale", type=int, default=0,
                     help="only a batched solve of this many 32-site Haldane sectors (for kernel profiling)")
+    ap.add_argument("--scale-slots", type=int, default=16,
+                    help="basis slots of the --solve-scale solve (fewer slots, smaller footprint)")
     ap.add_argument("--matvec-precision", type=int, default=0, choices=[0, 32, 64])
     ap.add_argument("--matvec-no-otf", action="store_true")
     ap.add_argument("--serving-only", action="store_true", help="only the 32-site served request stream")
@@ -1275,7 +1277,7 @@ def main():
         G = ed.build_translation_group(model.lattice)
         data = ed.build_ed_data(model, filling_fraction=Fraction(nf, model.lattice.n_site), symmetry_group=G)
         secs = list(range(args.solve_scale))
-        cfg = ed.SolverConfig((2,) * len(secs), 0, True, 16)
+        cfg = ed.SolverConfig((2,) * len(secs), 0, True, args.scale_slots)
         prm = ed.LanczosParams(block=2, precision=32, single_pass=not args.two_pass, stream=not args.no_stream,
                                stream_update=args.stream_update)
         res = ed.solve_sectors_batched(data, secs, nev=4, precision=32, params=prm, config=cfg,

@@ -161,8 +161,79 @@ __device__ __forceinline__ T ld_stream(const T* p) {
   return __ldcs(p);
 }
 
+// The hops of one row for an FP32 lane of 4 columns that form two sector
+// pairs (columns 0-1 in sector s0, 2-3 in s2) when the row belongs to every
+// sector of the warp: no per-column tests, one weight-character product per
+// pair, and the table entries of the next batch loaded while the current
+// batch gathers.  Missing entries past the row's end become (orbit 0,
+// weight 0), so the loop body has no branches (x is finite: the solver's
+// own Lanczos blocks).
+template <int L, int U>
+__device__ __forceinline__ void spmv_row_pairs32(const uint32_t* __restrict__ cgt, const float2* __restrict__ wt,
+                                                 int64_t e0, int64_t e1, int eslot, const char* __restrict__ xl,
+                                                 uint32_t rowb, const float2* ch0, const float2* ch2, int nsec,
+                                                 float2 acc[4]) {
+  constexpr int EPW = 32 / L;
+  constexpr int B = EPW * U;  // hops per batch and warp
+  float2 a0 = make_float2(0.f, 0.f), a1 = a0, a2 = a0, a3 = a0;
+  uint32_t cgn[U];
+  float2 wn[U];
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    const int64_t idx = e0 + u * EPW + eslot;
+    const bool ok = idx < e1;
+    cgn[u] = ok ? ld_stream(cgt + idx) : 0u;
+    wn[u] = ok ? ld_stream(wt + idx) : make_float2(0.f, 0.f);
+  }
+  for (int64_t base = e0; base < e1; base += B) {
+    uint32_t cgc[U];
+    float2 wc[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      cgc[u] = cgn[u];
+      wc[u] = wn[u];
+    }
+    if (base + B < e1) {
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int64_t idx = base + B + u * EPW + eslot;
+        const bool ok = idx < e1;
+        cgn[u] = ok ? ld_stream(cgt + idx) : 0u;
+        wn[u] = ok ? ld_stream(wt + idx) : make_float2(0.f, 0.f);
+      }
+    }
+    float4 xa[U], xc[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const char* px = xl + (size_t)(cgc[u] & kOrbitMask) * rowb;
+      xa[u] = __ldg(reinterpret_cast<const float4*>(px));
+      xc[u] = __ldg(reinterpret_cast<const float4*>(px + 16));
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int go = (int)(cgc[u] >> kOrbitBits) * nsec;
+      const float2 c0 = ch0[go], c2 = ch2[go];
+      const float2 w = wc[u];
+      const float p0x = w.x * c0.x - w.y * c0.y, p0y = w.x * c0.y + w.y * c0.x;
+      const float p2x = w.x * c2.x - w.y * c2.y, p2y = w.x * c2.y + w.y * c2.x;
+      a0.x += p0x * xa[u].x - p0y * xa[u].y;
+      a0.y += p0x * xa[u].y + p0y * xa[u].x;
+      a1.x += p0x * xa[u].z - p0y * xa[u].w;
+      a1.y += p0x * xa[u].w + p0y * xa[u].z;
+      a2.x += p2x * xc[u].x - p2y * xc[u].y;
+      a2.y += p2x * xc[u].y + p2y * xc[u].x;
+      a3.x += p2x * xc[u].z - p2y * xc[u].w;
+      a3.y += p2x * xc[u].w + p2y * xc[u].z;
+    }
+  }
+  acc[0] = a0;
+  acc[1] = a1;
+  acc[2] = a2;
+  acc[3] = a3;
+}
+
 template <int PREC, int L, int CPL, int U>
-__global__ void __launch_bounds__(256) k_proj_spmv(rsed_model_t md, rsed_sectors_t sc, const void* __restrict__ xin,
+__global__ void __launch_bounds__(256, 3) k_proj_spmv(rsed_model_t md, rsed_sectors_t sc, const void* __restrict__ xin,
                                                    double2* __restrict__ y, int chunk0) {
   using W = typename ProjTypes<PREC>::W;
   using Real = typename ProjTypes<PREC>::Real;
@@ -202,6 +273,20 @@ __global__ void __launch_bounds__(256) k_proj_spmv(rsed_model_t md, rsed_sectors
     fresh[j] = (j == 0) || sec[j] != sec[j - 1];
   }
   const char* xb = reinterpret_cast<const char*>(xin) + (size_t)c0 * sizeof(W);
+  // FP32 lanes of 4 columns in two sector pairs (blocks of 2 or 4 columns):
+  // the branch-free row loop whenever the row is in all of the warp's sectors.
+  // Lanes past the last column run it too, on column 0 of x (in bounds), and
+  // their sums are dropped.
+  bool pairs = false;
+  const char* xfast = xb;
+  int s0 = 0, s2 = 0;
+  if constexpr (PREC == 32 && CPL == 4) {
+    const bool lane_ok = colv[3] ? (sec[1] == sec[0] && sec[3] == sec[2]) : !colv[0];
+    pairs = __all_sync(0xffffffffu, lane_ok);
+    if (!colv[0]) xfast = reinterpret_cast<const char*>(xin);
+    s0 = colv[0] ? sec[0] : 0;
+    s2 = colv[0] ? sec[2] : 0;
+  }
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
   for (int64_t r = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < md.n_orbits; r += warps) {
     const uint64_t memr = sc.member[r];
@@ -215,7 +300,17 @@ __global__ void __launch_bounds__(256) k_proj_spmv(rsed_model_t md, rsed_sectors
     W acc[CPL];
 #pragma unroll
     for (int j = 0; j < CPL; ++j) acc[j].x = acc[j].y = (Real)0;
-    if (__any_sync(0xffffffffu, any)) {
+    bool done = false;
+    if constexpr (PREC == 32 && CPL == 4) {
+      if (pairs && __all_sync(0xffffffffu, !colv[0] || (on[0] && on[1] && on[2] && on[3]))) {
+        const float2* chb = reinterpret_cast<const float2*>(chi);
+        spmv_row_pairs32<L, U>(cgt, reinterpret_cast<const float2*>(wt), rp[r], rp[r + 1], eslot, xfast,
+                               (uint32_t)(ld * sizeof(float2)), chb + s0, chb + s2, nsec,
+                               reinterpret_cast<float2*>(acc));
+        done = true;
+      }
+    }
+    if (!done && __any_sync(0xffffffffu, any)) {
       const int64_t e0 = rp[r], e1 = rp[r + 1];
       for (int64_t base = e0; base < e1; base += EPW * U) {
         uint32_t cgv[U];
