@@ -493,26 +493,27 @@ __global__ void __launch_bounds__(256) k_lz_update(rsed_lanczos_t st, LzDims d, 
 
 // The same update for all instances at once (batches of 2+ instances whose
 // coefficients fit in shared memory): a block holds every instance's
-// coefficients and walks pairs of row groups (thread = one column of one row
-// in each group), so each slot is read as contiguous rows and every thread
-// keeps the loads of two rows in flight.  x R = w is solved per thread by
+// coefficients and walks RG row groups at a time (thread = one column of one
+// row in each group), so each slot is read as contiguous rows and every thread
+// keeps the loads of RG rows in flight.  BB bounds the block size.  x R = w is solved per thread by
 // forward substitution over its instance's columns, from the rows' w values
 // exchanged through shared memory.  Grid-stride over pairs of row groups.
 // The copy of a new block into the current-block slot is written only when
 // the matvec reads it (FP64 matvec); an FP32-matvec batch reads Xf.
+template <int RG, int BB>
 __global__ void __launch_bounds__(256, 3) k_lz_update_rows(rsed_lanczos_t st, LzDims d, int pass, int crows) {
   extern __shared__ __align__(16) unsigned char smem_u[];
+  const int bmax = st.bmax;
   double2* cs = reinterpret_cast<double2*>(smem_u);                    // [(s*bmax + p)][ld]: C[s p][q] of column c0+q
-  double2* Rs = cs + (size_t)crows * d.ld;                               // [k*kBMax + p][inst]
-  double2* wsh = Rs + (size_t)d.n_inst * kBMax * kBMax;                 // [2][256] row-group w values
-  int* meta = reinterpret_cast<int*>(wsh + 512);                        // [ld]: inst of each column
+  double2* Rs = cs + (size_t)crows * d.ld;                               // [k*bmax + p][inst]
+  double2* wsh = Rs + (size_t)d.n_inst * bmax * bmax;                    // [RG][256] row-group w values
+  int* meta = reinterpret_cast<int*>(wsh + RG * 256);                   // [ld]: inst of each column
   for (int c = threadIdx.x; c < d.ld; c += blockDim.x) meta[c] = -1;
   __syncthreads();
   for (int inst = threadIdx.x; inst < d.n_inst; inst += blockDim.x) {
     const int b = st.inst_b[inst], c0 = st.inst_col0[inst];
     for (int q = 0; q < b; ++q) meta[c0 + q] = inst;
   }
-  const int bmax = st.bmax;
   for (int inst = 0; inst < d.n_inst; ++inst) {
     const int* stt = st.state + inst * kStateInts;
     const int b = st.inst_b[inst], c0i = st.inst_col0[inst];
@@ -525,8 +526,8 @@ __global__ void __launch_bounds__(256, 3) k_lz_update_rows(rsed_lanczos_t st, Lz
       const int r = e / b, q = e % b;  // r = s * b + p
       cs[(size_t)((r / b) * bmax + r % b) * d.ld + c0i + q] = coef[(r / b) * kBMax * kBMax + (r % b) * kBMax + q];
     }
-    for (int e = threadIdx.x; e < kBMax * kBMax; e += blockDim.x)
-      Rs[e * d.n_inst + inst] = coef[(d.pslots - 1) * kBMax * kBMax + e];
+    for (int e = threadIdx.x; e < b * b; e += blockDim.x)
+      Rs[((e / b) * bmax + e % b) * d.n_inst + inst] = coef[(d.pslots - 1) * kBMax * kBMax + (e / b) * kBMax + e % b];
   }
   __syncthreads();
   const int rows_pg = blockDim.x / d.ld;  // rows per group
@@ -545,49 +546,59 @@ __global__ void __launch_bounds__(256, 3) k_lz_update_rows(rsed_lanczos_t st, Lz
     act = stt[S_ACTIVE] && nb * b <= kJacobiMax && !(pass == 2 && one);
   }
   const double2* ccol = cs + col;                    // C[s p][q] at ccol[(s*bmax + p)*ld]
-  const double2* Ri = Rs + (inst < 0 ? 0 : inst);  // R[k][p] at Ri[(k*kBMax + p)*n_inst]
+  const double2* Ri = Rs + (inst < 0 ? 0 : inst);  // R[k][p] at Ri[(k*bmax + p)*n_inst]
   const int ni = d.n_inst;
   double2* V = reinterpret_cast<double2*>(st.V);
   double2* W = reinterpret_cast<double2*>(st.W);
   const int64_t slot_stride = d.n_orb * d.ld;
   const int64_t n_groups = (d.n_orb + rows_pg - 1) / rows_pg;
+  const int64_t gstride = (int64_t)rows_pg * d.ld;  // one row group further
   const bool copy_cur = st.Xf == nullptr;  // the FP64 matvec reads the current-block slot
-  for (int64_t grp = 2 * (int64_t)blockIdx.x; grp < n_groups; grp += 2 * (int64_t)gridDim.x) {
-    const int64_t row0 = grp * rows_pg + rloc, row1 = row0 + rows_pg;
-    const bool live0 = act && lane_ok && row0 < d.n_orb;
-    const bool live1 = act && lane_ok && row1 < d.n_orb;
-    double2 w0 = make_double2(0.0, 0.0), w1 = make_double2(0.0, 0.0);
-    if (live0) {
-      w0 = W[row0 * d.ld + col];
-      if (live1) w1 = W[row1 * d.ld + col];
-#pragma unroll 4
+  for (int64_t grp = RG * (int64_t)blockIdx.x; grp < n_groups; grp += RG * (int64_t)gridDim.x) {
+    const int64_t row0 = grp * rows_pg + rloc;
+    bool live[RG];
+    double2 w[RG];
+#pragma unroll
+    for (int h = 0; h < RG; ++h) {
+      live[h] = act && lane_ok && row0 + h * rows_pg < d.n_orb;
+      w[h] = make_double2(0.0, 0.0);
+    }
+    if (live[0]) {
+#pragma unroll
+      for (int h = 0; h < RG; ++h)
+        if (live[h]) w[h] = W[row0 * d.ld + h * gstride + col];
+#pragma unroll 2
       for (int s = 0; s < nb; ++s) {
         const double2* Vs = V + s * slot_stride + row0 * d.ld + c0;
-        for (int p = 0; p < b; ++p) {
-          const double2 c = ccol[(size_t)(s * bmax + p) * d.ld];
-          w0 = csub(w0, cmul(Vs[p], c));
-          if (live1) w1 = csub(w1, cmul(Vs[(int64_t)rows_pg * d.ld + p], c));
+#pragma unroll
+        for (int p = 0; p < BB; ++p) {
+          if (p < b) {
+            const double2 c = ccol[(size_t)(s * bmax + p) * d.ld];
+#pragma unroll
+            for (int h = 0; h < RG; ++h)
+              if (live[h]) w[h] = csub(w[h], cmul(Vs[h * gstride + p], c));
+          }
         }
       }
     }
-    wsh[threadIdx.x] = w0;
-    wsh[256 + threadIdx.x] = w1;
+#pragma unroll
+    for (int h = 0; h < RG; ++h) wsh[h * 256 + threadIdx.x] = w[h];
     __syncthreads();
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const bool live = h == 0 ? live0 : live1;
-      if (!live) continue;
-      const int64_t row = h == 0 ? row0 : row1;
+    for (int h = 0; h < RG; ++h) {
+      if (!live[h]) continue;
+      const int64_t row = row0 + h * rows_pg;
       // forward substitution over this instance's columns 0..q
       const double2* wr = wsh + h * 256 + rloc * d.ld + c0;
-      double2 xs[kBMax];
+      double2 xs[BB];
       double2 xq = make_double2(0.0, 0.0);
 #pragma unroll
-      for (int pp = 0; pp < kBMax; ++pp) {
+      for (int pp = 0; pp < BB; ++pp) {
         if (pp > q) break;
         double2 v = wr[pp];
-        for (int k = 0; k < pp; ++k) v = csub(v, cmul(xs[k], Ri[(k * kBMax + pp) * ni]));
-        const double rr = Ri[(pp * kBMax + pp) * ni].x;
+#pragma unroll
+        for (int k = 0; k < pp; ++k) v = csub(v, cmul(xs[k], Ri[(k * bmax + pp) * ni]));
+        const double rr = Ri[(pp * bmax + pp) * ni].x;
         xs[pp] = make_double2(v.x / rr, v.y / rr);
         xq = xs[pp];
       }
@@ -2652,32 +2663,47 @@ int launch_restart(const rsed_lanczos_t& st, const LzDims& d, cudaStream_t strea
   return RSED_OK;
 }
 
+constexpr int kUpdRG = 4;  // row groups per thread iteration of k_lz_update_rows
+
+template <int BB>
+int launch_update_rows(const rsed_lanczos_t& st, const LzDims& d, int pass, size_t smem, int crows,
+                       cudaStream_t stream) {
+  static bool attr_set = false;
+  if (!attr_set) {
+    RSED_TRY_CUDA(cudaFuncSetAttribute(k_lz_update_rows<kUpdRG, BB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       160 * 1024));
+    attr_set = true;
+  }
+  const int rows_pg = 256 / d.ld;
+  const int64_t groups = (d.n_orb + rows_pg - 1) / rows_pg;
+  int dev = 0, n_sm = 148;
+  RSED_TRY_CUDA(cudaGetDevice(&dev));
+  RSED_TRY_CUDA(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
+  const int64_t iters = (groups + kUpdRG - 1) / kUpdRG;  // each block iteration takes kUpdRG row groups
+  const int64_t grid = iters < (int64_t)n_sm * 8 ? iters : (int64_t)n_sm * 8;
+  k_lz_update_rows<kUpdRG, BB><<<(unsigned)grid, 256, smem, stream>>>(st, d, pass, crows);
+  RSED_CHECK_LAUNCH();
+  return RSED_OK;
+}
+
 int launch_update(const rsed_lanczos_t& st, const LzDims& d, int pass, cudaStream_t stream) {
   // all instances per block when their coefficients fit in shared memory
   const int crows = st.n_slots * st.bmax;
-  const size_t smem = sizeof(double2) * ((size_t)crows * d.ld + (size_t)d.n_inst * kBMax * kBMax + 512) +
+  const size_t smem = sizeof(double2) * ((size_t)crows * d.ld + (size_t)d.n_inst * st.bmax * st.bmax +
+                                         kUpdRG * 256) +
                       sizeof(int) * (size_t)d.ld;
-  // (measured: above ~48 KB the lower occupancy costs more than whole-row reads save)
-  if (d.n_inst >= 2 && d.ld <= 256 && smem <= 48 * 1024) {
-    static bool attr_set = false;
-    if (!attr_set) {
-      RSED_TRY_CUDA(cudaFuncSetAttribute(k_lz_update_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
-      attr_set = true;
-    }
-    const int rows_pg = 256 / d.ld;
-    const int64_t groups = (d.n_orb + rows_pg - 1) / rows_pg;
-    int dev = 0, n_sm = 148;
-    RSED_TRY_CUDA(cudaGetDevice(&dev));
-    RSED_TRY_CUDA(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
-    const int64_t pairs = (groups + 1) / 2;  // each block iteration takes two row groups
-    const int64_t grid = pairs < (int64_t)n_sm * 8 ? pairs : (int64_t)n_sm * 8;
-    k_lz_update_rows<<<(unsigned)grid, 256, smem, stream>>>(st, d, pass, crows);
-  } else {
-    // rows per block: 8 warps x (32 / b) rows; sized for the largest block of the batch
-    const int64_t rows_per_block = 8 * (32 / st.bmax);
-    k_lz_update<<<(unsigned)(((d.n_orb + rows_per_block - 1) / rows_per_block) * d.n_inst), 256, 0, stream>>>(
-        st, d, pass);
+  // (three blocks of 256 per SM; above ~64 KB the lower occupancy costs more
+  // than whole-row reads save)
+  if (d.n_inst >= 2 && d.ld <= 256 && smem <= 64 * 1024) {
+    if (st.bmax <= 1) return launch_update_rows<1>(st, d, pass, smem, crows, stream);
+    if (st.bmax <= 2) return launch_update_rows<2>(st, d, pass, smem, crows, stream);
+    if (st.bmax <= 4) return launch_update_rows<4>(st, d, pass, smem, crows, stream);
+    return launch_update_rows<8>(st, d, pass, smem, crows, stream);
   }
+  // rows per block: 8 warps x (32 / b) rows; sized for the largest block of the batch
+  const int64_t rows_per_block = 8 * (32 / st.bmax);
+  k_lz_update<<<(unsigned)(((d.n_orb + rows_per_block - 1) / rows_per_block) * d.n_inst), 256, 0, stream>>>(
+      st, d, pass);
   RSED_CHECK_LAUNCH();
   return RSED_OK;
 }
