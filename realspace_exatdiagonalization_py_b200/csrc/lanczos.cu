@@ -1815,14 +1815,15 @@ __global__ void __launch_bounds__(256) k_lz_restart(rsed_lanczos_t st, LzDims d)
 }
 
 // The same restart for all instances at once: thread = (row, column c0 + q)
-// of two row groups per grid-stride iteration, so every basis slot is read
+// of RG row groups per grid-stride iteration, so every basis slot is read
 // as whole contiguous rows.  The Ritz coefficients of all restarting
 // instances sit in shared memory column-major,
 //   St[((l*bmax + p)*keep + jb)*ld + c0 + q] = S_i[l*b + p][jb*b + q],
 // so the lanes of a warp read consecutive words.  Every thread of the block
 // finishes reading its two rows (block barrier) before the rows are
-// overwritten in place.  KM bounds keep_blocks (register accumulators).
-template <int KM>
+// overwritten in place.  KM bounds keep_blocks (register accumulators); each
+// coefficient read from shared memory serves the RG rows.
+template <int KM, int RG>
 __global__ void __launch_bounds__(256, 2) k_lz_restart_rows(rsed_lanczos_t st, LzDims d) {
   extern __shared__ __align__(16) unsigned char smem_r[];
   const int keep = st.keep_blocks, bmax = st.bmax, ld = d.ld;
@@ -1863,47 +1864,50 @@ __global__ void __launch_bounds__(256, 2) k_lz_restart_rows(rsed_lanczos_t st, L
   const int64_t slot_stride = d.n_orb * d.ld;
   const int64_t n_groups = (d.n_orb + rows_pg - 1) / rows_pg;
   const double2* scol = St + col;
-  for (int64_t grp = 2 * (int64_t)blockIdx.x; grp < n_groups; grp += 2 * (int64_t)gridDim.x) {
-    const int64_t row0 = grp * rows_pg + rloc, row1 = row0 + rows_pg;
-    const bool live0 = inst >= 0 && row0 < d.n_orb;
-    const bool live1 = inst >= 0 && row1 < d.n_orb;
-    double2 a0[KM], a1[KM];
+  const int64_t gstride = (int64_t)rows_pg * ld;  // one row group further
+  for (int64_t grp = RG * (int64_t)blockIdx.x; grp < n_groups; grp += RG * (int64_t)gridDim.x) {
+    const int64_t row0 = grp * rows_pg + rloc;
+    bool live[RG];
+    double2 a[RG][KM], r[RG];
 #pragma unroll
-    for (int j = 0; j < KM; ++j) a0[j] = a1[j] = make_double2(0.0, 0.0);
-    double2 r0 = make_double2(0.0, 0.0), r1 = make_double2(0.0, 0.0);
-    if (live0) {
+    for (int h = 0; h < RG; ++h) {
+      live[h] = inst >= 0 && row0 + h * rows_pg < d.n_orb;
+      r[h] = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int j = 0; j < KM; ++j) a[h][j] = make_double2(0.0, 0.0);
+    }
+    if (live[0]) {
 #pragma unroll 2
       for (int l = 0; l < nslot; ++l) {
         const double2* Vs = V + (int64_t)l * slot_stride + row0 * ld + c0;
         for (int p = 0; p < b; ++p) {
-          const double2 v0 = Vs[p];
-          const double2 v1 = live1 ? Vs[(int64_t)rows_pg * ld + p] : make_double2(0.0, 0.0);
+          double2 v[RG];
+#pragma unroll
+          for (int h = 0; h < RG; ++h) v[h] = live[h] ? Vs[h * gstride + p] : make_double2(0.0, 0.0);
           const double2* sp = scol + (size_t)((l * bmax + p) * keep) * ld;
 #pragma unroll
           for (int j = 0; j < KM; ++j) {
             if (j < keep) {
               const double2 c = sp[(size_t)j * ld];
-              a0[j] = cadd(a0[j], cmul(v0, c));
-              a1[j] = cadd(a1[j], cmul(v1, c));
+#pragma unroll
+              for (int h = 0; h < RG; ++h) a[h][j] = cadd(a[h][j], cmul(v[h], c));
             }
           }
         }
       }
-      r0 = V[(int64_t)nslot * slot_stride + row0 * ld + col];
-      if (live1) r1 = V[(int64_t)nslot * slot_stride + row1 * ld + col];
+#pragma unroll
+      for (int h = 0; h < RG; ++h)
+        if (live[h]) r[h] = V[(int64_t)nslot * slot_stride + row0 * ld + h * gstride + col];
     }
-    __syncthreads();  // the rows of this pair are read by every thread before any is overwritten
-    if (live0) {
+    __syncthreads();  // the rows of these groups are read by every thread before any is overwritten
+#pragma unroll
+    for (int h = 0; h < RG; ++h) {
+      if (!live[h]) continue;
+      const int64_t at = row0 * ld + h * gstride + col;
 #pragma unroll
       for (int j = 0; j < KM; ++j)
-        if (j < keep) V[(int64_t)j * slot_stride + row0 * ld + col] = a0[j];
-      V[(int64_t)keep * slot_stride + row0 * ld + col] = r0;
-      if (live1) {
-#pragma unroll
-        for (int j = 0; j < KM; ++j)
-          if (j < keep) V[(int64_t)j * slot_stride + row1 * ld + col] = a1[j];
-        V[(int64_t)keep * slot_stride + row1 * ld + col] = r1;
-      }
+        if (j < keep) V[(int64_t)j * slot_stride + at] = a[h][j];
+      V[(int64_t)keep * slot_stride + at] = r[h];
     }
   }
 }
@@ -2630,6 +2634,8 @@ int check_lz(const rsed_model_t* md, const rsed_sectors_t* sc, const rsed_lanczo
   return RSED_OK;
 }
 
+constexpr int kRestartRG = 2;  // row groups per thread iteration of k_lz_restart_rows (keep <= 8)
+
 // Thick restart of every instance whose Ritz step asked for one: the
 // whole-row form when its coefficients fit shared memory (two blocks per SM
 // up to 115 KB, one up to 220 KB), else the per-instance form.
@@ -2639,9 +2645,9 @@ int launch_restart(const rsed_lanczos_t& st, const LzDims& d, cudaStream_t strea
   if (!(st.reserved & kFlagNoRowRestart) && d.ld <= 256 && smem <= 220 * 1024 && st.keep_blocks <= 16) {
     static bool attr_set = false;
     if (!attr_set) {
-      RSED_TRY_CUDA(cudaFuncSetAttribute(k_lz_restart_rows<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         220 * 1024));
-      RSED_TRY_CUDA(cudaFuncSetAttribute(k_lz_restart_rows<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      RSED_TRY_CUDA(cudaFuncSetAttribute(k_lz_restart_rows<8, kRestartRG>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+      RSED_TRY_CUDA(cudaFuncSetAttribute(k_lz_restart_rows<16, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          220 * 1024));
       attr_set = true;
     }
@@ -2649,13 +2655,14 @@ int launch_restart(const rsed_lanczos_t& st, const LzDims& d, cudaStream_t strea
     RSED_TRY_CUDA(cudaGetDevice(&dev));
     RSED_TRY_CUDA(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
     const int rows_pg = 256 / d.ld;
-    const int64_t pairs = ((d.n_orb + rows_pg - 1) / rows_pg + 1) / 2;
+    const int rg = st.keep_blocks <= 8 ? kRestartRG : 2;
+    const int64_t iters = ((d.n_orb + rows_pg - 1) / rows_pg + rg - 1) / rg;
     const int64_t per_sm = smem <= 115 * 1024 ? 2 : 1;  // 228 KB per SM, 1 KB reserved per block
-    const int64_t grid = pairs < n_sm * per_sm ? pairs : n_sm * per_sm;
+    const int64_t grid = iters < n_sm * per_sm ? iters : n_sm * per_sm;
     if (st.keep_blocks <= 8)
-      k_lz_restart_rows<8><<<(unsigned)grid, 256, smem, stream>>>(st, d);
+      k_lz_restart_rows<8, kRestartRG><<<(unsigned)grid, 256, smem, stream>>>(st, d);
     else
-      k_lz_restart_rows<16><<<(unsigned)grid, 256, smem, stream>>>(st, d);
+      k_lz_restart_rows<16, 2><<<(unsigned)grid, 256, smem, stream>>>(st, d);
   } else {
     k_lz_restart<<<(unsigned)(((d.n_orb + 255) / 256) * d.n_inst), 256, 0, stream>>>(st, d);
   }
