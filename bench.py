@@ -57,7 +57,10 @@ WORKLOADS = {
 # DRAM bytes per launch of the dominant kernels from one ncu capture each
 # (dram__bytes_read.sum + dram__bytes_write.sum); the capture commands and the
 # workloads are in the named profiles/ summaries.
-NCU_TRAFFIC: dict = {}
+NCU_TRAFFIC: dict = {
+    ("haldane32", "k_proj_spmv<32>"): {"bytes_per_launch": 2.903978e9 + 0.325e9,
+                                       "profile": "profiles/k_proj_spmv_fp32_haldane32_bench.md"},
+}
 
 
 def _dist():

@@ -2727,7 +2727,9 @@ bool stream_config(const rsed_lanczos_t& st, const LzDims& d, StreamConfig* c) {
   if (st.reserved & kFlagNoStream) return false;
   // lane = column in the Gram loop: below 16 columns most lanes would idle
   // (one sector of block 1 or 2: the per-instance kernel is faster)
-  if (d.ld < 16 || d.ld > 64 || d.n_inst > kStreamInstMax || d.n_orb < 1) return false;
+  // and below ~32k rows the ring's fill latency outweighs the streaming (a
+  // 892-row batch: 12.8 vs 8 ms per step), so small bases keep it too
+  if (d.ld < 16 || d.ld > 64 || d.n_inst > kStreamInstMax || d.n_orb < 32768) return false;
   const int crows = st.n_slots * st.bmax;
   constexpr size_t kBudget = 104 * 1024;  // dynamic shared memory per block (two blocks per SM)
   c->pr = kPanelElems / d.ld;
