@@ -205,9 +205,13 @@ __device__ __forceinline__ void spmv_row_pairs32(const uint32_t* __restrict__ cg
     float4 xa[U], xc[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
+      // the lane's 32-B segment in one 256-bit load (32-B aligned: see the caller)
       const char* px = xl + (size_t)(cgc[u] & kOrbitMask) * rowb;
-      xa[u] = __ldg(reinterpret_cast<const float4*>(px));
-      xc[u] = __ldg(reinterpret_cast<const float4*>(px + 16));
+      asm("{\n\t.reg .u64 ga;\n\tcvta.to.global.u64 ga, %8;\n\t"
+          "ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [ga];\n\t}"
+          : "=f"(xa[u].x), "=f"(xa[u].y), "=f"(xa[u].z), "=f"(xa[u].w), "=f"(xc[u].x), "=f"(xc[u].y),
+            "=f"(xc[u].z), "=f"(xc[u].w)
+          : "l"(px));
     }
 #pragma unroll
     for (int u = 0; u < U; ++u) {
@@ -281,8 +285,11 @@ __global__ void __launch_bounds__(256, 3) k_proj_spmv(rsed_model_t md, rsed_sect
   const char* xfast = xb;
   int s0 = 0, s2 = 0;
   if constexpr (PREC == 32 && CPL == 4) {
+    // a lane's 4 columns start at a multiple of 4: with ld a multiple of 4 too
+    // (and x 32-B aligned) each segment is 32-B aligned for one 256-bit load
     const bool lane_ok = colv[3] ? (sec[1] == sec[0] && sec[3] == sec[2]) : !colv[0];
-    pairs = __all_sync(0xffffffffu, lane_ok);
+    pairs = __all_sync(0xffffffffu, lane_ok) && (ld % 4) == 0 &&
+            (reinterpret_cast<uintptr_t>(xin) & 31) == 0;
     if (!colv[0]) xfast = reinterpret_cast<const char*>(xin);
     s0 = colv[0] ? sec[0] : 0;
     s2 = colv[0] ? sec[2] : 0;
