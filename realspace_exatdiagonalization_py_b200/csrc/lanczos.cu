@@ -1821,9 +1821,9 @@ __global__ void __launch_bounds__(256) k_lz_restart(rsed_lanczos_t st, LzDims d)
 //   St[((l*bmax + p)*keep + jb)*ld + c0 + q] = S_i[l*b + p][jb*b + q],
 // so the lanes of a warp read consecutive words.  Every thread of the block
 // finishes reading its two rows (block barrier) before the rows are
-// overwritten in place.  KM bounds keep_blocks (register accumulators); each
-// coefficient read from shared memory serves the RG rows.
-template <int KM, int RG>
+// overwritten in place.  KM bounds keep_blocks (register accumulators), BB
+// the block size; each coefficient read from shared memory serves the RG rows.
+template <int KM, int RG, int BB>
 __global__ void __launch_bounds__(256, 2) k_lz_restart_rows(rsed_lanczos_t st, LzDims d) {
   extern __shared__ __align__(16) unsigned char smem_r[];
   const int keep = st.keep_blocks, bmax = st.bmax, ld = d.ld;
@@ -1880,7 +1880,9 @@ __global__ void __launch_bounds__(256, 2) k_lz_restart_rows(rsed_lanczos_t st, L
 #pragma unroll 2
       for (int l = 0; l < nslot; ++l) {
         const double2* Vs = V + (int64_t)l * slot_stride + row0 * ld + c0;
-        for (int p = 0; p < b; ++p) {
+#pragma unroll
+        for (int p = 0; p < BB; ++p) {
+          if (p >= b) break;
           double2 v[RG];
 #pragma unroll
           for (int h = 0; h < RG; ++h) v[h] = live[h] ? Vs[h * gstride + p] : make_double2(0.0, 0.0);
@@ -2636,6 +2638,19 @@ int check_lz(const rsed_model_t* md, const rsed_sectors_t* sc, const rsed_lanczo
 
 constexpr int kRestartRG = 2;  // row groups per thread iteration of k_lz_restart_rows (keep <= 8)
 
+template <int KM, int RG, int BB>
+int launch_restart_rows(const rsed_lanczos_t& st, const LzDims& d, int64_t grid, size_t smem, cudaStream_t stream) {
+  static bool attr_set = false;
+  if (!attr_set) {
+    RSED_TRY_CUDA(cudaFuncSetAttribute(k_lz_restart_rows<KM, RG, BB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       220 * 1024));
+    attr_set = true;
+  }
+  k_lz_restart_rows<KM, RG, BB><<<(unsigned)grid, 256, smem, stream>>>(st, d);
+  RSED_CHECK_LAUNCH();
+  return RSED_OK;
+}
+
 // Thick restart of every instance whose Ritz step asked for one: the
 // whole-row form when its coefficients fit shared memory (two blocks per SM
 // up to 115 KB, one up to 220 KB), else the per-instance form.
@@ -2643,14 +2658,6 @@ int launch_restart(const rsed_lanczos_t& st, const LzDims& d, cudaStream_t strea
   const size_t smem = sizeof(double2) * (size_t)st.n_slots * st.bmax * st.keep_blocks * d.ld +
                       sizeof(int) * (size_t)d.ld;
   if (!(st.reserved & kFlagNoRowRestart) && d.ld <= 256 && smem <= 220 * 1024 && st.keep_blocks <= 16) {
-    static bool attr_set = false;
-    if (!attr_set) {
-      RSED_TRY_CUDA(cudaFuncSetAttribute(k_lz_restart_rows<8, kRestartRG>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
-      RSED_TRY_CUDA(cudaFuncSetAttribute(k_lz_restart_rows<16, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         220 * 1024));
-      attr_set = true;
-    }
     int dev = 0, n_sm = 148;
     RSED_TRY_CUDA(cudaGetDevice(&dev));
     RSED_TRY_CUDA(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
@@ -2659,10 +2666,16 @@ int launch_restart(const rsed_lanczos_t& st, const LzDims& d, cudaStream_t strea
     const int64_t iters = ((d.n_orb + rows_pg - 1) / rows_pg + rg - 1) / rg;
     const int64_t per_sm = smem <= 115 * 1024 ? 2 : 1;  // 228 KB per SM, 1 KB reserved per block
     const int64_t grid = iters < n_sm * per_sm ? iters : n_sm * per_sm;
-    if (st.keep_blocks <= 8)
-      k_lz_restart_rows<8, kRestartRG><<<(unsigned)grid, 256, smem, stream>>>(st, d);
-    else
-      k_lz_restart_rows<16, 2><<<(unsigned)grid, 256, smem, stream>>>(st, d);
+    int rc;
+    if (st.keep_blocks <= 8) {
+      rc = st.bmax <= 1   ? launch_restart_rows<8, kRestartRG, 1>(st, d, grid, smem, stream)
+           : st.bmax <= 2 ? launch_restart_rows<8, kRestartRG, 2>(st, d, grid, smem, stream)
+           : st.bmax <= 4 ? launch_restart_rows<8, kRestartRG, 4>(st, d, grid, smem, stream)
+                          : launch_restart_rows<8, kRestartRG, 8>(st, d, grid, smem, stream);
+    } else {
+      rc = launch_restart_rows<16, 2, 1>(st, d, grid, smem, stream);  // keep > 8 needs blocks of 1
+    }
+    if (rc != RSED_OK) return rc;
   } else {
     k_lz_restart<<<(unsigned)(((d.n_orb + 255) / 256) * d.n_inst), 256, 0, stream>>>(st, d);
   }

@@ -447,9 +447,10 @@ int rsed_proj_apply(const rsed_model_t& md, const rsed_sectors_t& sc, const void
   if (variant == 0) {
     // Measured on B200 (657,756 orbits, 64 columns): FP32 runs best with a
     // 32-B x segment per lane (4 columns) and one chunk covering up to 64
-    // columns (3.7 ms vs 4.5 ms with 16-B segments); FP64 with 16-B segments
-    // and 16-column chunks, one after another (7.5 ms; wider segments spill
-    // into lower occupancy).  Small (latency-bound) bases prefer 16 columns
+    // columns (3.7 ms vs 4.5 ms with 16-B segments; at 32 columns 1.48 ms in
+    // one chunk vs 1.95 ms in chunks of 16 that keep x in L2); FP64 with
+    // 16-B segments and 16-column chunks, one after another (7.5 ms; wider
+    // segments spill into lower occupancy), except at 17-32 columns.  Small (latency-bound) bases prefer 16 columns
     // per chunk with all chunks in one launch, for more warps in flight.
     if (md.n_orbits < 65536) {
       variant = 416;
@@ -457,6 +458,8 @@ int rsed_proj_apply(const rsed_model_t& md, const rsed_sectors_t& sc, const void
       int nc = 8;
       while (nc < sc.n_cols && nc < 64) nc *= 2;
       variant = 500 + nc;
+    } else if (sc.n_cols > 16 && sc.n_cols <= 32) {
+      variant = 632;  // 17-32 FP64 columns: 32-B segments, one launch (3.50 vs 3.76 ms at 32 columns)
     } else {
       int nc = 2;
       while (nc < sc.n_cols && nc < 16) nc *= 2;
