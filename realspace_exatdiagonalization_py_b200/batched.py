@@ -100,15 +100,17 @@ class BatchedSectorSolver:
         else:
             b.run(poll=poll, graph=False)
 
-    def solve(self, start_blocks=None, *, vectors: bool = True, host: bool = True):
-        """Solve every sector; ``start_blocks`` as in ``LanczosBatch.load_start``.
+    def solve(self, start_blocks=None, *, vectors: bool = True, host: bool = True, seeds=None):
+        """Solve every sector; ``start_blocks`` and ``seeds`` (per instance, for
+        the seeded blocks drawn where ``start_blocks`` is None) as in
+        ``LanczosBatch.load_start``.
 
         Returns ``(vals, vecs)``: ``vals [n_sectors, nev]`` and a list of
         ``[D_s, nev]`` eigenvector blocks (numpy if ``host`` else CUDA tensors,
         ``None`` when ``vectors`` is false).
         """
         b = self.batch
-        b.load_start(start_blocks)
+        b.load_start(start_blocks, seeds)
         self._run(b, self.poll)
         if self.precision == 32:
             self.last_fp32_vals = b.ritz_val[:, : self.nev].clone()

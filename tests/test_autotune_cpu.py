@@ -30,6 +30,9 @@ def test_candidates_large_basis_has_no_persistent_path():
     quick = candidate_configs([600000] * 4, nev=4, n_orbits=PERSISTENT_MAX_ORBITS + 1, quick=True)
     assert 0 < len(quick) < len(cands)
     assert all(c.projection for c in quick)
+    # shorter and longer basis lengths for blocks of 2 (measured: 12 slots fastest on the 32-site workload)
+    for n_slots in (10, 12, 16, 24):
+        assert SolverConfig((2,) * 4, 0, True, n_slots) in quick
 
 
 def test_candidates_without_projection_memory():
