@@ -479,7 +479,7 @@ def matvec_at_scale(ed, models, peak_gbs, n_launch=20, precisions=(32, 64), per_
     return out
 
 
-def serving_at_scale(ed, models, n_req=32, rate=20.0, block=2, plain_samples=2):
+def serving_at_scale(ed, models, n_req=32, rate=20.0, block=2, plain_samples=2, n_slots=16):
     """The request loop at the 32-site Haldane size: a Poisson stream (seed 0)
     of (sector, flux) requests over a 16 x 16 flux grid and 16 sectors,
     served with continuous batching (FP32 matvec + FP64 refinement, nev 4),
@@ -491,7 +491,7 @@ def serving_at_scale(ed, models, n_req=32, rate=20.0, block=2, plain_samples=2):
     model, nf = models.config_model("haldane32")
     sm = ed.ServingModel(model, nf, name="haldane32")
     reqs = poisson_requests(n_req, rate=rate, n_sectors=sm.n_sectors, flux_grid=16, model="haldane32", seed=0)
-    srv = ed.SolveServer(sm, nev=4, precision=32, block=block, poll=16)
+    srv = ed.SolveServer(sm, nev=4, precision=32, block=block, n_slots=n_slots, poll=16)
     srv.warm(48)  # start-up: lane buffers and captured graphs, before the stream begins
     res = srv.run([ed.SolveRequest(r.rid, r.sector, r.flux, r.model, r.arrival) for r in reqs], realtime=True)
     summ = ed.latency_summary(res)
