@@ -1967,7 +1967,9 @@ __global__ void k_rr_prepare(rsed_lanczos_t st) {
   }
 }
 
-__global__ void __launch_bounds__(128) k_rr_gram(rsed_lanczos_t st, LzDims d) {
+// Each task (row r of T, column block l2) is split over NP = blockDim / tasks
+// row phases (interleaved rows), summed in phase order in shared memory.
+__global__ void __launch_bounds__(256) k_rr_gram(rsed_lanczos_t st, LzDims d) {
   const int chunk = blockIdx.x / d.n_inst;
   const int inst = blockIdx.x % d.n_inst;
   int* stt = st.state + inst * kStateInts;
@@ -1983,24 +1985,50 @@ __global__ void __launch_bounds__(128) k_rr_gram(rsed_lanczos_t st, LzDims d) {
   double2* part = reinterpret_cast<double2*>(st.partial);
   const int64_t pbase = ((int64_t)chunk * d.n_inst + inst) * (int64_t)kRRMax * kRRMax;
   __shared__ int s_last;
-  // thread task: (row of T, column block l2) -> b accumulators
-  for (int task = threadIdx.x; task < M * nq; task += blockDim.x) {
+  // thread task: (row of T, column block l2, row phase) -> b accumulators
+  __shared__ double2 red[256][kBMax];
+  const int n_tasks = M * nq;
+  const int NP = n_tasks >= (int)blockDim.x ? 1 : (int)blockDim.x / n_tasks;
+  for (int t0 = 0; t0 < n_tasks * NP; t0 += blockDim.x) {  // one pass when NP > 1
+    const int t = t0 + (int)threadIdx.x;
+    const bool act = t < n_tasks * NP;
+    const int task = t % n_tasks, ph = t / n_tasks;
     const int r = task / nq, l2 = task % nq;
-    const double2* Q = V + (int64_t)(r / b) * slot_stride + c0 + (r % b);
-    const double2* Z = V + (int64_t)(nq + l2) * slot_stride + c0;
     double2 acc[kBMax];
 #pragma unroll
     for (int q = 0; q < kBMax; ++q) acc[q] = make_double2(0.0, 0.0);
+    if (act) {
+      const double2* Q = V + (int64_t)(r / b) * slot_stride + c0 + (r % b);
+      const double2* Z = V + (int64_t)(nq + l2) * slot_stride + c0;
 #pragma unroll 4
-    for (int64_t row = r0; row < r1; ++row) {
-      const double2 qv = Q[row * d.ld];
+      for (int64_t row = r0 + ph; row < r1; row += NP) {
+        const double2 qv = Q[row * d.ld];
 #pragma unroll
-      for (int q = 0; q < kBMax; ++q)
-        if (q < b) acc[q] = cadd(acc[q], cdotc(qv, Z[row * d.ld + q]));
+        for (int q = 0; q < kBMax; ++q)
+          if (q < b) acc[q] = cadd(acc[q], cdotc(qv, Z[row * d.ld + q]));
+      }
     }
+    if (NP == 1) {
+      if (act) {
 #pragma unroll
-    for (int q = 0; q < kBMax; ++q)
-      if (q < b) part[pbase + r * kRRMax + l2 * b + q] = acc[q];
+        for (int q = 0; q < kBMax; ++q)
+          if (q < b) part[pbase + r * kRRMax + l2 * b + q] = acc[q];
+      }
+    } else {
+#pragma unroll
+      for (int q = 0; q < kBMax; ++q) red[threadIdx.x][q] = acc[q];
+      __syncthreads();
+      if ((int)threadIdx.x < n_tasks) {
+#pragma unroll
+        for (int q = 0; q < kBMax; ++q) {
+          if (q >= b) continue;
+          double2 a = make_double2(0.0, 0.0);
+          for (int h = 0; h < NP; ++h) a = cadd(a, red[threadIdx.x + h * n_tasks][q]);
+          part[pbase + r * kRRMax + l2 * b + q] = a;
+        }
+      }
+      __syncthreads();
+    }
   }
   __threadfence();
   __syncthreads();
@@ -2980,7 +3008,7 @@ extern "C" int rsed_lanczos_rayleigh_ritz(const rsed_model_t* md, const rsed_sec
     if (rc) return rc;
   }
   const unsigned g = (unsigned)(d.n_chunks * d.n_inst);
-  k_rr_gram<<<g, 128, 0, stream>>>(*st, d);
+  k_rr_gram<<<g, 256, 0, stream>>>(*st, d);
   RSED_CHECK_LAUNCH();
   k_lz_ritz<<<d.n_inst, kRitzThreads, kRitzSmem, stream>>>(*st, d, 1, 1, 1);
   RSED_CHECK_LAUNCH();
