@@ -317,8 +317,8 @@ class ClockSampler:
 
 
 def sector_matvec_bytes(dm, sset, col_sector, x_bytes):
-    """Survey per-unit bytes of one apply over the given columns: per column
-    (one sector matvec) D_s * (8 + 2 s) + H_s * 16 -- the representative
+    """Per-column bytes of one apply over the given columns, counted per
+    sector matvec: D_s * (8 + 2 s) + H_s * 16 -- the representative
     mask, x read and y write per row and one 16-B table entry per hop of the
     sector's rows.  H_s comes from the projection table's row lengths."""
     import torch
