@@ -514,6 +514,10 @@ __global__ void __launch_bounds__(256, 3) k_lz_update_rows(rsed_lanczos_t st, Lz
     const int b = st.inst_b[inst], c0 = st.inst_col0[inst];
     for (int q = 0; q < b; ++q) meta[c0 + q] = inst;
   }
+  // any_work is the same in every thread (all read the same state words,
+  // which no kernel writes meanwhile), so a block with nothing to do (a
+  // pass-2 launch after every instance took the single pass) leaves at once
+  bool any_work = false;
   for (int inst = 0; inst < d.n_inst; ++inst) {
     const int* stt = st.state + inst * kStateInts;
     const int b = st.inst_b[inst], c0i = st.inst_col0[inst];
@@ -522,6 +526,7 @@ __global__ void __launch_bounds__(256, 3) k_lz_update_rows(rsed_lanczos_t st, Lz
     const double2* coef = reinterpret_cast<const double2*>(st.coef) +
                           (int64_t)inst * 2 * d.pslots * kBMax * kBMax + (pass - 1) * d.pslots * kBMax * kBMax;
     if (!stt[S_ACTIVE] || nb * b > kJacobiMax || (pass == 2 && one)) continue;
+    any_work = true;
     for (int e = threadIdx.x; e < nb * b * b; e += blockDim.x) {
       const int r = e / b, q = e % b;  // r = s * b + p
       cs[(size_t)((r / b) * bmax + r % b) * d.ld + c0i + q] = coef[(r / b) * kBMax * kBMax + (r % b) * kBMax + q];
@@ -530,6 +535,7 @@ __global__ void __launch_bounds__(256, 3) k_lz_update_rows(rsed_lanczos_t st, Lz
       Rs[((e / b) * bmax + e % b) * d.n_inst + inst] = coef[(d.pslots - 1) * kBMax * kBMax + (e / b) * kBMax + e % b];
   }
   __syncthreads();
+  if (!any_work) return;
   const int rows_pg = blockDim.x / d.ld;  // rows per group
   const int rloc = threadIdx.x / d.ld, col = threadIdx.x % d.ld;
   const bool lane_ok = rloc < rows_pg;
