@@ -65,6 +65,15 @@ class LanczosParams:
     row_restart: bool = True  # thick restart over whole rows (all instances per block)
 
 
+def reserved_bits(p: LanczosParams) -> int:
+    """The kernel-form switches of ``rsed_lanczos_t.reserved``: bit 0 adaptive
+    single Gram-Schmidt pass, bit 1 per-instance reduction (streaming off),
+    bit 2 row-group update after the streamed reduction, bit 3 per-instance
+    thick restart."""
+    return ((1 if p.single_pass else 0) | (0 if p.stream else 2) | (0 if p.stream_update else 4)
+            | (0 if p.row_restart else 8))
+
+
 def start_block(n: int, b: int, seed: int = 12345) -> np.ndarray:
     """Seeded complex-normal start block ``[n, b]``, each column normalised.
 
@@ -148,8 +157,7 @@ class LanczosBatch:
         self.state = torch.zeros((n_inst, STATE_INTS), dtype=torch.int32, device=dev)
         self.c = _lib.RsedLanczos(
             n_inst, S, nev, self.keep, p.max_restarts, p.precision, bmax, self.chunk_rows, self.pm,
-            (1 if p.single_pass else 0) | (0 if p.stream else 2) | (0 if p.stream_update else 4)
-            | (0 if p.row_restart else 8),
+            reserved_bits(p),
             float(p.tol if p.precision == 64 else max(p.tol, p.tol32)), _lib.ptr(self.inst_col0), _lib.ptr(self.inst_b), _lib.ptr(self.V),
             _lib.ptr(self.W), _lib.ptr(self.Xf), _lib.ptr(self.P), _lib.ptr(self.coef),
             _lib.ptr(self.partial), plen, _lib.ptr(self.ritz_val), _lib.ptr(self.ritz_vec),

@@ -347,3 +347,16 @@ def test_scalar_api_matches_reference():
         m = sum(1 << int(s) for s in rng.choice(n, size=k, replace=False))
         bt = sre._binom_table(n, k)
         assert ed.rank_combination(m, bt) == sre.rank_combination(m, bt)
+
+
+def test_lanczos_kernel_form_bits():
+    """LanczosParams switches -> rsed_lanczos_t.reserved bits (the C side reads
+    bit 0 single pass, bit 1 no streaming, bit 2 row-group update, bit 3
+    per-instance restart)."""
+    from realspace_exatdiagonalization_py_b200.lanczos import LanczosParams, reserved_bits
+
+    assert reserved_bits(LanczosParams()) == 1 | 4  # defaults: single pass, streamed reduction, row-group update
+    assert reserved_bits(LanczosParams(single_pass=False)) == 4
+    assert reserved_bits(LanczosParams(stream=False)) == 1 | 2 | 4
+    assert reserved_bits(LanczosParams(stream_update=True)) == 1
+    assert reserved_bits(LanczosParams(row_restart=False)) == 1 | 4 | 8
